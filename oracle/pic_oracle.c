@@ -1,0 +1,930 @@
+/* CPU restatement of Mandor's PIC time step -- TEST INFRASTRUCTURE ONLY.
+ *
+ * Every function below names the reference code it restates (paths are
+ * relative to the reference project).  The mesh is one global array per
+ * field component with two ghost layers on every side; the reference's
+ * boundary "caps" (core/em_caps.c) compute the same Yee update on boundary
+ * slabs with a single full-tau H step instead of two half steps, so fields
+ * near walls agree with the reference to round-off, not bit-for-bit.
+ *
+ * Build: oracle/Makefile target `port` -> oracle/_build/libpic_oracle.so.
+ */
+#include "pic_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define G 2                         /* ghost layers on every side */
+
+struct po_run {
+   int    n[3];
+   double h[3], tau, time;
+   int    bc[2][3];                 /* [min/max][axis] */
+   int    dim[3];                   /* n + 1 + 2G */
+   long   s[3];                     /* strides: s[2] = 1 */
+   double *e[3], *b[3], *j[3];      /* E, H, J components */
+   double *mur[2][3];               /* Mur history: 4 doubles per wall node */
+   double mur_alpha[3];
+   po_marker_t *p;
+   long   np;
+   po_laser_t laser;
+   int    has_laser;
+};
+
+static inline long IX (const po_run_t *r, int i, int j, int k)
+{
+   return (i + G)*r->s[0] + (j + G)*r->s[1] + (k + G);
+}
+
+/* Offset of node (a along axis ea, p along ep, q along eq). */
+static inline long IXA (const po_run_t *r, int ea, int a, int ep, int p, int eq, int q)
+{
+   int c[3];
+   c[ea] = a;
+   c[ep] = p;
+   c[eq] = q;
+   return IX (r, c[0], c[1], c[2]);
+}
+
+po_run_t *po_create (const int n[3], const double h[3], double tau,
+                     const int bc_min[3], const int bc_max[3], double time)
+{
+   po_run_t *r = (po_run_t *) calloc (1, sizeof (po_run_t));
+   for (int a = 0 ; a < 3 ; ++a) {
+      r->n[a] = n[a];
+      r->h[a] = h[a];
+      r->bc[0][a] = bc_min[a];
+      r->bc[1][a] = bc_max[a];
+      r->dim[a] = n[a] + 1 + 2*G;
+      r->mur_alpha[a] = (tau - h[a])/(tau + h[a]);   /* core/em_caps.c:380 via emCap_Mur.c:102 */
+   }
+   r->tau = tau;
+   r->time = time;
+   r->s[2] = 1;
+   r->s[1] = r->dim[2];
+   r->s[0] = (long) r->dim[1]*r->dim[2];
+   long total = (long) r->dim[0]*r->s[0];
+   for (int c = 0 ; c < 3 ; ++c) {
+      r->e[c] = (double *) calloc (total, sizeof (double));
+      r->b[c] = (double *) calloc (total, sizeof (double));
+      r->j[c] = (double *) calloc (total, sizeof (double));
+   }
+   for (int t = 0 ; t < 2 ; ++t)
+      for (int a = 0 ; a < 3 ; ++a) {
+         int ep = (a + 1) % 3, eq = (a + 2) % 3;
+         r->mur[t][a] = (double *) calloc ((size_t) 4*r->dim[ep]*r->dim[eq], sizeof (double));
+      }
+   return r;
+}
+
+void po_destroy (po_run_t *r)
+{
+   if (!r)
+      return;
+   for (int c = 0 ; c < 3 ; ++c) {
+      free (r->e[c]);
+      free (r->b[c]);
+      free (r->j[c]);
+   }
+   for (int t = 0 ; t < 2 ; ++t)
+      for (int a = 0 ; a < 3 ; ++a)
+         free (r->mur[t][a]);
+   free (r->p);
+   free (r);
+}
+
+double po_time (const po_run_t *r) { return r->time; }
+
+/* Checkpoint region [0,n]^3 in reference order (type_mesh.c:285-313). */
+void po_set_fields (po_run_t *r, const double *E, const double *H)
+{
+   long q = 0;
+   for (int i = 0 ; i <= r->n[0] ; ++i)
+   for (int j = 0 ; j <= r->n[1] ; ++j)
+   for (int k = 0 ; k <= r->n[2] ; ++k, q += 3) {
+      long o = IX (r, i, j, k);
+      for (int c = 0 ; c < 3 ; ++c) {
+         r->e[c][o] = E[q + c];
+         r->b[c][o] = H[q + c];
+      }
+   }
+}
+
+void po_get_fields (const po_run_t *r, double *E, double *H)
+{
+   long q = 0;
+   for (int i = 0 ; i <= r->n[0] ; ++i)
+   for (int j = 0 ; j <= r->n[1] ; ++j)
+   for (int k = 0 ; k <= r->n[2] ; ++k, q += 3) {
+      long o = IX (r, i, j, k);
+      for (int c = 0 ; c < 3 ; ++c) {
+         if (E) E[q + c] = r->e[c][o];
+         if (H) H[q + c] = r->b[c][o];
+      }
+   }
+}
+
+void po_get_current (const po_run_t *r, double *J)
+{
+   long q = 0;
+   for (int i = -G ; i <= r->n[0] + G ; ++i)
+   for (int j = -G ; j <= r->n[1] + G ; ++j)
+   for (int k = -G ; k <= r->n[2] + G ; ++k, q += 3) {
+      long o = IX (r, i, j, k);
+      for (int c = 0 ; c < 3 ; ++c)
+         J[q + c] = r->j[c][o];
+   }
+}
+
+void po_set_markers (po_run_t *r, const po_marker_t *m, long n)
+{
+   free (r->p);
+   r->p = (po_marker_t *) malloc ((n > 0 ? n : 1)*sizeof (po_marker_t));
+   if (n > 0)
+      memcpy (r->p, m, n*sizeof (po_marker_t));
+   r->np = n;
+}
+
+long po_marker_count (const po_run_t *r) { return r->np; }
+
+void po_get_markers (const po_run_t *r, po_marker_t *m)
+{
+   if (r->np > 0)
+      memcpy (m, r->p, r->np*sizeof (po_marker_t));
+}
+
+void po_set_laser (po_run_t *r, const po_laser_t *l)
+{
+   r->laser = *l;
+   r->has_laser = 1;
+}
+
+/* ------------------------------------------------------------------------
+ * Yee update ranges.  The union of the reference's inner loop and its six
+ * cap regions (core/em_caps.c:66-109 tables, core/em.c:55-163 loops) is a
+ * product of per-axis node ranges:
+ *   H: periodic [0,n], mirror [1,n], Mur [0,n]
+ *   E: lower bound 0 if periodic else 1; upper bound n-1 if periodic else n
+ * ---------------------------------------------------------------------- */
+static void h_range (const po_run_t *r, int a, int *lo, int *hi)
+{
+   *lo = (r->bc[0][a] == PO_BC_MIRROR) ? 1 : 0;
+   *hi = r->n[a];
+}
+
+static void e_range (const po_run_t *r, int a, int *lo, int *hi)
+{
+   *lo = (r->bc[0][a] == PO_BC_PERIODIC) ? 0 : 1;
+   *hi = (r->bc[1][a] == PO_BC_PERIODIC) ? r->n[a] - 1 : r->n[a];
+}
+
+/* H += frac*tau*(-curl E): core/em.c:55-77 (expression order kept). */
+static void h_advance (po_run_t *r, double frac)
+{
+   const double c1 = frac*r->tau/r->h[0], c2 = frac*r->tau/r->h[1], c3 = frac*r->tau/r->h[2];
+   const long sx = r->s[0], sy = r->s[1];
+   double *Ex = r->e[0], *Ey = r->e[1], *Ez = r->e[2];
+   double *Hx = r->b[0], *Hy = r->b[1], *Hz = r->b[2];
+   int lo[3], hi[3];
+   for (int a = 0 ; a < 3 ; ++a)
+      h_range (r, a, lo + a, hi + a);
+   for (int i = lo[0] ; i <= hi[0] ; ++i)
+   for (int j = lo[1] ; j <= hi[1] ; ++j)
+   for (int k = lo[2] ; k <= hi[2] ; ++k) {
+      long o = IX (r, i, j, k);
+      Hx[o] += c3*(Ey[o] - Ey[o - 1]) - c2*(Ez[o] - Ez[o - sy]);
+      Hy[o] += c1*(Ez[o] - Ez[o - sx]) - c3*(Ex[o] - Ex[o - 1]);
+      Hz[o] += c2*(Ex[o] - Ex[o - sy]) - c1*(Ey[o] - Ey[o - sx]);
+   }
+}
+
+/* E -= tau*(curl H) without the current: core/em.c:135-163. */
+static void e_advance (po_run_t *r)
+{
+   const double c1 = r->tau/r->h[0], c2 = r->tau/r->h[1], c3 = r->tau/r->h[2];
+   const long sx = r->s[0], sy = r->s[1];
+   double *Ex = r->e[0], *Ey = r->e[1], *Ez = r->e[2];
+   double *Hx = r->b[0], *Hy = r->b[1], *Hz = r->b[2];
+   int lo[3], hi[3];
+   for (int a = 0 ; a < 3 ; ++a)
+      e_range (r, a, lo + a, hi + a);
+   for (int i = lo[0] ; i <= hi[0] ; ++i)
+   for (int j = lo[1] ; j <= hi[1] ; ++j)
+   for (int k = lo[2] ; k <= hi[2] ; ++k) {
+      long o = IX (r, i, j, k);
+      Ex[o] -= c3*(Hy[o + 1] - Hy[o]) - c2*(Hz[o + sy] - Hz[o]);
+      Ey[o] -= c1*(Hz[o + sx] - Hz[o]) - c3*(Hx[o + 1] - Hx[o]);
+      Ez[o] -= c2*(Hx[o + sy] - Hx[o]) - c1*(Hy[o + sx] - Hy[o]);
+   }
+}
+
+/* Transverse extent of a wall operation: nodes [0, n+1] of the two other
+ * axes (the flush regions of the caps, core/em_caps.c:140-146). */
+#define FOR_WALL(r, ea, ep, eq, p, q)                          \
+   for (int p = 0 ; p <= (r)->n[ep] + 1 ; ++p)                 \
+   for (int q = 0 ; q <= (r)->n[eq] + 1 ; ++q)
+
+/* H boundary conditions, axis by axis, min side then max side:
+ * core/emCap_periodic.c:15-37, emCap_mirror.c:17-40, emCap_Mur.c:56-80. */
+static void h_bc (po_run_t *r)
+{
+   for (int ea = 0 ; ea < 3 ; ++ea) {
+      const int ep = (ea + 1) % 3, eq = (ea + 2) % 3, N = r->n[ea];
+      double *Ha = r->b[ea], *Hp = r->b[ep], *Hq = r->b[eq];
+      switch (r->bc[0][ea]) {
+      case PO_BC_PERIODIC:
+         FOR_WALL (r, ea, ep, eq, p, q) {
+            long b0 = IXA (r, ea, 0, ep, p, eq, q), t0 = IXA (r, ea, N, ep, p, eq, q);
+            long b1 = IXA (r, ea, 1, ep, p, eq, q), t1 = IXA (r, ea, N + 1, ep, p, eq, q);
+            for (int c = 0 ; c < 3 ; ++c) {
+               r->b[c][b0] = r->b[c][t0];
+               r->b[c][t1] = r->b[c][b1];
+            }
+         }
+         break;
+      case PO_BC_MIRROR:
+         FOR_WALL (r, ea, ep, eq, p, q) {
+            long w = IXA (r, ea, 0, ep, p, eq, q), in = IXA (r, ea, 1, ep, p, eq, q);
+            Ha[w] = 0;
+            Hp[w] = Hp[in];
+            Hq[w] = Hq[in];
+         }
+         break;
+      case PO_BC_OPEN:
+         FOR_WALL (r, ea, ep, eq, p, q) {
+            long w = IXA (r, ea, 0, ep, p, eq, q), in = IXA (r, ea, 1, ep, p, eq, q);
+            Hp[w] = Hp[in];
+            Hq[w] = Hq[in];
+         }
+         break;
+      }
+      switch (r->bc[1][ea]) {
+      case PO_BC_MIRROR:
+         FOR_WALL (r, ea, ep, eq, p, q) {
+            long w = IXA (r, ea, N, ep, p, eq, q), out = IXA (r, ea, N + 1, ep, p, eq, q);
+            Ha[w] = 0;
+            Hp[out] = Hp[w];
+            Hq[out] = Hq[w];
+         }
+         break;
+      case PO_BC_OPEN:
+         FOR_WALL (r, ea, ep, eq, p, q) {
+            long w = IXA (r, ea, N, ep, p, eq, q), out = IXA (r, ea, N + 1, ep, p, eq, q);
+            Hp[out] = Hp[w];
+            Hq[out] = Hq[w];
+         }
+         break;
+      }
+   }
+}
+
+/* Mur history index for wall node (p, q). */
+static inline long MUR (const po_run_t *r, int ea, int p, int q)
+{
+   const int eq = (ea + 2) % 3;
+   return 4*((long) p*r->dim[eq] + q);
+}
+
+/* E boundary conditions: core/emCap_periodic.c:42-67, emCap_mirror.c:45-70,
+ * emCap_Mur.c:117-166 (history holds wall and first inner node, pre-current). */
+static void e_bc (po_run_t *r)
+{
+   for (int ea = 0 ; ea < 3 ; ++ea) {
+      const int ep = (ea + 1) % 3, eq = (ea + 2) % 3, N = r->n[ea];
+      double *Ea = r->e[ea], *Ep = r->e[ep], *Eq = r->e[eq];
+      const double alpha = r->mur_alpha[ea];
+      switch (r->bc[0][ea]) {
+      case PO_BC_PERIODIC:
+         FOR_WALL (r, ea, ep, eq, p, q) {
+            long b0 = IXA (r, ea, 0, ep, p, eq, q), t0 = IXA (r, ea, N, ep, p, eq, q);
+            long b1 = IXA (r, ea, 1, ep, p, eq, q), t1 = IXA (r, ea, N + 1, ep, p, eq, q);
+            for (int c = 0 ; c < 3 ; ++c) {
+               r->e[c][t0] = r->e[c][b0];
+               r->e[c][t1] = r->e[c][b1];
+            }
+         }
+         break;
+      case PO_BC_MIRROR:
+         FOR_WALL (r, ea, ep, eq, p, q) {
+            long w = IXA (r, ea, 0, ep, p, eq, q), in = IXA (r, ea, 1, ep, p, eq, q);
+            Ep[w] = 0;
+            Eq[w] = 0;
+            Ea[w] = Ea[in];
+         }
+         break;
+      case PO_BC_OPEN: {
+         double *buf = r->mur[0][ea];
+         FOR_WALL (r, ea, ep, eq, p, q) {
+            long w = IXA (r, ea, 0, ep, p, eq, q), in = IXA (r, ea, 1, ep, p, eq, q);
+            double *o = buf + MUR (r, ea, p, q);
+            Ea[w] = Ea[in];
+            Ep[w] = o[2] + alpha*(Ep[in] - o[0]);
+            Eq[w] = o[3] + alpha*(Eq[in] - o[1]);
+            o[0] = Ep[w];
+            o[1] = Eq[w];
+            o[2] = Ep[in];
+            o[3] = Eq[in];
+         }
+         break;
+      }
+      }
+      switch (r->bc[1][ea]) {
+      case PO_BC_MIRROR:
+         FOR_WALL (r, ea, ep, eq, p, q) {
+            long w = IXA (r, ea, N, ep, p, eq, q), out = IXA (r, ea, N + 1, ep, p, eq, q);
+            Ep[w] = 0;
+            Eq[w] = 0;
+            Ea[out] = Ea[w];
+         }
+         break;
+      case PO_BC_OPEN: {
+         double *buf = r->mur[1][ea];
+         FOR_WALL (r, ea, ep, eq, p, q) {
+            long w = IXA (r, ea, N, ep, p, eq, q), out = IXA (r, ea, N + 1, ep, p, eq, q);
+            long in = IXA (r, ea, N - 1, ep, p, eq, q);
+            double *o = buf + MUR (r, ea, p, q);
+            Ea[out] = Ea[w];
+            Ep[w] = o[2] + alpha*(Ep[in] - o[0]);
+            Eq[w] = o[3] + alpha*(Eq[in] - o[1]);
+            o[0] = Ep[w];
+            o[1] = Eq[w];
+            o[2] = Ep[in];
+            o[3] = Eq[in];
+         }
+         break;
+      }
+      }
+   }
+}
+
+/* cap_init (core/em_caps.c:343-392): ghost refresh for periodic and mirror
+ * walls, Mur history from the loaded E and the normal-E ghost copy
+ * (emCap_Mur.c:86-112). */
+void po_init (po_run_t *r)
+{
+   for (int ea = 0 ; ea < 3 ; ++ea) {
+      const int ep = (ea + 1) % 3, eq = (ea + 2) % 3, N = r->n[ea];
+      if (r->bc[0][ea] == PO_BC_PERIODIC) {
+         FOR_WALL (r, ea, ep, eq, p, q) {
+            long b0 = IXA (r, ea, 0, ep, p, eq, q), t0 = IXA (r, ea, N, ep, p, eq, q);
+            long b1 = IXA (r, ea, 1, ep, p, eq, q), t1 = IXA (r, ea, N + 1, ep, p, eq, q);
+            for (int c = 0 ; c < 3 ; ++c) {
+               r->b[c][b0] = r->b[c][t0];
+               r->b[c][t1] = r->b[c][b1];
+               r->e[c][t0] = r->e[c][b0];
+               r->e[c][t1] = r->e[c][b1];
+            }
+         }
+      }
+      for (int top = 0 ; top < 2 ; ++top) {
+         int w_at = top ? N : 0;
+         int in_at = top ? N - 1 : 1;
+         if (r->bc[top][ea] == PO_BC_MIRROR) {
+            FOR_WALL (r, ea, ep, eq, p, q) {
+               long w = IXA (r, ea, w_at, ep, p, eq, q);
+               long hin = IXA (r, ea, top ? N : 1, ep, p, eq, q);
+               long hout = IXA (r, ea, top ? N + 1 : 0, ep, p, eq, q);
+               r->b[ea][w] = 0;
+               r->b[ep][hout] = r->b[ep][hin];
+               r->b[eq][hout] = r->b[eq][hin];
+               r->e[ep][w] = 0;
+               r->e[eq][w] = 0;
+               r->e[ea][hout] = r->e[ea][hin];
+            }
+         } else if (r->bc[top][ea] == PO_BC_OPEN) {
+            double *buf = r->mur[top][ea];
+            FOR_WALL (r, ea, ep, eq, p, q) {
+               long w = IXA (r, ea, w_at, ep, p, eq, q);
+               long in = IXA (r, ea, in_at, ep, p, eq, q);
+               long nin = IXA (r, ea, top ? N : 1, ep, p, eq, q);
+               long nout = IXA (r, ea, top ? N + 1 : 0, ep, p, eq, q);
+               double *o = buf + MUR (r, ea, p, q);
+               o[0] = r->e[ep][w];
+               o[1] = r->e[eq][w];
+               o[2] = r->e[ep][in];
+               o[3] = r->e[eq][in];
+               r->e[ea][nout] = r->e[ea][nin];
+            }
+         }
+      }
+   }
+}
+
+/* ------------------------------------------------------------------------
+ * Laser soft source (new analytic source on the reference's one-sided
+ * injection pattern, scpic/em_mirror.h:62-101 and scpic/em_mirror.c:666-717).
+ * ---------------------------------------------------------------------- */
+double po_laser_ey (const po_laser_t *l, double x, double y, double z,
+                    double t, double ymid, double zmid)
+{
+   const double k = 2*M_PI, xr = M_PI*l->waist*l->waist;
+   const double xi = x - l->x_focus;
+   const double w = l->waist*sqrt (1 + (xi/xr)*(xi/xr));
+   const double r2 = (y - ymid)*(y - ymid) + (z - zmid)*(z - zmid);
+   const double tr = t - l->t_start - x;
+   if (tr <= 0 || tr >= l->duration)
+      return 0;
+   const double s = sin (M_PI*tr/l->duration);
+   const double env = s*s;
+   const double phase = k*tr + atan (xi/xr) - k*r2*xi/(2*(xi*xi + xr*xr)) + l->phase;
+   return 2*M_PI*l->a0*(l->waist/w)*exp (-r2/(w*w))*env*sin (phase);
+}
+
+static void laser_h (po_run_t *r, double t)
+{
+   const po_laser_t *l = &r->laser;
+   const int I = l->plane;
+   const double c1 = r->tau/r->h[0];
+   const double ymid = 0.5*r->n[1]*r->h[1], zmid = 0.5*r->n[2]*r->h[2];
+   const double x = (I - 1)*r->h[0];
+   for (int j = l->margin ; j <= r->n[1] - l->margin ; ++j)
+   for (int k = l->margin ; k <= r->n[2] - l->margin ; ++k) {
+      double ey = po_laser_ey (l, x, (j - 0.5)*r->h[1], k*r->h[2], t, ymid, zmid);
+      r->b[2][IX (r, I, j, k)] += c1*ey;
+   }
+}
+
+static void laser_e (po_run_t *r, double t)
+{
+   const po_laser_t *l = &r->laser;
+   const int I = l->plane;
+   const double c1 = r->tau/r->h[0];
+   const double ymid = 0.5*r->n[1]*r->h[1], zmid = 0.5*r->n[2]*r->h[2];
+   const double x = (I - 0.5)*r->h[0];
+   for (int j = l->margin ; j <= r->n[1] - l->margin ; ++j)
+   for (int k = l->margin ; k <= r->n[2] - l->margin ; ++k) {
+      double hz = po_laser_ey (l, x, (j - 0.5)*r->h[1], k*r->h[2], t, ymid, zmid);
+      r->e[1][IX (r, I - 1, j, k)] += c1*hz;
+   }
+}
+
+/* ------------------------------------------------------------------------
+ * Particles.
+ * ---------------------------------------------------------------------- */
+
+/* MF_DBL_TO_INT (misc_PIC.h:18). */
+static inline int dbl_to_int (double x) { return (int) (x + 128.0) - 128; }
+
+/* One straight in-cell segment: plasmaCurrents_kernel
+ * (core/plasma_currentKernel.c:21-124), 3D branch. */
+static void deposit_segment (po_run_t *r, int i, int j, int k,
+                             double x1, double x2, double y1, double y2,
+                             double z1, double z2, double rho)
+{
+   const double h1 = r->h[0], h2 = r->h[1], h3 = r->h[2], tau = r->tau;
+   const double dX = x2 - x1, dY = y2 - y1, dZ = z2 - z1;
+   const double tX = 0.5*(x1 + x2) - i*h1;
+   const double tY = 0.5*(y1 + y2) - j*h2;
+   const double tZ = 0.5*(z1 + z2) - k*h3;
+   const long sx = r->s[0], sy = r->s[1];
+   double *Jx = r->j[0], *Jy = r->j[1], *Jz = r->j[2];
+   const long o = IX (r, i, j, k);
+
+   const double ax = rho*dX/(tau*h2*h3), dyz = dY*dZ/12;
+   Jx[o + sx]          += ax*((h2 - tY)*(h3 - tZ) + dyz);
+   Jx[o + sx + sy]     += ax*(tY*(h3 - tZ) - dyz);
+   Jx[o + sx + 1]      += ax*((h2 - tY)*tZ - dyz);
+   Jx[o + sx + sy + 1] += ax*(tY*tZ + dyz);
+
+   const double ay = rho*dY/(tau*h1*h3), dxz = dX*dZ/12;
+   Jy[o + sy]          += ay*((h1 - tX)*(h3 - tZ) + dxz);
+   Jy[o + sx + sy]     += ay*(tX*(h3 - tZ) - dxz);
+   Jy[o + sy + 1]      += ay*((h1 - tX)*tZ - dxz);
+   Jy[o + sx + sy + 1] += ay*(tX*tZ + dxz);
+
+   const double az = rho*dZ/(tau*h1*h2), dxy = dX*dY/12;
+   Jz[o + 1]           += az*((h1 - tX)*(h2 - tY) + dxy);
+   Jz[o + sx + 1]      += az*(tX*(h2 - tY) - dxy);
+   Jz[o + sy + 1]      += az*((h1 - tX)*tY - dxy);
+   Jz[o + sx + sy + 1] += az*(tX*tY + dxy);
+}
+
+#define SWAPI(a, b) do { int t_ = a; a = b; b = t_; } while (0)
+#define SWAPD(a, b) do { double t_ = a; a = b; b = t_; } while (0)
+
+/* plasmaCurrents_multiCellStep (core/plasma_currentKernel.c:157-279). */
+static void deposit_multicell (po_run_t *r, int i1, int j1, int k1,
+                               int i2, int j2, int k2,
+                               double x1, double y1, double z1,
+                               double x2, double y2, double z2, double rho)
+{
+   const double h1 = r->h[0], h2 = r->h[1], h3 = r->h[2];
+   const int di = abs (i2 - i1), dj = abs (j2 - j1), dk = abs (k2 - k1);
+
+   if (di + dj + dk == 2) {
+      int i = i1, j = j1, k = k1;
+      const double sX = di*((i1 + i2 + 1)*0.5*h1 - x1)/(x2 - x1 + ((1 - di) << 16));
+      const double sY = dj*((j1 + j2 + 1)*0.5*h2 - y1)/(y2 - y1 + ((1 - dj) << 16));
+      const double sZ = dk*((k1 + k2 + 1)*0.5*h3 - z1)/(z2 - z1 + ((1 - dk) << 16));
+      double kap1 = sX + (1 - di)*sY;
+      double kap2 = sZ + (1 - dk)*sY;
+      int dIdx[2][3] = {{0, 0, 0}, {0, 0, 0}};
+      int first = 0;
+      dIdx[0][0] = di*(i2 - i1);
+      dIdx[0][1] = (1 - di)*(j2 - j1);
+      dIdx[1][1] = (1 - dk)*(j2 - j1);
+      dIdx[1][2] = dk*(k2 - k1);
+      if (kap1 > kap2) {
+         SWAPD (kap1, kap2);
+         first = 1;
+      }
+      const double xA = x1 + kap1*(x2 - x1), yA = y1 + kap1*(y2 - y1), zA = z1 + kap1*(z2 - z1);
+      const double xB = x1 + kap2*(x2 - x1), yB = y1 + kap2*(y2 - y1), zB = z1 + kap2*(z2 - z1);
+      deposit_segment (r, i, j, k, x1, xA, y1, yA, z1, zA, rho);
+      i += dIdx[first][0];
+      j += dIdx[first][1];
+      k += dIdx[first][2];
+      deposit_segment (r, i, j, k, xA, xB, yA, yB, zA, zB, rho);
+      i += dIdx[1 - first][0];
+      j += dIdx[1 - first][1];
+      k += dIdx[1 - first][2];
+      deposit_segment (r, i, j, k, xB, x2, yB, y2, zB, z2, rho);
+      return;
+   }
+
+   const double xC = (i1 + i2 + 1)*0.5*h1, yC = (j1 + j2 + 1)*0.5*h2, zC = (k1 + k2 + 1)*0.5*h3;
+   double s1 = (xC - x1)/(x2 - x1), s2 = (yC - y1)/(y2 - y1), s3 = (zC - z1)/(z2 - z1);
+   double rc[3][3];
+   int dI[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+   int a = 0, b = 1, c = 2, i = i1, j = j1, k = k1;
+   rc[0][0] = xC;
+   rc[0][1] = y1 + s1*(y2 - y1);
+   rc[0][2] = z1 + s1*(z2 - z1);
+   dI[0][0] = i2 - i1;
+   rc[1][0] = x1 + s2*(x2 - x1);
+   rc[1][1] = yC;
+   rc[1][2] = z1 + s2*(z2 - z1);
+   dI[1][1] = j2 - j1;
+   rc[2][0] = x1 + s3*(x2 - x1);
+   rc[2][1] = y1 + s3*(y2 - y1);
+   rc[2][2] = zC;
+   dI[2][2] = k2 - k1;
+   if (s1 > s2) { SWAPI (a, b); SWAPD (s1, s2); }
+   if (s1 > s3) { SWAPI (a, c); SWAPD (s1, s3); }
+   if (s2 > s3) { SWAPI (b, c); SWAPD (s2, s3); }
+   deposit_segment (r, i, j, k, x1, rc[a][0], y1, rc[a][1], z1, rc[a][2], rho);
+   i += dI[a][0]; j += dI[a][1]; k += dI[a][2];
+   deposit_segment (r, i, j, k, rc[a][0], rc[b][0], rc[a][1], rc[b][1], rc[a][2], rc[b][2], rho);
+   i += dI[b][0]; j += dI[b][1]; k += dI[b][2];
+   deposit_segment (r, i, j, k, rc[b][0], rc[c][0], rc[b][1], rc[c][1], rc[b][2], rc[c][2], rho);
+   deposit_segment (r, i2, j2, k2, rc[c][0], x2, rc[c][1], y2, rc[c][2], z2, rho);
+}
+
+/* CIC read of one component (misc_PIC.h:72-126, 3D).  The macro expands to
+ * one flat left-to-right sum of eight terms; the same order is kept. */
+static inline double cic (const double *F, const po_run_t *r, int i, double sx,
+                          int j, double sy, int k, double sz)
+{
+   const long o = IX (r, i, j, k), Sx = r->s[0], Sy = r->s[1];
+   return F[o]*(1 - sx)*((1 - sy)*(1 - sz)) + F[o + Sx]*sx*((1 - sy)*(1 - sz))
+        + F[o + Sy]*(1 - sx)*(sy*(1 - sz)) + F[o + Sx + Sy]*sx*(sy*(1 - sz))
+        + F[o + 1]*(1 - sx)*((1 - sy)*sz) + F[o + Sx + 1]*sx*((1 - sy)*sz)
+        + F[o + Sy + 1]*(1 - sx)*(sy*sz) + F[o + Sx + Sy + 1]*sx*(sy*sz);
+}
+
+/* Particle boundary conditions, faces in the reference's order
+ * xMin, yMin, zMin, xMax, yMax, zMax (core/plasma_walls.c:27-104).
+ * Returns 1 if the marker is removed. */
+static int particle_bc (const po_run_t *r, po_marker_t *m)
+{
+   double *pos[3] = {&m->x, &m->y, &m->z};
+   double *vel[3] = {&m->vx, &m->vy, &m->vz};
+   const double L[3] = {r->n[0]*r->h[0], r->n[1]*r->h[1], r->n[2]*r->h[2]};
+   for (int f = 0 ; f < 6 ; ++f) {
+      const int a = f % 3, top = f / 3;
+      const int bc = r->bc[top][a];
+      double *x = pos[a];
+      if (bc == PO_BC_PERIODIC) {
+         if (!top && *x <= 0) *x += L[a];
+         if (top && *x >= L[a]) *x -= L[a];
+      } else if (bc == PO_BC_MIRROR) {
+         if (!top && *x <= 0) { *x = -*x; *vel[a] *= -1; }
+         if (top && *x >= L[a]) { *x = 2*L[a] - *x; *vel[a] *= -1; }
+      } else {
+         if (!top && *x <= r->h[a]) return 1;
+         if (top && *x >= L[a] - r->h[a]) return 1;
+      }
+   }
+   return 0;
+}
+
+/* plasma_timestep (core/plasma.c:95-263) over all markers; the shell/core
+ * split only orders the work and is dropped. */
+void po_plasma_move (po_run_t *r, double wt[3])
+{
+   const double h1 = r->h[0], h2 = r->h[1], h3 = r->h[2], tau = r->tau;
+   const long total = (long) r->dim[0]*r->s[0];
+   for (int c = 0 ; c < 3 ; ++c)
+      memset (r->j[c], 0, total*sizeof (double));
+   double Wx = 0, Wy = 0, Wz = 0;
+   long keep = 0;
+   for (long n = 0 ; n < r->np ; ++n) {
+      po_marker_t *p = r->p + n;
+      const double x1 = p->x, y1 = p->y, z1 = p->z;
+      double sX = x1/h1, sY = y1/h2, sZ = z1/h3;
+      double sX_ = sX + 0.5, sY_ = sY + 0.5, sZ_ = sZ + 0.5;
+      const int i = dbl_to_int (sX), j = dbl_to_int (sY), k = dbl_to_int (sZ);
+      const int i_ = dbl_to_int (sX_), j_ = dbl_to_int (sY_), k_ = dbl_to_int (sZ_);
+      sX -= i; sY -= j; sZ -= k;
+      sX_ -= i_; sY_ -= j_; sZ_ -= k_;
+
+      const double Ex = cic (r->e[0], r, i_, sX_, j, sY, k, sZ);
+      const double Ey = cic (r->e[1], r, i, sX, j_, sY_, k, sZ);
+      const double Ez = cic (r->e[2], r, i, sX, j, sY, k_, sZ_);
+      const double Hx = cic (r->b[0], r, i, sX, j_, sY_, k_, sZ_);
+      const double Hy = cic (r->b[1], r, i_, sX_, j, sY, k_, sZ_);
+      const double Hz = cic (r->b[2], r, i_, sX_, j_, sY_, k, sZ);
+
+      const double tm = 0.5*tau*p->qDivM;
+      const double px = p->vx + tm*Ex, py = p->vy + tm*Ey, pz = p->vz + tm*Ez;
+      const double gamma = sqrt (1 + px*px + py*py + pz*pz);
+      const double W = (gamma - 1.0)*p->rho/(px*px + py*py + pz*pz + 1e-19)*h1*h2*h3/p->qDivM;
+      Wx += W*px*px;
+      Wy += W*py*py;
+      Wz += W*pz*pz;
+
+      const double tg = tm/gamma;
+      const double ax = tg*Hx, ay = tg*Hy, az = tg*Hz;
+      const double u = px + py*az - pz*ay, v = py + pz*ax - px*az, w = pz + px*ay - py*ax;
+      const double bxx = ax*ax, byy = ay*ay, bzz = az*az;
+      const double bxy = ax*ay, byz = ay*az, bxz = az*ax;
+      const double delta = 1.0/(1 + bxx + byy + bzz);
+      p->vx = tm*Ex + ((1 + bxx)*u + (bxy + az)*v + (bxz - ay)*w)*delta;
+      p->vy = tm*Ey + ((bxy - az)*u + (1 + byy)*v + (byz + ax)*w)*delta;
+      p->vz = tm*Ez + ((bxz + ay)*u + (byz - ax)*v + (1 + bzz)*w)*delta;
+
+      const double tgi = tau/sqrt (1 + p->vx*p->vx + p->vy*p->vy + p->vz*p->vz);
+      const double x2 = p->x + p->vx*tgi, y2 = p->y + p->vy*tgi, z2 = p->z + p->vz*tgi;
+
+      int i2 = dbl_to_int (x2/h1), j2 = dbl_to_int (y2/h2), k2 = dbl_to_int (z2/h3);
+      int di = abs (i2 - i), dj = abs (j2 - j), dk = abs (k2 - k);
+      if (fabs (x2 - x1) < 1e-10*h1) { di = 0; i2 = i; }
+      if (fabs (y2 - y1) < 1e-10*h2) { dj = 0; j2 = j; }
+      if (fabs (z2 - z1) < 1e-10*h3) { dk = 0; k2 = k; }
+
+      if (di + dj + dk == 0) {
+         deposit_segment (r, i, j, k, x1, x2, y1, y2, z1, z2, p->rho);
+      } else if (di + dj + dk == 1) {
+         const double alpha = dk*((k + k2 + 1)*0.5*h3 - z1)/(z2 - z1 + ((1 - dk) << 16))
+                            + dj*((j + j2 + 1)*0.5*h2 - y1)/(y2 - y1 + ((1 - dj) << 16))
+                            + di*((i + i2 + 1)*0.5*h1 - x1)/(x2 - x1 + ((1 - di) << 16));
+         const double xC = x1 + alpha*(x2 - x1), yC = y1 + alpha*(y2 - y1), zC = z1 + alpha*(z2 - z1);
+         deposit_segment (r, i, j, k, x1, xC, y1, yC, z1, zC, p->rho);
+         deposit_segment (r, i2, j2, k2, xC, x2, yC, y2, zC, z2, p->rho);
+      } else {
+         deposit_multicell (r, i, j, k, i2, j2, k2, x1, y1, z1, x2, y2, z2, p->rho);
+      }
+      p->x = x2;
+      p->y = y2;
+      p->z = z2;
+      if (!particle_bc (r, p))
+         r->p[keep++] = *p;
+   }
+   r->np = keep;
+   wt[0] = Wx;
+   wt[1] = Wy;
+   wt[2] = Wz;
+}
+
+/* Current boundary conditions (core/plasma_currentWalls.c:27-121); faces in
+ * the order x-min, x-max, y-min, y-max, z-min, z-max; transverse extent
+ * [-2, n+2]. */
+void po_jbc (po_run_t *r)
+{
+   for (int f = 0 ; f < 6 ; ++f) {
+      const int ea = f >> 1, top = f & 1;
+      const int ep = (ea == 0) ? 1 : 0, eq = (ea == 2) ? 1 : 2;
+      const int N = r->n[ea];
+      const int bc = r->bc[top][ea];
+      double *J[3] = {r->j[0], r->j[1], r->j[2]};
+      if (bc == PO_BC_PERIODIC) {
+         if (top)
+            continue;
+         const long shift = (long) N*r->s[ea];
+         for (int p = -2 ; p <= r->n[ep] + 2 ; ++p)
+         for (int q = -2 ; q <= r->n[eq] + 2 ; ++q)
+         for (int a = -2 ; a <= 2 ; ++a) {
+            long o = IXA (r, ea, a, ep, p, eq, q);
+            for (int c = 0 ; c < 3 ; ++c) {
+               J[c][o + shift] += J[c][o];
+               J[c][o] = J[c][o + shift];
+            }
+         }
+         continue;
+      }
+      const long st = r->s[ea];
+      const long internal = (1 - top)*st, external = top*st;
+      const long out = st*(2*top - 1);
+      for (int p = -2 ; p <= r->n[ep] + 2 ; ++p)
+      for (int q = -2 ; q <= r->n[eq] + 2 ; ++q) {
+         const long o = IXA (r, ea, top ? N : 0, ep, p, eq, q);
+         double *Ja = J[ea], *Jp = J[ep], *Jq = J[eq];
+         Ja[o + internal] -= Ja[o + external];
+         Jp[o - out] += Jp[o + out];
+         Jq[o - out] += Jq[o + out];
+         Ja[o + internal - out] -= Ja[o + external + out];
+         Jp[o - 2*out] += Jp[o + 2*out];
+         Jq[o - 2*out] += Jq[o + 2*out];
+         Jp[o] = Jq[o] = 0;
+         Ja[o + external] = Ja[o + internal];
+         Jp[o + out] = -Jp[o - out];
+         Jq[o + out] = -Jq[o - out];
+         Ja[o + external + out] = Ja[o + internal - out];
+         Jp[o + 2*out] = -Jp[o - 2*out];
+         Jq[o + 2*out] = -Jq[o - 2*out];
+      }
+   }
+}
+
+/* em_EStep_addCurrents (core/em.c:167-184): E -= tau*J over [-1, n+1]. */
+static void e_sub_current (po_run_t *r)
+{
+   for (int i = -1 ; i <= r->n[0] + 1 ; ++i)
+   for (int j = -1 ; j <= r->n[1] + 1 ; ++j)
+   for (int k = -1 ; k <= r->n[2] + 1 ; ++k) {
+      long o = IX (r, i, j, k);
+      for (int c = 0 ; c < 3 ; ++c)
+         r->e[c][o] -= r->tau*r->j[c][o];
+   }
+}
+
+/* em_energy (core/em.c:227-252). */
+void po_em_energy (const po_run_t *r, double *we_out, double *wm_out)
+{
+   double we = 0, wb = 0;
+   const long sx = r->s[0], sy = r->s[1];
+   for (int i = 0 ; i < r->n[0] ; ++i)
+   for (int j = 0 ; j < r->n[1] ; ++j)
+   for (int k = 0 ; k < r->n[2] ; ++k) {
+      long o = IX (r, i, j, k);
+      double ex = r->e[0][o + sx], ey = r->e[1][o + sy], ez = r->e[2][o + 1];
+      double hx = r->b[0][o + sy + 1], hy = r->b[1][o + sx + 1], hz = r->b[2][o + sx + sy];
+      we += ex*ex + ey*ey + ez*ez;
+      wb += hx*hx + hy*hy + hz*hz;
+   }
+   const double v = r->h[0]*r->h[1]*r->h[2];
+   *we_out = 0.5*we*v;
+   *wm_out = 0.5*wb*v;
+}
+
+/* em_HHalfStep (core/em.c:85-110): H^(n-1/2) -> H^n. */
+void po_em_h_half (po_run_t *r)
+{
+   h_advance (r, 0.5);
+   h_bc (r);
+}
+
+/* em_HStep (core/em.c:115-131): H^n -> H^(n+1/2) plus source at t = n*tau. */
+void po_em_h_step (po_run_t *r)
+{
+   h_advance (r, 0.5);
+   if (r->has_laser)
+      laser_h (r, r->time);
+   h_bc (r);
+}
+
+/* em_EStep_start + cap E update and boundary conditions. */
+void po_em_e_step (po_run_t *r)
+{
+   e_advance (r);
+   e_bc (r);
+}
+
+/* em_EStep_finish (core/em.c:189-222): source at t + tau/2, E -= tau*J. */
+void po_em_e_finish (po_run_t *r)
+{
+   if (r->has_laser)
+      laser_e (r, r->time + 0.5*r->tau);
+   e_sub_current (r);
+}
+
+/* One step in core/main.c:353-478 order. */
+int po_step (po_run_t *r, double out[5])
+{
+   double we, wm, wt[3];
+   po_em_h_half (r);
+   po_em_energy (r, &we, &wm);
+   po_plasma_move (r, wt);
+   po_em_h_step (r);
+   po_em_e_step (r);
+   po_jbc (r);
+   po_em_e_finish (r);
+   r->time += r->tau;
+   if (out) {
+      out[0] = we;
+      out[1] = wm;
+      out[2] = wt[0];
+      out[3] = wt[1];
+      out[4] = wt[2];
+   }
+   return 0;
+}
+
+/* CIC charge density: core/plasma_rho.c:23-60 restated (no folding). */
+void po_rho (const po_run_t *r, double *rho)
+{
+   const int d1 = r->dim[1], d2 = r->dim[2];
+   memset (rho, 0, sizeof (double)*(long) r->dim[0]*d1*d2);
+   for (long n = 0 ; n < r->np ; ++n) {
+      const po_marker_t *p = r->p + n;
+      double sx = p->x/r->h[0], sy = p->y/r->h[1], sz = p->z/r->h[2];
+      int i = dbl_to_int (sx), j = dbl_to_int (sy), k = dbl_to_int (sz);
+      sx -= i; sy -= j; sz -= k;
+      long o = IX (r, i, j, k), Sx = r->s[0], Sy = r->s[1];
+      double v = p->rho;
+      rho[o]               += (1 - sx)*(1 - sy)*(1 - sz)*v;
+      rho[o + Sx]          += sx*(1 - sy)*(1 - sz)*v;
+      rho[o + Sy]          += (1 - sx)*sy*(1 - sz)*v;
+      rho[o + Sx + Sy]     += sx*sy*(1 - sz)*v;
+      rho[o + 1]           += (1 - sx)*(1 - sy)*sz*v;
+      rho[o + Sx + 1]      += sx*(1 - sy)*sz*v;
+      rho[o + Sy + 1]      += (1 - sx)*sy*sz*v;
+      rho[o + Sx + Sy + 1] += sx*sy*sz*v;
+   }
+}
+
+/* ------------------------------------------------------------------------
+ * ranmar: misc_ranmar.c:79-146 restated (Marsaglia & Zaman, FSU-SCRI-87-50,
+ * as modified by F. James).
+ * ---------------------------------------------------------------------- */
+void po_ranmar_init (po_ranmar_t *g, int ij, int kl)
+{
+   int i = (ij/177)%177 + 2, j = ij%177 + 2, k = (kl/169)%178 + 1, l = kl%169;
+   for (int ii = 0 ; ii < 97 ; ii++) {
+      double s = 0, t = 0.5;
+      for (int jj = 0 ; jj < 24 ; jj++) {
+         int m = (((i*j)%179)*k)%179;
+         i = j;
+         j = k;
+         k = m;
+         l = (53*l + 1)%169;
+         if ((l*m)%64 >= 32)
+            s += t;
+         t *= 0.5;
+      }
+      g->u[ii] = s;
+   }
+   g->c  = 362436.0/16777216.0;
+   g->cd = 7654321.0/16777216.0;
+   g->cm = 16777213.0/16777216.0;
+   g->i97 = 96;
+   g->j97 = 32;
+}
+
+void po_ranmar (po_ranmar_t *g, double *out, long n)
+{
+   for (long v = 0 ; v < n ; v++) {
+      double uni = g->u[g->i97] - g->u[g->j97];
+      if (uni < 0.0) uni += 1.0;
+      g->u[g->i97] = uni;
+      g->i97 = (g->i97 + 96)%97;
+      g->j97 = (g->j97 + 96)%97;
+      g->c -= g->cd;
+      if (g->c < 0.0) g->c += g->cm;
+      uni -= g->c;
+      if (uni < 0.0) uni += 1.0;
+      out[v] = uni;
+   }
+}
+
+long po_place_count (const po_place_t *s)
+{
+   long cells = 1;
+   for (int a = 0 ; a < 3 ; ++a)
+      cells *= (s->hi[a] > s->lo[a]) ? (s->hi[a] - s->lo[a]) : 0;
+   return cells*s->ppc;
+}
+
+long po_place (const po_place_t *s, const double h[3], po_marker_t *out)
+{
+   po_ranmar_t g;
+   po_ranmar_init (&g, s->seed_ij, s->seed_kl);
+   double d[7];
+   for (long k = s->skip ; k > 0 ; ) {
+      long c = (k > 7) ? 7 : k;
+      po_ranmar (&g, d, c);
+      k -= c;
+   }
+   long n = 0;
+   for (int i = s->lo[0] ; i < s->hi[0] ; ++i)
+   for (int j = s->lo[1] ; j < s->hi[1] ; ++j)
+   for (int k = s->lo[2] ; k < s->hi[2] ; ++k)
+   for (int q = 0 ; q < s->ppc ; ++q, ++n) {
+      po_ranmar (&g, d, 7);
+      po_marker_t *m = out + n;
+      m->x = (i + d[0])*h[0];
+      m->y = (j + d[1])*h[1];
+      m->z = (k + d[2])*h[2];
+      const double r1 = sqrt (-2.0*log (1.0 - d[3])), t1 = 2*M_PI*d[4];
+      const double r2 = sqrt (-2.0*log (1.0 - d[5])), t2 = 2*M_PI*d[6];
+      m->vx = s->drift[0] + s->uth[0]*(r1*cos (t1));
+      m->vy = s->drift[1] + s->uth[1]*(r1*sin (t1));
+      m->vz = s->drift[2] + s->uth[2]*(r2*cos (t2));
+      m->rho = (float) s->rho;
+      m->qDivM = (float) s->qDivM;
+      m->id = s->id0 + (int) n;
+      m->pad_ = 0;
+   }
+   return n;
+}

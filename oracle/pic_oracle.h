@@ -1,0 +1,122 @@
+/* CPU restatement of Mandor's PIC time step (TEST INFRASTRUCTURE ONLY).
+ *
+ * This is the oracle the CUDA path is checked against.  It restates, in
+ * plain C on one global mesh with ghost layers, what the reference core.out
+ * does per step (core/main.c:353-478): Yee H half-steps, E step, field
+ * boundary conditions, the relativistic Boris push with CIC gather and the
+ * charge-conserving current deposition, particle and current boundary
+ * conditions, and the energy diagnostics.  It is pinned against the
+ * reference binaries built from source (oracle/Makefile) by the tests.
+ *
+ * Only tests/, the package smoke check and the bench's CPU-baseline leg may
+ * load it.  It is never part of the product path.
+ */
+#ifndef PIC_ORACLE_H
+#define PIC_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Marker record of the reference with the tracer id (type_marker.h:12-25). */
+typedef struct {
+   double x, y, z;
+   double vx, vy, vz;
+   float  rho;
+   float  qDivM;
+   int    id;
+   int    pad_;
+} po_marker_t;
+
+/* Boundary condition codes (misc_parameters.h:38-42). */
+enum { PO_BC_PERIODIC = 0, PO_BC_MIRROR = 1, PO_BC_OPEN = 2 };
+
+/* Analytic laser: paraxial Gaussian beam, Ey-polarised, moving along +x,
+ * with a sin^2 field envelope, injected as a one-sided soft source at the
+ * x-planes i = plane (H) and i = plane - 1 (E). */
+typedef struct {
+   double a0;          /* normalised amplitude; E amplitude = 2*pi*a0      */
+   double waist;       /* w0, in wavelengths                               */
+   double x_focus;     /* focal plane position                             */
+   double duration;    /* sin^2 envelope length (field), in periods        */
+   double t_start;     /* time the envelope front crosses the source plane */
+   double phase;       /* carrier phase offset                             */
+   int    plane;       /* H plane index (E plane is plane - 1)             */
+   int    margin;      /* transverse nodes kept free next to each wall     */
+} po_laser_t;
+
+typedef struct po_run po_run_t;
+
+po_run_t *po_create (const int n[3], const double h[3], double tau,
+                     const int bc_min[3], const int bc_max[3], double time);
+void      po_destroy (po_run_t *r);
+
+/* Fields over the checkpoint region [0,n] per axis, reference AoS layout
+ * (vec3D_t, k fastest, i slowest). */
+void po_set_fields (po_run_t *r, const double *E, const double *H);
+void po_get_fields (const po_run_t *r, double *E, double *H);
+void po_get_current (const po_run_t *r, double *J);   /* region [-2,n+2] */
+
+void po_set_markers (po_run_t *r, const po_marker_t *m, long n);
+long po_marker_count (const po_run_t *r);
+void po_get_markers (const po_run_t *r, po_marker_t *m);
+
+void po_set_laser (po_run_t *r, const po_laser_t *l);
+
+/* em_init / cap_init equivalent: ghost fill and Mur history from E. */
+void po_init (po_run_t *r);
+
+/* One full time step; out[5] = {W_E, W_M, W_Tx, W_Ty, W_Tz} at t = n*tau
+ * (wDensity_addPoint arguments).  Returns 0. */
+int  po_step (po_run_t *r, double out[5]);
+double po_time (const po_run_t *r);
+
+/* Stage-level entry points (same order as core/main.c's loop). */
+void po_em_h_half (po_run_t *r);
+void po_em_energy (const po_run_t *r, double *we, double *wm);
+void po_plasma_move (po_run_t *r, double wt[3]);
+void po_em_h_step (po_run_t *r);
+void po_em_e_step (po_run_t *r);
+void po_jbc (po_run_t *r);
+void po_em_e_finish (po_run_t *r);
+
+/* Charge density (plasma_rho.c restated), region [-2,n+2]. */
+void po_rho (const po_run_t *r, double *rho);
+
+/* Marsaglia-Zaman "ranmar" generator (misc_ranmar.c:79-146 restated). */
+typedef struct {
+   double u[97], c, cd, cm;
+   int    i97, j97;
+} po_ranmar_t;
+
+void po_ranmar_init (po_ranmar_t *g, int ij, int kl);
+void po_ranmar (po_ranmar_t *g, double *out, long n);
+
+/* Uniform random placer (new component, no reference counterpart).  Cells
+ * [lo,hi) per axis in i-major, k-minor order; per marker seven draws:
+ * three in-cell offsets, then two Box-Muller pairs of which the first three
+ * normals scale u_th.  Stream = ranmar(ij,kl) after `skip` draws. */
+typedef struct {
+   int    lo[3], hi[3];
+   int    ppc;
+   double rho;          /* marker weight (charge density per marker)  */
+   double qDivM;
+   double drift[3];     /* mean u = gamma v / c                       */
+   double uth[3];       /* per-axis normal spread of u                */
+   int    seed_ij, seed_kl;
+   long   skip;
+   int    id0;          /* first id (ids are consecutive)             */
+} po_place_t;
+
+long po_place_count (const po_place_t *s);
+long po_place (const po_place_t *s, const double h[3], po_marker_t *out);
+
+/* Laser incident field used by the soft source (for tests). */
+double po_laser_ey (const po_laser_t *l, double x, double y, double z,
+                    double t, double ymid, double zmid);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

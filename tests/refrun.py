@@ -1,0 +1,172 @@
+"""Test infrastructure: run the reference Mandor binaries and read/write their
+binary formats with numpy.
+
+The reference ``setup.out`` / ``core.out`` are built from the reference
+sources by ``oracle/Makefile`` into ``oracle/_ref``.  A run directory gets the
+layout ``core.out`` expects (``binData/``, ``output/logs``, ``tmp``,
+``.EM_sources``) and a stub ``source/import.pl`` that hands the reference's
+command-line parser (source/commandLine.c:89) an empty option list.
+
+Formats (reference file:line):
+  * marker file: ``long N`` + N x ``marker_t`` (64 B with the tracer id),
+    core/plasma_IO.c:273-287, type_marker.h:12-25;
+  * mesh file: 6 x int32 valid region + the 88-byte ``mesh_t`` struct + the
+    region's nodes, k fastest, 24 B per vector node, type_mesh.c:285-313;
+  * ``diag.dat``: text, 10 columns, core/diag_WDensity.c:89-104.
+"""
+import os
+import shutil
+import subprocess
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+
+MARKER_DTYPE = np.dtype([("x", "<f8"), ("y", "<f8"), ("z", "<f8"),
+                         ("vx", "<f8"), ("vy", "<f8"), ("vz", "<f8"),
+                         ("rho", "<f4"), ("qDivM", "<f4"), ("id", "<i4"),
+                         ("pad", "<i4")])
+assert MARKER_DTYPE.itemsize == 64
+
+MESH_HEADER_BYTES = 6 * 4 + 88
+
+BC = {"periodic": 0, "mirror": 1, "open": 2, "mur": 2}
+
+
+def have_reference():
+    return all(os.path.exists(os.path.join(REF_DIR, f))
+               for f in ("setup.out", "core.out"))
+
+
+def read_markers(path):
+    with open(path, "rb") as fp:
+        n = int(np.frombuffer(fp.read(8), "<i8")[0])
+        return np.frombuffer(fp.read(n * 64), MARKER_DTYPE).copy()
+
+
+def write_markers(path, m):
+    m = np.ascontiguousarray(m, MARKER_DTYPE)
+    with open(path, "wb") as fp:
+        fp.write(np.array([len(m)], "<i8").tobytes())
+        fp.write(m.tobytes())
+
+
+def read_mesh(path):
+    """Returns (region(6 ints), raw header bytes, array[ni, nj, nk, 3])."""
+    with open(path, "rb") as fp:
+        raw = fp.read()
+    reg = np.frombuffer(raw[:24], "<i4")
+    ni, nj, nk = (reg[3] - reg[0] + 1, reg[4] - reg[1] + 1, reg[5] - reg[2] + 1)
+    data = np.frombuffer(raw[MESH_HEADER_BYTES:], "<f8")
+    return reg.copy(), raw[:MESH_HEADER_BYTES], data.reshape(ni, nj, nk, 3).copy()
+
+
+def write_mesh(path, header, arr):
+    with open(path, "wb") as fp:
+        fp.write(header)
+        fp.write(np.ascontiguousarray(arr, "<f8").tobytes())
+
+
+def read_domain(path):
+    with open(path, "rb") as fp:
+        raw = fp.read()
+    d = np.frombuffer(raw[:56], "<f8")
+    ints = np.frombuffer(raw[56:104], "<i4")
+    return {"h": d[0:3].copy(), "L": d[3:6].copy(), "tau": float(d[6]),
+            "dmn_min": ints[0:3].copy(), "dmn_max": ints[3:6].copy(),
+            "bc_min": ints[6:9].copy(), "bc_max": ints[9:12].copy()}
+
+
+def read_diag(path):
+    rows = []
+    with open(path) as fp:
+        for line in fp:
+            parts = line.split()
+            if len(parts) == 10:
+                try:
+                    rows.append([float(v) for v in parts])
+                except ValueError:
+                    pass
+    return np.array(rows)
+
+
+def deck_text(n, L_um, tau, bc_min, bc_max, lambda_um=1.0):
+    """A minimal setup deck: units, mesh and boundary tags only."""
+    lines = ["[units]", "@ %r\tlambda [microns]" % lambda_um, "",
+             "[mesh]"]
+    # Every value line carries a comment: cfg_readDouble's format
+    # "@ %le %*[^\n] " (misc_cfgReader.c:62) would otherwise swallow the
+    # next line as the comment.
+    lines += ["@ %d\tcells" % v for v in n]
+    lines += ["@ %.17g\tlength [microns]" % v for v in L_um]
+    lines += ["@ %.17g\ttau" % tau, "", "[boundaryConditions]"]
+    for a in range(3):
+        lines += ["@ %d\tmin" % bc_min[a], "@ %d\tmax" % bc_max[a]]
+    return "\n".join(lines) + "\n"
+
+
+class RefRun:
+    """One reference run directory."""
+
+    def __init__(self, workdir=None):
+        self.dir = workdir or tempfile.mkdtemp(prefix="mandor_ref_")
+        for d in ("source", "binData", "output/logs", "tmp",
+                  ".EM_sources/TFSF", ".EM_sources/laser"):
+            os.makedirs(os.path.join(self.dir, d), exist_ok=True)
+        stub = os.path.join(self.dir, "source", "import.pl")
+        with open(stub, "w") as fp:
+            fp.write("#!/bin/sh\necho BYE\n")
+        os.chmod(stub, 0o755)
+
+    def path(self, *p):
+        return os.path.join(self.dir, *p)
+
+    def setup(self, n, L_um, tau, bc_min, bc_max):
+        with open(self.path("deck.input"), "w") as fp:
+            fp.write(deck_text(n, L_um, tau, bc_min, bc_max))
+        self._run("setup.out", "deck.input", "create")
+        return read_domain(self.path("binData", "domain.bin"))
+
+    def set_state(self, markers=None, E=None, H=None):
+        if markers is not None:
+            write_markers(self.path("binData", "plasma_000000_000.bin"), markers)
+        for name, arr in (("E", E), ("H", H)):
+            if arr is not None:
+                f = self.path("binData", "sys_%s_000000(000).bin" % name)
+                _, hdr, _ = read_mesh(f)
+                write_mesh(f, hdr, arr)
+
+    def run(self, steps, exe="core.out", timeout=3600):
+        with open(self.path("run_mandor.cfg"), "w") as fp:
+            fp.write("@ %d\ttotal steps\n@ %d\tcheckpoint period\n@ -1\ttecplot\n"
+                     "@ 0\tcontinue\n@ %d\tstop-flag period\n@ -100\tspectral dumps\n"
+                     % (steps, 10 ** 8, 10 ** 8))
+        try:
+            os.remove(self.path("tmp", "stop.flag"))
+        except FileNotFoundError:
+            pass
+        out = self._run(exe, timeout=timeout)
+        return out
+
+    def final(self, record=1):
+        m = read_markers(self.path("binData", "plasma_%06d_000.bin" % record))
+        _, _, E = read_mesh(self.path("binData", "sys_E_%06d(000).bin" % record))
+        _, _, H = read_mesh(self.path("binData", "sys_H_%06d(000).bin" % record))
+        return m, E, H
+
+    def diag(self):
+        return read_diag(self.path("binData", "diag.dat"))
+
+    def _run(self, exe, *args, timeout=3600):
+        res = subprocess.run([os.path.join(REF_DIR, exe)] + list(args),
+                             cwd=self.dir, stdout=subprocess.PIPE,
+                             stderr=subprocess.STDOUT, timeout=timeout)
+        text = res.stdout.decode(errors="replace")
+        if res.returncode != 0:
+            raise RuntimeError("%s failed (%d):\n%s" % (exe, res.returncode, text[-3000:]))
+        return text
+
+    def cleanup(self):
+        shutil.rmtree(self.dir, ignore_errors=True)
