@@ -1,0 +1,191 @@
+/* mandor_b200.h -- C ABI of the B200 particle-in-cell core.
+ *
+ * The reference Mandor (cvarin/mandor3) exposes no plugin or FFI layer: its
+ * hot path is the in-process L2 C API that core/main.c calls once per time
+ * step (core/em.h:32-39, core/plasma.h:82-87) over global meshes and the
+ * global marker array.  This header replaces that API with an opaque,
+ * device-resident run object:
+ *
+ *   reference call (file:line)                    replacement
+ *   em_init            (core/em.c:40-49)          mg_run_init
+ *   plasma_init        (core/plasma.c:343-418)    mg_run_init
+ *   em_HHalfStep       (core/em.c:85-110)         mg_em_HHalfStep
+ *   em_energy          (core/em.c:227-252)        mg_em_energy
+ *   plasma_move        (core/plasma.c:269-305)    mg_plasma_move
+ *   plasma_temperature (core/plasma.c:311-316)    mg_plasma_temperature
+ *   em_HStep           (core/em.c:115-131)        mg_em_HStep
+ *   em_EStep_start     (core/em.c:135-163)        mg_em_EStep_start
+ *   jbc_finish         (core/plasma_currentWalls.c:172-209)  mg_jbc_finish
+ *   em_EStep_finish    (core/em.c:189-222)        mg_em_EStep_finish
+ *   plasma_rho         (core/plasma.c:321-329)    mg_plasma_rho
+ *   sysIO_loadEM / plasma_load (IO_sys.c:130-142, core/plasma_IO.c:227-266)
+ *                                                 mg_run_set_fields / mg_run_set_markers
+ *   sysIO_save / plasma_save   (IO_sys.c:99-124, core/plasma_IO.c:273-287)
+ *                                                 mg_run_get_fields / mg_run_get_markers
+ *   the whole step loop (core/main.c:353-478)     mg_run_step
+ *
+ * Data crossing the boundary keeps the reference's layouts: fields are the
+ * checkpoint region [0,n] per axis of vec3D_t nodes (k fastest), markers are
+ * the 64-byte marker_t records with the tracer id.  Every call returns an
+ * int status (MG_OK == 0, negative on error) instead of the reference's
+ * ENSURE/DIE exit; mg_last_error() returns the message of the last failure
+ * on the calling thread.  Calls on one run are not thread-safe; distinct
+ * runs may be driven from distinct threads.
+ */
+#ifndef MANDOR_B200_H
+#define MANDOR_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MG_OK             0
+#define MG_ERR_CUDA      (-1)   /* CUDA runtime error                        */
+#define MG_ERR_ARG       (-2)   /* bad argument                              */
+#define MG_ERR_OOM       (-3)   /* device allocation failed                  */
+#define MG_ERR_STATE     (-4)   /* stage called out of order                 */
+#define MG_ERR_CAPACITY  (-5)   /* marker capacity exceeded                  */
+#define MG_ERR_BOUNDS    (-6)   /* device bounds check tripped (marker left
+                                   the J ghost layers: Courant violated)     */
+#define MG_ERR_IO        (-7)   /* file error in the host driver             */
+#define MG_ERR_ADMISSION (-8)   /* serving admission refused (HBM budget)    */
+#define MG_ERR_TIMEOUT   (-9)   /* bounded device wait gave up               */
+
+/* Boundary condition codes, same values as misc_parameters.h:38-42. */
+enum { MG_BC_PERIODIC = 0, MG_BC_MIRROR = 1, MG_BC_OPEN = 2 };
+
+/* Precision forms. */
+enum {
+   MG_FP64 = 0,         /* reference arithmetic: FP64 positions, momenta, fields */
+   MG_FP32_OFFSET = 1   /* int cell + FP32 offset, FP32 u/E/H/J, FP64 reductions */
+};
+
+/* marker_t with ACTIVATE_TRACER=1 (type_marker.h:12-25): 64 bytes. */
+typedef struct {
+   double x, y, z;       /* absolute position, wavelengths            */
+   double vx, vy, vz;    /* u = gamma v / c                           */
+   float  rho;           /* charge density weight                     */
+   float  qDivM;         /* charge to mass ratio                      */
+   int    id;            /* tracer id                                 */
+   int    pad_;
+} mg_marker_t;
+
+typedef struct {
+   int       n[3];        /* cells per axis (dmn_max, dmn_min = 0)     */
+   double    h[3];        /* mesh steps h1, h2, h3                     */
+   double    tau;         /* time step                                 */
+   int       bc_min[3];   /* MG_BC_* per axis, lower wall              */
+   int       bc_max[3];   /* MG_BC_* per axis, upper wall              */
+   double    time;        /* start time                                */
+   int       precision;   /* MG_FP64 or MG_FP32_OFFSET                 */
+   int       device;      /* CUDA device ordinal                       */
+   long long capacity;    /* marker capacity (0: grows on upload)      */
+   int       sort_every;  /* re-sort markers by tile every k steps (0 = default) */
+} mg_params_t;
+
+/* Analytic laser source: paraxial Gaussian beam, Ey polarised, moving along
+ * +x, sin^2 field envelope, injected as a one-sided soft source on the
+ * x-planes i = plane (H) and i = plane - 1 (E), with the injection pattern
+ * of the reference's plane soft source (scpic/em_mirror.c:666-717). */
+typedef struct {
+   double a0;          /* normalised amplitude; E amplitude = 2*pi*a0      */
+   double waist;       /* w0, wavelengths                                  */
+   double x_focus;     /* focal plane x, wavelengths                       */
+   double duration;    /* sin^2 envelope length, periods                   */
+   double t_start;     /* time the envelope front leaves x = 0             */
+   double phase;       /* carrier phase offset                             */
+   int    plane;       /* H plane index (E plane is plane - 1)             */
+   int    margin;      /* transverse nodes kept free next to each wall     */
+} mg_laser_t;
+
+/* Uniform random marker placement driven by the reference's ranmar
+ * generator (misc_ranmar.c:79-146).  Cells [lo, hi) per axis, i-major and
+ * k-minor; per marker seven consecutive draws: three in-cell offsets, then
+ * two Box-Muller pairs whose first three normals scale uth.  The stream is
+ * ranmar(seed_ij, seed_kl) after `skip` draws; marker m of the box uses
+ * draws [skip + 7m, skip + 7m + 7). */
+typedef struct {
+   int       lo[3], hi[3];
+   int       ppc;
+   double    rho;        /* weight per marker                               */
+   double    qDivM;
+   double    drift[3];
+   double    uth[3];
+   int       seed_ij, seed_kl;
+   long long skip;
+   int       id0;        /* id of the first marker; ids are consecutive     */
+} mg_place_t;
+
+typedef struct mg_run mg_run_t;
+
+/* ---- run lifetime ----------------------------------------------------- */
+int  mg_run_create (const mg_params_t *params, mg_run_t **out);
+int  mg_run_destroy (mg_run_t *run);
+
+/* ---- state in the reference layouts (host buffers) ----------------------
+ * Fields: E and H over [0,n0]x[0,n1]x[0,n2], 3 doubles per node, k fastest
+ * (the checkpoint region written by sysIO_save, type_mesh.c:285-313).     */
+int  mg_run_set_fields (mg_run_t *run, const double *E, const double *H);
+int  mg_run_get_fields (mg_run_t *run, double *E, double *H);
+/* J over [-2,n0+2]x[-2,n1+2]x[-2,n2+2] after mg_jbc_finish.                */
+int  mg_run_get_current (mg_run_t *run, double *J);
+int  mg_run_set_markers (mg_run_t *run, const mg_marker_t *m, long long n);
+/* Live markers, in device order (ids identify them, as in the reference). */
+int  mg_run_get_markers (mg_run_t *run, mg_marker_t *m, long long cap, long long *n);
+int  mg_run_marker_count (mg_run_t *run, long long *n);
+int  mg_run_set_laser (mg_run_t *run, const mg_laser_t *laser);
+int  mg_run_set_time (mg_run_t *run, double time);
+int  mg_run_get_time (mg_run_t *run, double *time);
+/* Appends markers placed on the device (bit-exact with the CPU placement). */
+int  mg_run_place_uniform (mg_run_t *run, const mg_place_t *spec);
+
+/* em_init + plasma_init: ghost refresh, Mur history, checks. */
+int  mg_run_init (mg_run_t *run);
+
+/* ---- stage API, one call per reference call of core/main.c:353-478 ---- */
+int  mg_em_HHalfStep (mg_run_t *run);
+int  mg_em_energy (mg_run_t *run, double *W_E, double *W_M);
+int  mg_plasma_move (mg_run_t *run);
+int  mg_plasma_temperature (mg_run_t *run, double *WTx, double *WTy, double *WTz);
+int  mg_em_HStep (mg_run_t *run);
+int  mg_em_EStep_start (mg_run_t *run);
+int  mg_jbc_finish (mg_run_t *run);
+int  mg_em_EStep_finish (mg_run_t *run);
+/* CIC charge density over [-2,n+2]^3 (not folded), host buffer.           */
+int  mg_plasma_rho (mg_run_t *run, double *rho);
+
+/* ---- whole steps --------------------------------------------------------
+ * Runs nsteps full time steps on the device.  If energies is not NULL it
+ * receives nsteps rows {t, W_E, W_M, W_Tx, W_Ty, W_Tz} (the arguments of
+ * wDensity_addPoint, core/diag_WDensity.c:136-147), copied back once at the
+ * end.  Steps are replayed from a captured CUDA graph.                     */
+int  mg_run_step (mg_run_t *run, int nsteps, double *energies);
+/* Same, but the energy rows stay on the device (device pointer, nsteps*6
+ * doubles); no host synchronisation.                                      */
+int  mg_run_step_async (mg_run_t *run, int nsteps, double *energies_dev);
+int  mg_run_synchronize (mg_run_t *run);
+/* The CUDA stream (cudaStream_t) the run launches on.                     */
+int  mg_run_stream (mg_run_t *run, void **stream);
+/* Device kernels launched per step (for launch accounting).               */
+int  mg_run_kernels_per_step (mg_run_t *run, int *count);
+/* Device memory the run holds, bytes.                                     */
+int  mg_run_device_bytes (mg_run_t *run, long long *bytes);
+/* Estimated device bytes for a run with these parameters and markers.     */
+long long mg_estimate_bytes (const mg_params_t *params, long long markers);
+
+/* Kernel-level timing of the last mg_run_step: average device time of the
+ * push kernel and of the whole step, milliseconds (CUDA events on the run's
+ * stream).  Enabled by mg_run_profile(run, 1).                            */
+int  mg_run_profile (mg_run_t *run, int enable);
+int  mg_run_last_timing (mg_run_t *run, double *push_ms, double *step_ms);
+
+const char *mg_last_error (void);
+const char *mg_version (void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

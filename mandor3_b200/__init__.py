@@ -1,0 +1,304 @@
+"""B200-native particle-in-cell core with the capabilities of Mandor's
+``core.out`` hot path.
+
+The compute lives in ``libmandor_b200.so`` (hand-written sm_100a CUDA kernels
+behind the C ABI declared in ``include/mandor_b200.h``).  This module is a
+thin ctypes mirror of that ABI for Python callers; there is no CPU fallback:
+importing the package without the built library, or creating a run without
+a CUDA device, raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+__all__ = ["Run", "Params", "Laser", "Place", "MARKER_DTYPE", "MandorError",
+           "BC_PERIODIC", "BC_MIRROR", "BC_OPEN", "FP64", "FP32_OFFSET",
+           "library_path", "load"]
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libmandor_b200.so")
+
+BC_PERIODIC, BC_MIRROR, BC_OPEN = 0, 1, 2
+FP64, FP32_OFFSET = 0, 1
+
+# marker_t with the tracer id (reference type_marker.h:12-25), 64 bytes.
+MARKER_DTYPE = np.dtype([("x", "<f8"), ("y", "<f8"), ("z", "<f8"),
+                         ("vx", "<f8"), ("vy", "<f8"), ("vz", "<f8"),
+                         ("rho", "<f4"), ("qDivM", "<f4"), ("id", "<i4"),
+                         ("pad", "<i4")])
+
+ERRORS = {-1: "cuda", -2: "argument", -3: "out of memory", -4: "stage order",
+          -5: "capacity", -6: "bounds", -7: "io", -8: "admission", -9: "timeout"}
+
+
+class MandorError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s error (%d): %s" % (ERRORS.get(code, "unknown"), code, msg))
+        self.code = code
+
+
+class Params(C.Structure):
+    _fields_ = [("n", C.c_int * 3), ("h", C.c_double * 3), ("tau", C.c_double),
+                ("bc_min", C.c_int * 3), ("bc_max", C.c_int * 3), ("time", C.c_double),
+                ("precision", C.c_int), ("device", C.c_int), ("capacity", C.c_longlong),
+                ("sort_every", C.c_int)]
+
+
+class Laser(C.Structure):
+    _fields_ = [("a0", C.c_double), ("waist", C.c_double), ("x_focus", C.c_double),
+                ("duration", C.c_double), ("t_start", C.c_double), ("phase", C.c_double),
+                ("plane", C.c_int), ("margin", C.c_int)]
+
+
+class Place(C.Structure):
+    _fields_ = [("lo", C.c_int * 3), ("hi", C.c_int * 3), ("ppc", C.c_int),
+                ("rho", C.c_double), ("qDivM", C.c_double),
+                ("drift", C.c_double * 3), ("uth", C.c_double * 3),
+                ("seed_ij", C.c_int), ("seed_kl", C.c_int), ("skip", C.c_longlong),
+                ("id0", C.c_int)]
+
+
+_lib = None
+
+
+def library_path():
+    return LIB_PATH
+
+
+def load():
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libmandor_b200.so is not built; run `python -m mandor3_b200.build` "
+                          "(the B200 core has no CPU path)")
+    lib = C.CDLL(LIB_PATH)
+    vp, i, ll, d = C.c_void_p, C.c_int, C.c_longlong, C.c_double
+    sig = {
+        "mg_run_create": [C.POINTER(Params), C.POINTER(vp)],
+        "mg_run_destroy": [vp],
+        "mg_run_set_fields": [vp, vp, vp],
+        "mg_run_get_fields": [vp, vp, vp],
+        "mg_run_get_current": [vp, vp],
+        "mg_run_set_markers": [vp, vp, ll],
+        "mg_run_get_markers": [vp, vp, ll, C.POINTER(ll)],
+        "mg_run_marker_count": [vp, C.POINTER(ll)],
+        "mg_run_set_laser": [vp, vp],
+        "mg_run_set_time": [vp, d],
+        "mg_run_get_time": [vp, C.POINTER(d)],
+        "mg_run_place_uniform": [vp, C.POINTER(Place)],
+        "mg_run_init": [vp],
+        "mg_em_HHalfStep": [vp],
+        "mg_em_energy": [vp, C.POINTER(d), C.POINTER(d)],
+        "mg_plasma_move": [vp],
+        "mg_plasma_temperature": [vp, C.POINTER(d), C.POINTER(d), C.POINTER(d)],
+        "mg_em_HStep": [vp],
+        "mg_em_EStep_start": [vp],
+        "mg_jbc_finish": [vp],
+        "mg_em_EStep_finish": [vp],
+        "mg_plasma_rho": [vp, vp],
+        "mg_run_step": [vp, i, vp],
+        "mg_run_step_async": [vp, i, vp],
+        "mg_run_synchronize": [vp],
+        "mg_run_stream": [vp, C.POINTER(vp)],
+        "mg_run_kernels_per_step": [vp, C.POINTER(i)],
+        "mg_run_device_bytes": [vp, C.POINTER(ll)],
+        "mg_run_profile": [vp, i],
+        "mg_run_last_timing": [vp, C.POINTER(d), C.POINTER(d)],
+    }
+    for name, args in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = i
+    lib.mg_estimate_bytes.argtypes = [C.POINTER(Params), ll]
+    lib.mg_estimate_bytes.restype = ll
+    lib.mg_last_error.restype = C.c_char_p
+    lib.mg_version.restype = C.c_char_p
+    _lib = lib
+    return lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise MandorError(rc, load().mg_last_error().decode(errors="replace"))
+
+
+def _f8(a):
+    return np.ascontiguousarray(a, dtype="<f8")
+
+
+class Run:
+    """One simulation held on one GPU (the reference's global meshes and
+    marker array, core/main.c:90-91, core/plasma.c:40-43)."""
+
+    def __init__(self, n, h, tau, bc_min, bc_max, time=0.0, precision=FP64,
+                 device=0, capacity=0, sort_every=0):
+        lib = load()
+        self.n = tuple(int(v) for v in n)
+        self.h = tuple(float(v) for v in h)
+        self.tau = float(tau)
+        self.precision = precision
+        p = Params((C.c_int * 3)(*self.n), (C.c_double * 3)(*self.h), self.tau,
+                   (C.c_int * 3)(*bc_min), (C.c_int * 3)(*bc_max), float(time),
+                   int(precision), int(device), int(capacity), int(sort_every))
+        self._params = p
+        ptr = C.c_void_p()
+        _check(lib.mg_run_create(C.byref(p), C.byref(ptr)))
+        self.ptr = ptr
+
+    def close(self):
+        if getattr(self, "ptr", None):
+            load().mg_run_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- state ------------------------------------------------------------
+    def field_shape(self):
+        return (self.n[0] + 1, self.n[1] + 1, self.n[2] + 1, 3)
+
+    def set_fields(self, E=None, H=None):
+        Ea = _f8(E) if E is not None else None
+        Ha = _f8(H) if H is not None else None
+        for a in (Ea, Ha):
+            if a is not None and a.size != int(np.prod(self.field_shape())):
+                raise ValueError("field arrays must hold %s doubles" % (self.field_shape(),))
+        _check(load().mg_run_set_fields(self.ptr, Ea.ctypes.data if Ea is not None else None,
+                                        Ha.ctypes.data if Ha is not None else None))
+
+    def fields(self):
+        E = np.zeros(self.field_shape())
+        H = np.zeros(self.field_shape())
+        _check(load().mg_run_get_fields(self.ptr, E.ctypes.data, H.ctypes.data))
+        return E, H
+
+    def current(self):
+        J = np.zeros((self.n[0] + 5, self.n[1] + 5, self.n[2] + 5, 3))
+        _check(load().mg_run_get_current(self.ptr, J.ctypes.data))
+        return J
+
+    def rho(self):
+        r = np.zeros((self.n[0] + 5, self.n[1] + 5, self.n[2] + 5))
+        _check(load().mg_plasma_rho(self.ptr, r.ctypes.data))
+        return r
+
+    def set_markers(self, m):
+        m = np.ascontiguousarray(m, MARKER_DTYPE)
+        _check(load().mg_run_set_markers(self.ptr, m.ctypes.data if len(m) else None, len(m)))
+
+    def marker_count(self):
+        n = C.c_longlong()
+        _check(load().mg_run_marker_count(self.ptr, C.byref(n)))
+        return n.value
+
+    def markers(self):
+        n = self.marker_count()
+        out = np.zeros(n, MARKER_DTYPE)
+        got = C.c_longlong()
+        _check(load().mg_run_get_markers(self.ptr, out.ctypes.data if n else None, n, C.byref(got)))
+        return out[:got.value]
+
+    def set_laser(self, **kw):
+        self._laser = Laser(**kw)
+        _check(load().mg_run_set_laser(self.ptr, C.byref(self._laser)))
+
+    def place_uniform(self, lo, hi, ppc, rho, qDivM, drift=(0, 0, 0), uth=(0, 0, 0),
+                      seed=(1802, 9373), skip=0, id0=1):
+        s = Place((C.c_int * 3)(*lo), (C.c_int * 3)(*hi), int(ppc), float(rho), float(qDivM),
+                  (C.c_double * 3)(*drift), (C.c_double * 3)(*uth), int(seed[0]), int(seed[1]),
+                  int(skip), int(id0))
+        _check(load().mg_run_place_uniform(self.ptr, C.byref(s)))
+
+    def set_time(self, t):
+        _check(load().mg_run_set_time(self.ptr, float(t)))
+
+    def time(self):
+        t = C.c_double()
+        _check(load().mg_run_get_time(self.ptr, C.byref(t)))
+        return t.value
+
+    def init(self):
+        _check(load().mg_run_init(self.ptr))
+
+    # -- stage API (core/main.c:353-478) -----------------------------------
+    def em_HHalfStep(self):
+        _check(load().mg_em_HHalfStep(self.ptr))
+
+    def em_energy(self):
+        we, wm = C.c_double(), C.c_double()
+        _check(load().mg_em_energy(self.ptr, C.byref(we), C.byref(wm)))
+        return we.value, wm.value
+
+    def plasma_move(self):
+        _check(load().mg_plasma_move(self.ptr))
+
+    def plasma_temperature(self):
+        v = [C.c_double() for _ in range(3)]
+        _check(load().mg_plasma_temperature(self.ptr, *[C.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
+    def em_HStep(self):
+        _check(load().mg_em_HStep(self.ptr))
+
+    def em_EStep_start(self):
+        _check(load().mg_em_EStep_start(self.ptr))
+
+    def jbc_finish(self):
+        _check(load().mg_jbc_finish(self.ptr))
+
+    def em_EStep_finish(self):
+        _check(load().mg_em_EStep_finish(self.ptr))
+
+    # -- whole steps -----------------------------------------------------------
+    def step(self, nsteps=1):
+        """Runs nsteps steps; returns rows {t, W_E, W_M, W_Tx, W_Ty, W_Tz}."""
+        rows = np.zeros((nsteps, 6))
+        _check(load().mg_run_step(self.ptr, int(nsteps), rows.ctypes.data if nsteps else None))
+        return rows
+
+    def step_async(self, nsteps, energies_dev=None):
+        _check(load().mg_run_step_async(self.ptr, int(nsteps), energies_dev))
+
+    def synchronize(self):
+        _check(load().mg_run_synchronize(self.ptr))
+
+    def stream(self):
+        s = C.c_void_p()
+        _check(load().mg_run_stream(self.ptr, C.byref(s)))
+        return s.value
+
+    def kernels_per_step(self):
+        k = C.c_int()
+        _check(load().mg_run_kernels_per_step(self.ptr, C.byref(k)))
+        return k.value
+
+    def device_bytes(self):
+        b = C.c_longlong()
+        _check(load().mg_run_device_bytes(self.ptr, C.byref(b)))
+        return b.value
+
+    def profile(self, enable=True):
+        _check(load().mg_run_profile(self.ptr, int(enable)))
+
+    def last_timing(self):
+        a, b = C.c_double(), C.c_double()
+        _check(load().mg_run_last_timing(self.ptr, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+
+def estimate_bytes(n, h, tau, bc_min, bc_max, markers, precision=FP64):
+    p = Params((C.c_int * 3)(*n), (C.c_double * 3)(*h), float(tau), (C.c_int * 3)(*bc_min),
+               (C.c_int * 3)(*bc_max), 0.0, int(precision), 0, 0, 0)
+    return load().mg_estimate_bytes(C.byref(p), int(markers))

@@ -1,0 +1,999 @@
+// C ABI of the B200 PIC core (declared in include/mandor_b200.h): run
+// lifetime, host<->device transfers in the reference's layouts, the stage
+// API that mirrors core/main.c's step, and the graph-replayed step loop.
+#include <cuda_runtime.h>
+
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "mg_internal.cuh"
+
+// ---------------------------------------------------------------------------
+// Errors.
+// ---------------------------------------------------------------------------
+static thread_local char g_err[1024];
+
+void mg_set_error (const char *fmt, ...)
+{
+   va_list ap;
+   va_start (ap, fmt);
+   vsnprintf (g_err, sizeof (g_err), fmt, ap);
+   va_end (ap);
+}
+
+extern "C" const char *mg_last_error (void) { return g_err; }
+extern "C" const char *mg_version (void) { return "mandor_b200 1.0 (sm_100a)"; }
+
+int mg_sm_count (void)
+{
+   static int count = 0;
+   if (!count) {
+      int dev = 0;
+      cudaGetDevice (&dev);
+      if (cudaDeviceGetAttribute (&count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || count <= 0)
+         count = 148;
+   }
+   return count;
+}
+
+#define CHECK_RUN(r)                                                         \
+   do {                                                                      \
+      if (!(r)) {                                                            \
+         mg_set_error ("%s: null run", __func__);                            \
+         return MG_ERR_ARG;                                                  \
+      }                                                                      \
+      cudaSetDevice ((r)->device);                                           \
+   } while (0)
+
+#define TRY(x)                                                               \
+   do {                                                                      \
+      int rc_ = (x);                                                         \
+      if (rc_ != MG_OK)                                                      \
+         return rc_;                                                         \
+   } while (0)
+
+// ---------------------------------------------------------------------------
+// Layout conversion kernels.
+// ---------------------------------------------------------------------------
+namespace {
+
+// Reference AoS region [0,n]^3 (k fastest) <-> device SoA.
+__global__ void k_fields_in (Grid g, const double *aos, double *c0, double *c1, double *c2)
+{
+   const long nk = g.n[2] + 1, nj = g.n[1] + 1, ni = g.n[0] + 1;
+   const long vol = ni*nj*nk;
+   for (long t = blockIdx.x*(long) blockDim.x + threadIdx.x ; t < vol ; t += (long) gridDim.x*blockDim.x) {
+      const int k = (int) (t % nk), j = (int) ((t / nk) % nj), i = (int) (t / (nk*nj));
+      const long o = g.at (i, j, k);
+      c0[o] = aos[3*t];
+      c1[o] = aos[3*t + 1];
+      c2[o] = aos[3*t + 2];
+   }
+}
+
+__global__ void k_fields_out (Grid g, double *aos, const double *c0, const double *c1, const double *c2,
+                              int ghost)
+{
+   const int lo = -ghost;
+   const long nk = g.n[2] + 1 + 2*ghost, nj = g.n[1] + 1 + 2*ghost, ni = g.n[0] + 1 + 2*ghost;
+   const long vol = ni*nj*nk;
+   for (long t = blockIdx.x*(long) blockDim.x + threadIdx.x ; t < vol ; t += (long) gridDim.x*blockDim.x) {
+      const int k = lo + (int) (t % nk), j = lo + (int) ((t / nk) % nj), i = lo + (int) (t / (nk*nj));
+      const long o = g.at (i, j, k);
+      aos[3*t] = c0[o];
+      aos[3*t + 1] = c1[o];
+      aos[3*t + 2] = c2[o];
+   }
+}
+
+__global__ void k_markers_in (const mg_marker_t *src, long long n, Markers64 m, long long at)
+{
+   for (long long t = blockIdx.x*(long long) blockDim.x + threadIdx.x ; t < n ; t += (long long) gridDim.x*blockDim.x) {
+      const mg_marker_t p = src[t];
+      const long long o = at + t;
+      m.x[o] = p.x;
+      m.y[o] = p.y;
+      m.z[o] = p.z;
+      m.ux[o] = p.vx;
+      m.uy[o] = p.vy;
+      m.uz[o] = p.vz;
+      m.rho[o] = p.rho;
+      m.qm[o] = p.qDivM;
+      m.id[o] = p.id;
+   }
+}
+
+// Live-marker flags and packing (removed markers carry qDivM = 0).
+__global__ void k_markers_out (Markers64 m, long long from, long long n, mg_marker_t *dst,
+                               const long long *slot)
+{
+   for (long long t = blockIdx.x*(long long) blockDim.x + threadIdx.x ; t < n ; t += (long long) gridDim.x*blockDim.x) {
+      const long long o = from + t;
+      const float qm = m.qm[o];
+      if (qm == 0.0f)
+         continue;
+      mg_marker_t p;
+      p.x = m.x[o];
+      p.y = m.y[o];
+      p.z = m.z[o];
+      p.vx = m.ux[o];
+      p.vy = m.uy[o];
+      p.vz = m.uz[o];
+      p.rho = m.rho[o];
+      p.qDivM = qm;
+      p.id = m.id[o];
+      p.pad_ = 0;
+      dst[slot[t]] = p;
+   }
+}
+
+// Exclusive scan of live flags within one chunk, single block (chunks are
+// at most a few million markers; this runs only on download).
+__global__ void k_live_scan (const float *qm, long long from, long long n, long long *slot,
+                             long long *total)
+{
+   __shared__ long long part[1024];
+   const int T = blockDim.x;
+   const long long per = (n + T - 1)/T;
+   const long long b = threadIdx.x*per, e = (b + per < n) ? b + per : n;
+   long long cnt = 0;
+   for (long long t = b ; t < e ; ++t)
+      cnt += (qm[from + t] != 0.0f);
+   part[threadIdx.x] = cnt;
+   __syncthreads ();
+   if (threadIdx.x == 0) {
+      long long s = 0;
+      for (int q = 0 ; q < T ; ++q) {
+         const long long v = part[q];
+         part[q] = s;
+         s += v;
+      }
+      *total = s;
+   }
+   __syncthreads ();
+   long long s = part[threadIdx.x];
+   for (long long t = b ; t < e ; ++t) {
+      slot[t] = s;
+      s += (qm[from + t] != 0.0f);
+   }
+}
+
+// End of a step: energy row {t, W_E, W_M, W_Tx, W_Ty, W_Tz} into the ring,
+// accumulators cleared, time advanced (parameter_setTime, core/main.c:435).
+__global__ void k_end_step (DevScalars *dsc, double *ring, double volume, double tau)
+{
+   const int s = dsc->step % MG_RING;
+   double *row = ring + 6*s;
+   row[0] = dsc->time;
+   row[1] = 0.5*dsc->acc[0]*volume;
+   row[2] = 0.5*dsc->acc[1]*volume;
+   row[3] = dsc->acc[2];
+   row[4] = dsc->acc[3];
+   row[5] = dsc->acc[4];
+   for (int q = 0 ; q < 8 ; ++q)
+      dsc->acc[q] = 0;
+   dsc->time += tau;
+   dsc->step += 1;
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+// Allocation.
+// ---------------------------------------------------------------------------
+static int dev_alloc (mg_run_t *r, void **p, size_t bytes)
+{
+   cudaError_t e = cudaMalloc (p, bytes ? bytes : 16);
+   if (e != cudaSuccess) {
+      cudaGetLastError ();
+      mg_set_error ("device allocation of %.3f GB failed: %s", bytes/1e9, cudaGetErrorString (e));
+      *p = nullptr;
+      return MG_ERR_OOM;
+   }
+   r->dev_bytes += bytes;
+   return MG_OK;
+}
+
+static int ensure_stage (mg_run_t *r, size_t bytes)
+{
+   if (r->stage_bytes >= bytes)
+      return MG_OK;
+   if (r->stage) {
+      cudaFree (r->stage);
+      r->dev_bytes -= r->stage_bytes;
+      r->stage = nullptr;
+      r->stage_bytes = 0;
+   }
+   TRY (dev_alloc (r, &r->stage, bytes));
+   r->stage_bytes = bytes;
+   return MG_OK;
+}
+
+static void free_markers (mg_run_t *r)
+{
+   void *ptrs[] = {r->m64.x, r->m64.y, r->m64.z, r->m64.ux, r->m64.uy, r->m64.uz,
+                   r->m64.rho, r->m64.qm, r->m64.id};
+   for (void *p : ptrs)
+      if (p)
+         cudaFree (p);
+   memset (&r->m64, 0, sizeof (r->m64));
+}
+
+static size_t marker_bytes64 (long long cap) { return (size_t) cap*(6*8 + 4 + 4 + 4); }
+
+static int ensure_capacity (mg_run_t *r, long long need)
+{
+   if (need <= r->cap)
+      return MG_OK;
+   long long cap = need + need/8 + 1024;
+   Markers64 old = r->m64;
+   long long old_np = r->np;
+   Markers64 nm;
+   memset (&nm, 0, sizeof (nm));
+   void **d[] = {(void **) &nm.x, (void **) &nm.y, (void **) &nm.z, (void **) &nm.ux,
+                 (void **) &nm.uy, (void **) &nm.uz};
+   for (void **p : d)
+      TRY (dev_alloc (r, p, (size_t) cap*8));
+   TRY (dev_alloc (r, (void **) &nm.rho, (size_t) cap*4));
+   TRY (dev_alloc (r, (void **) &nm.qm, (size_t) cap*4));
+   TRY (dev_alloc (r, (void **) &nm.id, (size_t) cap*4));
+   if (old.x && old_np > 0) {
+      MG_CUDA (cudaMemcpyAsync (nm.x, old.x, old_np*8, cudaMemcpyDeviceToDevice, r->stream));
+      MG_CUDA (cudaMemcpyAsync (nm.y, old.y, old_np*8, cudaMemcpyDeviceToDevice, r->stream));
+      MG_CUDA (cudaMemcpyAsync (nm.z, old.z, old_np*8, cudaMemcpyDeviceToDevice, r->stream));
+      MG_CUDA (cudaMemcpyAsync (nm.ux, old.ux, old_np*8, cudaMemcpyDeviceToDevice, r->stream));
+      MG_CUDA (cudaMemcpyAsync (nm.uy, old.uy, old_np*8, cudaMemcpyDeviceToDevice, r->stream));
+      MG_CUDA (cudaMemcpyAsync (nm.uz, old.uz, old_np*8, cudaMemcpyDeviceToDevice, r->stream));
+      MG_CUDA (cudaMemcpyAsync (nm.rho, old.rho, old_np*4, cudaMemcpyDeviceToDevice, r->stream));
+      MG_CUDA (cudaMemcpyAsync (nm.qm, old.qm, old_np*4, cudaMemcpyDeviceToDevice, r->stream));
+      MG_CUDA (cudaMemcpyAsync (nm.id, old.id, old_np*4, cudaMemcpyDeviceToDevice, r->stream));
+      MG_CUDA (cudaStreamSynchronize (r->stream));
+   }
+   if (old.x) {
+      r->dev_bytes -= marker_bytes64 (r->cap);
+      free_markers (r);
+   }
+   r->m64 = nm;
+   r->cap = cap;
+   // The captured graph holds the old pointers.
+   if (r->graph_exec) {
+      cudaGraphExecDestroy (r->graph_exec);
+      r->graph_exec = nullptr;
+   }
+   if (r->graph) {
+      cudaGraphDestroy (r->graph);
+      r->graph = nullptr;
+   }
+   r->graph_ok = 0;
+   return MG_OK;
+}
+
+static int check_params (const mg_params_t *p)
+{
+   for (int a = 0 ; a < 3 ; ++a) {
+      if (p->n[a] < 8) {
+         mg_set_error ("axis %d: %d cells; at least 8 are needed (core/plasma.c:392-396)", a, p->n[a]);
+         return MG_ERR_ARG;
+      }
+      if (!(p->h[a] > 0)) {
+         mg_set_error ("axis %d: mesh step %g", a, p->h[a]);
+         return MG_ERR_ARG;
+      }
+      for (int t = 0 ; t < 2 ; ++t) {
+         const int bc = t ? p->bc_max[a] : p->bc_min[a];
+         if (bc < MG_BC_PERIODIC || bc > MG_BC_OPEN) {
+            mg_set_error ("axis %d: unknown boundary condition %d", a, bc);
+            return MG_ERR_ARG;
+         }
+      }
+      if ((p->bc_min[a] == MG_BC_PERIODIC) != (p->bc_max[a] == MG_BC_PERIODIC)) {
+         mg_set_error ("axis %d: periodic must be set on both walls", a);
+         return MG_ERR_ARG;
+      }
+   }
+   const double c = 1.0/(p->tau*p->tau), s = 1.0/(p->h[0]*p->h[0]) + 1.0/(p->h[1]*p->h[1]) + 1.0/(p->h[2]*p->h[2]);
+   if (!(p->tau > 0) || !(c > s)) {
+      mg_set_error ("Yee-solver is unstable: tau = %g (core/em.c:43-44)", p->tau);
+      return MG_ERR_ARG;
+   }
+   if (p->precision != MG_FP64 && p->precision != MG_FP32_OFFSET) {
+      mg_set_error ("unknown precision form %d", p->precision);
+      return MG_ERR_ARG;
+   }
+   return MG_OK;
+}
+
+extern "C" long long mg_estimate_bytes (const mg_params_t *p, long long markers)
+{
+   if (!p)
+      return -1;
+   Grid g = make_grid (p->n, p->h, p->tau, p->bc_min, p->bc_max);
+   const long long elt = (p->precision == MG_FP64) ? 8 : 4;
+   long long b = 9LL*g.total*elt;
+   for (int a = 0 ; a < 3 ; ++a)
+      b += 2LL*4*elt*(p->n[(a + 1) % 3] + 2)*(p->n[(a + 2) % 3] + 2);
+   const long long per_marker = (p->precision == MG_FP64) ? 60 : 40;
+   b += (markers + markers/8 + 1024)*per_marker;
+   b += (long long) MG_RING*6*8 + (1 << 20);
+   return b;
+}
+
+extern "C" int mg_run_create (const mg_params_t *params, mg_run_t **out)
+{
+   if (!params || !out) {
+      mg_set_error ("mg_run_create: null argument");
+      return MG_ERR_ARG;
+   }
+   *out = nullptr;
+   TRY (check_params (params));
+   if (params->precision == MG_FP32_OFFSET) {
+      return mg_run_create32 (params, out);
+   }
+   int ndev = 0;
+   if (cudaGetDeviceCount (&ndev) != cudaSuccess || ndev == 0) {
+      cudaGetLastError ();
+      mg_set_error ("no CUDA device available: the B200 core has no CPU path");
+      return MG_ERR_CUDA;
+   }
+   if (params->device < 0 || params->device >= ndev) {
+      mg_set_error ("device %d out of range (%d devices)", params->device, ndev);
+      return MG_ERR_ARG;
+   }
+   MG_CUDA (cudaSetDevice (params->device));
+   mg_run_t *r = (mg_run_t *) calloc (1, sizeof (mg_run_t));
+   r->prm = *params;
+   r->device = params->device;
+   r->g = make_grid (params->n, params->h, params->tau, params->bc_min, params->bc_max);
+   r->time = params->time;
+   if (cudaStreamCreateWithFlags (&r->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      free (r);
+      mg_set_error ("cannot create a stream");
+      return MG_ERR_CUDA;
+   }
+   int rc = MG_OK;
+   const size_t fb = (size_t) r->g.total*sizeof (double);
+   for (int c = 0 ; c < 3 && rc == MG_OK ; ++c) {
+      rc = dev_alloc (r, (void **) &r->E[c], fb);
+      if (rc == MG_OK) rc = dev_alloc (r, (void **) &r->H[c], fb);
+      if (rc == MG_OK) rc = dev_alloc (r, (void **) &r->J[c], fb);
+      if (rc == MG_OK) {
+         cudaMemsetAsync (r->E[c], 0, fb, r->stream);
+         cudaMemsetAsync (r->H[c], 0, fb, r->stream);
+         cudaMemsetAsync (r->J[c], 0, fb, r->stream);
+      }
+   }
+   for (int t = 0 ; t < 2 && rc == MG_OK ; ++t)
+      for (int a = 0 ; a < 3 && rc == MG_OK ; ++a) {
+         const size_t mb = 4*sizeof (double)*(size_t) (params->n[(a + 1) % 3] + 2)*(params->n[(a + 2) % 3] + 2);
+         rc = dev_alloc (r, (void **) &r->mur[t][a], mb);
+         if (rc == MG_OK)
+            cudaMemsetAsync (r->mur[t][a], 0, mb, r->stream);
+      }
+   if (rc == MG_OK) rc = dev_alloc (r, (void **) &r->dsc, sizeof (DevScalars));
+   if (rc == MG_OK) rc = dev_alloc (r, (void **) &r->ring, sizeof (double)*6*MG_RING);
+   if (rc == MG_OK) {
+      DevScalars s;
+      memset (&s, 0, sizeof (s));
+      s.time = r->time;
+      cudaMemcpyAsync (r->dsc, &s, sizeof (s), cudaMemcpyHostToDevice, r->stream);
+   }
+   if (rc == MG_OK && params->capacity > 0)
+      rc = ensure_capacity (r, params->capacity);
+   for (int e = 0 ; e < 4 && rc == MG_OK ; ++e)
+      if (cudaEventCreate (&r->ev[e]) != cudaSuccess)
+         rc = MG_ERR_CUDA;
+   if (rc == MG_OK && cudaStreamSynchronize (r->stream) != cudaSuccess) {
+      mg_set_error ("initialisation failed: %s", cudaGetErrorString (cudaGetLastError ()));
+      rc = MG_ERR_CUDA;
+   }
+   if (rc != MG_OK) {
+      char keep[1024];
+      strncpy (keep, g_err, sizeof (keep) - 1);
+      keep[sizeof (keep) - 1] = 0;
+      mg_run_destroy (r);
+      mg_set_error ("%s", keep);
+      return rc;
+   }
+   *out = r;
+   return MG_OK;
+}
+
+extern "C" int mg_run_destroy (mg_run_t *r)
+{
+   if (!r)
+      return MG_OK;
+   if (r->prm.precision == MG_FP32_OFFSET) {
+      return mg_run_destroy32 (r);
+   }
+   cudaSetDevice (r->device);
+   if (r->stream)
+      cudaStreamSynchronize (r->stream);
+   if (r->graph_exec) cudaGraphExecDestroy (r->graph_exec);
+   if (r->graph) cudaGraphDestroy (r->graph);
+   for (int c = 0 ; c < 3 ; ++c) {
+      if (r->E[c]) cudaFree (r->E[c]);
+      if (r->H[c]) cudaFree (r->H[c]);
+      if (r->J[c]) cudaFree (r->J[c]);
+   }
+   for (int t = 0 ; t < 2 ; ++t)
+      for (int a = 0 ; a < 3 ; ++a)
+         if (r->mur[t][a]) cudaFree (r->mur[t][a]);
+   free_markers (r);
+   if (r->dsc) cudaFree (r->dsc);
+   if (r->ring) cudaFree (r->ring);
+   if (r->stage) cudaFree (r->stage);
+   if (r->sort_tmp) cudaFree (r->sort_tmp);
+   for (int e = 0 ; e < 4 ; ++e)
+      if (r->ev[e]) cudaEventDestroy (r->ev[e]);
+   if (r->stream) cudaStreamDestroy (r->stream);
+   free (r);
+   return MG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Transfers.
+// ---------------------------------------------------------------------------
+extern "C" int mg_run_set_fields (mg_run_t *r, const double *E, const double *H)
+{
+   CHECK_RUN (r);
+   if (r->prm.precision != MG_FP64) {
+      return mg_run_set_fields32 (r, E, H);
+   }
+   const long vol = (long) (r->g.n[0] + 1)*(r->g.n[1] + 1)*(r->g.n[2] + 1);
+   const size_t bytes = (size_t) vol*3*sizeof (double);
+   TRY (ensure_stage (r, bytes));
+   const double *src[2] = {E, H};
+   double **dst[2] = {r->E, r->H};
+   for (int f = 0 ; f < 2 ; ++f) {
+      if (!src[f])
+         continue;
+      MG_CUDA (cudaMemcpyAsync (r->stage, src[f], bytes, cudaMemcpyHostToDevice, r->stream));
+      k_fields_in<<<mg_blocks_for (vol, 256, 8), 256, 0, r->stream>>> (r->g, (const double *) r->stage,
+                                                                       dst[f][0], dst[f][1], dst[f][2]);
+      MG_LAUNCH_CHECK ();
+   }
+   MG_CUDA (cudaStreamSynchronize (r->stream));
+   r->inited = 0;
+   return MG_OK;
+}
+
+extern "C" int mg_run_get_fields (mg_run_t *r, double *E, double *H)
+{
+   CHECK_RUN (r);
+   if (r->prm.precision != MG_FP64) {
+      return mg_run_get_fields32 (r, E, H);
+   }
+   const long vol = (long) (r->g.n[0] + 1)*(r->g.n[1] + 1)*(r->g.n[2] + 1);
+   const size_t bytes = (size_t) vol*3*sizeof (double);
+   TRY (ensure_stage (r, bytes));
+   double *dst[2] = {E, H};
+   double **src[2] = {r->E, r->H};
+   for (int f = 0 ; f < 2 ; ++f) {
+      if (!dst[f])
+         continue;
+      k_fields_out<<<mg_blocks_for (vol, 256, 8), 256, 0, r->stream>>> (r->g, (double *) r->stage,
+                                                                        src[f][0], src[f][1], src[f][2], 0);
+      MG_LAUNCH_CHECK ();
+      MG_CUDA (cudaMemcpyAsync (dst[f], r->stage, bytes, cudaMemcpyDeviceToHost, r->stream));
+      MG_CUDA (cudaStreamSynchronize (r->stream));
+   }
+   return MG_OK;
+}
+
+extern "C" int mg_run_get_current (mg_run_t *r, double *J)
+{
+   CHECK_RUN (r);
+   if (r->prm.precision != MG_FP64) {
+      return mg_run_get_current32 (r, J);
+   }
+   const long vol = (long) (r->g.n[0] + 5)*(r->g.n[1] + 5)*(r->g.n[2] + 5);
+   const size_t bytes = (size_t) vol*3*sizeof (double);
+   TRY (ensure_stage (r, bytes));
+   k_fields_out<<<mg_blocks_for (vol, 256, 8), 256, 0, r->stream>>> (r->g, (double *) r->stage,
+                                                                     r->J[0], r->J[1], r->J[2], 2);
+   MG_LAUNCH_CHECK ();
+   MG_CUDA (cudaMemcpyAsync (J, r->stage, bytes, cudaMemcpyDeviceToHost, r->stream));
+   MG_CUDA (cudaStreamSynchronize (r->stream));
+   return MG_OK;
+}
+
+static const long long CHUNK = 1LL << 22;   // markers per staged transfer
+
+extern "C" int mg_run_set_markers (mg_run_t *r, const mg_marker_t *m, long long n)
+{
+   CHECK_RUN (r);
+   if (n < 0 || (n > 0 && !m)) {
+      mg_set_error ("mg_run_set_markers: bad arguments");
+      return MG_ERR_ARG;
+   }
+   if (r->prm.precision != MG_FP64) {
+      return mg_run_set_markers32 (r, m, n);
+   }
+   TRY (ensure_capacity (r, n));
+   const long long chunk = n < CHUNK ? n : CHUNK;
+   TRY (ensure_stage (r, (size_t) (chunk > 0 ? chunk : 1)*sizeof (mg_marker_t)));
+   for (long long at = 0 ; at < n ; at += CHUNK) {
+      const long long c = (n - at < CHUNK) ? n - at : CHUNK;
+      MG_CUDA (cudaMemcpyAsync (r->stage, m + at, c*sizeof (mg_marker_t), cudaMemcpyHostToDevice, r->stream));
+      k_markers_in<<<mg_blocks_for (c, 256, 8), 256, 0, r->stream>>> ((const mg_marker_t *) r->stage, c, r->m64, at);
+      MG_LAUNCH_CHECK ();
+   }
+   r->np = n;
+   MG_CUDA (cudaMemsetAsync (&r->dsc->dead, 0, sizeof (long long), r->stream));
+   MG_CUDA (cudaStreamSynchronize (r->stream));
+   return MG_OK;
+}
+
+extern "C" int mg_run_marker_count (mg_run_t *r, long long *n)
+{
+   CHECK_RUN (r);
+   if (!n) {
+      mg_set_error ("mg_run_marker_count: null output");
+      return MG_ERR_ARG;
+   }
+   long long dead = 0;
+   MG_CUDA (cudaMemcpyAsync (&dead, &r->dsc->dead, sizeof (dead), cudaMemcpyDeviceToHost, r->stream));
+   MG_CUDA (cudaStreamSynchronize (r->stream));
+   *n = r->np - dead;
+   return MG_OK;
+}
+
+extern "C" int mg_run_get_markers (mg_run_t *r, mg_marker_t *out, long long cap, long long *n)
+{
+   CHECK_RUN (r);
+   if (r->prm.precision != MG_FP64) {
+      return mg_run_get_markers32 (r, out, cap, n);
+   }
+   long long live = 0;
+   TRY (mg_run_marker_count (r, &live));
+   if (n)
+      *n = live;
+   if (!out)
+      return MG_OK;
+   if (cap < live) {
+      mg_set_error ("mg_run_get_markers: buffer holds %lld markers, %lld live", cap, live);
+      return MG_ERR_CAPACITY;
+   }
+   const long long chunk = r->np < CHUNK ? r->np : CHUNK;
+   const size_t need = (size_t) (chunk > 0 ? chunk : 1)*(sizeof (mg_marker_t) + sizeof (long long)) + 64;
+   TRY (ensure_stage (r, need));
+   mg_marker_t *dst = (mg_marker_t *) r->stage;
+   long long *slot = (long long *) ((char *) r->stage + (size_t) (chunk > 0 ? chunk : 1)*sizeof (mg_marker_t));
+   long long *total_d = slot + (chunk > 0 ? chunk : 1);
+   long long written = 0;
+   for (long long at = 0 ; at < r->np ; at += CHUNK) {
+      const long long c = (r->np - at < CHUNK) ? r->np - at : CHUNK;
+      k_live_scan<<<1, 1024, 0, r->stream>>> (r->m64.qm, at, c, slot, total_d);
+      k_markers_out<<<mg_blocks_for (c, 256, 8), 256, 0, r->stream>>> (r->m64, at, c, dst, slot);
+      MG_LAUNCH_CHECK ();
+      long long got = 0;
+      MG_CUDA (cudaMemcpyAsync (&got, total_d, sizeof (got), cudaMemcpyDeviceToHost, r->stream));
+      MG_CUDA (cudaStreamSynchronize (r->stream));
+      if (written + got > cap) {
+         mg_set_error ("mg_run_get_markers: live count changed during download");
+         return MG_ERR_STATE;
+      }
+      MG_CUDA (cudaMemcpyAsync (out + written, dst, got*sizeof (mg_marker_t), cudaMemcpyDeviceToHost, r->stream));
+      MG_CUDA (cudaStreamSynchronize (r->stream));
+      written += got;
+   }
+   if (n)
+      *n = written;
+   return MG_OK;
+}
+
+extern "C" int mg_run_set_laser (mg_run_t *r, const mg_laser_t *l)
+{
+   CHECK_RUN (r);
+   if (!l) {
+      r->has_laser = 0;
+   } else {
+      if (l->plane < 2 || l->plane > r->g.n[0] - 2 || l->margin < 0 || !(l->waist > 0) || !(l->duration > 0)) {
+         mg_set_error ("mg_run_set_laser: plane %d / margin %d / waist %g / duration %g out of range",
+                       l->plane, l->margin, l->waist, l->duration);
+         return MG_ERR_ARG;
+      }
+      r->laser = *l;
+      r->has_laser = 1;
+   }
+   if (r->graph_exec) { cudaGraphExecDestroy (r->graph_exec); r->graph_exec = nullptr; }
+   if (r->graph) { cudaGraphDestroy (r->graph); r->graph = nullptr; }
+   r->graph_ok = 0;
+   return MG_OK;
+}
+
+extern "C" int mg_run_set_time (mg_run_t *r, double t)
+{
+   CHECK_RUN (r);
+   r->time = t;
+   MG_CUDA (cudaMemcpyAsync (&r->dsc->time, &r->time, sizeof (double), cudaMemcpyHostToDevice, r->stream));
+   MG_CUDA (cudaStreamSynchronize (r->stream));
+   return MG_OK;
+}
+
+extern "C" int mg_run_get_time (mg_run_t *r, double *t)
+{
+   CHECK_RUN (r);
+   MG_CUDA (cudaMemcpyAsync (&r->time, &r->dsc->time, sizeof (double), cudaMemcpyDeviceToHost, r->stream));
+   MG_CUDA (cudaStreamSynchronize (r->stream));
+   if (t)
+      *t = r->time;
+   return MG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Stage API (core/main.c:353-478).  The order is checked like the
+// reference's emStage flag (core/em.c:32).
+// ---------------------------------------------------------------------------
+static int expect_stage (mg_run_t *r, int want, const char *who)
+{
+   if (!r->inited) {
+      mg_set_error ("%s: mg_run_init has not been called since the state was loaded", who);
+      return MG_ERR_STATE;
+   }
+   if (r->stage_no != want) {
+      mg_set_error ("%s: called at stage %d, expected stage %d", who, r->stage_no, want);
+      return MG_ERR_STATE;
+   }
+   return MG_OK;
+}
+
+static bool is32 (const mg_run_t *r) { return r->prm.precision == MG_FP32_OFFSET; }
+
+int mg_walls64 (mg_run_t *r);
+int mg_walls32 (mg_run_t *r);
+
+extern "C" int mg_run_init (mg_run_t *r)
+{
+   CHECK_RUN (r);
+   TRY (is32 (r) ? mg_fields32_init (r) : mg_fields64_init (r));
+   TRY (is32 (r) ? mg_walls32 (r) : mg_walls64 (r));
+   MG_CUDA (cudaStreamSynchronize (r->stream));
+   r->inited = 1;
+   r->stage_no = 0;
+   return MG_OK;
+}
+
+extern "C" int mg_em_HHalfStep (mg_run_t *r)
+{
+   CHECK_RUN (r);
+   TRY (expect_stage (r, 0, __func__));
+   TRY (is32 (r) ? mg_fields32_h_half (r) : mg_fields64_h_half (r));
+   r->stage_no = 1;
+   return MG_OK;
+}
+
+extern "C" int mg_em_energy (mg_run_t *r, double *we, double *wm)
+{
+   CHECK_RUN (r);
+   TRY (expect_stage (r, 1, __func__));
+   MG_CUDA (cudaMemsetAsync (r->dsc->acc, 0, 2*sizeof (double), r->stream));
+   TRY (is32 (r) ? mg_fields32_energy (r) : mg_fields64_energy (r));
+   double acc[2];
+   MG_CUDA (cudaMemcpyAsync (acc, r->dsc->acc, sizeof (acc), cudaMemcpyDeviceToHost, r->stream));
+   MG_CUDA (cudaStreamSynchronize (r->stream));
+   const double v = r->g.h[0]*r->g.h[1]*r->g.h[2];
+   if (we) *we = 0.5*acc[0]*v;
+   if (wm) *wm = 0.5*acc[1]*v;
+   r->stage_no = 2;
+   return MG_OK;
+}
+
+static int check_err (mg_run_t *r)
+{
+   int info[5];
+   MG_CUDA (cudaMemcpyAsync (info, &r->dsc->err, sizeof (int)*5, cudaMemcpyDeviceToHost, r->stream));
+   MG_CUDA (cudaStreamSynchronize (r->stream));
+   if (info[0]) {
+      mg_set_error ("marker %d left the mesh or moved more than one cell per step "
+                    "(flags %d, cell %d %d %d); the step is invalid", info[1], info[0], info[2], info[3], info[4]);
+      return MG_ERR_BOUNDS;
+   }
+   return MG_OK;
+}
+
+extern "C" int mg_plasma_move (mg_run_t *r)
+{
+   CHECK_RUN (r);
+   if (r->stage_no == 1) {
+      // Energy stage skipped by the caller: keep the accumulators clear.
+      MG_CUDA (cudaMemsetAsync (r->dsc->acc, 0, 2*sizeof (double), r->stream));
+      r->stage_no = 2;
+   }
+   TRY (expect_stage (r, 2, __func__));
+   MG_CUDA (cudaMemsetAsync (r->dsc->acc + 2, 0, 3*sizeof (double), r->stream));
+   TRY (is32 (r) ? mg_fields32_zero_j (r) : mg_fields64_zero_j (r));
+   TRY (is32 (r) ? mg_push32 (r) : mg_push64 (r));
+   TRY (check_err (r));
+   r->stage_no = 3;
+   return MG_OK;
+}
+
+extern "C" int mg_plasma_temperature (mg_run_t *r, double *wx, double *wy, double *wz)
+{
+   CHECK_RUN (r);
+   double acc[3];
+   MG_CUDA (cudaMemcpyAsync (acc, r->dsc->acc + 2, sizeof (acc), cudaMemcpyDeviceToHost, r->stream));
+   MG_CUDA (cudaStreamSynchronize (r->stream));
+   if (wx) *wx = acc[0];
+   if (wy) *wy = acc[1];
+   if (wz) *wz = acc[2];
+   return MG_OK;
+}
+
+extern "C" int mg_em_HStep (mg_run_t *r)
+{
+   CHECK_RUN (r);
+   TRY (expect_stage (r, 3, __func__));
+   TRY (is32 (r) ? mg_fields32_h_step (r) : mg_fields64_h_step (r));
+   r->stage_no = 4;
+   return MG_OK;
+}
+
+extern "C" int mg_em_EStep_start (mg_run_t *r)
+{
+   CHECK_RUN (r);
+   TRY (expect_stage (r, 4, __func__));
+   TRY (is32 (r) ? mg_fields32_e_step (r) : mg_fields64_e_step (r));
+   r->stage_no = 5;
+   return MG_OK;
+}
+
+extern "C" int mg_jbc_finish (mg_run_t *r)
+{
+   CHECK_RUN (r);
+   TRY (expect_stage (r, 5, __func__));
+   TRY (is32 (r) ? mg_fields32_jbc (r) : mg_fields64_jbc (r));
+   r->stage_no = 6;
+   return MG_OK;
+}
+
+extern "C" int mg_em_EStep_finish (mg_run_t *r)
+{
+   CHECK_RUN (r);
+   TRY (expect_stage (r, 6, __func__));
+   TRY (is32 (r) ? mg_fields32_e_finish (r) : mg_fields64_e_finish (r));
+   // Time advances at the end of the step (core/main.c:435).
+   k_end_step<<<1, 1, 0, r->stream>>> (r->dsc, r->ring, r->g.h[0]*r->g.h[1]*r->g.h[2], r->g.tau);
+   MG_LAUNCH_CHECK ();
+   MG_CUDA (cudaStreamSynchronize (r->stream));
+   r->time += r->g.tau;
+   r->stage_no = 0;
+   return MG_OK;
+}
+
+extern "C" int mg_plasma_rho (mg_run_t *r, double *rho)
+{
+   CHECK_RUN (r);
+   if (is32 (r)) {
+      return mg_plasma_rho32 (r, rho);
+   }
+   const size_t fb = (size_t) r->g.total*sizeof (double);
+   double *d = nullptr;
+   TRY (dev_alloc (r, (void **) &d, fb));
+   cudaMemsetAsync (d, 0, fb, r->stream);
+   int rc = mg_rho64 (r, d);
+   if (rc == MG_OK) {
+      const long vol = (long) (r->g.n[0] + 5)*(r->g.n[1] + 5)*(r->g.n[2] + 5);
+      rc = ensure_stage (r, vol*3*sizeof (double));
+      if (rc == MG_OK) {
+         k_fields_out<<<mg_blocks_for (vol, 256, 8), 256, 0, r->stream>>> (r->g, (double *) r->stage, d, d, d, 2);
+         // Take one component of the triplets on the host.
+         double *tmp = (double *) malloc (vol*3*sizeof (double));
+         cudaMemcpyAsync (tmp, r->stage, vol*3*sizeof (double), cudaMemcpyDeviceToHost, r->stream);
+         cudaStreamSynchronize (r->stream);
+         for (long t = 0 ; t < vol ; ++t)
+            rho[t] = tmp[3*t];
+         free (tmp);
+      }
+   }
+   cudaFree (d);
+   r->dev_bytes -= fb;
+   return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Whole steps.
+// ---------------------------------------------------------------------------
+int mg_enqueue_step64 (mg_run_t *r)
+{
+   TRY (mg_fields64_h_half (r));
+   TRY (mg_fields64_energy (r));
+   TRY (mg_fields64_zero_j (r));
+   TRY (mg_push64 (r));
+   TRY (mg_fields64_h_step (r));
+   TRY (mg_fields64_e_step (r));
+   TRY (mg_fields64_jbc (r));
+   TRY (mg_fields64_e_finish (r));
+   k_end_step<<<1, 1, 0, r->stream>>> (r->dsc, r->ring, r->g.h[0]*r->g.h[1]*r->g.h[2], r->g.tau);
+   MG_LAUNCH_CHECK ();
+   return MG_OK;
+}
+
+int mg_enqueue_step32 (mg_run_t *r);
+
+static int count_kernels (mg_run_t *r)
+{
+   size_t n = 0;
+   if (cudaGraphGetNodes (r->graph, nullptr, &n) != cudaSuccess)
+      return 0;
+   cudaGraphNode_t *nodes = (cudaGraphNode_t *) malloc (n*sizeof (cudaGraphNode_t));
+   cudaGraphGetNodes (r->graph, nodes, &n);
+   int k = 0;
+   for (size_t q = 0 ; q < n ; ++q) {
+      cudaGraphNodeType t;
+      if (cudaGraphNodeGetType (nodes[q], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel)
+         ++k;
+   }
+   free (nodes);
+   return k;
+}
+
+static int build_graph (mg_run_t *r)
+{
+   if (r->graph_ok)
+      return MG_OK;
+   if (r->graph_exec) { cudaGraphExecDestroy (r->graph_exec); r->graph_exec = nullptr; }
+   if (r->graph) { cudaGraphDestroy (r->graph); r->graph = nullptr; }
+   MG_CUDA (cudaStreamBeginCapture (r->stream, cudaStreamCaptureModeThreadLocal));
+   int rc = is32 (r) ? mg_enqueue_step32 (r) : mg_enqueue_step64 (r);
+   cudaGraph_t g = nullptr;
+   cudaError_t e = cudaStreamEndCapture (r->stream, &g);
+   if (rc != MG_OK) {
+      if (g) cudaGraphDestroy (g);
+      return rc;
+   }
+   if (e != cudaSuccess) {
+      mg_set_error ("graph capture failed: %s", cudaGetErrorString (e));
+      return MG_ERR_CUDA;
+   }
+   r->graph = g;
+   MG_CUDA (cudaGraphInstantiate (&r->graph_exec, g, 0));
+   r->kernels_per_step = count_kernels (r);
+   r->graph_ok = 1;
+   return MG_OK;
+}
+
+static int run_steps (mg_run_t *r, int nsteps, double *host_rows, double *dev_rows, bool sync)
+{
+   if (!r->inited) {
+      mg_set_error ("mg_run_step: mg_run_init has not been called since the state was loaded");
+      return MG_ERR_STATE;
+   }
+   if (r->stage_no != 0) {
+      mg_set_error ("mg_run_step: a stage-by-stage step is in progress (stage %d)", r->stage_no);
+      return MG_ERR_STATE;
+   }
+   if (nsteps < 0) {
+      mg_set_error ("mg_run_step: nsteps = %d", nsteps);
+      return MG_ERR_ARG;
+   }
+   TRY (build_graph (r));
+   for (int done = 0 ; done < nsteps ; ) {
+      const int chunk = (nsteps - done < MG_RING) ? nsteps - done : MG_RING;
+      MG_CUDA (cudaMemsetAsync (&r->dsc->step, 0, sizeof (int), r->stream));
+      if (r->profile)
+         MG_CUDA (cudaEventRecord (r->ev[0], r->stream));
+      for (int s = 0 ; s < chunk ; ++s)
+         MG_CUDA (cudaGraphLaunch (r->graph_exec, r->stream));
+      if (r->profile)
+         MG_CUDA (cudaEventRecord (r->ev[1], r->stream));
+      if (host_rows)
+         MG_CUDA (cudaMemcpyAsync (host_rows + 6*(size_t) done, r->ring, sizeof (double)*6*chunk,
+                                   cudaMemcpyDeviceToHost, r->stream));
+      if (dev_rows)
+         MG_CUDA (cudaMemcpyAsync (dev_rows + 6*(size_t) done, r->ring, sizeof (double)*6*chunk,
+                                   cudaMemcpyDeviceToDevice, r->stream));
+      done += chunk;
+      if (host_rows || sync || done < nsteps)
+         MG_CUDA (cudaStreamSynchronize (r->stream));
+      if (r->profile && (host_rows || sync)) {
+         float ms = 0;
+         cudaEventElapsedTime (&ms, r->ev[0], r->ev[1]);
+         r->last_step_ms = ms/chunk;
+      }
+   }
+   r->time += nsteps*r->g.tau;
+   if (sync)
+      TRY (check_err (r));
+   return MG_OK;
+}
+
+extern "C" int mg_run_step (mg_run_t *r, int nsteps, double *energies)
+{
+   CHECK_RUN (r);
+   return run_steps (r, nsteps, energies, nullptr, true);
+}
+
+extern "C" int mg_run_step_async (mg_run_t *r, int nsteps, double *energies_dev)
+{
+   CHECK_RUN (r);
+   return run_steps (r, nsteps, nullptr, energies_dev, false);
+}
+
+extern "C" int mg_run_synchronize (mg_run_t *r)
+{
+   CHECK_RUN (r);
+   MG_CUDA (cudaStreamSynchronize (r->stream));
+   return check_err (r);
+}
+
+extern "C" int mg_run_stream (mg_run_t *r, void **stream)
+{
+   CHECK_RUN (r);
+   if (stream)
+      *stream = (void *) r->stream;
+   return MG_OK;
+}
+
+extern "C" int mg_run_kernels_per_step (mg_run_t *r, int *count)
+{
+   CHECK_RUN (r);
+   TRY (build_graph (r));
+   if (count)
+      *count = r->kernels_per_step;
+   return MG_OK;
+}
+
+extern "C" int mg_run_device_bytes (mg_run_t *r, long long *bytes)
+{
+   CHECK_RUN (r);
+   if (bytes)
+      *bytes = r->dev_bytes;
+   return MG_OK;
+}
+
+extern "C" int mg_run_profile (mg_run_t *r, int enable)
+{
+   CHECK_RUN (r);
+   r->profile = enable;
+   return MG_OK;
+}
+
+extern "C" int mg_run_last_timing (mg_run_t *r, double *push_ms, double *step_ms)
+{
+   CHECK_RUN (r);
+   if (push_ms) *push_ms = r->last_push_ms;
+   if (step_ms) *step_ms = r->last_step_ms;
+   return MG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Device placement.
+// ---------------------------------------------------------------------------
+int mg_place64 (mg_run_t *r, const mg_place_t *spec, long long at, long long count);
+int mg_place32 (mg_run_t *r, const mg_place_t *spec, long long at, long long count);
+int mg_ensure_capacity32 (mg_run_t *r, long long need);
+
+extern "C" int mg_run_place_uniform (mg_run_t *r, const mg_place_t *s)
+{
+   CHECK_RUN (r);
+   if (!s || s->ppc <= 0) {
+      mg_set_error ("mg_run_place_uniform: bad spec");
+      return MG_ERR_ARG;
+   }
+   long long cells = 1;
+   for (int a = 0 ; a < 3 ; ++a) {
+      if (s->lo[a] < 0 || s->hi[a] > r->g.n[a] || s->hi[a] < s->lo[a]) {
+         mg_set_error ("mg_run_place_uniform: box [%d,%d) outside axis %d of %d cells",
+                       s->lo[a], s->hi[a], a, r->g.n[a]);
+         return MG_ERR_ARG;
+      }
+      cells *= s->hi[a] - s->lo[a];
+   }
+   const long long count = cells*s->ppc;
+   if (count == 0)
+      return MG_OK;
+   if (is32 (r)) {
+      TRY (mg_ensure_capacity32 (r, r->np + count));
+      TRY (mg_place32 (r, s, r->np, count));
+   } else {
+      TRY (ensure_capacity (r, r->np + count));
+      TRY (mg_place64 (r, s, r->np, count));
+   }
+   r->np += count;
+   r->inited = 0;
+   return MG_OK;
+}

@@ -1,0 +1,207 @@
+// Internal definitions shared by the CUDA translation units of the B200
+// particle-in-cell core.  Nothing here is part of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "mandor_b200.h"
+
+// ---------------------------------------------------------------------------
+// Device mesh layout.
+//
+// Every field component (Ex, Ey, Ez, Hx, Hy, Hz, Jx, Jy, Jz) is its own
+// array ("structure of arrays") over nodes i in [-2, n0+2], j in [-2, n1+2],
+// k in [-4, n2+2+pad]: two ghost layers on every side (the reference keeps
+// one for E, H and two for J, core/main.c:108-115) and a z row padded so
+// that k = 0 of every row starts on a 32-byte sector.  k is the fastest
+// index, as in the reference's meshes (type_mesh.h:134-141).
+// ---------------------------------------------------------------------------
+#define MG_GX 2
+#define MG_GZ_FRONT 4
+
+struct Grid {
+   int    n[3];
+   long   sx, sy;          // strides of i and j (k stride is 1)
+   long   origin;          // linear offset of node (0,0,0)
+   long   total;           // elements per component array
+   double h[3];
+   double tau;
+   int    bc[2][3];        // [min/max][axis]
+
+   __host__ __device__ __forceinline__ long at (int i, int j, int k) const
+   {
+      return origin + i*sx + j*sy + k;
+   }
+};
+
+static inline Grid make_grid (const int n[3], const double h[3], double tau,
+                              const int bc_min[3], const int bc_max[3])
+{
+   Grid g;
+   for (int a = 0 ; a < 3 ; ++a) {
+      g.n[a] = n[a];
+      g.h[a] = h[a];
+      g.bc[0][a] = bc_min[a];
+      g.bc[1][a] = bc_max[a];
+   }
+   g.tau = tau;
+   long row = MG_GZ_FRONT + n[2] + 1 + MG_GX;
+   row = (row + 3) & ~3L;                       // 32-byte rows
+   g.sy = row;
+   g.sx = row*(n[1] + 1 + 2*MG_GX);
+   g.total = g.sx*(n[0] + 1 + 2*MG_GX);
+   g.origin = MG_GX*g.sx + MG_GX*g.sy + MG_GZ_FRONT;
+   return g;
+}
+
+// Device-side per-run scalars (one small allocation).
+struct DevScalars {
+   double time;            // t = n*tau of the step being advanced
+   double acc[8];          // W_E, W_M, WTx, WTy, WTz of the current step
+   long long dead;         // markers removed by open walls (not compacted)
+   int    step;            // steps done since the energy ring was reset
+   int    err;             // sticky error flags (1: start cell outside the
+                           // ghost layers, 2: more than one cell per step)
+   int    err_info[4];     // first offending marker index and cell
+};
+
+#define MG_RING 4096       // energy rows kept on the device between copies
+
+// FP64 particle arrays (structure of arrays).
+struct Markers64 {
+   double *x, *y, *z, *ux, *uy, *uz;
+   float  *rho, *qm;
+   int    *id;
+};
+
+// FP32-offset particle arrays.
+struct Markers32 {
+   int    *cell;           // linear cell index i*ny*nz + j*nz + k
+   float  *ox, *oy, *oz;   // offsets in [0,1) in units of h
+   float  *ux, *uy, *uz;
+   float  *rho, *qm;
+   int    *id;
+};
+
+struct mg_run {
+   mg_params_t prm;
+   Grid        g;
+   int         device;
+   cudaStream_t stream;
+
+   // fields
+   double *E[3], *H[3], *J[3];
+   double *mur[2][3];      // Mur history, 4 doubles per wall node
+   float  *E32[3], *H32[3], *J32[3];
+   float  *mur32[2][3];
+
+   // markers
+   long long  np, cap;
+   Markers64  m64;
+   Markers32  m32;
+   void      *sort_tmp;    // scratch for sorting / compaction
+   size_t     sort_tmp_bytes;
+   int       *tile_key;
+   long long  steps_since_sort;
+
+   // scalars and energy ring
+   DevScalars *dsc;
+   double     *ring;       // MG_RING rows of 6 doubles
+   double      time;       // host mirror
+
+   // laser
+   int         has_laser;
+   mg_laser_t  laser;
+
+   // staging
+   void       *stage;
+   size_t      stage_bytes;
+
+   // graph
+   cudaGraph_t     graph;
+   cudaGraphExec_t graph_exec;
+   int             graph_ok;
+   int             kernels_per_step;
+
+   // stage ordering (like core/em.c:32's emStage)
+   int         stage_no;
+   int         inited;
+
+   // profiling
+   int         profile;
+   cudaEvent_t ev[4];
+   double      last_push_ms, last_step_ms;
+
+   long long   dev_bytes;
+};
+
+// Error handling -----------------------------------------------------------
+void mg_set_error (const char *fmt, ...);
+
+#define MG_CUDA(call)                                                        \
+   do {                                                                      \
+      cudaError_t e_ = (call);                                               \
+      if (e_ != cudaSuccess) {                                               \
+         mg_set_error ("%s:%d: %s: %s", __FILE__, __LINE__, #call,           \
+                       cudaGetErrorString (e_));                             \
+         return MG_ERR_CUDA;                                                 \
+      }                                                                      \
+   } while (0)
+
+#define MG_LAUNCH_CHECK()                                                    \
+   do {                                                                      \
+      cudaError_t e_ = cudaGetLastError ();                                  \
+      if (e_ != cudaSuccess) {                                               \
+         mg_set_error ("%s:%d: kernel launch: %s", __FILE__, __LINE__,       \
+                       cudaGetErrorString (e_));                             \
+         return MG_ERR_CUDA;                                                 \
+      }                                                                      \
+   } while (0)
+
+// Launch helpers shared between translation units ---------------------------
+int mg_fields64_h_half (mg_run_t *r);
+int mg_fields64_energy (mg_run_t *r);
+int mg_fields64_h_step (mg_run_t *r);
+int mg_fields64_e_step (mg_run_t *r);
+int mg_fields64_jbc (mg_run_t *r);
+int mg_fields64_e_finish (mg_run_t *r);
+int mg_fields64_init (mg_run_t *r);
+int mg_fields64_zero_j (mg_run_t *r);
+int mg_push64 (mg_run_t *r);
+int mg_rho64 (mg_run_t *r, double *rho_dev);
+int mg_end_step (mg_run_t *r);
+
+int mg_fields32_h_half (mg_run_t *r);
+int mg_fields32_energy (mg_run_t *r);
+int mg_fields32_h_step (mg_run_t *r);
+int mg_fields32_e_step (mg_run_t *r);
+int mg_fields32_jbc (mg_run_t *r);
+int mg_fields32_e_finish (mg_run_t *r);
+int mg_fields32_init (mg_run_t *r);
+int mg_fields32_zero_j (mg_run_t *r);
+int mg_push32 (mg_run_t *r);
+int mg_sort32 (mg_run_t *r);
+int mg_walls32 (mg_run_t *r);
+int mg_enqueue_step32 (mg_run_t *r);
+int mg_place32 (mg_run_t *r, const mg_place_t *spec, long long at, long long count);
+int mg_ensure_capacity32 (mg_run_t *r, long long need);
+int mg_run_create32 (const mg_params_t *params, mg_run_t **out);
+int mg_run_destroy32 (mg_run_t *r);
+int mg_run_set_fields32 (mg_run_t *r, const double *E, const double *H);
+int mg_run_get_fields32 (mg_run_t *r, double *E, double *H);
+int mg_run_get_current32 (mg_run_t *r, double *J);
+int mg_run_set_markers32 (mg_run_t *r, const mg_marker_t *m, long long n);
+int mg_run_get_markers32 (mg_run_t *r, mg_marker_t *m, long long cap, long long *n);
+int mg_plasma_rho32 (mg_run_t *r, double *rho);
+
+// Grid sizing: a multiple of the SM count (148 on B200).
+int mg_sm_count (void);
+static inline int mg_blocks_for (long long work, int threads, int per_sm = 8)
+{
+   long long b = (work + threads - 1)/threads;
+   long long cap = (long long) mg_sm_count ()*per_sm;
+   if (b > cap) b = cap;
+   if (b < 1) b = 1;
+   return (int) b;
+}

@@ -1,0 +1,244 @@
+// Device marker placement driven by the reference's ranmar generator
+// (Marsaglia-Zaman lagged Fibonacci with lags 97 and 33 plus an arithmetic
+// sequence, misc_ranmar.c:79-146).  The reference ships the generator but
+// no placer that uses it; the placement rule here is this project's
+// (documented in include/mandor_b200.h at mg_place_t).
+//
+// Every ranmar value is a multiple of 2^-24, so the generator runs in
+// integers: F_n = (F_{n-97} - F_{n-33}) mod 2^24 and C_n = (C_0 - n CD) mod
+// CM, output_n = (F_n - C_{n+1}) mod 2^24 scaled by 2^-24 -- bit-identical
+// to the reference's doubles.  The Fibonacci part is linear over
+// Z/2^24, so the state after L draws is A^L s_0 for the 97x97 companion
+// matrix A; the host computes one start state per chunk by repeated
+// squaring and every device thread then generates its own chunk.
+#include <cuda_runtime.h>
+
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "mg_internal.cuh"
+
+#define RM_LAG 97
+#define RM_MASK 0xFFFFFFu
+#define RM_CD 7654321LL
+#define RM_CM 16777213LL
+#define RM_C0 362436LL
+
+namespace {
+
+// ranmar_init (misc_ranmar.c:79-119) in integer form: F_{-1-s} = u[s].
+static void rm_seed (int ij, int kl, uint32_t F[RM_LAG])
+{
+   int i = (ij/177)%177 + 2, j = ij%177 + 2, k = (kl/169)%178 + 1, l = kl%169;
+   uint32_t u[RM_LAG];
+   for (int ii = 0 ; ii < RM_LAG ; ii++) {
+      uint32_t s = 0;
+      for (int bit = 0 ; bit < 24 ; bit++) {
+         int m = (((i*j)%179)*k)%179;
+         i = j;
+         j = k;
+         k = m;
+         l = (53*l + 1)%169;
+         if ((l*m)%64 >= 32)
+            s |= 1u << (23 - bit);
+      }
+      u[ii] = s;
+   }
+   // State vector s[q] = F_{q-97}, q = 0..96  (F_{-97} .. F_{-1}).
+   for (int q = 0 ; q < RM_LAG ; ++q)
+      F[q] = u[96 - q];
+}
+
+typedef uint32_t Mat[RM_LAG][RM_LAG];
+
+// y = M x over Z/2^24.
+static void mat_vec (const Mat &M, const uint32_t x[RM_LAG], uint32_t y[RM_LAG])
+{
+   for (int r = 0 ; r < RM_LAG ; ++r) {
+      uint64_t acc = 0;
+      for (int c = 0 ; c < RM_LAG ; ++c)
+         acc += (uint64_t) M[r][c]*x[c];
+      y[r] = (uint32_t) (acc & RM_MASK);
+   }
+}
+
+static void mat_mul (const Mat &A, const Mat &B, Mat &C)
+{
+   for (int r = 0 ; r < RM_LAG ; ++r)
+      for (int c = 0 ; c < RM_LAG ; ++c) {
+         uint64_t acc = 0;
+         for (int q = 0 ; q < RM_LAG ; ++q)
+            acc += (uint64_t) A[r][q]*B[q][c];
+         C[r][c] = (uint32_t) (acc & RM_MASK);
+      }
+}
+
+// Companion matrix of one draw: new state s'[q] = s[q+1], s'[96] = s[0] - s[64].
+static void mat_step (Mat &A)
+{
+   memset (&A, 0, sizeof (Mat));
+   for (int q = 0 ; q < RM_LAG - 1 ; ++q)
+      A[q][q + 1] = 1;
+   A[96][0] = 1;
+   A[96][64] = RM_MASK;           // -1 mod 2^24
+}
+
+static void mat_pow (long long e, Mat &R)
+{
+   Mat *base = (Mat *) malloc (sizeof (Mat)), *tmp = (Mat *) malloc (sizeof (Mat));
+   mat_step (*base);
+   memset (&R, 0, sizeof (Mat));
+   for (int q = 0 ; q < RM_LAG ; ++q)
+      R[q][q] = 1;
+   while (e > 0) {
+      if (e & 1) {
+         mat_mul (R, *base, *tmp);
+         memcpy (&R, tmp, sizeof (Mat));
+      }
+      e >>= 1;
+      if (e) {
+         mat_mul (*base, *base, *tmp);
+         memcpy (base, tmp, sizeof (Mat));
+      }
+   }
+   free (base);
+   free (tmp);
+}
+
+struct PlaceArgs {
+   mg_place_t s;
+   double h[3];
+   long long nmarkers;     // markers in the box
+   long long per_thread;   // markers per thread
+   long long at;           // first device slot
+};
+
+// One thread: markers [t*per, (t+1)*per) of the box, draws starting at
+// skip + 7*t*per, whose generator state the host put in states[t].
+__global__ void __launch_bounds__ (128)
+k_place (PlaceArgs a, const uint32_t *states, Markers64 m)
+{
+   extern __shared__ uint32_t ring[];           // RM_LAG words per thread
+   const long long t = blockIdx.x*(long long) blockDim.x + threadIdx.x;
+   const long long first = t*a.per_thread;
+   if (first >= a.nmarkers)
+      return;
+   uint32_t *F = ring + threadIdx.x*RM_LAG;
+   for (int q = 0 ; q < RM_LAG ; ++q)
+      F[q] = states[t*RM_LAG + q];               // F_{d-97} .. F_{d-1}
+   long long d = a.s.skip + 7*first;             // absolute draw index
+   int head = 0;                                 // slot of F_{d-97}
+   const int ex = a.s.hi[0] - a.s.lo[0], ey = a.s.hi[1] - a.s.lo[1], ez = a.s.hi[2] - a.s.lo[2];
+   long long last = first + a.per_thread;
+   if (last > a.nmarkers)
+      last = a.nmarkers;
+   for (long long n = first ; n < last ; ++n) {
+      double u[7];
+      for (int q = 0 ; q < 7 ; ++q, ++d) {
+         // F_d = F_{d-97} - F_{d-33}; F_{d-97} sits at slot head, F_{d-33}
+         // at slot head + 64.
+         int s33 = head + 64;
+         if (s33 >= RM_LAG) s33 -= RM_LAG;
+         const uint32_t f = (F[head] - F[s33]) & RM_MASK;
+         F[head] = f;
+         head = (head + 1 == RM_LAG) ? 0 : head + 1;
+         long long c = (RM_C0 - ((d + 1) % RM_CM)*RM_CD) % RM_CM;
+         if (c < 0) c += RM_CM;
+         const uint32_t out = (f - (uint32_t) c) & RM_MASK;
+         u[q] = (double) out*(1.0/16777216.0);
+      }
+      const long long cell = n / a.s.ppc;
+      const int k = a.s.lo[2] + (int) (cell % ez);
+      const int j = a.s.lo[1] + (int) ((cell / ez) % ey);
+      const int i = a.s.lo[0] + (int) (cell / ((long long) ez*ey));
+      (void) ex;
+      const long long o = a.at + n;
+      m.x[o] = (i + u[0])*a.h[0];
+      m.y[o] = (j + u[1])*a.h[1];
+      m.z[o] = (k + u[2])*a.h[2];
+      const double r1 = sqrt (-2.0*log (1.0 - u[3])), t1 = 2*M_PI*u[4];
+      const double r2 = sqrt (-2.0*log (1.0 - u[5])), t2 = 2*M_PI*u[6];
+      m.ux[o] = a.s.drift[0] + a.s.uth[0]*(r1*cos (t1));
+      m.uy[o] = a.s.drift[1] + a.s.uth[1]*(r1*sin (t1));
+      m.uz[o] = a.s.drift[2] + a.s.uth[2]*(r2*cos (t2));
+      m.rho[o] = (float) a.s.rho;
+      m.qm[o] = (float) a.s.qDivM;
+      m.id[o] = a.s.id0 + (int) n;
+   }
+}
+
+} // namespace
+
+// Host: generator states for `nthreads` chunks of `chunk_draws` draws
+// starting at draw `skip`.  states[t] = (F_{d_t-97} .. F_{d_t-1}).
+int mg_ranmar_states (int ij, int kl, long long skip, long long chunk_draws, int nthreads,
+                      uint32_t *states)
+{
+   if (ij < 0 || ij > 31328 || kl < 0 || kl > 30081) {
+      mg_set_error ("ranmar seeds must satisfy 0 <= ij <= 31328, 0 <= kl <= 30081 (misc_ranmar.c:81-84)");
+      return MG_ERR_ARG;
+   }
+   uint32_t s[RM_LAG], tmp[RM_LAG];
+   rm_seed (ij, kl, s);
+   Mat *M = (Mat *) malloc (sizeof (Mat));
+   if (skip > 0) {
+      mat_pow (skip, *M);
+      mat_vec (*M, s, tmp);
+      memcpy (s, tmp, sizeof (s));
+   }
+   if (nthreads > 1)
+      mat_pow (chunk_draws, *M);
+   for (int t = 0 ; t < nthreads ; ++t) {
+      memcpy (states + (size_t) t*RM_LAG, s, sizeof (s));
+      if (t + 1 < nthreads) {
+         mat_vec (*M, s, tmp);
+         memcpy (s, tmp, sizeof (s));
+      }
+   }
+   free (M);
+   return MG_OK;
+}
+
+int mg_place64 (mg_run_t *r, const mg_place_t *spec, long long at, long long count)
+{
+   PlaceArgs a;
+   a.s = *spec;
+   for (int q = 0 ; q < 3 ; ++q)
+      a.h[q] = r->g.h[q];
+   a.nmarkers = count;
+   a.at = at;
+   // Threads: enough to fill the GPU, bounded so the host jump-ahead stays
+   // cheap (one 97x97 mat-vec per thread).
+   int nthreads = mg_sm_count ()*128;
+   if (count < nthreads) nthreads = (int) count;
+   if (nthreads < 1) nthreads = 1;
+   a.per_thread = (count + nthreads - 1)/nthreads;
+   nthreads = (int) ((count + a.per_thread - 1)/a.per_thread);
+   uint32_t *hs = (uint32_t *) malloc ((size_t) nthreads*RM_LAG*sizeof (uint32_t));
+   int rc = mg_ranmar_states (spec->seed_ij, spec->seed_kl, spec->skip, 7*a.per_thread, nthreads, hs);
+   if (rc != MG_OK) {
+      free (hs);
+      return rc;
+   }
+   uint32_t *ds = nullptr;
+   if (cudaMalloc (&ds, (size_t) nthreads*RM_LAG*sizeof (uint32_t)) != cudaSuccess) {
+      free (hs);
+      mg_set_error ("placer: device allocation failed");
+      return MG_ERR_OOM;
+   }
+   cudaMemcpyAsync (ds, hs, (size_t) nthreads*RM_LAG*sizeof (uint32_t), cudaMemcpyHostToDevice, r->stream);
+   const int T = 128, B = (nthreads + T - 1)/T;
+   const int smem = T*RM_LAG*sizeof (uint32_t);          // 49,664 bytes
+   cudaFuncSetAttribute (k_place, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+   k_place<<<B, T, smem, r->stream>>> (a, ds, r->m64);
+   cudaError_t e = cudaGetLastError ();
+   cudaStreamSynchronize (r->stream);
+   cudaFree (ds);
+   free (hs);
+   if (e != cudaSuccess) {
+      mg_set_error ("placer launch: %s", cudaGetErrorString (e));
+      return MG_ERR_CUDA;
+   }
+   return MG_OK;
+}

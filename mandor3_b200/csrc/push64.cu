@@ -1,0 +1,541 @@
+// FP64 particle push: CIC gather of the staggered E and H, relativistic
+// Boris rotation, position update, charge-conserving current deposition
+// and particle boundary conditions, fused in one kernel.
+//
+// Reference semantics (paths relative to the reference project):
+//   gather + Boris + move      core/plasma.c:106-171, misc_PIC.h:18-126
+//   crossing classification    core/plasma.c:176-225
+//   in-cell segment deposit    core/plasma_currentKernel.c:21-124
+//   2- and 3-face crossings    core/plasma_currentKernel.c:157-279
+//   thermal energy tally       core/plasma.c:140-143
+//   particle walls             core/plasma_walls.c:27-104
+//
+// Compiled with --fmad=false: every product and sum rounds as the
+// reference's C expressions do, so cell indices and per-marker updates are
+// bit-identical given identical fields.
+//
+// Deposition: markers are stored in cell order (placement order, kept by
+// the periodic sort), so consecutive lanes of a warp usually start in the
+// same cell.  The twelve contributions of each marker's first segment (which
+// always lies in its start cell) are summed across lanes that share the
+// cell with a segmented warp scan, and one lane per run of equal cells
+// issues the twelve atomics.  Further segments of cell-crossing markers add
+// their contributions directly.
+#include <cuda_runtime.h>
+
+#include "mg_internal.cuh"
+
+namespace {
+
+__device__ __forceinline__ int dbl_to_int (double x) { return (int) (x + 128.0) - 128; }
+
+struct Ctx {
+   Grid   g;
+   const double *E0, *E1, *E2, *H0, *H1, *H2;
+   double *J0, *J1, *J2;
+};
+
+__device__ __forceinline__ double cic (const double *F, const Grid &g, int i, double sx,
+                                       int j, double sy, int k, double sz)
+{
+   const long o = g.at (i, j, k), Sx = g.sx, Sy = g.sy;
+   return F[o]*(1 - sx)*((1 - sy)*(1 - sz)) + F[o + Sx]*sx*((1 - sy)*(1 - sz))
+        + F[o + Sy]*(1 - sx)*(sy*(1 - sz)) + F[o + Sx + Sy]*sx*(sy*(1 - sz))
+        + F[o + 1]*(1 - sx)*((1 - sy)*sz) + F[o + Sx + 1]*sx*((1 - sy)*sz)
+        + F[o + Sy + 1]*(1 - sx)*(sy*sz) + F[o + Sx + Sy + 1]*sx*(sy*sz);
+}
+
+// The twelve weights of one in-cell segment, in the reference's order:
+// Jx at (i+1, j|j+1, k|k+1), Jy at (i|i+1, j+1, k|k+1), Jz at (i|i+1, j|j+1, k+1).
+__device__ __forceinline__ void segment_weights (const Grid &g, int i, int j, int k,
+                                                 double x1, double x2, double y1, double y2,
+                                                 double z1, double z2, double rho, double w[12])
+{
+   const double h1 = g.h[0], h2 = g.h[1], h3 = g.h[2], tau = g.tau;
+   const double dX = x2 - x1, dY = y2 - y1, dZ = z2 - z1;
+   const double tX = 0.5*(x1 + x2) - i*h1;
+   const double tY = 0.5*(y1 + y2) - j*h2;
+   const double tZ = 0.5*(z1 + z2) - k*h3;
+   const double ax = rho*dX/(tau*h2*h3), dyz = dY*dZ/12;
+   w[0] = ax*((h2 - tY)*(h3 - tZ) + dyz);
+   w[1] = ax*(tY*(h3 - tZ) - dyz);
+   w[2] = ax*((h2 - tY)*tZ - dyz);
+   w[3] = ax*(tY*tZ + dyz);
+   const double ay = rho*dY/(tau*h1*h3), dxz = dX*dZ/12;
+   w[4] = ay*((h1 - tX)*(h3 - tZ) + dxz);
+   w[5] = ay*(tX*(h3 - tZ) - dxz);
+   w[6] = ay*((h1 - tX)*tZ - dxz);
+   w[7] = ay*(tX*tZ + dxz);
+   const double az = rho*dZ/(tau*h1*h2), dxy = dX*dY/12;
+   w[8] = az*((h1 - tX)*(h2 - tY) + dxy);
+   w[9] = az*(tX*(h2 - tY) - dxy);
+   w[10] = az*((h1 - tX)*tY - dxy);
+   w[11] = az*(tX*tY + dxy);
+}
+
+__device__ __forceinline__ void scatter12 (const Ctx &c, int i, int j, int k, const double w[12])
+{
+   const long o = c.g.at (i, j, k), sx = c.g.sx, sy = c.g.sy;
+   atomicAdd (c.J0 + o + sx, w[0]);
+   atomicAdd (c.J0 + o + sx + sy, w[1]);
+   atomicAdd (c.J0 + o + sx + 1, w[2]);
+   atomicAdd (c.J0 + o + sx + sy + 1, w[3]);
+   atomicAdd (c.J1 + o + sy, w[4]);
+   atomicAdd (c.J1 + o + sx + sy, w[5]);
+   atomicAdd (c.J1 + o + sy + 1, w[6]);
+   atomicAdd (c.J1 + o + sx + sy + 1, w[7]);
+   atomicAdd (c.J2 + o + 1, w[8]);
+   atomicAdd (c.J2 + o + sx + 1, w[9]);
+   atomicAdd (c.J2 + o + sy + 1, w[10]);
+   atomicAdd (c.J2 + o + sx + sy + 1, w[11]);
+}
+
+__device__ __forceinline__ void deposit_direct (const Ctx &c, int i, int j, int k,
+                                                double x1, double x2, double y1, double y2,
+                                                double z1, double z2, double rho)
+{
+   double w[12];
+   segment_weights (c.g, i, j, k, x1, x2, y1, y2, z1, z2, rho, w);
+   scatter12 (c, i, j, k, w);
+}
+
+// plasmaCurrents_multiCellStep (core/plasma_currentKernel.c:157-279) for
+// everything after the first segment, which the caller has deposited.
+// Returns the end point of the first segment in (xa, ya, za).
+__device__ void multicell_first (const Grid &g, int i1, int j1, int k1, int i2, int j2, int k2,
+                                 double x1, double y1, double z1, double x2, double y2, double z2,
+                                 double &xa, double &ya, double &za)
+{
+   const double h1 = g.h[0], h2 = g.h[1], h3 = g.h[2];
+   const int di = abs (i2 - i1), dj = abs (j2 - j1), dk = abs (k2 - k1);
+   if (di + dj + dk == 2) {
+      const double sX = di*((i1 + i2 + 1)*0.5*h1 - x1)/(x2 - x1 + ((1 - di) << 16));
+      const double sY = dj*((j1 + j2 + 1)*0.5*h2 - y1)/(y2 - y1 + ((1 - dj) << 16));
+      const double sZ = dk*((k1 + k2 + 1)*0.5*h3 - z1)/(z2 - z1 + ((1 - dk) << 16));
+      double kap1 = sX + (1 - di)*sY;
+      double kap2 = sZ + (1 - dk)*sY;
+      if (kap1 > kap2) {
+         const double t = kap1;
+         kap1 = kap2;
+         kap2 = t;
+      }
+      xa = x1 + kap1*(x2 - x1);
+      ya = y1 + kap1*(y2 - y1);
+      za = z1 + kap1*(z2 - z1);
+      return;
+   }
+   const double xC = (i1 + i2 + 1)*0.5*h1, yC = (j1 + j2 + 1)*0.5*h2, zC = (k1 + k2 + 1)*0.5*h3;
+   double s1 = (xC - x1)/(x2 - x1), s2 = (yC - y1)/(y2 - y1), s3 = (zC - z1)/(z2 - z1);
+   double rc[3][3];
+   rc[0][0] = xC;
+   rc[0][1] = y1 + s1*(y2 - y1);
+   rc[0][2] = z1 + s1*(z2 - z1);
+   rc[1][0] = x1 + s2*(x2 - x1);
+   rc[1][1] = yC;
+   rc[1][2] = z1 + s2*(z2 - z1);
+   rc[2][0] = x1 + s3*(x2 - x1);
+   rc[2][1] = y1 + s3*(y2 - y1);
+   rc[2][2] = zC;
+   int a = 0, b = 1, cc = 2;
+   if (s1 > s2) { int t = a; a = b; b = t; double u = s1; s1 = s2; s2 = u; }
+   if (s1 > s3) { int t = a; a = cc; cc = t; double u = s1; s1 = s3; s3 = u; }
+   (void) b;
+   xa = rc[a][0];
+   ya = rc[a][1];
+   za = rc[a][2];
+}
+
+__device__ void multicell_rest (const Ctx &c, int i1, int j1, int k1, int i2, int j2, int k2,
+                                double x1, double y1, double z1, double x2, double y2, double z2,
+                                double rho)
+{
+   const Grid &g = c.g;
+   const double h1 = g.h[0], h2 = g.h[1], h3 = g.h[2];
+   const int di = abs (i2 - i1), dj = abs (j2 - j1), dk = abs (k2 - k1);
+   if (di + dj + dk == 2) {
+      int i = i1, j = j1, k = k1;
+      const double sX = di*((i1 + i2 + 1)*0.5*h1 - x1)/(x2 - x1 + ((1 - di) << 16));
+      const double sY = dj*((j1 + j2 + 1)*0.5*h2 - y1)/(y2 - y1 + ((1 - dj) << 16));
+      const double sZ = dk*((k1 + k2 + 1)*0.5*h3 - z1)/(z2 - z1 + ((1 - dk) << 16));
+      double kap1 = sX + (1 - di)*sY;
+      double kap2 = sZ + (1 - dk)*sY;
+      int d[2][3] = {{0, 0, 0}, {0, 0, 0}};
+      int first = 0;
+      d[0][0] = di*(i2 - i1);
+      d[0][1] = (1 - di)*(j2 - j1);
+      d[1][1] = (1 - dk)*(j2 - j1);
+      d[1][2] = dk*(k2 - k1);
+      if (kap1 > kap2) {
+         const double t = kap1;
+         kap1 = kap2;
+         kap2 = t;
+         first = 1;
+      }
+      const double xA = x1 + kap1*(x2 - x1), yA = y1 + kap1*(y2 - y1), zA = z1 + kap1*(z2 - z1);
+      const double xB = x1 + kap2*(x2 - x1), yB = y1 + kap2*(y2 - y1), zB = z1 + kap2*(z2 - z1);
+      i += d[first][0];
+      j += d[first][1];
+      k += d[first][2];
+      deposit_direct (c, i, j, k, xA, xB, yA, yB, zA, zB, rho);
+      i += d[1 - first][0];
+      j += d[1 - first][1];
+      k += d[1 - first][2];
+      deposit_direct (c, i, j, k, xB, x2, yB, y2, zB, z2, rho);
+      return;
+   }
+   const double xC = (i1 + i2 + 1)*0.5*h1, yC = (j1 + j2 + 1)*0.5*h2, zC = (k1 + k2 + 1)*0.5*h3;
+   double s1 = (xC - x1)/(x2 - x1), s2 = (yC - y1)/(y2 - y1), s3 = (zC - z1)/(z2 - z1);
+   double rc[3][3];
+   int dI[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+   rc[0][0] = xC;
+   rc[0][1] = y1 + s1*(y2 - y1);
+   rc[0][2] = z1 + s1*(z2 - z1);
+   dI[0][0] = i2 - i1;
+   rc[1][0] = x1 + s2*(x2 - x1);
+   rc[1][1] = yC;
+   rc[1][2] = z1 + s2*(z2 - z1);
+   dI[1][1] = j2 - j1;
+   rc[2][0] = x1 + s3*(x2 - x1);
+   rc[2][1] = y1 + s3*(y2 - y1);
+   rc[2][2] = zC;
+   dI[2][2] = k2 - k1;
+   int a = 0, b = 1, cc = 2;
+   if (s1 > s2) { int t = a; a = b; b = t; double u = s1; s1 = s2; s2 = u; }
+   if (s1 > s3) { int t = a; a = cc; cc = t; double u = s1; s1 = s3; s3 = u; }
+   if (s2 > s3) { int t = b; b = cc; cc = t; double u = s2; s2 = s3; s3 = u; }
+   int i = i1 + dI[a][0], j = j1 + dI[a][1], k = k1 + dI[a][2];
+   deposit_direct (c, i, j, k, rc[a][0], rc[b][0], rc[a][1], rc[b][1], rc[a][2], rc[b][2], rho);
+   i += dI[b][0];
+   j += dI[b][1];
+   k += dI[b][2];
+   deposit_direct (c, i, j, k, rc[b][0], rc[cc][0], rc[b][1], rc[cc][1], rc[b][2], rc[cc][2], rho);
+   deposit_direct (c, i2, j2, k2, rc[cc][0], x2, rc[cc][1], y2, rc[cc][2], z2, rho);
+}
+
+__device__ __forceinline__ double warp_sum (double v)
+{
+   for (int d = 16 ; d > 0 ; d >>= 1)
+      v += __shfl_xor_sync (0xffffffffu, v, d);
+   return v;
+}
+
+// Segmented inclusive sum over lanes: lanes [seg_start, lane] of the run of
+// equal keys that contains this lane.
+__device__ __forceinline__ double seg_scan (double v, int lane, int seg_start)
+{
+#pragma unroll
+   for (int d = 1 ; d < 32 ; d <<= 1) {
+      const double t = __shfl_up_sync (0xffffffffu, v, d);
+      if (lane - d >= seg_start)
+         v += t;
+   }
+   return v;
+}
+
+__global__ void __launch_bounds__ (256)
+k_push64 (Ctx c, Markers64 m, long long np, DevScalars *dsc)
+{
+   const Grid &g = c.g;
+   const double h1 = g.h[0], h2 = g.h[1], h3 = g.h[2], tau = g.tau;
+   const double L0 = g.n[0]*h1, L1 = g.n[1]*h2, L2 = g.n[2]*h3;
+   const int lane = threadIdx.x & 31;
+   double Wx = 0, Wy = 0, Wz = 0;
+   long long dead = 0;
+
+   const long long warps_total = ((long long) gridDim.x*blockDim.x) >> 5;
+   const long long warp0 = ((long long) blockIdx.x*blockDim.x + threadIdx.x) >> 5;
+   for (long long base = warp0*32 ; base < np ; base += warps_total*32) {
+      const long long n = base + lane;
+      bool valid = n < np;
+      double qm = 0;
+      if (valid) {
+         qm = m.qm[n];
+         valid = (qm != 0.0);             // removed markers carry qDivM = 0
+      }
+      int i = 0, j = 0, k = 0, i2 = 0, j2 = 0, k2 = 0, nseg = 0;
+      double x1 = 0, y1 = 0, z1 = 0, x2 = 0, y2 = 0, z2 = 0, rho = 0;
+      double xa = 0, ya = 0, za = 0;         // end of the first segment
+      if (valid) {
+         x1 = m.x[n];
+         y1 = m.y[n];
+         z1 = m.z[n];
+         double sX = x1/h1, sY = y1/h2, sZ = z1/h3;
+         double sX_ = sX + 0.5, sY_ = sY + 0.5, sZ_ = sZ + 0.5;
+         i = dbl_to_int (sX);
+         j = dbl_to_int (sY);
+         k = dbl_to_int (sZ);
+         const int i_ = dbl_to_int (sX_), j_ = dbl_to_int (sY_), k_ = dbl_to_int (sZ_);
+         // Start cells outside [-1, n] would read or write past the two
+         // ghost layers: flag and skip the marker.
+         if (i < -1 || i > g.n[0] || j < -1 || j > g.n[1] || k < -1 || k > g.n[2]) {
+            if (atomicOr (&dsc->err, 1) == 0) {
+               dsc->err_info[0] = (int) n;
+               dsc->err_info[1] = i;
+               dsc->err_info[2] = j;
+               dsc->err_info[3] = k;
+            }
+            valid = false;
+         } else {
+            sX -= i; sY -= j; sZ -= k;
+            sX_ -= i_; sY_ -= j_; sZ_ -= k_;
+            const double Ex = cic (c.E0, g, i_, sX_, j, sY, k, sZ);
+            const double Ey = cic (c.E1, g, i, sX, j_, sY_, k, sZ);
+            const double Ez = cic (c.E2, g, i, sX, j, sY, k_, sZ_);
+            const double Hx = cic (c.H0, g, i, sX, j_, sY_, k_, sZ_);
+            const double Hy = cic (c.H1, g, i_, sX_, j, sY, k_, sZ_);
+            const double Hz = cic (c.H2, g, i_, sX_, j_, sY_, k, sZ);
+
+            rho = (double) m.rho[n];
+            const double tm = 0.5*tau*qm;
+            const double px = m.ux[n] + tm*Ex, py = m.uy[n] + tm*Ey, pz = m.uz[n] + tm*Ez;
+            const double gamma = sqrt (1 + px*px + py*py + pz*pz);
+            const double W = (gamma - 1.0)*rho/(px*px + py*py + pz*pz + 1e-19)*h1*h2*h3/qm;
+            Wx += W*px*px;
+            Wy += W*py*py;
+            Wz += W*pz*pz;
+
+            const double tg = tm/gamma;
+            const double ax = tg*Hx, ay = tg*Hy, az = tg*Hz;
+            const double u = px + py*az - pz*ay, v = py + pz*ax - px*az, w = pz + px*ay - py*ax;
+            const double bxx = ax*ax, byy = ay*ay, bzz = az*az;
+            const double bxy = ax*ay, byz = ay*az, bxz = az*ax;
+            const double delta = 1.0/(1 + bxx + byy + bzz);
+            const double vx = tm*Ex + ((1 + bxx)*u + (bxy + az)*v + (bxz - ay)*w)*delta;
+            const double vy = tm*Ey + ((bxy - az)*u + (1 + byy)*v + (byz + ax)*w)*delta;
+            const double vz = tm*Ez + ((bxz + ay)*u + (byz - ax)*v + (1 + bzz)*w)*delta;
+
+            const double tgi = tau/sqrt (1 + vx*vx + vy*vy + vz*vz);
+            x2 = x1 + vx*tgi;
+            y2 = y1 + vy*tgi;
+            z2 = z1 + vz*tgi;
+
+            i2 = dbl_to_int (x2/h1);
+            j2 = dbl_to_int (y2/h2);
+            k2 = dbl_to_int (z2/h3);
+            int di = abs (i2 - i), dj = abs (j2 - j), dk = abs (k2 - k);
+            if (fabs (x2 - x1) < 1e-10*h1) { di = 0; i2 = i; }
+            if (fabs (y2 - y1) < 1e-10*h2) { dj = 0; j2 = j; }
+            if (fabs (z2 - z1) < 1e-10*h3) { dk = 0; k2 = k; }
+            if (di > 1 || dj > 1 || dk > 1) {
+               // More than one cell per step (Courant violated): flag, no deposit.
+               if (atomicOr (&dsc->err, 2) == 0) {
+                  dsc->err_info[0] = (int) n;
+                  dsc->err_info[1] = i2;
+                  dsc->err_info[2] = j2;
+                  dsc->err_info[3] = k2;
+               }
+               valid = false;
+            }
+            nseg = di + dj + dk;
+            if (nseg == 0) {
+               xa = x2; ya = y2; za = z2;
+            } else if (nseg == 1) {
+               const double alpha = dk*((k + k2 + 1)*0.5*h3 - z1)/(z2 - z1 + ((1 - dk) << 16))
+                                  + dj*((j + j2 + 1)*0.5*h2 - y1)/(y2 - y1 + ((1 - dj) << 16))
+                                  + di*((i + i2 + 1)*0.5*h1 - x1)/(x2 - x1 + ((1 - di) << 16));
+               xa = x1 + alpha*(x2 - x1);
+               ya = y1 + alpha*(y2 - y1);
+               za = z1 + alpha*(z2 - z1);
+            } else {
+               multicell_first (g, i, j, k, i2, j2, k2, x1, y1, z1, x2, y2, z2, xa, ya, za);
+            }
+
+            // Store the advanced marker, then apply the walls in the
+            // reference's order xMin, yMin, zMin, xMax, yMax, zMax.
+            double pos[3] = {x2, y2, z2};
+            double vel[3] = {vx, vy, vz};
+            const double L[3] = {L0, L1, L2};
+            bool gone = false;
+            for (int f = 0 ; f < 6 ; ++f) {
+               const int a = (f < 3) ? f : f - 3, top = (f >= 3);
+               const int bc = g.bc[top][a];
+               if (bc == MG_BC_PERIODIC) {
+                  if (!top && pos[a] <= 0) pos[a] += L[a];
+                  if (top && pos[a] >= L[a]) pos[a] -= L[a];
+               } else if (bc == MG_BC_MIRROR) {
+                  if (!top && pos[a] <= 0) { pos[a] = -pos[a]; vel[a] *= -1; }
+                  if (top && pos[a] >= L[a]) { pos[a] = 2*L[a] - pos[a]; vel[a] *= -1; }
+               } else {
+                  const double hh = g.h[a];
+                  if ((!top && pos[a] <= hh) || (top && pos[a] >= L[a] - hh)) {
+                     gone = true;
+                     break;
+                  }
+               }
+            }
+            m.x[n] = pos[0];
+            m.y[n] = pos[1];
+            m.z[n] = pos[2];
+            m.ux[n] = vel[0];
+            m.uy[n] = vel[1];
+            m.uz[n] = vel[2];
+            if (gone) {
+               m.qm[n] = 0.0f;
+               ++dead;
+            }
+         }
+      }
+
+      // First segment: warp-aggregated by start cell.
+      double wgt[12];
+      if (valid)
+         segment_weights (g, i, j, k, x1, xa, y1, ya, z1, za, rho, wgt);
+      else
+         for (int q = 0 ; q < 12 ; ++q) wgt[q] = 0;
+      const long long key = valid ? g.at (i, j, k) : -1 - lane;
+      const long long prev = __shfl_up_sync (0xffffffffu, key, 1);
+      const long long next = __shfl_down_sync (0xffffffffu, key, 1);
+      const bool head = (lane == 0) || (prev != key);
+      const bool tail = (lane == 31) || (next != key);
+      const unsigned heads = __ballot_sync (0xffffffffu, head);
+      const unsigned le = (lane == 31) ? 0xffffffffu : ((1u << (lane + 1)) - 1);
+      const int seg_start = 31 - __clz (heads & le);
+#pragma unroll
+      for (int q = 0 ; q < 12 ; ++q)
+         wgt[q] = seg_scan (wgt[q], lane, seg_start);
+      if (valid && tail) {
+         Ctx cc = c;
+         scatter12 (cc, i, j, k, wgt);
+      }
+
+      // Remaining segments of markers that crossed cell faces.
+      if (valid && nseg == 1)
+         deposit_direct (c, i2, j2, k2, xa, x2, ya, y2, za, z2, rho);
+      else if (valid && nseg >= 2)
+         multicell_rest (c, i, j, k, i2, j2, k2, x1, y1, z1, x2, y2, z2, rho);
+   }
+
+   // Thermal energy tally: block reduction, one atomic per block.
+   __shared__ double sw[3][8];
+   Wx = warp_sum (Wx);
+   Wy = warp_sum (Wy);
+   Wz = warp_sum (Wz);
+   const int wid = threadIdx.x >> 5;
+   if (lane == 0) {
+      sw[0][wid] = Wx;
+      sw[1][wid] = Wy;
+      sw[2][wid] = Wz;
+   }
+   for (int d = 16 ; d > 0 ; d >>= 1)
+      dead += __shfl_xor_sync (0xffffffffu, dead, d);
+   if (lane == 0 && dead)
+      atomicAdd ((unsigned long long *) &dsc->dead, (unsigned long long) dead);
+   __syncthreads ();
+   if (wid == 0) {
+      const int nw = blockDim.x >> 5;
+      Wx = lane < nw ? sw[0][lane] : 0;
+      Wy = lane < nw ? sw[1][lane] : 0;
+      Wz = lane < nw ? sw[2][lane] : 0;
+      Wx = warp_sum (Wx);
+      Wy = warp_sum (Wy);
+      Wz = warp_sum (Wz);
+      if (lane == 0) {
+         atomicAdd (&dsc->acc[2], Wx);
+         atomicAdd (&dsc->acc[3], Wy);
+         atomicAdd (&dsc->acc[4], Wz);
+      }
+   }
+}
+
+// CIC charge density (core/plasma_rho.c:23-60), no folding.
+__global__ void k_rho64 (Grid g, Markers64 m, long long np, double *rho)
+{
+   for (long long n = blockIdx.x*(long long) blockDim.x + threadIdx.x ; n < np ;
+        n += (long long) gridDim.x*blockDim.x) {
+      const double qm = m.qm[n];
+      if (qm == 0.0)
+         continue;
+      double sx = m.x[n]/g.h[0], sy = m.y[n]/g.h[1], sz = m.z[n]/g.h[2];
+      const int i = dbl_to_int (sx), j = dbl_to_int (sy), k = dbl_to_int (sz);
+      if (i < -1 || i > g.n[0] || j < -1 || j > g.n[1] || k < -1 || k > g.n[2])
+         continue;
+      sx -= i; sy -= j; sz -= k;
+      const long o = g.at (i, j, k), Sx = g.sx, Sy = g.sy;
+      const double v = m.rho[n];
+      atomicAdd (rho + o, (1 - sx)*(1 - sy)*(1 - sz)*v);
+      atomicAdd (rho + o + Sx, sx*(1 - sy)*(1 - sz)*v);
+      atomicAdd (rho + o + Sy, (1 - sx)*sy*(1 - sz)*v);
+      atomicAdd (rho + o + Sx + Sy, sx*sy*(1 - sz)*v);
+      atomicAdd (rho + o + 1, (1 - sx)*(1 - sy)*sz*v);
+      atomicAdd (rho + o + Sx + 1, sx*(1 - sy)*sz*v);
+      atomicAdd (rho + o + Sy + 1, (1 - sx)*sy*sz*v);
+      atomicAdd (rho + o + Sx + Sy + 1, sx*sy*sz*v);
+   }
+}
+
+// Particle walls applied once to freshly loaded markers (plasma_init,
+// core/plasma.c:399-404, on markers that all start in the shell).
+__global__ void k_walls64 (Grid g, Markers64 m, long long np, DevScalars *dsc)
+{
+   long long dead = 0;
+   const double L[3] = {g.n[0]*g.h[0], g.n[1]*g.h[1], g.n[2]*g.h[2]};
+   for (long long n = blockIdx.x*(long long) blockDim.x + threadIdx.x ; n < np ;
+        n += (long long) gridDim.x*blockDim.x) {
+      if (m.qm[n] == 0.0f)
+         continue;
+      double pos[3] = {m.x[n], m.y[n], m.z[n]};
+      double vel[3] = {m.ux[n], m.uy[n], m.uz[n]};
+      bool gone = false;
+      for (int f = 0 ; f < 6 && !gone ; ++f) {
+         const int a = (f < 3) ? f : f - 3, top = (f >= 3);
+         const int bc = g.bc[top][a];
+         if (bc == MG_BC_PERIODIC) {
+            if (!top && pos[a] <= 0) pos[a] += L[a];
+            if (top && pos[a] >= L[a]) pos[a] -= L[a];
+         } else if (bc == MG_BC_MIRROR) {
+            if (!top && pos[a] <= 0) { pos[a] = -pos[a]; vel[a] *= -1; }
+            if (top && pos[a] >= L[a]) { pos[a] = 2*L[a] - pos[a]; vel[a] *= -1; }
+         } else if ((!top && pos[a] <= g.h[a]) || (top && pos[a] >= L[a] - g.h[a])) {
+            gone = true;
+         }
+      }
+      m.x[n] = pos[0];
+      m.y[n] = pos[1];
+      m.z[n] = pos[2];
+      m.ux[n] = vel[0];
+      m.uy[n] = vel[1];
+      m.uz[n] = vel[2];
+      if (gone) {
+         m.qm[n] = 0.0f;
+         ++dead;
+      }
+   }
+   if (dead)
+      atomicAdd ((unsigned long long *) &dsc->dead, (unsigned long long) dead);
+}
+
+} // namespace
+
+int mg_walls64 (mg_run_t *r)
+{
+   if (r->np == 0)
+      return MG_OK;
+   k_walls64<<<mg_blocks_for (r->np, 256, 8), 256, 0, r->stream>>> (r->g, r->m64, r->np, r->dsc);
+   MG_LAUNCH_CHECK ();
+   return MG_OK;
+}
+
+int mg_push64 (mg_run_t *r)
+{
+   if (r->np == 0)
+      return MG_OK;
+   Ctx c;
+   c.g = r->g;
+   c.E0 = r->E[0]; c.E1 = r->E[1]; c.E2 = r->E[2];
+   c.H0 = r->H[0]; c.H1 = r->H[1]; c.H2 = r->H[2];
+   c.J0 = r->J[0]; c.J1 = r->J[1]; c.J2 = r->J[2];
+   const int T = 256;
+   k_push64<<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (c, r->m64, r->np, r->dsc);
+   MG_LAUNCH_CHECK ();
+   return MG_OK;
+}
+
+int mg_rho64 (mg_run_t *r, double *rho_dev)
+{
+   if (r->np == 0)
+      return MG_OK;
+   const int T = 256;
+   k_rho64<<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (r->g, r->m64, r->np, rho_dev);
+   MG_LAUNCH_CHECK ();
+   return MG_OK;
+}

@@ -358,11 +358,21 @@ static void e_bc (po_run_t *r)
    }
 }
 
+static int particle_bc (const po_run_t *r, po_marker_t *m);
+
 /* cap_init (core/em_caps.c:343-392): ghost refresh for periodic and mirror
  * walls, Mur history from the loaded E and the normal-E ghost copy
- * (emCap_Mur.c:86-112). */
+ * (emCap_Mur.c:86-112).  plasma_init (core/plasma.c:399-404) applies the
+ * particle walls once to the loaded markers, which all start in the shell
+ * (core/plasma_IO.c:265): markers within one cell of an open wall go. */
 void po_init (po_run_t *r)
 {
+   long keep = 0;
+   for (long n = 0 ; n < r->np ; ++n)
+      if (!particle_bc (r, r->p + n))
+         r->p[keep++] = r->p[n];
+   r->np = keep;
+
    for (int ea = 0 ; ea < 3 ; ++ea) {
       const int ep = (ea + 1) % 3, eq = (ea + 2) % 3, N = r->n[ea];
       if (r->bc[0][ea] == PO_BC_PERIODIC) {
