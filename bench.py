@@ -1,0 +1,397 @@
+"""Throughput benchmark of the B200 PIC core.
+
+Workload (default): the plain FP64 3D laser-foil interaction -- a 256x128x128
+grid at 20 cells per wavelength (h = 0.05), Courant 0.5, Mur absorbing walls
+on all six faces, an Ey-polarised Gaussian laser (lambda = 1, a0 = 3, waist
+3 lambda, 10-cycle sin^2 envelope) injected at x-plane 5 and focused on the
+front of a 30 n_cr, 0.5-lambda (10-cell) foil of electrons and protons at 16
+markers per cell each (4.46e6 markers, uniform random in-cell positions from
+ranmar seeds (1802, 9373), cold), run for 2000 steps: W warm-up steps, then
+K timed steps of the same run.  Data are synthetic (no benchmark suite).
+
+One JSON line on rank 0:
+  value      particle-steps/s over all ranks, device-resident state, CUDA
+             events on the run's stream around K graph-replayed steps;
+  e2e        the same metric through the C ABI from pinned host buffers:
+             upload of markers and fields, K steps with the energy rows read
+             back, download of markers and fields, all inside the timed region;
+  roofline   the push kernel (the largest kernel of the step): algorithmic
+             bytes per launch (100 B per marker: x and u read and written in
+             FP64, the weight read) over its mean launch time, against the
+             measured HBM copy bandwidth;
+  cpu_baseline  the reference core.out (built from the reference sources,
+             oracle/_ref/core_fast.out) on a bounded sample of the same
+             workload on this host's cores.
+
+--impl reference times that reference path alone on rank 0 and prints the
+same metric.  Under torchrun every rank runs an independent replica (the
+path has no data-parallel exchange: replicas only, weak scaling).
+"""
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_CR = 4 * math.pi ** 2
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def workload(name="laser_foil"):
+    if name != "laser_foil":
+        raise SystemExit("unknown workload %r" % name)
+    n = (256, 128, 128)
+    h = (0.05, 0.05, 0.05)
+    tau = 0.5 / math.sqrt(sum(1.0 / v ** 2 for v in h))
+    bc = (2, 2, 2)
+    ppc = 16
+    foil = ((120, 5, 5), (130, 123, 123))           # 10 cells, 5-cell wall margins
+    n_each = (foil[1][0] - foil[0][0]) * (foil[1][1] - foil[0][1]) * (foil[1][2] - foil[0][2]) * ppc
+    species = [
+        dict(lo=foil[0], hi=foil[1], ppc=ppc, rho=-30 * N_CR / ppc, qDivM=-1.0,
+             drift=(0, 0, 0), uth=(0, 0, 0), seed=(1802, 9373), skip=0, id0=1),
+        dict(lo=foil[0], hi=foil[1], ppc=ppc, rho=30 * N_CR / ppc, qDivM=1.0 / 1836,
+             drift=(0, 0, 0), uth=(0, 0, 0), seed=(1802, 9373), skip=7 * n_each, id0=1 + n_each),
+    ]
+    laser = dict(a0=3.0, waist=3.0, x_focus=foil[0][0] * h[0], duration=10.0, t_start=0.0,
+                 phase=0.0, plane=5, margin=5)
+    return dict(name="laser_foil_fp64_256x128x128", n=n, h=h, tau=tau, bc=bc, species=species,
+                laser=laser, markers=2 * n_each, total_steps=2000)
+
+
+def make_run(w, device):
+    import mandor3_b200 as mg
+    r = mg.Run(w["n"], w["h"], w["tau"], w["bc"], w["bc"], device=device, capacity=w["markers"])
+    z = np.zeros(r.field_shape())
+    r.set_fields(z, z)
+    r.set_laser(**w["laser"])
+    for s in w["species"]:
+        r.place_uniform(**s)
+    r.init()
+    return r
+
+
+class Clocks:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.lines = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.QUERY,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+            time.sleep(0.3)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [v.strip() for v in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_FILE) as fp:
+            return float(json.load(fp)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per push launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "push64_laser_foil.md")
+    try:
+        text = open(path).read()
+    except OSError:
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", text)
+    return float(m.group(1)) if m else None
+
+
+# ---------------------------------------------------------------------------
+# Reference CPU path (the reference core.out built from its sources).
+# ---------------------------------------------------------------------------
+def reference_sample(w, steps):
+    """Runs the reference core_fast.out on the workload's grid and markers for
+    `steps` steps; returns (particle-steps/s, seconds, markers, description)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_port
+    from refrun import RefRun, have_reference
+    exe = os.path.join(ROOT, "oracle", "_ref", "core_fast.out")
+    if not have_reference() or not os.path.exists(exe):
+        return None
+    m = np.concatenate([oracle_port.place(h=w["h"], **s) for s in w["species"]])
+    rr = RefRun(tempfile.mkdtemp(prefix="mandor_bench_ref_"))
+    try:
+        h_um = [v for v in w["h"]]
+        L_um = [w["n"][a] * h_um[a] for a in range(3)]
+        rr.setup(w["n"], L_um, -0.5, w["bc"], w["bc"])
+        rr.set_state(m)
+        out = rr.run(steps, exe="core_fast.out", timeout=1800)
+    finally:
+        rr.cleanup()
+    sec = float(re.search(r"main loop have taken ([0-9.eE+-]+) sec", out).group(1))
+    desc = ("reference core.out (-O3, single-rank MPI shim, 1 process) on the laser-foil grid "
+            "and markers, %d steps from t=0, laser source omitted (the reference has no "
+            "analytic sin^2 source; the source plane is O(n^2) work)" % steps)
+    return len(m) * steps / sec, sec, len(m), desc
+
+
+# ---------------------------------------------------------------------------
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def dist_max(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v)], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_sum(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v)], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_reference_arm(args, w, world, rank):
+    if rank != 0:
+        return
+    steps = args.ref_steps
+    res = reference_sample(w, steps)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference binaries not built (make -C oracle ref)"}))
+        return
+    rate, sec, nm, desc = res
+    line = {"metric": "particle-steps/s", "value": rate, "unit": "particle-steps/s",
+            "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sec / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w["name"], "markers": nm, "grid": list(w["n"]),
+                       "bc": "mur x6", "courant": 0.5},
+            "cpu_baseline": {"value": rate, "unit": "particle-steps/s", "cores": 1,
+                             "kind": "reference", "sample": desc},
+            "e2e": {"value": rate, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1990)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="laser_foil")
+    ap.add_argument("--ref-steps", type=int, default=12)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("at least 3 warm-up steps")
+
+    w = workload(args.workload)
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference_arm(args, w, world, rank)
+        barrier(world)
+        return
+
+    import mandor3_b200 as mg
+    import torch
+
+    device = local
+    torch.cuda.set_device(device)
+    r = make_run(w, device)
+    r.step(args.warmup)
+    launches_per_step = r.kernels_per_step()
+    n_before = r.marker_count()
+    stream = torch.cuda.ExternalStream(r.stream(), device=device)
+
+    # Timed region: K graph-replayed steps, events on the run's stream.
+    r.profile(True)
+    barrier(world)
+    torch.cuda.synchronize()
+    with Clocks(device) as clocks:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r.step_async(args.steps)
+        e1.record(stream)
+        r.synchronize()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    push_ms, step_ms = r.last_timing()
+    n_after = r.marker_count()
+    r.close()
+    n_avg = 0.5 * (n_before + n_after)
+    ms_max = dist_max(ms, world)
+    total_ps = dist_sum(n_avg * args.steps, world)
+    value = total_ps / (ms_max / 1e3)
+
+    # End to end through the C ABI from pinned host buffers.
+    e2e = None
+    if not args.no_e2e:
+        e2e = end_to_end(w, device, args.steps, args.warmup, world)
+
+    peak, peak_kind = hbm_peak()
+    algo_bytes = 100.0 * n_avg
+    achieved = algo_bytes / (push_ms / 1e3) / 1e9 if push_ms > 0 else None
+    roofline = {"bound": "hbm", "kernel": "k_push64", "achieved": achieved, "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s",
+                "frac": achieved / peak if achieved else None,
+                "traffic": ncu_traffic(), "push_ms": push_ms, "step_ms": step_ms,
+                "algorithmic_bytes_per_launch": algo_bytes}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        res = reference_sample(w, args.ref_steps)
+        if res:
+            rate, sec, nm, desc = res
+            cpu = {"value": rate, "unit": "particle-steps/s", "cores": 1, "kind": "reference",
+                   "sample": desc}
+    barrier(world)
+    if rank != 0:
+        return
+    line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w["name"], "markers": w["markers"], "grid": list(w["n"]),
+                       "bc": "mur x6", "courant": 0.5, "laser": "a0=3 w0=3 sin^2 10 cycles",
+                       "foil": "30 n_cr, 10 cells, e- and p+ at 16 ppc",
+                       "parallelism": "replicas x%d" % world,
+                       "l2": "inputs larger than L2 (fields 0.34 GB + markers 0.27 GB per step)"},
+            "clocks": clocks.summary(), "e2e": e2e,
+            "gpu_launches": launches_per_step * args.steps, "roofline": roofline,
+            "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+
+
+def end_to_end(w, device, steps, warmup, world):
+    """Host buffers in, host buffers out, through the reference-facing ABI."""
+    import mandor3_b200 as mg
+    import torch
+    # The initial state as host data (what core.out would load from binData).
+    r0 = make_run(w, device)
+    markers = r0.markers()
+    r0.close()
+    shape = (w["n"][0] + 1, w["n"][1] + 1, w["n"][2] + 1, 3)
+    pin = lambda nbytes: torch.empty(nbytes, dtype=torch.uint8, pin_memory=True).numpy()
+    hm = pin(markers.nbytes).view(mg.MARKER_DTYPE)
+    hm[:] = markers
+    hE = pin(8 * int(np.prod(shape))).view("<f8").reshape(shape)
+    hH = pin(8 * int(np.prod(shape))).view("<f8").reshape(shape)
+    hE[:] = 0
+    hH[:] = 0
+    rows = pin(8 * 6 * steps).view("<f8").reshape(steps, 6)
+    out_m = pin(markers.nbytes).view(mg.MARKER_DTYPE)
+    r = mg.Run(w["n"], w["h"], w["tau"], w["bc"], w["bc"], device=device, capacity=len(markers))
+    r.set_laser(**w["laser"])
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r.set_fields(hE, hH)
+    r.set_markers(hm)
+    r.init()
+    lib = mg.load()
+    rc = lib.mg_run_step(r.ptr, steps, rows.ctypes.data)
+    if rc:
+        raise mg.MandorError(rc, lib.mg_last_error().decode())
+    import ctypes
+    got = ctypes.c_longlong()
+    rc = lib.mg_run_get_markers(r.ptr, out_m.ctypes.data, len(out_m), ctypes.byref(got))
+    if rc:
+        raise mg.MandorError(rc, lib.mg_last_error().decode())
+    rc = lib.mg_run_get_fields(r.ptr, hE.ctypes.data, hH.ctypes.data)
+    if rc:
+        raise mg.MandorError(rc, lib.mg_last_error().decode())
+    sec = time.perf_counter() - t0
+    r.close()
+    sec = dist_max(sec, world)
+    ps = dist_sum(0.5 * (len(markers) + got.value) * steps, world)
+    h2d = markers.nbytes + hE.nbytes + hH.nbytes
+    d2h = got.value * 64 + hE.nbytes + hH.nbytes + rows.nbytes
+    return {"value": ps / sec, "unit": "particle-steps/s",
+            "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps,
+            "seconds": sec, "note": "wall clock, max over ranks; upload + %d steps + download" % steps}
+
+
+if __name__ == "__main__":
+    main()

@@ -54,6 +54,9 @@ int mg_sm_count (void)
          return rc_;                                                         \
    } while (0)
 
+static void drop_graphs (mg_run_t *r);
+#define MG_PROFILE_CHUNK 512
+
 // ---------------------------------------------------------------------------
 // Layout conversion kernels.
 // ---------------------------------------------------------------------------
@@ -257,16 +260,8 @@ static int ensure_capacity (mg_run_t *r, long long need)
    }
    r->m64 = nm;
    r->cap = cap;
-   // The captured graph holds the old pointers.
-   if (r->graph_exec) {
-      cudaGraphExecDestroy (r->graph_exec);
-      r->graph_exec = nullptr;
-   }
-   if (r->graph) {
-      cudaGraphDestroy (r->graph);
-      r->graph = nullptr;
-   }
-   r->graph_ok = 0;
+   // The captured graphs hold the old pointers.
+   drop_graphs (r);
    return MG_OK;
 }
 
@@ -410,8 +405,12 @@ extern "C" int mg_run_destroy (mg_run_t *r)
    cudaSetDevice (r->device);
    if (r->stream)
       cudaStreamSynchronize (r->stream);
-   if (r->graph_exec) cudaGraphExecDestroy (r->graph_exec);
-   if (r->graph) cudaGraphDestroy (r->graph);
+   drop_graphs (r);
+   if (r->pev) {
+      for (int q = 0 ; q < 2*MG_PROFILE_CHUNK ; ++q)
+         if (r->pev[q]) cudaEventDestroy (r->pev[q]);
+      free (r->pev);
+   }
    for (int c = 0 ; c < 3 ; ++c) {
       if (r->E[c]) cudaFree (r->E[c]);
       if (r->H[c]) cudaFree (r->H[c]);
@@ -598,9 +597,7 @@ extern "C" int mg_run_set_laser (mg_run_t *r, const mg_laser_t *l)
       r->laser = *l;
       r->has_laser = 1;
    }
-   if (r->graph_exec) { cudaGraphExecDestroy (r->graph_exec); r->graph_exec = nullptr; }
-   if (r->graph) { cudaGraphDestroy (r->graph); r->graph = nullptr; }
-   r->graph_ok = 0;
+   drop_graphs (r);
    return MG_OK;
 }
 
@@ -797,30 +794,37 @@ extern "C" int mg_plasma_rho (mg_run_t *r, double *rho)
 // ---------------------------------------------------------------------------
 // Whole steps.
 // ---------------------------------------------------------------------------
-int mg_enqueue_step64 (mg_run_t *r)
+// One step as three parts: fields before the push, the push, and the rest
+// (core/main.c:353-478 order).  part < 0 enqueues all three.
+int mg_enqueue_step64 (mg_run_t *r, int part)
 {
-   TRY (mg_fields64_h_half (r));
-   TRY (mg_fields64_energy (r));
-   TRY (mg_fields64_zero_j (r));
-   TRY (mg_push64 (r));
-   TRY (mg_fields64_h_step (r));
-   TRY (mg_fields64_e_step (r));
-   TRY (mg_fields64_jbc (r));
-   TRY (mg_fields64_e_finish (r));
-   k_end_step<<<1, 1, 0, r->stream>>> (r->dsc, r->ring, r->g.h[0]*r->g.h[1]*r->g.h[2], r->g.tau);
-   MG_LAUNCH_CHECK ();
+   if (part < 0 || part == 0) {
+      TRY (mg_fields64_h_half (r));
+      TRY (mg_fields64_energy (r));
+      TRY (mg_fields64_zero_j (r));
+   }
+   if (part < 0 || part == 1)
+      TRY (mg_push64 (r));
+   if (part < 0 || part == 2) {
+      TRY (mg_fields64_h_step (r));
+      TRY (mg_fields64_e_step (r));
+      TRY (mg_fields64_jbc (r));
+      TRY (mg_fields64_e_finish (r));
+      k_end_step<<<1, 1, 0, r->stream>>> (r->dsc, r->ring, r->g.h[0]*r->g.h[1]*r->g.h[2], r->g.tau);
+      MG_LAUNCH_CHECK ();
+   }
    return MG_OK;
 }
 
-int mg_enqueue_step32 (mg_run_t *r);
+int mg_enqueue_step32 (mg_run_t *r, int part);
 
-static int count_kernels (mg_run_t *r)
+static int count_kernels (cudaGraph_t graph)
 {
    size_t n = 0;
-   if (cudaGraphGetNodes (r->graph, nullptr, &n) != cudaSuccess)
+   if (cudaGraphGetNodes (graph, nullptr, &n) != cudaSuccess)
       return 0;
    cudaGraphNode_t *nodes = (cudaGraphNode_t *) malloc (n*sizeof (cudaGraphNode_t));
-   cudaGraphGetNodes (r->graph, nodes, &n);
+   cudaGraphGetNodes (graph, nodes, &n);
    int k = 0;
    for (size_t q = 0 ; q < n ; ++q) {
       cudaGraphNodeType t;
@@ -831,27 +835,42 @@ static int count_kernels (mg_run_t *r)
    return k;
 }
 
+static void drop_graphs (mg_run_t *r)
+{
+   for (int q = 0 ; q < 4 ; ++q) {
+      if (r->gexec[q]) cudaGraphExecDestroy (r->gexec[q]);
+      if (r->gr[q]) cudaGraphDestroy (r->gr[q]);
+      r->gexec[q] = nullptr;
+      r->gr[q] = nullptr;
+   }
+   r->graph_ok = 0;
+}
+
+// Graph 0: the whole step; graphs 1..3: its three parts (profiling mode, so
+// that events can bracket the push on the run's stream).
 static int build_graph (mg_run_t *r)
 {
    if (r->graph_ok)
       return MG_OK;
-   if (r->graph_exec) { cudaGraphExecDestroy (r->graph_exec); r->graph_exec = nullptr; }
-   if (r->graph) { cudaGraphDestroy (r->graph); r->graph = nullptr; }
-   MG_CUDA (cudaStreamBeginCapture (r->stream, cudaStreamCaptureModeThreadLocal));
-   int rc = is32 (r) ? mg_enqueue_step32 (r) : mg_enqueue_step64 (r);
-   cudaGraph_t g = nullptr;
-   cudaError_t e = cudaStreamEndCapture (r->stream, &g);
-   if (rc != MG_OK) {
-      if (g) cudaGraphDestroy (g);
-      return rc;
+   drop_graphs (r);
+   for (int q = 0 ; q < 4 ; ++q) {
+      MG_CUDA (cudaStreamBeginCapture (r->stream, cudaStreamCaptureModeThreadLocal));
+      const int part = q - 1;
+      int rc = is32 (r) ? mg_enqueue_step32 (r, part) : mg_enqueue_step64 (r, part);
+      cudaGraph_t g = nullptr;
+      cudaError_t e = cudaStreamEndCapture (r->stream, &g);
+      if (rc != MG_OK) {
+         if (g) cudaGraphDestroy (g);
+         return rc;
+      }
+      if (e != cudaSuccess) {
+         mg_set_error ("graph capture failed: %s", cudaGetErrorString (e));
+         return MG_ERR_CUDA;
+      }
+      r->gr[q] = g;
+      MG_CUDA (cudaGraphInstantiate (&r->gexec[q], g, 0));
    }
-   if (e != cudaSuccess) {
-      mg_set_error ("graph capture failed: %s", cudaGetErrorString (e));
-      return MG_ERR_CUDA;
-   }
-   r->graph = g;
-   MG_CUDA (cudaGraphInstantiate (&r->graph_exec, g, 0));
-   r->kernels_per_step = count_kernels (r);
+   r->kernels_per_step = count_kernels (r->gr[0]);
    r->graph_ok = 1;
    return MG_OK;
 }
@@ -871,15 +890,26 @@ static int run_steps (mg_run_t *r, int nsteps, double *host_rows, double *dev_ro
       return MG_ERR_ARG;
    }
    TRY (build_graph (r));
+   double push_sum = 0, step_sum = 0;
    for (int done = 0 ; done < nsteps ; ) {
-      const int chunk = (nsteps - done < MG_RING) ? nsteps - done : MG_RING;
+      int chunk = (nsteps - done < MG_RING) ? nsteps - done : MG_RING;
+      if (r->profile && chunk > MG_PROFILE_CHUNK)
+         chunk = MG_PROFILE_CHUNK;
       MG_CUDA (cudaMemsetAsync (&r->dsc->step, 0, sizeof (int), r->stream));
-      if (r->profile)
+      if (r->profile) {
          MG_CUDA (cudaEventRecord (r->ev[0], r->stream));
-      for (int s = 0 ; s < chunk ; ++s)
-         MG_CUDA (cudaGraphLaunch (r->graph_exec, r->stream));
-      if (r->profile)
+         for (int s = 0 ; s < chunk ; ++s) {
+            MG_CUDA (cudaGraphLaunch (r->gexec[1], r->stream));
+            MG_CUDA (cudaEventRecord (r->pev[2*s], r->stream));
+            MG_CUDA (cudaGraphLaunch (r->gexec[2], r->stream));
+            MG_CUDA (cudaEventRecord (r->pev[2*s + 1], r->stream));
+            MG_CUDA (cudaGraphLaunch (r->gexec[3], r->stream));
+         }
          MG_CUDA (cudaEventRecord (r->ev[1], r->stream));
+      } else {
+         for (int s = 0 ; s < chunk ; ++s)
+            MG_CUDA (cudaGraphLaunch (r->gexec[0], r->stream));
+      }
       if (host_rows)
          MG_CUDA (cudaMemcpyAsync (host_rows + 6*(size_t) done, r->ring, sizeof (double)*6*chunk,
                                    cudaMemcpyDeviceToHost, r->stream));
@@ -887,13 +917,21 @@ static int run_steps (mg_run_t *r, int nsteps, double *host_rows, double *dev_ro
          MG_CUDA (cudaMemcpyAsync (dev_rows + 6*(size_t) done, r->ring, sizeof (double)*6*chunk,
                                    cudaMemcpyDeviceToDevice, r->stream));
       done += chunk;
-      if (host_rows || sync || done < nsteps)
+      if (host_rows || sync || r->profile || done < nsteps)
          MG_CUDA (cudaStreamSynchronize (r->stream));
-      if (r->profile && (host_rows || sync)) {
+      if (r->profile) {
          float ms = 0;
+         for (int s = 0 ; s < chunk ; ++s) {
+            cudaEventElapsedTime (&ms, r->pev[2*s], r->pev[2*s + 1]);
+            push_sum += ms;
+         }
          cudaEventElapsedTime (&ms, r->ev[0], r->ev[1]);
-         r->last_step_ms = ms/chunk;
+         step_sum += ms;
       }
+   }
+   if (r->profile && nsteps > 0) {
+      r->last_push_ms = push_sum/nsteps;
+      r->last_step_ms = step_sum/nsteps;
    }
    r->time += nsteps*r->g.tau;
    if (sync)
@@ -948,6 +986,11 @@ extern "C" int mg_run_device_bytes (mg_run_t *r, long long *bytes)
 extern "C" int mg_run_profile (mg_run_t *r, int enable)
 {
    CHECK_RUN (r);
+   if (enable && !r->pev) {
+      r->pev = (cudaEvent_t *) calloc (2*MG_PROFILE_CHUNK, sizeof (cudaEvent_t));
+      for (int q = 0 ; q < 2*MG_PROFILE_CHUNK ; ++q)
+         MG_CUDA (cudaEventCreate (&r->pev[q]));
+   }
    r->profile = enable;
    return MG_OK;
 }

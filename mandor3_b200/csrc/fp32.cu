@@ -25,7 +25,7 @@ int mg_fields32_e_finish (mg_run_t *) { NOT_BUILT ("e_finish"); }
 int mg_fields32_init (mg_run_t *) { NOT_BUILT ("init"); }
 int mg_fields32_zero_j (mg_run_t *) { NOT_BUILT ("zero_j"); }
 int mg_push32 (mg_run_t *) { NOT_BUILT ("push"); }
-int mg_enqueue_step32 (mg_run_t *) { NOT_BUILT ("step"); }
+int mg_enqueue_step32 (mg_run_t *, int) { NOT_BUILT ("step"); }
 int mg_place32 (mg_run_t *, const mg_place_t *, long long, long long) { NOT_BUILT ("place"); }
 int mg_ensure_capacity32 (mg_run_t *, long long) { NOT_BUILT ("capacity"); }
 int mg_walls32 (mg_run_t *) { NOT_BUILT ("walls"); }

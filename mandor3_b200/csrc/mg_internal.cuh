@@ -119,8 +119,8 @@ struct mg_run {
    size_t      stage_bytes;
 
    // graph
-   cudaGraph_t     graph;
-   cudaGraphExec_t graph_exec;
+   cudaGraph_t     gr[4];      // whole step, then its three parts
+   cudaGraphExec_t gexec[4];
    int             graph_ok;
    int             kernels_per_step;
 
@@ -131,6 +131,7 @@ struct mg_run {
    // profiling
    int         profile;
    cudaEvent_t ev[4];
+   cudaEvent_t *pev;       // event pairs around the push, profiling mode
    double      last_push_ms, last_step_ms;
 
    long long   dev_bytes;
@@ -183,7 +184,7 @@ int mg_fields32_zero_j (mg_run_t *r);
 int mg_push32 (mg_run_t *r);
 int mg_sort32 (mg_run_t *r);
 int mg_walls32 (mg_run_t *r);
-int mg_enqueue_step32 (mg_run_t *r);
+int mg_enqueue_step32 (mg_run_t *r, int part);
 int mg_place32 (mg_run_t *r, const mg_place_t *spec, long long at, long long count);
 int mg_ensure_capacity32 (mg_run_t *r, long long need);
 int mg_run_create32 (const mg_params_t *params, mg_run_t **out);
