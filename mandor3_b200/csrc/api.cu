@@ -353,7 +353,9 @@ extern "C" int mg_run_create (const mg_params_t *params, mg_run_t **out)
       rc = dev_alloc (r, (void **) &r->E[c], fb);
       if (rc == MG_OK) rc = dev_alloc (r, (void **) &r->H[c], fb);
       if (rc == MG_OK) rc = dev_alloc (r, (void **) &r->J[c], fb);
+      if (rc == MG_OK) rc = dev_alloc (r, (void **) &r->Hn[c], fb);
       if (rc == MG_OK) {
+         cudaMemsetAsync (r->Hn[c], 0, fb, r->stream);
          cudaMemsetAsync (r->E[c], 0, fb, r->stream);
          cudaMemsetAsync (r->H[c], 0, fb, r->stream);
          cudaMemsetAsync (r->J[c], 0, fb, r->stream);
@@ -415,6 +417,7 @@ extern "C" int mg_run_destroy (mg_run_t *r)
       if (r->E[c]) cudaFree (r->E[c]);
       if (r->H[c]) cudaFree (r->H[c]);
       if (r->J[c]) cudaFree (r->J[c]);
+      if (r->Hn[c]) cudaFree (r->Hn[c]);
    }
    for (int t = 0 ; t < 2 ; ++t)
       for (int a = 0 ; a < 3 ; ++a)
@@ -468,7 +471,8 @@ extern "C" int mg_run_get_fields (mg_run_t *r, double *E, double *H)
    const size_t bytes = (size_t) vol*3*sizeof (double);
    TRY (ensure_stage (r, bytes));
    double *dst[2] = {E, H};
-   double **src[2] = {r->E, r->H};
+   // Between mg_em_HHalfStep and mg_em_HStep the reference's H is H^n.
+   double **src[2] = {r->E, (r->stage_no >= 1 && r->stage_no <= 3) ? r->Hn : r->H};
    for (int f = 0 ; f < 2 ; ++f) {
       if (!dst[f])
          continue;
@@ -589,9 +593,13 @@ extern "C" int mg_run_set_laser (mg_run_t *r, const mg_laser_t *l)
    if (!l) {
       r->has_laser = 0;
    } else {
-      if (l->plane < 2 || l->plane > r->g.n[0] - 2 || l->margin < 0 || !(l->waist > 0) || !(l->duration > 0)) {
-         mg_set_error ("mg_run_set_laser: plane %d / margin %d / waist %g / duration %g out of range",
-                       l->plane, l->margin, l->waist, l->duration);
+      // The E plane (plane - 1) and the transverse range must stay clear of
+      // the two rim layers next to every wall: plane in [3, n-1], margin >= 2.
+      if (l->plane < 3 || l->plane > r->g.n[0] - 1 || l->margin < 2 || !(l->waist > 0) ||
+          !(l->duration > 0)) {
+         mg_set_error ("mg_run_set_laser: plane %d (allowed 3..%d) / margin %d (>= 2) / waist %g / "
+                       "duration %g out of range", l->plane, r->g.n[0] - 1, l->margin, l->waist,
+                       l->duration);
          return MG_ERR_ARG;
       }
       r->laser = *l;
@@ -666,7 +674,6 @@ extern "C" int mg_em_energy (mg_run_t *r, double *we, double *wm)
 {
    CHECK_RUN (r);
    TRY (expect_stage (r, 1, __func__));
-   MG_CUDA (cudaMemsetAsync (r->dsc->acc, 0, 2*sizeof (double), r->stream));
    TRY (is32 (r) ? mg_fields32_energy (r) : mg_fields64_energy (r));
    double acc[2];
    MG_CUDA (cudaMemcpyAsync (acc, r->dsc->acc, sizeof (acc), cudaMemcpyDeviceToHost, r->stream));
@@ -694,11 +701,8 @@ static int check_err (mg_run_t *r)
 extern "C" int mg_plasma_move (mg_run_t *r)
 {
    CHECK_RUN (r);
-   if (r->stage_no == 1) {
-      // Energy stage skipped by the caller: keep the accumulators clear.
-      MG_CUDA (cudaMemsetAsync (r->dsc->acc, 0, 2*sizeof (double), r->stream));
-      r->stage_no = 2;
-   }
+   if (r->stage_no == 1)
+      r->stage_no = 2;       // the energy stage is optional
    TRY (expect_stage (r, 2, __func__));
    MG_CUDA (cudaMemsetAsync (r->dsc->acc + 2, 0, 3*sizeof (double), r->stream));
    TRY (is32 (r) ? mg_fields32_zero_j (r) : mg_fields64_zero_j (r));
@@ -799,17 +803,14 @@ extern "C" int mg_plasma_rho (mg_run_t *r, double *rho)
 int mg_enqueue_step64 (mg_run_t *r, int part)
 {
    if (part < 0 || part == 0) {
-      TRY (mg_fields64_h_half (r));
-      TRY (mg_fields64_energy (r));
+      TRY (mg_fields64_h_both (r));
       TRY (mg_fields64_zero_j (r));
    }
    if (part < 0 || part == 1)
       TRY (mg_push64 (r));
    if (part < 0 || part == 2) {
-      TRY (mg_fields64_h_step (r));
-      TRY (mg_fields64_e_step (r));
       TRY (mg_fields64_jbc (r));
-      TRY (mg_fields64_e_finish (r));
+      TRY (mg_fields64_e_fused (r));
       k_end_step<<<1, 1, 0, r->stream>>> (r->dsc, r->ring, r->g.h[0]*r->g.h[1]*r->g.h[2], r->g.tau);
       MG_LAUNCH_CHECK ();
    }

@@ -92,6 +92,7 @@ struct mg_run {
 
    // fields
    double *E[3], *H[3], *J[3];
+   double *Hn[3];          // H at t = n tau (H holds n-1/2, then n+1/2)
    double *mur[2][3];      // Mur history, 4 doubles per wall node
    float  *E32[3], *H32[3], *J32[3];
    float  *mur32[2][3];
@@ -169,6 +170,8 @@ int mg_fields64_jbc (mg_run_t *r);
 int mg_fields64_e_finish (mg_run_t *r);
 int mg_fields64_init (mg_run_t *r);
 int mg_fields64_zero_j (mg_run_t *r);
+int mg_fields64_h_both (mg_run_t *r);
+int mg_fields64_e_fused (mg_run_t *r);
 int mg_push64 (mg_run_t *r);
 int mg_rho64 (mg_run_t *r, double *rho_dev);
 int mg_end_step (mg_run_t *r);

@@ -22,6 +22,7 @@
 // issues the twelve atomics.  Further segments of cell-crossing markers add
 // their contributions directly.
 #include <cuda_runtime.h>
+#include <stdlib.h>
 
 #include "mg_internal.cuh"
 
@@ -29,11 +30,51 @@ namespace {
 
 __device__ __forceinline__ int dbl_to_int (double x) { return (int) (x + 128.0) - 128; }
 
+// MF_DBL_TO_INT (misc_PIC.h:18) without conversion instructions: for
+// y = s + 128 in [0, 2^31), t = y + 1.5*2^52 holds round(y) in the low bits
+// of its significand, t - 1.5*2^52 is that integer as a double (exact), and
+// one comparison turns rounding into truncation.  Returns the index as an
+// int and, in fs, the same index as a double -- the values the reference's
+// (int) cast and its int-to-double promotions produce.  Out-of-range input
+// gives some integer, which the caller's range check rejects.
+__device__ __forceinline__ int cell_of (double s, double &fs)
+{
+   const double M = 6755399441055744.0;
+   const double y = s + 128.0;
+   const double t = y + M;
+   double r = t - M;
+   int n = __double2loint (t);
+   if (r > y) {
+      r -= 1.0;
+      n -= 1;
+   }
+   fs = r - 128.0;
+   return n - 128;
+}
+
 struct Ctx {
    Grid   g;
    const double *E0, *E1, *E2, *H0, *H1, *H2;
    double *J0, *J1, *J2;
+   // Correctly rounded reciprocals of the run's constant divisors: 1/h,
+   // 1/((tau h2) h3), 1/((tau h1) h3), 1/((tau h1) h2) and 1/12.
+   double rh[3], rjx, rjy, rjz, jdx, jdy, jdz;
 };
+
+// a/b for a divisor b known in advance, with y = RN(1/b): q0 = RN(a y),
+// r = a - q0 b (exact with one fused multiply-add), q = RN(q0 + r y).  By
+// Markstein's theorem (P. Markstein, IBM J. Res. Dev. 34(1), 1990; see also
+// Muller et al., Handbook of Floating-Point Arithmetic, ch. 4) q is the
+// correctly rounded quotient, i.e. bit-identical to the IEEE division the
+// reference performs, for normal a and b.
+__device__ __forceinline__ double div_by (double a, double b, double y)
+{
+   const double q0 = a*y;
+   const double r = __fma_rn (-q0, b, a);
+   return __fma_rn (r, y, q0);
+}
+
+#define R12 (1.0/12.0)
 
 __device__ __forceinline__ double cic (const double *F, const Grid &g, int i, double sx,
                                        int j, double sy, int k, double sz)
@@ -47,26 +88,27 @@ __device__ __forceinline__ double cic (const double *F, const Grid &g, int i, do
 
 // The twelve weights of one in-cell segment, in the reference's order:
 // Jx at (i+1, j|j+1, k|k+1), Jy at (i|i+1, j+1, k|k+1), Jz at (i|i+1, j|j+1, k+1).
-__device__ __forceinline__ void segment_weights (const Grid &g, int i, int j, int k,
+__device__ __forceinline__ void segment_weights (const Ctx &c, double fi, double fj, double fk,
                                                  double x1, double x2, double y1, double y2,
                                                  double z1, double z2, double rho, double w[12])
 {
-   const double h1 = g.h[0], h2 = g.h[1], h3 = g.h[2], tau = g.tau;
+   const Grid &g = c.g;
+   const double h1 = g.h[0], h2 = g.h[1], h3 = g.h[2];
    const double dX = x2 - x1, dY = y2 - y1, dZ = z2 - z1;
-   const double tX = 0.5*(x1 + x2) - i*h1;
-   const double tY = 0.5*(y1 + y2) - j*h2;
-   const double tZ = 0.5*(z1 + z2) - k*h3;
-   const double ax = rho*dX/(tau*h2*h3), dyz = dY*dZ/12;
+   const double tX = 0.5*(x1 + x2) - fi*h1;
+   const double tY = 0.5*(y1 + y2) - fj*h2;
+   const double tZ = 0.5*(z1 + z2) - fk*h3;
+   const double ax = div_by (rho*dX, c.jdx, c.rjx), dyz = div_by (dY*dZ, 12.0, R12);
    w[0] = ax*((h2 - tY)*(h3 - tZ) + dyz);
    w[1] = ax*(tY*(h3 - tZ) - dyz);
    w[2] = ax*((h2 - tY)*tZ - dyz);
    w[3] = ax*(tY*tZ + dyz);
-   const double ay = rho*dY/(tau*h1*h3), dxz = dX*dZ/12;
+   const double ay = div_by (rho*dY, c.jdy, c.rjy), dxz = div_by (dX*dZ, 12.0, R12);
    w[4] = ay*((h1 - tX)*(h3 - tZ) + dxz);
    w[5] = ay*(tX*(h3 - tZ) - dxz);
    w[6] = ay*((h1 - tX)*tZ - dxz);
    w[7] = ay*(tX*tZ + dxz);
-   const double az = rho*dZ/(tau*h1*h2), dxy = dX*dY/12;
+   const double az = div_by (rho*dZ, c.jdz, c.rjz), dxy = div_by (dX*dY, 12.0, R12);
    w[8] = az*((h1 - tX)*(h2 - tY) + dxy);
    w[9] = az*(tX*(h2 - tY) - dxy);
    w[10] = az*((h1 - tX)*tY - dxy);
@@ -95,7 +137,7 @@ __device__ __forceinline__ void deposit_direct (const Ctx &c, int i, int j, int 
                                                 double z1, double z2, double rho)
 {
    double w[12];
-   segment_weights (c.g, i, j, k, x1, x2, y1, y2, z1, z2, rho, w);
+   segment_weights (c, (double) i, (double) j, (double) k, x1, x2, y1, y2, z1, z2, rho, w);
    scatter12 (c, i, j, k, w);
 }
 
@@ -232,7 +274,25 @@ __device__ __forceinline__ double seg_scan (double v, int lane, int seg_start)
    return v;
 }
 
-__global__ void __launch_bounds__ (256)
+// One wall of core/plasma_walls.c:27-104; returns true if the marker goes.
+// Once removed, later walls leave it alone (it is dropped by the caller).
+__device__ __forceinline__ bool wall (int bc, bool top, double &x, double &v, double L, double h)
+{
+   if (bc == MG_BC_PERIODIC) {
+      if (!top && x <= 0) x += L;
+      if (top && x >= L) x -= L;
+      return false;
+   }
+   if (bc == MG_BC_MIRROR) {
+      if (!top && x <= 0) { x = -x; v = -v; }
+      if (top && x >= L) { x = 2*L - x; v = -v; }
+      return false;
+   }
+   return (!top && x <= h) || (top && x >= L - h);
+}
+
+template <int MINB>
+__global__ void __launch_bounds__ (256, MINB)
 k_push64 (Ctx c, Markers64 m, long long np, DevScalars *dsc)
 {
    const Grid &g = c.g;
@@ -253,18 +313,20 @@ k_push64 (Ctx c, Markers64 m, long long np, DevScalars *dsc)
          valid = (qm != 0.0);             // removed markers carry qDivM = 0
       }
       int i = 0, j = 0, k = 0, i2 = 0, j2 = 0, k2 = 0, nseg = 0;
+      double fi = 0, fj = 0, fk = 0, fi2 = 0, fj2 = 0, fk2 = 0;   // the same as doubles
       double x1 = 0, y1 = 0, z1 = 0, x2 = 0, y2 = 0, z2 = 0, rho = 0;
       double xa = 0, ya = 0, za = 0;         // end of the first segment
       if (valid) {
          x1 = m.x[n];
          y1 = m.y[n];
          z1 = m.z[n];
-         double sX = x1/h1, sY = y1/h2, sZ = z1/h3;
+         double sX = div_by (x1, h1, c.rh[0]), sY = div_by (y1, h2, c.rh[1]), sZ = div_by (z1, h3, c.rh[2]);
          double sX_ = sX + 0.5, sY_ = sY + 0.5, sZ_ = sZ + 0.5;
-         i = dbl_to_int (sX);
-         j = dbl_to_int (sY);
-         k = dbl_to_int (sZ);
-         const int i_ = dbl_to_int (sX_), j_ = dbl_to_int (sY_), k_ = dbl_to_int (sZ_);
+         double fi_, fj_, fk_;
+         i = cell_of (sX, fi);
+         j = cell_of (sY, fj);
+         k = cell_of (sZ, fk);
+         const int i_ = cell_of (sX_, fi_), j_ = cell_of (sY_, fj_), k_ = cell_of (sZ_, fk_);
          // Start cells outside [-1, n] would read or write past the two
          // ghost layers: flag and skip the marker.
          if (i < -1 || i > g.n[0] || j < -1 || j > g.n[1] || k < -1 || k > g.n[2]) {
@@ -276,8 +338,8 @@ k_push64 (Ctx c, Markers64 m, long long np, DevScalars *dsc)
             }
             valid = false;
          } else {
-            sX -= i; sY -= j; sZ -= k;
-            sX_ -= i_; sY_ -= j_; sZ_ -= k_;
+            sX -= fi; sY -= fj; sZ -= fk;
+            sX_ -= fi_; sY_ -= fj_; sZ_ -= fk_;
             const double Ex = cic (c.E0, g, i_, sX_, j, sY, k, sZ);
             const double Ey = cic (c.E1, g, i, sX, j_, sY_, k, sZ);
             const double Ez = cic (c.E2, g, i, sX, j, sY, k_, sZ_);
@@ -288,7 +350,7 @@ k_push64 (Ctx c, Markers64 m, long long np, DevScalars *dsc)
             rho = (double) m.rho[n];
             const double tm = 0.5*tau*qm;
             const double px = m.ux[n] + tm*Ex, py = m.uy[n] + tm*Ey, pz = m.uz[n] + tm*Ez;
-            const double gamma = sqrt (1 + px*px + py*py + pz*pz);
+            const double gamma = sqrt (1.0 + px*px + py*py + pz*pz);
             const double W = (gamma - 1.0)*rho/(px*px + py*py + pz*pz + 1e-19)*h1*h2*h3/qm;
             Wx += W*px*px;
             Wy += W*py*py;
@@ -299,23 +361,23 @@ k_push64 (Ctx c, Markers64 m, long long np, DevScalars *dsc)
             const double u = px + py*az - pz*ay, v = py + pz*ax - px*az, w = pz + px*ay - py*ax;
             const double bxx = ax*ax, byy = ay*ay, bzz = az*az;
             const double bxy = ax*ay, byz = ay*az, bxz = az*ax;
-            const double delta = 1.0/(1 + bxx + byy + bzz);
-            const double vx = tm*Ex + ((1 + bxx)*u + (bxy + az)*v + (bxz - ay)*w)*delta;
-            const double vy = tm*Ey + ((bxy - az)*u + (1 + byy)*v + (byz + ax)*w)*delta;
-            const double vz = tm*Ez + ((bxz + ay)*u + (byz - ax)*v + (1 + bzz)*w)*delta;
+            const double delta = 1.0/(1.0 + bxx + byy + bzz);
+            const double vx = tm*Ex + ((1.0 + bxx)*u + (bxy + az)*v + (bxz - ay)*w)*delta;
+            const double vy = tm*Ey + ((bxy - az)*u + (1.0 + byy)*v + (byz + ax)*w)*delta;
+            const double vz = tm*Ez + ((bxz + ay)*u + (byz - ax)*v + (1.0 + bzz)*w)*delta;
 
-            const double tgi = tau/sqrt (1 + vx*vx + vy*vy + vz*vz);
+            const double tgi = tau/sqrt (1.0 + vx*vx + vy*vy + vz*vz);
             x2 = x1 + vx*tgi;
             y2 = y1 + vy*tgi;
             z2 = z1 + vz*tgi;
 
-            i2 = dbl_to_int (x2/h1);
-            j2 = dbl_to_int (y2/h2);
-            k2 = dbl_to_int (z2/h3);
+            i2 = cell_of (div_by (x2, h1, c.rh[0]), fi2);
+            j2 = cell_of (div_by (y2, h2, c.rh[1]), fj2);
+            k2 = cell_of (div_by (z2, h3, c.rh[2]), fk2);
             int di = abs (i2 - i), dj = abs (j2 - j), dk = abs (k2 - k);
-            if (fabs (x2 - x1) < 1e-10*h1) { di = 0; i2 = i; }
-            if (fabs (y2 - y1) < 1e-10*h2) { dj = 0; j2 = j; }
-            if (fabs (z2 - z1) < 1e-10*h3) { dk = 0; k2 = k; }
+            if (fabs (x2 - x1) < 1e-10*h1) { di = 0; i2 = i; fi2 = fi; }
+            if (fabs (y2 - y1) < 1e-10*h2) { dj = 0; j2 = j; fj2 = fj; }
+            if (fabs (z2 - z1) < 1e-10*h3) { dk = 0; k2 = k; fk2 = fk; }
             if (di > 1 || dj > 1 || dk > 1) {
                // More than one cell per step (Courant violated): flag, no deposit.
                if (atomicOr (&dsc->err, 2) == 0) {
@@ -330,9 +392,13 @@ k_push64 (Ctx c, Markers64 m, long long np, DevScalars *dsc)
             if (nseg == 0) {
                xa = x2; ya = y2; za = z2;
             } else if (nseg == 1) {
-               const double alpha = dk*((k + k2 + 1)*0.5*h3 - z1)/(z2 - z1 + ((1 - dk) << 16))
-                                  + dj*((j + j2 + 1)*0.5*h2 - y1)/(y2 - y1 + ((1 - dj) << 16))
-                                  + di*((i + i2 + 1)*0.5*h1 - x1)/(x2 - x1 + ((1 - di) << 16));
+               // core/plasma.c:214-216: d*(...)/(... + ((1 - d) << 16)) with d in
+               // {0, 1}; a zero term adds a signed zero, which leaves the
+               // crossing point unchanged, so it is skipped.
+               double alpha = 0.0;
+               if (dk) alpha = ((fk + fk2 + 1.0)*0.5*h3 - z1)/(z2 - z1);
+               if (dj) alpha = ((fj + fj2 + 1.0)*0.5*h2 - y1)/(y2 - y1);
+               if (di) alpha = ((fi + fi2 + 1.0)*0.5*h1 - x1)/(x2 - x1);
                xa = x1 + alpha*(x2 - x1);
                ya = y1 + alpha*(y2 - y1);
                za = z1 + alpha*(z2 - z1);
@@ -342,33 +408,20 @@ k_push64 (Ctx c, Markers64 m, long long np, DevScalars *dsc)
 
             // Store the advanced marker, then apply the walls in the
             // reference's order xMin, yMin, zMin, xMax, yMax, zMax.
-            double pos[3] = {x2, y2, z2};
-            double vel[3] = {vx, vy, vz};
-            const double L[3] = {L0, L1, L2};
+            double px_ = x2, py_ = y2, pz_ = z2, vx_ = vx, vy_ = vy, vz_ = vz;
             bool gone = false;
-            for (int f = 0 ; f < 6 ; ++f) {
-               const int a = (f < 3) ? f : f - 3, top = (f >= 3);
-               const int bc = g.bc[top][a];
-               if (bc == MG_BC_PERIODIC) {
-                  if (!top && pos[a] <= 0) pos[a] += L[a];
-                  if (top && pos[a] >= L[a]) pos[a] -= L[a];
-               } else if (bc == MG_BC_MIRROR) {
-                  if (!top && pos[a] <= 0) { pos[a] = -pos[a]; vel[a] *= -1; }
-                  if (top && pos[a] >= L[a]) { pos[a] = 2*L[a] - pos[a]; vel[a] *= -1; }
-               } else {
-                  const double hh = g.h[a];
-                  if ((!top && pos[a] <= hh) || (top && pos[a] >= L[a] - hh)) {
-                     gone = true;
-                     break;
-                  }
-               }
-            }
-            m.x[n] = pos[0];
-            m.y[n] = pos[1];
-            m.z[n] = pos[2];
-            m.ux[n] = vel[0];
-            m.uy[n] = vel[1];
-            m.uz[n] = vel[2];
+            gone |= wall (g.bc[0][0], false, px_, vx_, L0, h1);
+            gone |= wall (g.bc[0][1], false, py_, vy_, L1, h2);
+            gone |= wall (g.bc[0][2], false, pz_, vz_, L2, h3);
+            gone |= wall (g.bc[1][0], true, px_, vx_, L0, h1);
+            gone |= wall (g.bc[1][1], true, py_, vy_, L1, h2);
+            gone |= wall (g.bc[1][2], true, pz_, vz_, L2, h3);
+            m.x[n] = px_;
+            m.y[n] = py_;
+            m.z[n] = pz_;
+            m.ux[n] = vx_;
+            m.uy[n] = vy_;
+            m.uz[n] = vz_;
             if (gone) {
                m.qm[n] = 0.0f;
                ++dead;
@@ -376,10 +429,19 @@ k_push64 (Ctx c, Markers64 m, long long np, DevScalars *dsc)
          }
       }
 
+      // Segments after the first, for markers that crossed cell faces.
+      if (valid && nseg == 1) {
+         double w2[12];
+         segment_weights (c, fi2, fj2, fk2, xa, x2, ya, y2, za, z2, rho, w2);
+         scatter12 (c, i2, j2, k2, w2);
+      }
+      else if (valid && nseg >= 2)
+         multicell_rest (c, i, j, k, i2, j2, k2, x1, y1, z1, x2, y2, z2, rho);
+
       // First segment: warp-aggregated by start cell.
       double wgt[12];
       if (valid)
-         segment_weights (g, i, j, k, x1, xa, y1, ya, z1, za, rho, wgt);
+         segment_weights (c, fi, fj, fk, x1, xa, y1, ya, z1, za, rho, wgt);
       else
          for (int q = 0 ; q < 12 ; ++q) wgt[q] = 0;
       const long long key = valid ? g.at (i, j, k) : -1 - lane;
@@ -393,16 +455,8 @@ k_push64 (Ctx c, Markers64 m, long long np, DevScalars *dsc)
 #pragma unroll
       for (int q = 0 ; q < 12 ; ++q)
          wgt[q] = seg_scan (wgt[q], lane, seg_start);
-      if (valid && tail) {
-         Ctx cc = c;
-         scatter12 (cc, i, j, k, wgt);
-      }
-
-      // Remaining segments of markers that crossed cell faces.
-      if (valid && nseg == 1)
-         deposit_direct (c, i2, j2, k2, xa, x2, ya, y2, za, z2, rho);
-      else if (valid && nseg >= 2)
-         multicell_rest (c, i, j, k, i2, j2, k2, x1, y1, z1, x2, y2, z2, rho);
+      if (valid && tail)
+         scatter12 (c, i, j, k, wgt);
    }
 
    // Thermal energy tally: block reduction, one atomic per block.
@@ -522,10 +576,29 @@ int mg_push64 (mg_run_t *r)
    Ctx c;
    c.g = r->g;
    c.E0 = r->E[0]; c.E1 = r->E[1]; c.E2 = r->E[2];
-   c.H0 = r->H[0]; c.H1 = r->H[1]; c.H2 = r->H[2];
+   c.H0 = r->Hn[0]; c.H1 = r->Hn[1]; c.H2 = r->Hn[2];   // H at t = n tau
    c.J0 = r->J[0]; c.J1 = r->J[1]; c.J2 = r->J[2];
+   const double *h = r->g.h, tau = r->g.tau;
+   for (int a = 0 ; a < 3 ; ++a)
+      c.rh[a] = 1.0/h[a];
+   c.jdx = tau*h[1]*h[2];
+   c.jdy = tau*h[0]*h[2];
+   c.jdz = tau*h[0]*h[1];
+   c.rjx = 1.0/c.jdx;
+   c.rjy = 1.0/c.jdy;
+   c.rjz = 1.0/c.jdz;
    const int T = 256;
-   k_push64<<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (c, r->m64, r->np, r->dsc);
+   // Blocks resident per SM the kernel is compiled for (register budget):
+   // 2 (no spills) or 3 (some spills, more warps to hide gather latency).
+   static int minb = 0;
+   if (!minb) {
+      const char *e = getenv ("MG_PUSH_MINB");
+      minb = (e && atoi (e) == 3) ? 3 : 2;
+   }
+   if (minb == 3)
+      k_push64<3><<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (c, r->m64, r->np, r->dsc);
+   else
+      k_push64<2><<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (c, r->m64, r->np, r->dsc);
    MG_LAUNCH_CHECK ();
    return MG_OK;
 }
