@@ -181,6 +181,36 @@ long long mg_estimate_bytes (const mg_params_t *params, long long markers);
 int  mg_run_profile (mg_run_t *run, int enable);
 int  mg_run_last_timing (mg_run_t *run, double *push_ms, double *step_ms);
 
+/* ---- placement into caller-owned device memory ---------------------------
+ * No counterpart in the reference.  Device arrays of one marker population
+ * in structure-of-arrays form, each with room for `capacity` markers. */
+typedef struct {
+   double *x, *y, *z, *vx, *vy, *vz;
+   float  *rho, *qDivM;
+   int    *id;
+} mg_device_markers_t;
+
+/* Writes the markers of `spec` (the placement rule of mg_place_t, cell box
+ * measured with steps h) to out[0 .. count), allocating nothing on the
+ * device or the host: for callers that cannot call cudaMalloc -- code that
+ * runs while a stream is being captured into a CUDA graph (where
+ * allocation calls are not allowed), or hosts that have handed all of HBM
+ * to their own memory pool and pass this library slices of it.  The
+ * generator start states go through a file-scope device array of at most
+ * 4096 states (1.59 MB, resident on every GPU that loads the library until
+ * the process exits); `threads` (0 = 4096) sets how many states, i.e.
+ * parallel generator streams, are used and is rejected above 4096.  The
+ * first call on a device looks up that array's device address, so make the
+ * first call before any stream capture.  Calls run on `stream` (a
+ * cudaStream_t, NULL for the legacy stream) of the current device and
+ * return after the kernel has finished; the scratch is shared by every call
+ * in the process (calls are serialised by a lock) and overwritten each
+ * time, so launches that overlap on the GPU from outside this process would
+ * race on it.  Output is bit-identical to mg_run_place_uniform. */
+int  mg_place_uniform_static (const mg_place_t *spec, const double h[3],
+                              const mg_device_markers_t *out, long long capacity,
+                              int threads, void *stream);
+
 const char *mg_last_error (void);
 const char *mg_version (void);
 

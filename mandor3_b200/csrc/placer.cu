@@ -13,6 +13,7 @@
 // squaring and every device thread then generates its own chunk.
 #include <cuda_runtime.h>
 
+#include <mutex>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -24,6 +25,7 @@
 #define RM_CD 7654321LL
 #define RM_CM 16777213LL
 #define RM_C0 362436LL
+#define MG_PLACE_STATIC_STATES 4096
 
 namespace {
 
@@ -240,5 +242,145 @@ int mg_place64 (mg_run_t *r, const mg_place_t *spec, long long at, long long cou
       mg_set_error ("placer launch: %s", cudaGetErrorString (e));
       return MG_ERR_CUDA;
    }
+   return MG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Placement without allocation.
+//
+// mg_place_uniform_static writes the markers of one placement box into
+// device arrays the caller owns, and allocates nothing: the generator start
+// states live in a file-scope device array (MG_PLACE_STATIC_STATES states of
+// 97 words, 1.59 MB, held by every GPU that loads the library until the
+// process exits), and the host-side jump-ahead works in static host buffers.
+// Every call overwrites the states it uses, so nothing needs clearing.
+// Calls are serialised inside the process by a mutex and each call waits for
+// its kernel before returning; work launched concurrently on the same device
+// by two processes, or by another user of this array, would race on it.
+// ---------------------------------------------------------------------------
+static __device__ __align__ (256) uint32_t g_place_states[MG_PLACE_STATIC_STATES*RM_LAG];
+
+namespace {
+
+std::mutex g_place_mutex;
+uint32_t   g_host_states[MG_PLACE_STATIC_STATES*RM_LAG];
+Mat        g_mat[3];
+uint32_t  *g_states_dev[64];          // cudaGetSymbolAddress of g_place_states per device
+
+// Jump-ahead with the static matrices: R = A^e.
+void mat_pow_static (long long e, Mat &R, Mat &base, Mat &tmp)
+{
+   mat_step (base);
+   memset (&R, 0, sizeof (Mat));
+   for (int q = 0 ; q < RM_LAG ; ++q)
+      R[q][q] = 1;
+   while (e > 0) {
+      if (e & 1) {
+         mat_mul (R, base, tmp);
+         memcpy (&R, &tmp, sizeof (Mat));
+      }
+      e >>= 1;
+      if (e) {
+         mat_mul (base, base, tmp);
+         memcpy (&base, &tmp, sizeof (Mat));
+      }
+   }
+}
+
+} // namespace
+
+extern "C" int mg_place_uniform_static (const mg_place_t *spec, const double h[3],
+                                        const mg_device_markers_t *out, long long capacity,
+                                        int threads, void *stream)
+{
+   if (!spec || !h || !out || spec->ppc <= 0) {
+      mg_set_error ("mg_place_uniform_static: null or empty argument");
+      return MG_ERR_ARG;
+   }
+   long long cells = 1;
+   for (int a = 0 ; a < 3 ; ++a) {
+      if (spec->hi[a] < spec->lo[a]) {
+         mg_set_error ("mg_place_uniform_static: empty box on axis %d", a);
+         return MG_ERR_ARG;
+      }
+      cells *= spec->hi[a] - spec->lo[a];
+   }
+   const long long count = cells*spec->ppc;
+   if (count > capacity) {
+      mg_set_error ("mg_place_uniform_static: %lld markers do not fit the %lld-marker arrays",
+                    count, capacity);
+      return MG_ERR_CAPACITY;
+   }
+   if (threads < 0 || threads > MG_PLACE_STATIC_STATES) {
+      mg_set_error ("mg_place_uniform_static: %d generator streams requested; the static scratch "
+                    "holds at most %d", threads, MG_PLACE_STATIC_STATES);
+      return MG_ERR_ARG;
+   }
+   if (count == 0)
+      return MG_OK;
+   if (spec->seed_ij < 0 || spec->seed_ij > 31328 || spec->seed_kl < 0 || spec->seed_kl > 30081) {
+      mg_set_error ("ranmar seeds must satisfy 0 <= ij <= 31328, 0 <= kl <= 30081 (misc_ranmar.c:81-84)");
+      return MG_ERR_ARG;
+   }
+   int dev = 0;
+   if (cudaGetDevice (&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+      mg_set_error ("mg_place_uniform_static: no current CUDA device");
+      return MG_ERR_CUDA;
+   }
+   std::lock_guard<std::mutex> lock (g_place_mutex);
+   // First call on this device: resolve the device address of the static
+   // scratch with the device current.
+   if (!g_states_dev[dev]) {
+      void *ptr = nullptr;
+      cudaError_t e = cudaGetSymbolAddress (&ptr, g_place_states);
+      if (e != cudaSuccess || !ptr) {
+         mg_set_error ("mg_place_uniform_static: cudaGetSymbolAddress: %s", cudaGetErrorString (e));
+         return MG_ERR_CUDA;
+      }
+      g_states_dev[dev] = (uint32_t *) ptr;
+   }
+   int nthreads = threads ? threads : MG_PLACE_STATIC_STATES;
+   if (count < nthreads)
+      nthreads = (int) count;
+   PlaceArgs a;
+   a.s = *spec;
+   for (int q = 0 ; q < 3 ; ++q)
+      a.h[q] = h[q];
+   a.nmarkers = count;
+   a.at = 0;
+   a.per_thread = (count + nthreads - 1)/nthreads;
+   nthreads = (int) ((count + a.per_thread - 1)/a.per_thread);
+
+   uint32_t st[RM_LAG], tmp[RM_LAG];
+   rm_seed (spec->seed_ij, spec->seed_kl, st);
+   if (spec->skip > 0) {
+      mat_pow_static (spec->skip, g_mat[0], g_mat[1], g_mat[2]);
+      mat_vec (g_mat[0], st, tmp);
+      memcpy (st, tmp, sizeof (st));
+   }
+   if (nthreads > 1)
+      mat_pow_static (7*a.per_thread, g_mat[0], g_mat[1], g_mat[2]);
+   for (int t = 0 ; t < nthreads ; ++t) {
+      memcpy (g_host_states + (size_t) t*RM_LAG, st, sizeof (st));
+      if (t + 1 < nthreads) {
+         mat_vec (g_mat[0], st, tmp);
+         memcpy (st, tmp, sizeof (st));
+      }
+   }
+   cudaStream_t s = (cudaStream_t) stream;
+   MG_CUDA (cudaMemcpyAsync (g_states_dev[dev], g_host_states, (size_t) nthreads*RM_LAG*sizeof (uint32_t),
+                             cudaMemcpyHostToDevice, s));
+   Markers64 m;
+   m.x = out->x; m.y = out->y; m.z = out->z;
+   m.ux = out->vx; m.uy = out->vy; m.uz = out->vz;
+   m.rho = out->rho; m.qm = out->qDivM; m.id = out->id;
+   const int T = 128, B = (nthreads + T - 1)/T;
+   const int smem = T*RM_LAG*sizeof (uint32_t);
+   MG_CUDA (cudaFuncSetAttribute (k_place, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+   k_place<<<B, T, smem, s>>> (a, g_states_dev[dev], m);
+   MG_LAUNCH_CHECK ();
+   // The host states buffer and the device scratch are reused by the next
+   // call: wait here.
+   MG_CUDA (cudaStreamSynchronize (s));
    return MG_OK;
 }
