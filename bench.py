@@ -50,6 +50,8 @@ FALLBACK_HBM_GBS = 6650.0
 
 
 def workload(name="laser_foil"):
+    if name == "weibel":
+        return weibel()
     if name != "laser_foil":
         raise SystemExit("unknown workload %r" % name)
     n = (256, 128, 128)
@@ -68,15 +70,42 @@ def workload(name="laser_foil"):
     laser = dict(a0=3.0, waist=3.0, x_focus=foil[0][0] * h[0], duration=10.0, t_start=0.0,
                  phase=0.0, plane=5, margin=5)
     return dict(name="laser_foil_fp64_256x128x128", n=n, h=h, tau=tau, bc=bc, species=species,
-                laser=laser, markers=2 * n_each, total_steps=2000)
+                laser=laser, markers=2 * n_each, total_steps=2000, precision=0, dtype="f64",
+                bytes_per_marker=100.0)
+
+
+def weibel():
+    """Counter-streaming electron beams (two-stream/Weibel), precision form:
+    256^3 periodic cells, h = 0.05 c/omega_p at the total density n_cr,
+    Courant 0.5, beams at u_x = +-0.2 (gamma v = 0.2/sqrt(1 - 0.04)) with
+    32 markers per cell each, thermal spread 0.01, 500 steps."""
+    n = (256, 256, 256)
+    hh = 0.05 / (2 * math.pi)
+    h = (hh, hh, hh)
+    tau = 0.5 / math.sqrt(3 / hh ** 2)
+    ppc = 32
+    each = n[0] * n[1] * n[2] * ppc
+    u = 0.2 / math.sqrt(1 - 0.04)
+    species = [
+        dict(lo=(0, 0, 0), hi=n, ppc=ppc, rho=-0.5 * N_CR / ppc, qDivM=-1.0,
+             drift=(u, 0, 0), uth=(0.01, 0.01, 0.01), seed=(1802, 9373), skip=0, id0=1),
+        dict(lo=(0, 0, 0), hi=n, ppc=ppc, rho=-0.5 * N_CR / ppc, qDivM=-1.0,
+             drift=(-u, 0, 0), uth=(0.01, 0.01, 0.01), seed=(1802, 9373), skip=7 * each,
+             id0=1 + each),
+    ]
+    return dict(name="weibel_fp32_256cubed", n=n, h=h, tau=tau, bc=(0, 0, 0), species=species,
+                laser=None, markers=2 * each, total_steps=500, precision=1, dtype="f32",
+                bytes_per_marker=60.0)
 
 
 def make_run(w, device):
     import mandor3_b200 as mg
-    r = mg.Run(w["n"], w["h"], w["tau"], w["bc"], w["bc"], device=device, capacity=w["markers"])
+    r = mg.Run(w["n"], w["h"], w["tau"], w["bc"], w["bc"], device=device, capacity=w["markers"],
+               precision=w["precision"])
     z = np.zeros(r.field_shape())
     r.set_fields(z, z)
-    r.set_laser(**w["laser"])
+    if w["laser"]:
+        r.set_laser(**w["laser"])
     for s in w["species"]:
         r.place_uniform(**s)
     r.init()
@@ -255,7 +284,7 @@ def run_reference_arm(args, w, world, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1990)
+    ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="laser_foil")
@@ -267,6 +296,8 @@ def main():
         raise SystemExit("at least 3 warm-up steps")
 
     w = workload(args.workload)
+    if args.steps is None:
+        args.steps = w["total_steps"] - args.warmup
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference_arm(args, w, world, rank)
@@ -311,9 +342,9 @@ def main():
         e2e = end_to_end(w, device, args.steps, args.warmup, world)
 
     peak, peak_kind = hbm_peak()
-    algo_bytes = 100.0 * n_avg
+    algo_bytes = w["bytes_per_marker"] * n_avg
     achieved = algo_bytes / (push_ms / 1e3) / 1e9 if push_ms > 0 else None
-    roofline = {"bound": "hbm", "kernel": "k_push64", "achieved": achieved, "peak": peak,
+    roofline = {"bound": "hbm", "kernel": "k_push64" if w["precision"] == 0 else "k_push32", "achieved": achieved, "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s",
                 "frac": achieved / peak if achieved else None,
                 "traffic": ncu_traffic(), "push_ms": push_ms, "step_ms": step_ms,
@@ -332,16 +363,26 @@ def main():
     line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": w["name"], "markers": w["markers"], "grid": list(w["n"]),
-                       "bc": "mur x6", "courant": 0.5, "laser": "a0=3 w0=3 sin^2 10 cycles",
-                       "foil": "30 n_cr, 10 cells, e- and p+ at 16 ppc",
-                       "parallelism": "replicas x%d" % world,
-                       "l2": "inputs larger than L2 (fields 0.34 GB + markers 0.27 GB per step)"},
+            "vs_baseline": None, "dtype": w["dtype"], "data": "synthetic",
+            "config": config_of(w, world),
             "clocks": clocks.summary(), "e2e": e2e,
             "gpu_launches": launches_per_step * args.steps, "roofline": roofline,
             "cpu_baseline": cpu}
     print(json.dumps(line), flush=True)
+
+
+def config_of(w, world):
+    if w["precision"] == 0:
+        return {"workload": w["name"], "markers": w["markers"], "grid": list(w["n"]),
+                "bc": "mur x6", "courant": 0.5, "laser": "a0=3 w0=3 sin^2 10 cycles",
+                "foil": "30 n_cr, 10 cells, e- and p+ at 16 ppc",
+                "parallelism": "replicas x%d" % world,
+                "l2": "inputs larger than L2 (fields 0.34 GB + markers 0.27 GB per step)"}
+    return {"workload": w["name"], "markers": w["markers"], "grid": list(w["n"]), "bc": "periodic",
+            "courant": 0.5, "beams": "u_x = +-0.2c, 32 ppc each, u_th 0.01",
+            "precision": "int cell + FP32 offset, FP32 u/E/H/J, FP64 reductions",
+            "parallelism": "replicas x%d" % world,
+            "l2": "inputs larger than L2 (43 GB of markers per step)"}
 
 
 def end_to_end(w, device, steps, warmup, world):
@@ -362,8 +403,10 @@ def end_to_end(w, device, steps, warmup, world):
     hH[:] = 0
     rows = pin(8 * 6 * steps).view("<f8").reshape(steps, 6)
     out_m = pin(markers.nbytes).view(mg.MARKER_DTYPE)
-    r = mg.Run(w["n"], w["h"], w["tau"], w["bc"], w["bc"], device=device, capacity=len(markers))
-    r.set_laser(**w["laser"])
+    r = mg.Run(w["n"], w["h"], w["tau"], w["bc"], w["bc"], device=device, capacity=len(markers),
+               precision=w["precision"])
+    if w["laser"]:
+        r.set_laser(**w["laser"])
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()

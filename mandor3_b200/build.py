@@ -31,7 +31,9 @@ CUDA_UNITS = {
     "fields64.cu": ["-fmad=false"],
     "push64.cu": ["-fmad=false"],
     "placer.cu": ["-fmad=false"],
-    "fp32.cu": [],
+    "api32.cu": [],
+    "fields32.cu": [],
+    "push32.cu": [],
 }
 HOST_UNITS = ["mgio.c"]
 

@@ -54,7 +54,7 @@ int mg_sm_count (void)
          return rc_;                                                         \
    } while (0)
 
-static void drop_graphs (mg_run_t *r);
+void mg_drop_graphs (mg_run_t *r);
 #define MG_PROFILE_CHUNK 512
 
 // ---------------------------------------------------------------------------
@@ -186,7 +186,7 @@ __global__ void k_end_step (DevScalars *dsc, double *ring, double volume, double
 // ---------------------------------------------------------------------------
 // Allocation.
 // ---------------------------------------------------------------------------
-static int dev_alloc (mg_run_t *r, void **p, size_t bytes)
+int mg_dev_alloc (mg_run_t *r, void **p, size_t bytes)
 {
    cudaError_t e = cudaMalloc (p, bytes ? bytes : 16);
    if (e != cudaSuccess) {
@@ -199,7 +199,7 @@ static int dev_alloc (mg_run_t *r, void **p, size_t bytes)
    return MG_OK;
 }
 
-static int ensure_stage (mg_run_t *r, size_t bytes)
+int mg_ensure_stage (mg_run_t *r, size_t bytes)
 {
    if (r->stage_bytes >= bytes)
       return MG_OK;
@@ -209,7 +209,7 @@ static int ensure_stage (mg_run_t *r, size_t bytes)
       r->stage = nullptr;
       r->stage_bytes = 0;
    }
-   TRY (dev_alloc (r, &r->stage, bytes));
+   TRY (mg_dev_alloc (r, &r->stage, bytes));
    r->stage_bytes = bytes;
    return MG_OK;
 }
@@ -238,10 +238,10 @@ static int ensure_capacity (mg_run_t *r, long long need)
    void **d[] = {(void **) &nm.x, (void **) &nm.y, (void **) &nm.z, (void **) &nm.ux,
                  (void **) &nm.uy, (void **) &nm.uz};
    for (void **p : d)
-      TRY (dev_alloc (r, p, (size_t) cap*8));
-   TRY (dev_alloc (r, (void **) &nm.rho, (size_t) cap*4));
-   TRY (dev_alloc (r, (void **) &nm.qm, (size_t) cap*4));
-   TRY (dev_alloc (r, (void **) &nm.id, (size_t) cap*4));
+      TRY (mg_dev_alloc (r, p, (size_t) cap*8));
+   TRY (mg_dev_alloc (r, (void **) &nm.rho, (size_t) cap*4));
+   TRY (mg_dev_alloc (r, (void **) &nm.qm, (size_t) cap*4));
+   TRY (mg_dev_alloc (r, (void **) &nm.id, (size_t) cap*4));
    if (old.x && old_np > 0) {
       MG_CUDA (cudaMemcpyAsync (nm.x, old.x, old_np*8, cudaMemcpyDeviceToDevice, r->stream));
       MG_CUDA (cudaMemcpyAsync (nm.y, old.y, old_np*8, cudaMemcpyDeviceToDevice, r->stream));
@@ -261,7 +261,7 @@ static int ensure_capacity (mg_run_t *r, long long need)
    r->m64 = nm;
    r->cap = cap;
    // The captured graphs hold the old pointers.
-   drop_graphs (r);
+   mg_drop_graphs (r);
    return MG_OK;
 }
 
@@ -323,9 +323,6 @@ extern "C" int mg_run_create (const mg_params_t *params, mg_run_t **out)
    }
    *out = nullptr;
    TRY (check_params (params));
-   if (params->precision == MG_FP32_OFFSET) {
-      return mg_run_create32 (params, out);
-   }
    int ndev = 0;
    if (cudaGetDeviceCount (&ndev) != cudaSuccess || ndev == 0) {
       cudaGetLastError ();
@@ -348,28 +345,30 @@ extern "C" int mg_run_create (const mg_params_t *params, mg_run_t **out)
       return MG_ERR_CUDA;
    }
    int rc = MG_OK;
-   const size_t fb = (size_t) r->g.total*sizeof (double);
+   const bool f32 = (params->precision == MG_FP32_OFFSET);
+   const size_t elt = f32 ? sizeof (float) : sizeof (double);
+   const size_t fb = (size_t) r->g.total*elt;
    for (int c = 0 ; c < 3 && rc == MG_OK ; ++c) {
-      rc = dev_alloc (r, (void **) &r->E[c], fb);
-      if (rc == MG_OK) rc = dev_alloc (r, (void **) &r->H[c], fb);
-      if (rc == MG_OK) rc = dev_alloc (r, (void **) &r->J[c], fb);
-      if (rc == MG_OK) rc = dev_alloc (r, (void **) &r->Hn[c], fb);
-      if (rc == MG_OK) {
-         cudaMemsetAsync (r->Hn[c], 0, fb, r->stream);
-         cudaMemsetAsync (r->E[c], 0, fb, r->stream);
-         cudaMemsetAsync (r->H[c], 0, fb, r->stream);
-         cudaMemsetAsync (r->J[c], 0, fb, r->stream);
+      void **arrs[4] = {f32 ? (void **) &r->E32[c] : (void **) &r->E[c],
+                        f32 ? (void **) &r->H32[c] : (void **) &r->H[c],
+                        f32 ? (void **) &r->J32[c] : (void **) &r->J[c],
+                        f32 ? (void **) &r->Hn32[c] : (void **) &r->Hn[c]};
+      for (int q = 0 ; q < 4 && rc == MG_OK ; ++q) {
+         rc = mg_dev_alloc (r, arrs[q], fb);
+         if (rc == MG_OK)
+            cudaMemsetAsync (*arrs[q], 0, fb, r->stream);
       }
    }
    for (int t = 0 ; t < 2 && rc == MG_OK ; ++t)
       for (int a = 0 ; a < 3 && rc == MG_OK ; ++a) {
-         const size_t mb = 4*sizeof (double)*(size_t) (params->n[(a + 1) % 3] + 2)*(params->n[(a + 2) % 3] + 2);
-         rc = dev_alloc (r, (void **) &r->mur[t][a], mb);
+         const size_t mb = 4*elt*(size_t) (params->n[(a + 1) % 3] + 2)*(params->n[(a + 2) % 3] + 2);
+         void **mp = f32 ? (void **) &r->mur32[t][a] : (void **) &r->mur[t][a];
+         rc = mg_dev_alloc (r, mp, mb);
          if (rc == MG_OK)
-            cudaMemsetAsync (r->mur[t][a], 0, mb, r->stream);
+            cudaMemsetAsync (*mp, 0, mb, r->stream);
       }
-   if (rc == MG_OK) rc = dev_alloc (r, (void **) &r->dsc, sizeof (DevScalars));
-   if (rc == MG_OK) rc = dev_alloc (r, (void **) &r->ring, sizeof (double)*6*MG_RING);
+   if (rc == MG_OK) rc = mg_dev_alloc (r, (void **) &r->dsc, sizeof (DevScalars));
+   if (rc == MG_OK) rc = mg_dev_alloc (r, (void **) &r->ring, sizeof (double)*6*MG_RING);
    if (rc == MG_OK) {
       DevScalars s;
       memset (&s, 0, sizeof (s));
@@ -377,7 +376,7 @@ extern "C" int mg_run_create (const mg_params_t *params, mg_run_t **out)
       cudaMemcpyAsync (r->dsc, &s, sizeof (s), cudaMemcpyHostToDevice, r->stream);
    }
    if (rc == MG_OK && params->capacity > 0)
-      rc = ensure_capacity (r, params->capacity);
+      rc = f32 ? mg_ensure_capacity32 (r, params->capacity) : ensure_capacity (r, params->capacity);
    for (int e = 0 ; e < 4 && rc == MG_OK ; ++e)
       if (cudaEventCreate (&r->ev[e]) != cudaSuccess)
          rc = MG_ERR_CUDA;
@@ -401,13 +400,10 @@ extern "C" int mg_run_destroy (mg_run_t *r)
 {
    if (!r)
       return MG_OK;
-   if (r->prm.precision == MG_FP32_OFFSET) {
-      return mg_run_destroy32 (r);
-   }
    cudaSetDevice (r->device);
    if (r->stream)
       cudaStreamSynchronize (r->stream);
-   drop_graphs (r);
+   mg_drop_graphs (r);
    if (r->pev) {
       for (int q = 0 ; q < 2*MG_PROFILE_CHUNK ; ++q)
          if (r->pev[q]) cudaEventDestroy (r->pev[q]);
@@ -418,11 +414,19 @@ extern "C" int mg_run_destroy (mg_run_t *r)
       if (r->H[c]) cudaFree (r->H[c]);
       if (r->J[c]) cudaFree (r->J[c]);
       if (r->Hn[c]) cudaFree (r->Hn[c]);
+      if (r->E32[c]) cudaFree (r->E32[c]);
+      if (r->H32[c]) cudaFree (r->H32[c]);
+      if (r->J32[c]) cudaFree (r->J32[c]);
+      if (r->Hn32[c]) cudaFree (r->Hn32[c]);
    }
    for (int t = 0 ; t < 2 ; ++t)
       for (int a = 0 ; a < 3 ; ++a)
          if (r->mur[t][a]) cudaFree (r->mur[t][a]);
+   for (int t = 0 ; t < 2 ; ++t)
+      for (int a = 0 ; a < 3 ; ++a)
+         if (r->mur32[t][a]) cudaFree (r->mur32[t][a]);
    free_markers (r);
+   mg_free_markers32 (r);
    if (r->dsc) cudaFree (r->dsc);
    if (r->ring) cudaFree (r->ring);
    if (r->stage) cudaFree (r->stage);
@@ -445,7 +449,7 @@ extern "C" int mg_run_set_fields (mg_run_t *r, const double *E, const double *H)
    }
    const long vol = (long) (r->g.n[0] + 1)*(r->g.n[1] + 1)*(r->g.n[2] + 1);
    const size_t bytes = (size_t) vol*3*sizeof (double);
-   TRY (ensure_stage (r, bytes));
+   TRY (mg_ensure_stage (r, bytes));
    const double *src[2] = {E, H};
    double **dst[2] = {r->E, r->H};
    for (int f = 0 ; f < 2 ; ++f) {
@@ -469,7 +473,7 @@ extern "C" int mg_run_get_fields (mg_run_t *r, double *E, double *H)
    }
    const long vol = (long) (r->g.n[0] + 1)*(r->g.n[1] + 1)*(r->g.n[2] + 1);
    const size_t bytes = (size_t) vol*3*sizeof (double);
-   TRY (ensure_stage (r, bytes));
+   TRY (mg_ensure_stage (r, bytes));
    double *dst[2] = {E, H};
    // Between mg_em_HHalfStep and mg_em_HStep the reference's H is H^n.
    double **src[2] = {r->E, (r->stage_no >= 1 && r->stage_no <= 3) ? r->Hn : r->H};
@@ -493,7 +497,7 @@ extern "C" int mg_run_get_current (mg_run_t *r, double *J)
    }
    const long vol = (long) (r->g.n[0] + 5)*(r->g.n[1] + 5)*(r->g.n[2] + 5);
    const size_t bytes = (size_t) vol*3*sizeof (double);
-   TRY (ensure_stage (r, bytes));
+   TRY (mg_ensure_stage (r, bytes));
    k_fields_out<<<mg_blocks_for (vol, 256, 8), 256, 0, r->stream>>> (r->g, (double *) r->stage,
                                                                      r->J[0], r->J[1], r->J[2], 2);
    MG_LAUNCH_CHECK ();
@@ -516,7 +520,7 @@ extern "C" int mg_run_set_markers (mg_run_t *r, const mg_marker_t *m, long long 
    }
    TRY (ensure_capacity (r, n));
    const long long chunk = n < CHUNK ? n : CHUNK;
-   TRY (ensure_stage (r, (size_t) (chunk > 0 ? chunk : 1)*sizeof (mg_marker_t)));
+   TRY (mg_ensure_stage (r, (size_t) (chunk > 0 ? chunk : 1)*sizeof (mg_marker_t)));
    for (long long at = 0 ; at < n ; at += CHUNK) {
       const long long c = (n - at < CHUNK) ? n - at : CHUNK;
       MG_CUDA (cudaMemcpyAsync (r->stage, m + at, c*sizeof (mg_marker_t), cudaMemcpyHostToDevice, r->stream));
@@ -561,7 +565,7 @@ extern "C" int mg_run_get_markers (mg_run_t *r, mg_marker_t *out, long long cap,
    }
    const long long chunk = r->np < CHUNK ? r->np : CHUNK;
    const size_t need = (size_t) (chunk > 0 ? chunk : 1)*(sizeof (mg_marker_t) + sizeof (long long)) + 64;
-   TRY (ensure_stage (r, need));
+   TRY (mg_ensure_stage (r, need));
    mg_marker_t *dst = (mg_marker_t *) r->stage;
    long long *slot = (long long *) ((char *) r->stage + (size_t) (chunk > 0 ? chunk : 1)*sizeof (mg_marker_t));
    long long *total_d = slot + (chunk > 0 ? chunk : 1);
@@ -605,7 +609,7 @@ extern "C" int mg_run_set_laser (mg_run_t *r, const mg_laser_t *l)
       r->laser = *l;
       r->has_laser = 1;
    }
-   drop_graphs (r);
+   mg_drop_graphs (r);
    return MG_OK;
 }
 
@@ -773,12 +777,12 @@ extern "C" int mg_plasma_rho (mg_run_t *r, double *rho)
    }
    const size_t fb = (size_t) r->g.total*sizeof (double);
    double *d = nullptr;
-   TRY (dev_alloc (r, (void **) &d, fb));
+   TRY (mg_dev_alloc (r, (void **) &d, fb));
    cudaMemsetAsync (d, 0, fb, r->stream);
    int rc = mg_rho64 (r, d);
    if (rc == MG_OK) {
       const long vol = (long) (r->g.n[0] + 5)*(r->g.n[1] + 5)*(r->g.n[2] + 5);
-      rc = ensure_stage (r, vol*3*sizeof (double));
+      rc = mg_ensure_stage (r, vol*3*sizeof (double));
       if (rc == MG_OK) {
          k_fields_out<<<mg_blocks_for (vol, 256, 8), 256, 0, r->stream>>> (r->g, (double *) r->stage, d, d, d, 2);
          // Take one component of the triplets on the host.
@@ -819,6 +823,13 @@ int mg_enqueue_step64 (mg_run_t *r, int part)
 
 int mg_enqueue_step32 (mg_run_t *r, int part);
 
+int mg_end_step (mg_run_t *r)
+{
+   k_end_step<<<1, 1, 0, r->stream>>> (r->dsc, r->ring, r->g.h[0]*r->g.h[1]*r->g.h[2], r->g.tau);
+   MG_LAUNCH_CHECK ();
+   return MG_OK;
+}
+
 static int count_kernels (cudaGraph_t graph)
 {
    size_t n = 0;
@@ -836,7 +847,7 @@ static int count_kernels (cudaGraph_t graph)
    return k;
 }
 
-static void drop_graphs (mg_run_t *r)
+void mg_drop_graphs (mg_run_t *r)
 {
    for (int q = 0 ; q < 4 ; ++q) {
       if (r->gexec[q]) cudaGraphExecDestroy (r->gexec[q]);
@@ -853,7 +864,7 @@ static int build_graph (mg_run_t *r)
 {
    if (r->graph_ok)
       return MG_OK;
-   drop_graphs (r);
+   mg_drop_graphs (r);
    for (int q = 0 ; q < 4 ; ++q) {
       MG_CUDA (cudaStreamBeginCapture (r->stream, cudaStreamCaptureModeThreadLocal));
       const int part = q - 1;
@@ -874,6 +885,19 @@ static int build_graph (mg_run_t *r)
    r->kernels_per_step = count_kernels (r->gr[0]);
    r->graph_ok = 1;
    return MG_OK;
+}
+
+// Precision form: markers are re-sorted by cell every sort_every steps
+// (default 8) so that warps keep sharing cells; the sort runs between graph
+// launches on the run's stream.
+static int maybe_sort (mg_run_t *r)
+{
+   if (!is32 (r))
+      return MG_OK;
+   const int every = r->prm.sort_every > 0 ? r->prm.sort_every : 8;
+   if (r->steps_since_sort++ < every)
+      return MG_OK;
+   return mg_sort32 (r);
 }
 
 static int run_steps (mg_run_t *r, int nsteps, double *host_rows, double *dev_rows, bool sync)
@@ -900,6 +924,7 @@ static int run_steps (mg_run_t *r, int nsteps, double *host_rows, double *dev_ro
       if (r->profile) {
          MG_CUDA (cudaEventRecord (r->ev[0], r->stream));
          for (int s = 0 ; s < chunk ; ++s) {
+            TRY (maybe_sort (r));
             MG_CUDA (cudaGraphLaunch (r->gexec[1], r->stream));
             MG_CUDA (cudaEventRecord (r->pev[2*s], r->stream));
             MG_CUDA (cudaGraphLaunch (r->gexec[2], r->stream));
@@ -908,8 +933,10 @@ static int run_steps (mg_run_t *r, int nsteps, double *host_rows, double *dev_ro
          }
          MG_CUDA (cudaEventRecord (r->ev[1], r->stream));
       } else {
-         for (int s = 0 ; s < chunk ; ++s)
+         for (int s = 0 ; s < chunk ; ++s) {
+            TRY (maybe_sort (r));
             MG_CUDA (cudaGraphLaunch (r->gexec[0], r->stream));
+         }
       }
       if (host_rows)
          MG_CUDA (cudaMemcpyAsync (host_rows + 6*(size_t) done, r->ring, sizeof (double)*6*chunk,

@@ -1,937 +1,28 @@
-// FP64 Yee solver, field boundary conditions, current folding and energy
-// reductions of the B200 PIC core.
-//
-// Reference semantics (paths relative to the reference project):
-//   H half step   core/em.c:55-77, caps core/em_caps.c:406-729
-//   E step        core/em.c:135-163, E -= tau*J core/em.c:167-184
-//   periodic BC   core/emCap_periodic.c:15-67
-//   mirror BC     core/emCap_mirror.c:17-70
-//   Mur BC        core/emCap_Mur.c:56-166
-//   J folding     core/plasma_currentWalls.c:27-121
-//   field energy  core/em.c:227-252
-//
-// The reference splits every update into an inner box and six boundary
-// "caps" so that MPI exchange overlaps compute.  With the whole domain on
-// one GPU the union of those regions is one box per field (per axis:
-// H over [0,n] or [1,n] at a mirror wall; E over [0 or 1, n-1 or n]), so
-// each update is a single launch over that box followed by thin wall
-// kernels.  The caps advance H by one tau instead of two tau/2 halves, so
-// near-wall values agree with the reference to round-off.
-//
-// Arithmetic is compiled with --fmad=false so that every expression rounds
-// exactly as the reference's C does.
-#include <cuda_runtime.h>
+// FP64 instantiation of the field kernels (fields_tmpl.cuh): the
+// reference's arithmetic, compiled with --fmad=false.
+#include "fields_tmpl.cuh"
 
-#include <limits.h>
-
-#include "mg_internal.cuh"
-
-#define TRY_MG(x)                                                            \
-   do {                                                                      \
-      int rc_ = (x);                                                         \
-      if (rc_ != MG_OK)                                                      \
-         return rc_;                                                         \
-   } while (0)
-
-namespace {
-
-struct F3 {
-   double *c[3];
-};
-
-__device__ __forceinline__ void box_index (long t, const int lo[3], const int ext[3],
-                                           int &i, int &j, int &k)
+static FS<double> fs_of (mg_run_t *r)
 {
-   k = lo[2] + (int) (t % ext[2]);
-   t /= ext[2];
-   j = lo[1] + (int) (t % ext[1]);
-   i = lo[0] + (int) (t / ext[1]);
-}
-
-struct Box {
-   int lo[3], ext[3];
-   long vol;
-};
-
-static Box make_box (const int lo[3], const int hi[3])
-{
-   Box b;
-   b.vol = 1;
-   for (int a = 0 ; a < 3 ; ++a) {
-      b.lo[a] = lo[a];
-      b.ext[a] = hi[a] - lo[a] + 1;
-      if (b.ext[a] < 0) b.ext[a] = 0;
-      b.vol *= b.ext[a];
+   FS<double> fs;
+   for (int c = 0 ; c < 3 ; ++c) {
+      fs.E[c] = r->E[c];
+      fs.H[c] = r->H[c];
+      fs.Hn[c] = r->Hn[c];
+      fs.J[c] = r->J[c];
+      fs.mur[0][c] = r->mur[0][c];
+      fs.mur[1][c] = r->mur[1][c];
    }
-   return b;
+   return fs;
 }
 
-// Both H half steps in one pass (core/em.c:55-77, called twice per step
-// with the same E^n): Hn = H + c curl E is H at t = n tau (gathered by the
-// push, summed by the energy), H = Hn + c curl E is H at t = (n+1/2) tau.
-// Each result rounds exactly as the reference's two successive updates do.
-// The field energy of core/em.c:227-252 is summed on the way: E^n at the
-// staggered picks and Hn at its picks, where a node whose value the walls
-// will replace is represented by the node the walls copy it from.
-struct EnergyPick {
-   int lo[3][3], hi[3][3];    // [component][axis] index ranges of E picks
-   int hlo[3][3], hhi[3][3];  // same for H picks (after the periodic remap)
-};
-
-__global__ void __launch_bounds__ (256)
-k_h_fused (Grid g, F3 E, F3 H, F3 Hn, Box b, double c1, double c2, double c3,
-           EnergyPick ep, DevScalars *dsc)
-{
-   __shared__ double sw[2][8];
-   const double *Ex = E.c[0], *Ey = E.c[1], *Ez = E.c[2];
-   const long sx = g.sx, sy = g.sy;
-   double we = 0, wb = 0;
-   for (long t = blockIdx.x*(long) blockDim.x + threadIdx.x ; t < b.vol ; t += (long) gridDim.x*blockDim.x) {
-      int i, j, k;
-      box_index (t, b.lo, b.ext, i, j, k);
-      const long o = g.at (i, j, k);
-      const double ex = Ex[o], ey = Ey[o], ez = Ez[o];
-      const double cx = c3*(ey - Ey[o - 1]) - c2*(ez - Ez[o - sy]);
-      const double cy = c1*(ez - Ez[o - sx]) - c3*(ex - Ex[o - 1]);
-      const double cz = c2*(ex - Ex[o - sy]) - c1*(ey - Ey[o - sx]);
-      const double hx = H.c[0][o] + cx, hy = H.c[1][o] + cy, hz = H.c[2][o] + cz;
-      Hn.c[0][o] = hx;
-      Hn.c[1][o] = hy;
-      Hn.c[2][o] = hz;
-      H.c[0][o] = hx + cx;
-      H.c[1][o] = hy + cy;
-      H.c[2][o] = hz + cz;
-      const int I[3] = {i, j, k};
-      const double ev[3] = {ex, ey, ez}, hv[3] = {hx, hy, hz};
-#pragma unroll
-      for (int c = 0 ; c < 3 ; ++c) {
-         bool in_e = true, in_h = true;
-#pragma unroll
-         for (int a = 0 ; a < 3 ; ++a) {
-            in_e &= (I[a] >= ep.lo[c][a]) & (I[a] <= ep.hi[c][a]);
-            in_h &= (I[a] >= ep.hlo[c][a]) & (I[a] <= ep.hhi[c][a]);
-         }
-         if (in_e) we += ev[c]*ev[c];
-         if (in_h) wb += hv[c]*hv[c];
-      }
-   }
-   for (int d = 16 ; d > 0 ; d >>= 1) {
-      we += __shfl_xor_sync (0xffffffffu, we, d);
-      wb += __shfl_xor_sync (0xffffffffu, wb, d);
-   }
-   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-   if (lane == 0) {
-      sw[0][wid] = we;
-      sw[1][wid] = wb;
-   }
-   __syncthreads ();
-   if (wid == 0) {
-      we = lane < (int) (blockDim.x >> 5) ? sw[0][lane] : 0;
-      wb = lane < (int) (blockDim.x >> 5) ? sw[1][lane] : 0;
-      for (int d = 16 ; d > 0 ; d >>= 1) {
-         we += __shfl_xor_sync (0xffffffffu, we, d);
-         wb += __shfl_xor_sync (0xffffffffu, wb, d);
-      }
-      if (lane == 0) {
-         atomicAdd (&dsc->acc[0], we);
-         atomicAdd (&dsc->acc[1], wb);
-      }
-   }
-}
-
-// E -= tau*(curl H) over the E box (core/em.c:155-162 expression order).
-__global__ void k_e_advance (Grid g, F3 E, F3 H, Box b, double c1, double c2, double c3)
-{
-   double *Ex = E.c[0], *Ey = E.c[1], *Ez = E.c[2];
-   const double *Hx = H.c[0], *Hy = H.c[1], *Hz = H.c[2];
-   const long sx = g.sx, sy = g.sy;
-   for (long t = blockIdx.x*(long) blockDim.x + threadIdx.x ; t < b.vol ; t += (long) gridDim.x*blockDim.x) {
-      int i, j, k;
-      box_index (t, b.lo, b.ext, i, j, k);
-      const long o = g.at (i, j, k);
-      const double hx = Hx[o], hy = Hy[o], hz = Hz[o];
-      Ex[o] -= c3*(Hy[o + 1] - hy) - c2*(Hz[o + sy] - hz);
-      Ey[o] -= c1*(Hz[o + sx] - hz) - c3*(Hx[o + 1] - hx);
-      Ez[o] -= c2*(Hx[o + sy] - hx) - c1*(Hy[o + sx] - hy);
-   }
-}
-
-// E step with the current term (core/em.c:155-162 then 167-184) for nodes
-// that no wall operation or source touches between the two: rim nodes
-// (indices -1, 0, 1, n-1, n, n+1 on any axis, and the laser E plane) get
-// only the curl here and their -tau J after the walls (k_e_rim).
-struct Rim {
-   int lo[3], hi[3];       // a node is inner on axis a if lo[a] <= idx <= hi[a]
-   int laser_i;            // x index of the laser E plane, or INT_MIN
-   int laser_lo[2], laser_hi[2];   // its j and k ranges
-};
-
-__device__ __forceinline__ bool rim_node (const Rim &rm, int i, int j, int k)
-{
-   return i < rm.lo[0] || i > rm.hi[0] || j < rm.lo[1] || j > rm.hi[1] ||
-          k < rm.lo[2] || k > rm.hi[2] ||
-          (i == rm.laser_i && j >= rm.laser_lo[0] && j <= rm.laser_hi[0] &&
-           k >= rm.laser_lo[1] && k <= rm.laser_hi[1]);
-}
-
-__global__ void __launch_bounds__ (256)
-k_e_fused (Grid g, F3 E, F3 H, F3 J, Box b, double c1, double c2, double c3, Rim rm)
-{
-   double *Ex = E.c[0], *Ey = E.c[1], *Ez = E.c[2];
-   const double *Hx = H.c[0], *Hy = H.c[1], *Hz = H.c[2];
-   const long sx = g.sx, sy = g.sy;
-   const double tau = g.tau;
-   for (long t = blockIdx.x*(long) blockDim.x + threadIdx.x ; t < b.vol ; t += (long) gridDim.x*blockDim.x) {
-      int i, j, k;
-      box_index (t, b.lo, b.ext, i, j, k);
-      const long o = g.at (i, j, k);
-      const double hx = Hx[o], hy = Hy[o], hz = Hz[o];
-      double ex = Ex[o] - (c3*(Hy[o + 1] - hy) - c2*(Hz[o + sy] - hz));
-      double ey = Ey[o] - (c1*(Hz[o + sx] - hz) - c3*(Hx[o + 1] - hx));
-      double ez = Ez[o] - (c2*(Hx[o + sy] - hx) - c1*(Hy[o + sx] - hy));
-      if (!rim_node (rm, i, j, k)) {
-         ex -= tau*J.c[0][o];
-         ey -= tau*J.c[1][o];
-         ez -= tau*J.c[2][o];
-      }
-      Ex[o] = ex;
-      Ey[o] = ey;
-      Ez[o] = ez;
-   }
-}
-
-
-// Wall kernels run over the two transverse axes, nodes [0, n+1] each (the
-// flush extent of the reference's caps, core/em_caps.c:140-146).
-struct Wall {
-   int ea, ep, eq;
-   int np_, nq_;           // extents n[ep]+2, n[eq]+2
-   long s_a, s_p, s_q;     // strides along the three axes
-};
-
-static Wall make_wall (const Grid &g, int ea)
-{
-   Wall w;
-   w.ea = ea;
-   w.ep = (ea + 1) % 3;
-   w.eq = (ea + 2) % 3;
-   w.np_ = g.n[w.ep] + 2;
-   w.nq_ = g.n[w.eq] + 2;
-   const long s[3] = {g.sx, g.sy, 1};
-   w.s_a = s[ea];
-   w.s_p = s[w.ep];
-   w.s_q = s[w.eq];
-   return w;
-}
-
-__device__ __forceinline__ bool wall_node (const Grid &g, const Wall &w, int a,
-                                           long &o, int &p, int &q)
-{
-   const long t = blockIdx.x*(long) blockDim.x + threadIdx.x;
-   if (t >= (long) w.np_*w.nq_)
-      return false;
-   p = (int) (t / w.nq_);
-   q = (int) (t % w.nq_);
-   o = g.origin + a*w.s_a + p*w.s_p + q*w.s_q;
-   return true;
-}
-
-enum { OP_PERIODIC = 0, OP_MIRROR_MIN, OP_MIRROR_MAX, OP_OPEN_MIN, OP_OPEN_MAX };
-
-// H wall operations (core/emCap_periodic.c:15-37, emCap_mirror.c:17-40,
-// emCap_Mur.c:56-80).
-__global__ void k_h_wall (Grid g, F3 H, Wall w, int op)
-{
-   long o;
-   int p, q;
-   const int N = g.n[w.ea];
-   if (!wall_node (g, w, 0, o, p, q))
-      return;
-   double *Ha = H.c[w.ea], *Hp = H.c[w.ep], *Hq = H.c[w.eq];
-   switch (op) {
-   case OP_PERIODIC:
-      for (int c = 0 ; c < 3 ; ++c) {
-         H.c[c][o] = H.c[c][o + N*w.s_a];
-         H.c[c][o + (N + 1)*w.s_a] = H.c[c][o + w.s_a];
-      }
-      break;
-   case OP_MIRROR_MIN:
-      Ha[o] = 0;
-      Hp[o] = Hp[o + w.s_a];
-      Hq[o] = Hq[o + w.s_a];
-      break;
-   case OP_MIRROR_MAX:
-      o += N*w.s_a;
-      Ha[o] = 0;
-      Hp[o + w.s_a] = Hp[o];
-      Hq[o + w.s_a] = Hq[o];
-      break;
-   case OP_OPEN_MIN:
-      Hp[o] = Hp[o + w.s_a];
-      Hq[o] = Hq[o + w.s_a];
-      break;
-   case OP_OPEN_MAX:
-      o += N*w.s_a;
-      Hp[o + w.s_a] = Hp[o];
-      Hq[o + w.s_a] = Hq[o];
-      break;
-   }
-}
-
-// E wall operations (core/emCap_periodic.c:42-67, emCap_mirror.c:45-70,
-// emCap_Mur.c:117-166).  The Mur history holds, per wall node, the wall and
-// first inner tangential values of the previous step before E -= tau*J.
-__global__ void k_e_wall (Grid g, F3 E, Wall w, int op, double *mur, double alpha)
-{
-   long o;
-   int p, q;
-   const int N = g.n[w.ea];
-   if (!wall_node (g, w, 0, o, p, q))
-      return;
-   double *Ea = E.c[w.ea], *Ep = E.c[w.ep], *Eq = E.c[w.eq];
-   switch (op) {
-   case OP_PERIODIC:
-      for (int c = 0 ; c < 3 ; ++c) {
-         E.c[c][o + N*w.s_a] = E.c[c][o];
-         E.c[c][o + (N + 1)*w.s_a] = E.c[c][o + w.s_a];
-      }
-      break;
-   case OP_MIRROR_MIN:
-      Ep[o] = 0;
-      Eq[o] = 0;
-      Ea[o] = Ea[o + w.s_a];
-      break;
-   case OP_MIRROR_MAX:
-      o += N*w.s_a;
-      Ep[o] = 0;
-      Eq[o] = 0;
-      Ea[o + w.s_a] = Ea[o];
-      break;
-   case OP_OPEN_MIN:
-   case OP_OPEN_MAX: {
-      const bool top = (op == OP_OPEN_MAX);
-      if (top)
-         o += N*w.s_a;
-      const long in = top ? o - w.s_a : o + w.s_a;
-      double *h = mur + 4*((long) p*w.nq_ + q);
-      if (top)
-         Ea[o + w.s_a] = Ea[o];
-      else
-         Ea[o] = Ea[o + w.s_a];
-      const double ep = h[2] + alpha*(Ep[in] - h[0]);
-      const double eq = h[3] + alpha*(Eq[in] - h[1]);
-      Ep[o] = ep;
-      Eq[o] = eq;
-      h[0] = ep;
-      h[1] = eq;
-      h[2] = Ep[in];
-      h[3] = Eq[in];
-      break;
-   }
-   }
-}
-
-// Mur history from the loaded E and normal-E ghost copy (emCap_Mur.c:86-112).
-__global__ void k_mur_init (Grid g, F3 E, Wall w, int top, double *mur)
-{
-   long o;
-   int p, q;
-   const int N = g.n[w.ea];
-   if (!wall_node (g, w, 0, o, p, q))
-      return;
-   if (top)
-      o += N*w.s_a;
-   const long in = top ? o - w.s_a : o + w.s_a;
-   double *h = mur + 4*((long) p*w.nq_ + q);
-   h[0] = E.c[w.ep][o];
-   h[1] = E.c[w.eq][o];
-   h[2] = E.c[w.ep][in];
-   h[3] = E.c[w.eq][in];
-   if (top)
-      E.c[w.ea][o + w.s_a] = E.c[w.ea][o];
-   else
-      E.c[w.ea][o] = E.c[w.ea][o + w.s_a];
-}
-
-// All wall operations of one axis in one launch: the lower wall, then the
-// upper wall (they touch disjoint nodes for n >= 3).  H walls act on both
-// H arrays (H at n and at n+1/2).
-__global__ void k_h_walls (Grid g, F3 H, F3 Hn, Wall w, int op_min, int op_max, int both)
-{
-   long o;
-   int p, q;
-   if (!wall_node (g, w, 0, o, p, q))
-      return;
-   const int N = g.n[w.ea];
-   const long s = w.s_a;
-   for (int arr = 0 ; arr < (both ? 2 : 1) ; ++arr) {
-      F3 &F = arr ? Hn : H;
-      double *Ha = F.c[w.ea], *Hp = F.c[w.ep], *Hq = F.c[w.eq];
-      // Loads first, then stores: the wall nodes never alias the sources.
-      if (op_min == OP_PERIODIC) {
-         double top[3], one[3];
-#pragma unroll
-         for (int c = 0 ; c < 3 ; ++c) {
-            top[c] = F.c[c][o + N*s];
-            one[c] = F.c[c][o + s];
-         }
-#pragma unroll
-         for (int c = 0 ; c < 3 ; ++c) {
-            F.c[c][o] = top[c];
-            F.c[c][o + (N + 1)*s] = one[c];
-         }
-         continue;
-      }
-      const double p1 = Hp[o + s], q1 = Hq[o + s];
-      const long t = o + N*s;
-      const double pN = Hp[t], qN = Hq[t];
-      Hp[o] = p1;
-      Hq[o] = q1;
-      if (op_min == OP_MIRROR_MIN)
-         Ha[o] = 0;
-      Hp[t + s] = pN;
-      Hq[t + s] = qN;
-      if (op_max == OP_MIRROR_MAX)
-         Ha[t] = 0;
-   }
-}
-
-__device__ __forceinline__ void e_wall_op (const Grid &g, F3 &E, const Wall &w, int op,
-                                           long o, int p, int q, double *mur, double alpha)
-{
-   const int N = g.n[w.ea];
-   double *Ea = E.c[w.ea], *Ep = E.c[w.ep], *Eq = E.c[w.eq];
-   switch (op) {
-   case OP_PERIODIC:
-      for (int c = 0 ; c < 3 ; ++c) {
-         E.c[c][o + N*w.s_a] = E.c[c][o];
-         E.c[c][o + (N + 1)*w.s_a] = E.c[c][o + w.s_a];
-      }
-      break;
-   case OP_MIRROR_MIN:
-      Ep[o] = 0;
-      Eq[o] = 0;
-      Ea[o] = Ea[o + w.s_a];
-      break;
-   case OP_MIRROR_MAX:
-      o += N*w.s_a;
-      Ep[o] = 0;
-      Eq[o] = 0;
-      Ea[o + w.s_a] = Ea[o];
-      break;
-   case OP_OPEN_MIN:
-   case OP_OPEN_MAX: {
-      const bool top = (op == OP_OPEN_MAX);
-      if (top)
-         o += N*w.s_a;
-      const long in = top ? o - w.s_a : o + w.s_a;
-      double *h = mur + 4*((long) p*w.nq_ + q);
-      if (top)
-         Ea[o + w.s_a] = Ea[o];
-      else
-         Ea[o] = Ea[o + w.s_a];
-      const double ep = h[2] + alpha*(Ep[in] - h[0]);
-      const double eq = h[3] + alpha*(Eq[in] - h[1]);
-      Ep[o] = ep;
-      Eq[o] = eq;
-      h[0] = ep;
-      h[1] = eq;
-      h[2] = Ep[in];
-      h[3] = Eq[in];
-      break;
-   }
-   default:
-      break;
-   }
-}
-
-// E walls of one axis, then -tau J on the rim nodes of the wall lines this
-// thread owns.  Rim nodes are those of [-1, n+1]^3 outside [2, n-2]^3; the
-// z walls own every node with a rim z index, the y walls those with a rim y
-// index and an inner z index, the x walls the rest.  After its own axis no
-// later wall reads or writes such a node, so its -tau J comes after every
-// wall operation on it, as in core/em.c:189-222.  Threads cover transverse
-// indices [-1, n+1]; the wall operations act on [0, n+1].
-__global__ void k_e_walls (Grid g, F3 E, F3 J, Wall w, int op_min, int op_max, double *mur_min,
-                           double *mur_max, double alpha, int sub_j)
-{
-   const long t = blockIdx.x*(long) blockDim.x + threadIdx.x;
-   const int np1 = w.np_ + 1, nq1 = w.nq_ + 1;          // [-1, n+1]
-   if (t >= (long) np1*nq1)
-      return;
-   const int p = (int) (t / nq1) - 1, q = (int) (t % nq1) - 1;
-   const long o = g.origin + p*w.s_p + q*w.s_q;
-   if (p >= 0 && q >= 0) {
-      e_wall_op (g, E, w, op_min, o, p, q, mur_min, alpha);
-      e_wall_op (g, E, w, op_max, o, p, q, mur_max, alpha);
-   }
-   if (!sub_j)
-      return;
-   const int N = g.n[w.ea];
-   const int Np = g.n[w.ep], Nq = g.n[w.eq];
-   const bool p_rim = p < 2 || p > Np - 2, q_rim = q < 2 || q > Nq - 2;
-   bool own;
-   if (w.ea == 2)
-      own = true;
-   else if (w.ea == 1)
-      own = !p_rim;                 // ep = z
-   else
-      own = !p_rim && !q_rim;       // ep = y, eq = z
-   if (!own)
-      return;
-   const double tau = g.tau;
-   const int vs[6] = {-1, 0, 1, N - 1, N, N + 1};
-   double e[6][3], jv[6][3];
-#pragma unroll
-   for (int u = 0 ; u < 6 ; ++u) {
-      const long x = o + vs[u]*w.s_a;
-#pragma unroll
-      for (int c = 0 ; c < 3 ; ++c) {
-         e[u][c] = E.c[c][x];
-         jv[u][c] = __ldg (J.c[c] + x);
-      }
-   }
-#pragma unroll
-   for (int u = 0 ; u < 6 ; ++u) {
-      const long x = o + vs[u]*w.s_a;
-#pragma unroll
-      for (int c = 0 ; c < 3 ; ++c)
-         E.c[c][x] = e[u][c] - tau*jv[u][c];
-   }
-}
-
-// Current folding of one axis, lower wall then upper wall
-// (plasma_currentWalls.c:27-121); transverse extent [-2, n+2].  The five
-// nodes around a wall are loaded, folded in registers in the reference's
-// order and stored back.
-__device__ __forceinline__ void j_fold_wall (double a[5], double pp[5], double qq[5], int top)
-{
-   // Index u = 2 + offset along the axis from the wall node (u = 0..4 for
-   // offsets -2..2).  out = +1 at the upper wall, -1 at the lower wall;
-   // internal/external pick the normal component's staggered neighbours.
-   const int out = top ? 1 : -1;
-   const int in_ = top ? 2 : 3, ex_ = top ? 3 : 2;          // wall + internal / external
-   a[in_] -= a[ex_];
-   pp[2 - out] += pp[2 + out];
-   qq[2 - out] += qq[2 + out];
-   a[in_ - out] -= a[ex_ + out];
-   pp[2 - 2*out] += pp[2 + 2*out];
-   qq[2 - 2*out] += qq[2 + 2*out];
-   pp[2] = 0;
-   qq[2] = 0;
-   a[ex_] = a[in_];
-   pp[2 + out] = -pp[2 - out];
-   qq[2 + out] = -qq[2 - out];
-   a[ex_ + out] = a[in_ - out];
-   pp[2 + 2*out] = -pp[2 - 2*out];
-   qq[2 + 2*out] = -qq[2 - 2*out];
-}
-
-__device__ __forceinline__ void j_fold (const Grid &g, F3 &J, int ea, int top, int bc, long base,
-                                        const long s[3])
-{
-   const long st = s[ea];
-   if (bc == MG_BC_PERIODIC) {
-      if (top)
-         return;
-      const long shift = (long) g.n[ea]*st;
-      double lo[3][5], hi[3][5];
-#pragma unroll
-      for (int c = 0 ; c < 3 ; ++c)
-#pragma unroll
-         for (int u = 0 ; u < 5 ; ++u) {
-            lo[c][u] = J.c[c][base + (u - 2)*st];
-            hi[c][u] = J.c[c][base + (u - 2)*st + shift];
-         }
-#pragma unroll
-      for (int c = 0 ; c < 3 ; ++c)
-#pragma unroll
-         for (int u = 0 ; u < 5 ; ++u) {
-            const double v = hi[c][u] + lo[c][u];
-            J.c[c][base + (u - 2)*st + shift] = v;
-            J.c[c][base + (u - 2)*st] = v;
-         }
-      return;
-   }
-   const int ep = (ea == 0) ? 1 : 0, eq = (ea == 2) ? 1 : 2;
-   const long o = base + (top ? g.n[ea] : 0)*st;
-   double a[5], pp[5], qq[5];
-#pragma unroll
-   for (int u = 0 ; u < 5 ; ++u) {
-      a[u] = J.c[ea][o + (u - 2)*st];
-      pp[u] = J.c[ep][o + (u - 2)*st];
-      qq[u] = J.c[eq][o + (u - 2)*st];
-   }
-   j_fold_wall (a, pp, qq, top);
-#pragma unroll
-   for (int u = 0 ; u < 5 ; ++u) {
-      J.c[ea][o + (u - 2)*st] = a[u];
-      J.c[ep][o + (u - 2)*st] = pp[u];
-      J.c[eq][o + (u - 2)*st] = qq[u];
-   }
-}
-
-__global__ void k_j_walls (Grid g, F3 J, int ea)
-{
-   const int ep = (ea == 0) ? 1 : 0, eq = (ea == 2) ? 1 : 2;
-   const int np_ = g.n[ep] + 5, nq_ = g.n[eq] + 5;
-   const long t = blockIdx.x*(long) blockDim.x + threadIdx.x;
-   if (t >= (long) np_*nq_)
-      return;
-   const long s[3] = {g.sx, g.sy, 1};
-   const int p = (int) (t / nq_) - 2, q = (int) (t % nq_) - 2;
-   const long base = g.origin + p*s[ep] + q*s[eq];
-   j_fold (g, J, ea, 0, g.bc[0][ea], base, s);
-   j_fold (g, J, ea, 1, g.bc[1][ea], base, s);
-}
-
-
-
-// E -= tau*J over [-1, n+1]^3 (core/em.c:167-184).
-__global__ void k_e_sub_j (Grid g, F3 E, F3 J, Box b)
-{
-   const double tau = g.tau;
-   for (long t = blockIdx.x*(long) blockDim.x + threadIdx.x ; t < b.vol ; t += (long) gridDim.x*blockDim.x) {
-      int i, j, k;
-      box_index (t, b.lo, b.ext, i, j, k);
-      const long o = g.at (i, j, k);
-      E.c[0][o] -= tau*J.c[0][o];
-      E.c[1][o] -= tau*J.c[1][o];
-      E.c[2][o] -= tau*J.c[2][o];
-   }
-}
-
-
-
-// Laser soft source (one-sided injection of scpic/em_mirror.h:62-101 with an
-// analytic paraxial Gaussian beam and sin^2 envelope).  The incident field
-// is evaluated in FP64 from the device time.
-__device__ double laser_ey (const mg_laser_t &l, double x, double y, double z,
-                            double t, double ymid, double zmid)
-{
-   const double k = 2*M_PI, xr = M_PI*l.waist*l.waist;
-   const double xi = x - l.x_focus;
-   const double w = l.waist*sqrt (1 + (xi/xr)*(xi/xr));
-   const double r2 = (y - ymid)*(y - ymid) + (z - zmid)*(z - zmid);
-   const double tr = t - l.t_start - x;
-   if (tr <= 0 || tr >= l.duration)
-      return 0;
-   const double s = sin (M_PI*tr/l.duration);
-   const double env = s*s;
-   const double phase = k*tr + atan (xi/xr) - k*r2*xi/(2*(xi*xi + xr*xr)) + l.phase;
-   return 2*M_PI*l.a0*(l.waist/w)*exp (-r2/(w*w))*env*sin (phase);
-}
-
-// Hz[I] += (tau/h1) * Ey_inc(x = (I-1) h1, t = n tau)   (after the H step)
-// Ey[I-1] += (tau/h1) * Hz_inc(x = (I-1/2) h1, t = (n+1/2) tau)
-__global__ void k_laser (Grid g, double *F, mg_laser_t l, const DevScalars *dsc,
-                         int is_e, F3 E, F3 J, int sub_j)
-{
-   const int nj = g.n[1] - 2*l.margin + 1, nk = g.n[2] - 2*l.margin + 1;
-   const long t = blockIdx.x*(long) blockDim.x + threadIdx.x;
-   if (nj <= 0 || nk <= 0 || t >= (long) nj*nk)
-      return;
-   const int j = l.margin + (int) (t / nk), k = l.margin + (int) (t % nk);
-   const double ymid = 0.5*g.n[1]*g.h[1], zmid = 0.5*g.n[2]*g.h[2];
-   const double c1 = g.tau/g.h[0];
-   const double time = dsc->time + (is_e ? 0.5*g.tau : 0.0);
-   const double x = is_e ? (l.plane - 0.5)*g.h[0] : (l.plane - 1)*g.h[0];
-   const int i = is_e ? l.plane - 1 : l.plane;
-   const double v = laser_ey (l, x, (j - 0.5)*g.h[1], k*g.h[2], time, ymid, zmid);
-   const long o = g.at (i, j, k);
-   F[o] += c1*v;
-   if (sub_j) {
-      // These nodes skip -tau J in the fused E pass: it comes after the
-      // source here (core/em.c:210-215 order).
-      for (int c = 0 ; c < 3 ; ++c)
-         E.c[c][o] -= g.tau*J.c[c][o];
-   }
-}
-
-static F3 f3 (double *const c[3])
-{
-   F3 f;
-   for (int a = 0 ; a < 3 ; ++a)
-      f.c[a] = c[a];
-   return f;
-}
-
-static int wall_ops (const Grid &g, int ea, int &op_min, int &op_max)
-{
-   const int b0 = g.bc[0][ea], b1 = g.bc[1][ea];
-   if (b0 == MG_BC_PERIODIC) {
-      op_min = OP_PERIODIC;
-      op_max = -1;
-      return 0;
-   }
-   op_min = (b0 == MG_BC_MIRROR) ? OP_MIRROR_MIN : OP_OPEN_MIN;
-   op_max = (b1 == MG_BC_MIRROR) ? OP_MIRROR_MAX : OP_OPEN_MAX;
-   return 0;
-}
-
-static int launch_h_walls (mg_run_t *r, int both)
-{
-   const Grid &g = r->g;
-   for (int ea = 0 ; ea < 3 ; ++ea) {
-      Wall w = make_wall (g, ea);
-      const long nodes = (long) w.np_*w.nq_;
-      const int T = 256, B = (int) ((nodes + T - 1)/T);
-      int op0, op1;
-      wall_ops (g, ea, op0, op1);
-      k_h_walls<<<B, T, 0, r->stream>>> (g, f3 (r->H), f3 (r->Hn), w, op0, op1, both);
-      MG_LAUNCH_CHECK ();
-   }
-   return MG_OK;
-}
-
-static int launch_hn_walls (mg_run_t *r)
-{
-   const Grid &g = r->g;
-   for (int ea = 0 ; ea < 3 ; ++ea) {
-      Wall w = make_wall (g, ea);
-      const long nodes = (long) w.np_*w.nq_;
-      const int T = 256, B = (int) ((nodes + T - 1)/T);
-      int op0, op1;
-      wall_ops (g, ea, op0, op1);
-      k_h_walls<<<B, T, 0, r->stream>>> (g, f3 (r->Hn), f3 (r->Hn), w, op0, op1, 0);
-      MG_LAUNCH_CHECK ();
-   }
-   return MG_OK;
-}
-
-// E walls of all axes; with sub_j the rim nodes also get their -tau J.
-static int launch_e_walls (mg_run_t *r, int sub_j)
-{
-   const Grid &g = r->g;
-   for (int ea = 0 ; ea < 3 ; ++ea) {
-      Wall w = make_wall (g, ea);
-      const long nodes = (long) (w.np_ + 1)*(w.nq_ + 1);
-      const int T = 128, B = (int) ((nodes + T - 1)/T);
-      const double alpha = (g.tau - g.h[ea])/(g.tau + g.h[ea]);
-      int op0, op1;
-      wall_ops (g, ea, op0, op1);
-      k_e_walls<<<B, T, 0, r->stream>>> (g, f3 (r->E), f3 (r->J), w, op0, op1, r->mur[0][ea],
-                                         r->mur[1][ea], alpha, sub_j);
-      MG_LAUNCH_CHECK ();
-   }
-   return MG_OK;
-}
-
-static int launch_laser (mg_run_t *r, int is_e, int sub_j = 0)
-{
-   if (!r->has_laser)
-      return MG_OK;
-   const mg_laser_t &l = r->laser;
-   const long nj = r->g.n[1] - 2*l.margin + 1, nk = r->g.n[2] - 2*l.margin + 1;
-   if (nj <= 0 || nk <= 0)
-      return MG_OK;
-   const int T = 256, B = (int) ((nj*nk + T - 1)/T);
-   k_laser<<<B, T, 0, r->stream>>> (r->g, is_e ? r->E[1] : r->H[2], l, r->dsc, is_e,
-                                    f3 (r->E), f3 (r->J), sub_j);
-   MG_LAUNCH_CHECK ();
-   return MG_OK;
-}
-
-static Box h_box (const Grid &g)
-{
-   int lo[3], hi[3];
-   for (int a = 0 ; a < 3 ; ++a) {
-      lo[a] = (g.bc[0][a] == MG_BC_MIRROR) ? 1 : 0;
-      hi[a] = g.n[a];
-   }
-   return make_box (lo, hi);
-}
-
-static Box e_box (const Grid &g)
-{
-   int lo[3], hi[3];
-   for (int a = 0 ; a < 3 ; ++a) {
-      lo[a] = (g.bc[0][a] == MG_BC_PERIODIC) ? 0 : 1;
-      hi[a] = (g.bc[1][a] == MG_BC_PERIODIC) ? g.n[a] - 1 : g.n[a];
-   }
-   return make_box (lo, hi);
-}
-
-// Pick ranges of em_energy (core/em.c:241-247): component c sums nodes with
-// index in [1, n] on its own axis and [0, n-1] on the others (E), and
-// [0, n-1] on its own axis and [1, n] on the others (H).  On a periodic axis
-// the H value at node 0 is the copy of node n, so node n stands in for it.
-static EnergyPick energy_pick (const Grid &g)
-{
-   EnergyPick ep;
-   for (int c = 0 ; c < 3 ; ++c)
-      for (int a = 0 ; a < 3 ; ++a) {
-         const int N = g.n[a];
-         if (a == c) {
-            ep.lo[c][a] = 1; ep.hi[c][a] = N;
-            const bool per = (g.bc[0][a] == MG_BC_PERIODIC);
-            ep.hlo[c][a] = per ? 1 : 0;
-            ep.hhi[c][a] = per ? N : N - 1;
-         } else {
-            ep.lo[c][a] = 0; ep.hi[c][a] = N - 1;
-            ep.hlo[c][a] = 1; ep.hhi[c][a] = N;
-         }
-      }
-   return ep;
-}
-
-static Rim rim (const mg_run_t *r)
-{
-   Rim rm;
-   for (int a = 0 ; a < 3 ; ++a) {
-      rm.lo[a] = 2;
-      rm.hi[a] = r->g.n[a] - 2;
-   }
-   rm.laser_i = r->has_laser ? r->laser.plane - 1 : INT_MIN;
-   const int margin = r->has_laser ? r->laser.margin : 0;
-   rm.laser_lo[0] = margin;
-   rm.laser_hi[0] = r->g.n[1] - margin;
-   rm.laser_lo[1] = margin;
-   rm.laser_hi[1] = r->g.n[2] - margin;
-   return rm;
-}
-
-} // namespace
-
-// H^(n-1/2) -> H^n (kept in Hn) and on to H^(n+1/2) (kept in H), with the
-// field energy at t = n tau summed on the way; walls on Hn.
-int mg_fields64_h_half (mg_run_t *r)
-{
-   const Grid &g = r->g;
-   Box b = h_box (g);
-   const int T = 256;
-   MG_CUDA (cudaMemsetAsync (r->dsc->acc, 0, 2*sizeof (double), r->stream));
-   k_h_fused<<<mg_blocks_for (b.vol, T, 8), T, 0, r->stream>>> (
-      g, f3 (r->E), f3 (r->H), f3 (r->Hn), b, 0.5*g.tau/g.h[0], 0.5*g.tau/g.h[1], 0.5*g.tau/g.h[2],
-      energy_pick (g), r->dsc);
-   MG_LAUNCH_CHECK ();
-   return launch_hn_walls (r);
-}
-
-int mg_fields64_energy (mg_run_t *r)
-{
-   (void) r;                      // summed by mg_fields64_h_half
-   return MG_OK;
-}
-
-// Source at t = n tau on H^(n+1/2), then its walls (core/em.c:115-131).
-int mg_fields64_h_step (mg_run_t *r)
-{
-   TRY_MG (launch_laser (r, 0));
-   const Grid &g = r->g;
-   for (int ea = 0 ; ea < 3 ; ++ea) {
-      Wall w = make_wall (g, ea);
-      const long nodes = (long) w.np_*w.nq_;
-      const int T = 256, B = (int) ((nodes + T - 1)/T);
-      int op0, op1;
-      wall_ops (g, ea, op0, op1);
-      k_h_walls<<<B, T, 0, r->stream>>> (g, f3 (r->H), f3 (r->H), w, op0, op1, 0);
-      MG_LAUNCH_CHECK ();
-   }
-   return MG_OK;
-}
-
-// Graph path: both half steps, the source on H^(n+1/2), walls on both.
-int mg_fields64_h_both (mg_run_t *r)
-{
-   const Grid &g = r->g;
-   Box b = h_box (g);
-   const int T = 256;
-   MG_CUDA (cudaMemsetAsync (r->dsc->acc, 0, 2*sizeof (double), r->stream));
-   k_h_fused<<<mg_blocks_for (b.vol, T, 8), T, 0, r->stream>>> (
-      g, f3 (r->E), f3 (r->H), f3 (r->Hn), b, 0.5*g.tau/g.h[0], 0.5*g.tau/g.h[1], 0.5*g.tau/g.h[2],
-      energy_pick (g), r->dsc);
-   MG_LAUNCH_CHECK ();
-   TRY_MG (launch_laser (r, 0));
-   return launch_h_walls (r, 1);
-}
-
-// Stage path: E += curl H only, then the E walls (Mur history before -tau J).
-int mg_fields64_e_step (mg_run_t *r)
-{
-   const Grid &g = r->g;
-   Box b = e_box (g);
-   const int T = 256;
-   k_e_advance<<<mg_blocks_for (b.vol, T, 16), T, 0, r->stream>>> (
-      g, f3 (r->E), f3 (r->H), b, g.tau/g.h[0], g.tau/g.h[1], g.tau/g.h[2]);
-   MG_LAUNCH_CHECK ();
-   return launch_e_walls (r, 0);
-}
-
-int mg_fields64_jbc (mg_run_t *r)
-{
-   const Grid &g = r->g;
-   for (int ea = 0 ; ea < 3 ; ++ea) {
-      const int ep = (ea == 0) ? 1 : 0, eq = (ea == 2) ? 1 : 2;
-      const long nodes = (long) (g.n[ep] + 5)*(g.n[eq] + 5);
-      const int T = 256, B = (int) ((nodes + T - 1)/T);
-      k_j_walls<<<B, T, 0, r->stream>>> (g, f3 (r->J), ea);
-      MG_LAUNCH_CHECK ();
-   }
-   return MG_OK;
-}
-
-// Stage path: source at t + tau/2, then E -= tau J over [-1, n+1]^3.
-int mg_fields64_e_finish (mg_run_t *r)
-{
-   TRY_MG (launch_laser (r, 1));
-   const int lo[3] = {-1, -1, -1};
-   const int hi[3] = {r->g.n[0] + 1, r->g.n[1] + 1, r->g.n[2] + 1};
-   Box b = make_box (lo, hi);
-   const int T = 256;
-   k_e_sub_j<<<mg_blocks_for (b.vol, T, 16), T, 0, r->stream>>> (r->g, f3 (r->E), f3 (r->J), b);
-   MG_LAUNCH_CHECK ();
-   return MG_OK;
-}
-
-// Graph path: E += curl H - tau J in one pass away from the rim, E walls,
-// source, then -tau J on the rim.  Bit-identical to the stage path: every
-// node sees the same operations in the same order.  Needs the J walls done.
-int mg_fields64_e_fused (mg_run_t *r)
-{
-   const Grid &g = r->g;
-   Box b = e_box (g);
-   Rim rm = rim (r);
-   const int T = 256;
-   k_e_fused<<<mg_blocks_for (b.vol, T, 8), T, 0, r->stream>>> (
-      g, f3 (r->E), f3 (r->H), f3 (r->J), b, g.tau/g.h[0], g.tau/g.h[1], g.tau/g.h[2], rm);
-   MG_LAUNCH_CHECK ();
-   TRY_MG (launch_e_walls (r, 1));
-   TRY_MG (launch_laser (r, 1, 1));
-   return MG_OK;
-}
-
-int mg_fields64_zero_j (mg_run_t *r)
-{
-   for (int c = 0 ; c < 3 ; ++c)
-      MG_CUDA (cudaMemsetAsync (r->J[c], 0, r->g.total*sizeof (double), r->stream));
-   return MG_OK;
-}
-
-// cap_init equivalent (core/em_caps.c:343-392), axis by axis.
-int mg_fields64_init (mg_run_t *r)
-{
-   const Grid &g = r->g;
-   for (int ea = 0 ; ea < 3 ; ++ea) {
-      Wall w = make_wall (g, ea);
-      const long nodes = (long) w.np_*w.nq_;
-      const int T = 256, B = (int) ((nodes + T - 1)/T);
-      if (g.bc[0][ea] == MG_BC_PERIODIC) {
-         k_h_wall<<<B, T, 0, r->stream>>> (g, f3 (r->H), w, OP_PERIODIC);
-         k_e_wall<<<B, T, 0, r->stream>>> (g, f3 (r->E), w, OP_PERIODIC, nullptr, 0.0);
-         MG_LAUNCH_CHECK ();
-         continue;
-      }
-      for (int top = 0 ; top < 2 ; ++top) {
-         if (g.bc[top][ea] == MG_BC_MIRROR) {
-            const int op = top ? OP_MIRROR_MAX : OP_MIRROR_MIN;
-            k_h_wall<<<B, T, 0, r->stream>>> (g, f3 (r->H), w, op);
-            k_e_wall<<<B, T, 0, r->stream>>> (g, f3 (r->E), w, op, nullptr, 0.0);
-         } else if (g.bc[top][ea] == MG_BC_OPEN) {
-            k_mur_init<<<B, T, 0, r->stream>>> (g, f3 (r->E), w, top, r->mur[top][ea]);
-         }
-         MG_LAUNCH_CHECK ();
-      }
-   }
-   return MG_OK;
-}
+int mg_fields64_h_half (mg_run_t *r) { return fields_h_half<double> (r, fs_of (r)); }
+int mg_fields64_energy (mg_run_t *r) { return fields_energy<double> (r, fs_of (r)); }
+int mg_fields64_h_step (mg_run_t *r) { return fields_h_step<double> (r, fs_of (r)); }
+int mg_fields64_h_both (mg_run_t *r) { return fields_h_both<double> (r, fs_of (r)); }
+int mg_fields64_e_step (mg_run_t *r) { return fields_e_step<double> (r, fs_of (r)); }
+int mg_fields64_jbc (mg_run_t *r) { return fields_jbc<double> (r, fs_of (r)); }
+int mg_fields64_e_finish (mg_run_t *r) { return fields_e_finish<double> (r, fs_of (r)); }
+int mg_fields64_e_fused (mg_run_t *r) { return fields_e_fused<double> (r, fs_of (r)); }
+int mg_fields64_zero_j (mg_run_t *r) { return fields_zero_j<double> (r, fs_of (r)); }
+int mg_fields64_init (mg_run_t *r) { return fields_init<double> (r, fs_of (r)); }

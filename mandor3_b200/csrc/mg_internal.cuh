@@ -94,7 +94,7 @@ struct mg_run {
    double *E[3], *H[3], *J[3];
    double *Hn[3];          // H at t = n tau (H holds n-1/2, then n+1/2)
    double *mur[2][3];      // Mur history, 4 doubles per wall node
-   float  *E32[3], *H32[3], *J32[3];
+   float  *E32[3], *H32[3], *J32[3], *Hn32[3];
    float  *mur32[2][3];
 
    // markers
@@ -184,14 +184,18 @@ int mg_fields32_jbc (mg_run_t *r);
 int mg_fields32_e_finish (mg_run_t *r);
 int mg_fields32_init (mg_run_t *r);
 int mg_fields32_zero_j (mg_run_t *r);
+int mg_fields32_h_both (mg_run_t *r);
+int mg_fields32_e_fused (mg_run_t *r);
 int mg_push32 (mg_run_t *r);
 int mg_sort32 (mg_run_t *r);
 int mg_walls32 (mg_run_t *r);
 int mg_enqueue_step32 (mg_run_t *r, int part);
 int mg_place32 (mg_run_t *r, const mg_place_t *spec, long long at, long long count);
 int mg_ensure_capacity32 (mg_run_t *r, long long need);
-int mg_run_create32 (const mg_params_t *params, mg_run_t **out);
-int mg_run_destroy32 (mg_run_t *r);
+void mg_free_markers32 (mg_run_t *r);
+int mg_dev_alloc (mg_run_t *r, void **p, size_t bytes);
+int mg_ensure_stage (mg_run_t *r, size_t bytes);
+void mg_drop_graphs (mg_run_t *r);
 int mg_run_set_fields32 (mg_run_t *r, const double *E, const double *H);
 int mg_run_get_fields32 (mg_run_t *r, double *E, double *H);
 int mg_run_get_current32 (mg_run_t *r, double *J);
