@@ -43,9 +43,13 @@ def test_fp32_matches_reference_within_single_precision(name):
     u = np.stack([want["vx"], want["vy"], want["vz"]])
     for ax in ("vx", "vy", "vz"):
         assert np.max(np.abs(got[ax] - want[ax])) < 1e-4 * max(np.max(np.abs(u)), 1e-30)
+    # Energy rows: each quantity within 1e-4 of the run's total energy scale
+    # (small quantities such as a cold slab's thermal energy carry FP32
+    # rounding relative to the whole system, not to themselves).
     d = g["diag"]
+    scale = float(np.max(np.abs(d[:, 1:6].sum(1))))
     for c in range(5):
-        np.testing.assert_allclose(rows[1:, 1 + c], d[:, 1 + c], rtol=1e-4, atol=1e-12)
+        np.testing.assert_allclose(rows[1:, 1 + c], d[:, 1 + c], rtol=1e-4, atol=1e-4 * scale)
 
 
 def thermal_plasma(precision, steps, sort_every=0):
