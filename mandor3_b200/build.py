@@ -35,7 +35,7 @@ CUDA_UNITS = {
     "fields32.cu": [],
     "push32.cu": [],
 }
-HOST_UNITS = ["mgio.c"]
+HOST_UNITS = []
 
 
 def _newer(src, dst, extra=()):
@@ -67,7 +67,7 @@ def build(force=False, verbose=False):
         if not os.path.exists(src):
             continue
         obj = os.path.join(OBJ, unit + ".o")
-        if force or _newer(src, obj, headers + [os.path.join(HOST, "mgio.h")]):
+        if force or _newer(src, obj, headers):
             _run(["gcc", "-O2", "-std=gnu99", "-fPIC", "-Wall", "-I" + INCLUDE, "-I" + HOST,
                   "-c", src, "-o", obj], verbose)
         objs.append(obj)

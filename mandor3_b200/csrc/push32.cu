@@ -126,7 +126,27 @@ __device__ __forceinline__ bool wall32 (int bc, bool top, int n, int &c, float &
    return (!top && (c < 1 || (c == 1 && o == 0.0f))) || (top && c >= n - 1);
 }
 
-__global__ void __launch_bounds__ (256, 4)
+// Segment of the path between times ta and tb (start-cell coordinates),
+// in the cell shifted by (si, sj, sk) from the start cell.
+__device__ __forceinline__ void deposit_piece (const Ctx32 &c, float rho, int i, int j, int k,
+                                               int si, int sj, int sk, float ox, float oy, float oz,
+                                               float dx, float dy, float dz, float ta, float tb)
+{
+   float w[12];
+   weights32 (c, rho, ox + ta*dx - si, ox + tb*dx - si, oy + ta*dy - sj, oy + tb*dy - sj,
+              oz + ta*dz - sk, oz + tb*dz - sk, w);
+   scatter32 (c, i + si, j + sj, k + sk, w);
+}
+
+#define CSWAP(ta, aa, tb, ab)                                                 \
+   do {                                                                      \
+      if (tb < ta) {                                                         \
+         const float t_ = ta; ta = tb; tb = t_;                              \
+         const int a_ = aa; aa = ab; ab = a_;                                \
+      }                                                                      \
+   } while (0)
+
+__global__ void __launch_bounds__ (256, 3)
 k_push32 (Ctx32 c, Markers32 m, long long np, DevScalars *dsc)
 {
    const Grid &g = c.g;
@@ -178,17 +198,20 @@ k_push32 (Ctx32 c, Markers32 m, long long np, DevScalars *dsc)
             const float tm = 0.5f*c.tau*qm;
             const float px = m.ux[n] + tm*Ex, py = m.uy[n] + tm*Ey, pz = m.uz[n] + tm*Ez;
             const float p2 = px*px + py*py + pz*pz;
-            const float gamma = sqrtf (1.0f + p2);
-            const float W = (gamma - 1.0f)*rho/(p2 + 1e-19f)*(float) c.vol/qm;
+            const float rg = rsqrtf (1.0f + p2);             // 1/gamma
+            const float gamma = (1.0f + p2)*rg;
+            // (gamma - 1)/(p^2 + 1e-19) of core/plasma.c:140 written as
+            // 1/(gamma + 1) up to the 1e-19 guard: no cancellation in FP32.
+            const float W = __fdividef (p2, (gamma + 1.0f)*(p2 + 1e-19f))*rho*(float) c.vol/qm;
             Wx += (double) (W*px*px);
             Wy += (double) (W*py*py);
             Wz += (double) (W*pz*pz);
-            const float tg = tm/gamma;
+            const float tg = tm*rg;
             const float ax = tg*Hx, ay = tg*Hy, az = tg*Hz;
             const float u = px + py*az - pz*ay, v = py + pz*ax - px*az, w = pz + px*ay - py*ax;
             const float bxx = ax*ax, byy = ay*ay, bzz = az*az;
             const float bxy = ax*ay, byz = ay*az, bxz = az*ax;
-            const float delta = 1.0f/(1.0f + bxx + byy + bzz);
+            const float delta = __frcp_rn (1.0f + bxx + byy + bzz);
             float vx = tm*Ex + ((1.0f + bxx)*u + (bxy + az)*v + (bxz - ay)*w)*delta;
             float vy = tm*Ey + ((bxy - az)*u + (1.0f + byy)*v + (byz + ax)*w)*delta;
             float vz = tm*Ez + ((bxz + ay)*u + (byz - ax)*v + (1.0f + bzz)*w)*delta;
@@ -233,67 +256,63 @@ k_push32 (Ctx32 c, Markers32 m, long long np, DevScalars *dsc)
          }
       }
 
-      // Split the path at the faces it crosses (times along the path in
-      // [0, 1]); segment s runs from time t[s] to t[s+1] in cell cs.
-      float ta = 1.0f;
-      int na = 0;
-      float tcr[3];
-      int axc[3];
+      // Crossing times of the faces the path crosses (2 = none), sorted with
+      // a three-element network; the path splits at each of them.
+      float t0 = 2.0f, t1 = 2.0f, t2 = 2.0f;
+      int a0 = 0, a1 = 1, a2 = 2;
       if (valid) {
-         if (di) { tcr[na] = ((di > 0 ? 1.0f : 0.0f) - ox)/dx; axc[na++] = 0; }
-         if (dj) { tcr[na] = ((dj > 0 ? 1.0f : 0.0f) - oy)/dy; axc[na++] = 1; }
-         if (dk) { tcr[na] = ((dk > 0 ? 1.0f : 0.0f) - oz)/dz; axc[na++] = 2; }
-         // Sort the (at most three) crossing times.
-         for (int a = 0 ; a < na ; ++a)
-            for (int b = a + 1 ; b < na ; ++b)
-               if (tcr[b] < tcr[a]) {
-                  const float t = tcr[a]; tcr[a] = tcr[b]; tcr[b] = t;
-                  const int x = axc[a]; axc[a] = axc[b]; axc[b] = x;
-               }
-         ta = na > 0 ? tcr[0] : 1.0f;
+         if (di) t0 = __fdividef ((di > 0 ? 1.0f : 0.0f) - ox, dx);
+         if (dj) t1 = __fdividef ((dj > 0 ? 1.0f : 0.0f) - oy, dy);
+         if (dk) t2 = __fdividef ((dk > 0 ? 1.0f : 0.0f) - oz, dz);
+         CSWAP (t0, a0, t1, a1);
+         CSWAP (t1, a1, t2, a2);
+         CSWAP (t0, a0, t1, a1);
       }
+      const float ta = fminf (t0, 1.0f);
 
-      // Later segments first (direct atomics), in the cells the path enters.
-      if (valid && na > 0) {
-         int ci = i, cj = j, ck = k;
-         float sx0 = ox + ta*dx, sy0 = oy + ta*dy, sz0 = oz + ta*dz;   // start point, start-cell coords
-         float off[3] = {0.0f, 0.0f, 0.0f};                           // start-cell to segment-cell shift
-         for (int s = 0 ; s < na ; ++s) {
-            const int a = axc[s];
-            const int d = a == 0 ? di : (a == 1 ? dj : dk);
-            if (a == 0) ci += d; else if (a == 1) cj += d; else ck += d;
-            off[a] += (float) d;
-            const float t2 = (s + 1 < na) ? tcr[s + 1] : 1.0f;
-            float ex = ox + t2*dx, ey = oy + t2*dy, ez = oz + t2*dz;
-            float wseg[12];
-            weights32 (c, rho, sx0 - off[0], ex - off[0], sy0 - off[1], ey - off[1],
-                       sz0 - off[2], ez - off[2], wseg);
-            scatter32 (c, ci, cj, ck, wseg);
-            sx0 = ex;
-            sy0 = ey;
-            sz0 = ez;
+      // Segments after the first: direct atomics in the cells entered.
+      if (valid && t0 <= 1.0f) {
+         int si = 0, sj = 0, sk = 0;
+         const int d3[3] = {di, dj, dk};
+         si += (a0 == 0) ? d3[0] : 0; sj += (a0 == 1) ? d3[1] : 0; sk += (a0 == 2) ? d3[2] : 0;
+         deposit_piece (c, rho, i, j, k, si, sj, sk, ox, oy, oz, dx, dy, dz, t0, fminf (t1, 1.0f));
+         if (t1 <= 1.0f) {
+            si += (a1 == 0) ? d3[0] : 0; sj += (a1 == 1) ? d3[1] : 0; sk += (a1 == 2) ? d3[2] : 0;
+            deposit_piece (c, rho, i, j, k, si, sj, sk, ox, oy, oz, dx, dy, dz, t1, fminf (t2, 1.0f));
+            if (t2 <= 1.0f) {
+               si += (a2 == 0) ? d3[0] : 0; sj += (a2 == 1) ? d3[1] : 0; sk += (a2 == 2) ? d3[2] : 0;
+               deposit_piece (c, rho, i, j, k, si, sj, sk, ox, oy, oz, dx, dy, dz, t2, 1.0f);
+            }
          }
       }
 
-      // First segment (in the start cell): warp-aggregated by cell.
+      // First segment (in the start cell): summed across lanes that share
+      // the cell, one lane per run of equal cells issues the atomics.
       float wgt[12];
       if (valid)
          weights32 (c, rho, ox, ox + ta*dx, oy, oy + ta*dy, oz, oz + ta*dz, wgt);
       else
          for (int q = 0 ; q < 12 ; ++q) wgt[q] = 0.0f;
-      const long long key = valid ? g.at (i, j, k) : -1 - lane;
-      const long long prev = __shfl_up_sync (0xffffffffu, key, 1);
-      const long long next = __shfl_down_sync (0xffffffffu, key, 1);
-      const bool head = (lane == 0) || (prev != key);
-      const bool tail = (lane == 31) || (next != key);
-      const unsigned heads = __ballot_sync (0xffffffffu, head);
-      const unsigned le = (lane == 31) ? 0xffffffffu : ((1u << (lane + 1)) - 1);
-      const int seg_start = 31 - __clz (heads & le);
-      if (__all_sync (0xffffffffu, seg_start == lane)) {
-         // No two lanes share a cell: no reduction.
-         if (valid)
+      const int key = valid ? (int) g.at (i, j, k) : -1 - lane;
+      const int key0 = __shfl_sync (0xffffffffu, key, 0);
+      if (__all_sync (0xffffffffu, key == key0 || !valid)) {
+         // One cell for the whole warp: butterfly sums, lane 0 scatters.
+#pragma unroll
+         for (int q = 0 ; q < 12 ; ++q)
+#pragma unroll
+            for (int d = 16 ; d > 0 ; d >>= 1)
+               wgt[q] += __shfl_xor_sync (0xffffffffu, wgt[q], d);
+         const unsigned any = __ballot_sync (0xffffffffu, valid);
+         if (any && lane == __ffs (any) - 1)
             scatter32 (c, i, j, k, wgt);
       } else {
+         const int prev = __shfl_up_sync (0xffffffffu, key, 1);
+         const int next = __shfl_down_sync (0xffffffffu, key, 1);
+         const bool head = (lane == 0) || (prev != key);
+         const bool tail = (lane == 31) || (next != key);
+         const unsigned heads = __ballot_sync (0xffffffffu, head);
+         const unsigned le = (lane == 31) ? 0xffffffffu : ((1u << (lane + 1)) - 1);
+         const int seg_start = 31 - __clz (heads & le);
 #pragma unroll
          for (int q = 0 ; q < 12 ; ++q)
             wgt[q] = seg_scan (wgt[q], lane, seg_start);

@@ -1,0 +1,472 @@
+/* core_b200.out -- drop-in replacement for the reference's core.out.
+ *
+ * Run it in a Mandor run directory prepared by the reference's setup.out:
+ * it reads the same inputs (run_mandor.cfg, binData/domain.bin, the last or
+ * the first checkpoint record, tmp/stop.flag) and writes the same outputs
+ * (checkpoint records, binData/diag.dat), so the reference's tools read its
+ * results unchanged.  The time stepping runs on one B200 through the C ABI
+ * of include/mandor_b200.h.
+ *
+ * Files and their reference writers/readers:
+ *   run_mandor.cfg             core/main.c:205-213 (six "@ int" lines)
+ *   binData/domain.bin         misc_parameters.c:98-131
+ *   binData/sys.N, sys_%06d.txt, sys_E/H_%06d(000).bin, sys_prtn_%06d.bin
+ *                              IO_sys.c:99-142, type_mesh.c:285-313
+ *   binData/fileMap*.txt/.N    IO_fileMap.c:129-157
+ *   binData/plasma_%06d_000.bin  core/plasma_IO.c:273-287
+ *   binData/diag.dat           core/diag_WDensity.c:30-157
+ *   tmp/stop.flag              core/main.c:120-189
+ *
+ *   core_b200.out [--fp32] [--device N]
+ */
+#include <errno.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#include "mandor_b200.h"
+
+#define HEADER_BYTES 112            /* 6 ints of valid region + 88-byte mesh_t */
+
+static void die (const char *fmt, const char *arg)
+{
+   fprintf (stderr, "core_b200.out: ");
+   fprintf (stderr, fmt, arg);
+   fprintf (stderr, "\n");
+   exit (EXIT_FAILURE);
+}
+
+static void check (int rc, const char *what)
+{
+   if (rc != MG_OK) {
+      fprintf (stderr, "core_b200.out: %s: %s\n", what, mg_last_error ());
+      exit (EXIT_FAILURE);
+   }
+}
+
+static double now (void)
+{
+   struct timespec ts;
+   clock_gettime (CLOCK_MONOTONIC, &ts);
+   return ts.tv_sec + 1e-9*ts.tv_nsec;
+}
+
+static FILE *open_or_die (const char *path, const char *mode)
+{
+   FILE *fp = fopen (path, mode);
+   if (!fp)
+      die ("cannot open '%s'", path);
+   return fp;
+}
+
+/* "@ value ..." lines, as cfg_readInt reads them (misc_cfgReader.c:71-81). */
+static int read_at_int (FILE *fp, const char *path)
+{
+   int c, v;
+   while ((c = fgetc (fp)) != EOF && c != '@')
+      ;
+   if (c == EOF || fscanf (fp, "%d", &v) != 1)
+      die ("bad integer line in '%s'", path);
+   while ((c = fgetc (fp)) != EOF && c != '\n')
+      ;
+   return v;
+}
+
+static double read_at_double (FILE *fp, const char *path)
+{
+   int c;
+   double v;
+   while ((c = fgetc (fp)) != EOF && c != '@')
+      ;
+   if (c == EOF || fscanf (fp, "%lf", &v) != 1)
+      die ("bad number line in '%s'", path);
+   while ((c = fgetc (fp)) != EOF && c != '\n')
+      ;
+   return v;
+}
+
+static void read_exact (void *p, size_t n, FILE *fp, const char *path)
+{
+   if (fread (p, 1, n, fp) != n)
+      die ("'%s' is truncated", path);
+}
+
+static void write_exact (const void *p, size_t n, FILE *fp, const char *path)
+{
+   if (fwrite (p, 1, n, fp) != n)
+      die ("cannot write '%s'", path);
+}
+
+typedef struct {
+   int    total, full, tecplot, cont, stop, spectr;
+} run_cfg_t;
+
+typedef struct {
+   double h[3], L[3], tau;
+   int    dmin[3], dmax[3], bcmin[3], bcmax[3];
+} domain_t;
+
+static domain_t read_domain (void)
+{
+   domain_t d;
+   const char *path = "binData/domain.bin";
+   FILE *fp = open_or_die (path, "rb");
+   double v[7];
+   int iv[12];
+   read_exact (v, sizeof (v), fp, path);
+   read_exact (iv, sizeof (iv), fp, path);
+   fclose (fp);
+   for (int a = 0 ; a < 3 ; ++a) {
+      d.h[a] = v[a];
+      d.L[a] = v[3 + a];
+      d.dmin[a] = iv[a];
+      d.dmax[a] = iv[3 + a];
+      d.bcmin[a] = iv[6 + a];
+      d.bcmax[a] = iv[9 + a];
+   }
+   d.tau = v[6];
+   return d;
+}
+
+static void write_domain (const domain_t *d)
+{
+   const char *path = "binData/domain.bin";
+   FILE *fp = open_or_die (path, "wb");
+   double v[7] = {d->h[0], d->h[1], d->h[2], d->L[0], d->L[1], d->L[2], d->tau};
+   int iv[12];
+   for (int a = 0 ; a < 3 ; ++a) {
+      iv[a] = d->dmin[a];
+      iv[3 + a] = d->dmax[a];
+      iv[6 + a] = d->bcmin[a];
+      iv[9 + a] = d->bcmax[a];
+   }
+   write_exact (v, sizeof (v), fp, path);
+   write_exact (iv, sizeof (iv), fp, path);
+   fclose (fp);
+}
+
+/* Mesh file: region, the mesh_t struct, nodes of the region (k fastest). */
+static double *read_mesh (const char *path, unsigned char header[HEADER_BYTES], long nodes)
+{
+   FILE *fp = open_or_die (path, "rb");
+   read_exact (header, HEADER_BYTES, fp, path);
+   int reg[6];
+   memcpy (reg, header, sizeof (reg));
+   const long n = (long) (reg[3] - reg[0] + 1)*(reg[4] - reg[1] + 1)*(reg[5] - reg[2] + 1);
+   if (n != nodes || reg[0] || reg[1] || reg[2])
+      die ("'%s': region does not match the domain", path);
+   double *data = (double *) malloc (sizeof (double)*3*n);
+   read_exact (data, sizeof (double)*3*n, fp, path);
+   fclose (fp);
+   return data;
+}
+
+static void write_mesh (const char *path, const unsigned char header[HEADER_BYTES], const double *data,
+                        long nodes)
+{
+   FILE *fp = open_or_die (path, "wb");
+   write_exact (header, HEADER_BYTES, fp, path);
+   write_exact (data, sizeof (double)*3*nodes, fp, path);
+   fclose (fp);
+}
+
+static mg_marker_t *read_markers (const char *path, long long *n)
+{
+   FILE *fp = open_or_die (path, "rb");
+   long count = 0;
+   read_exact (&count, sizeof (long), fp, path);
+   mg_marker_t *m = (mg_marker_t *) malloc (sizeof (mg_marker_t)*(count > 0 ? count : 1));
+   if (count > 0)
+      read_exact (m, sizeof (mg_marker_t)*count, fp, path);
+   fclose (fp);
+   *n = count;
+   return m;
+}
+
+static void write_markers (const char *path, const mg_marker_t *m, long long n)
+{
+   FILE *fp = open_or_die (path, "wb");
+   long count = (long) n;
+   write_exact (&count, sizeof (long), fp, path);
+   if (n > 0)
+      write_exact (m, sizeof (mg_marker_t)*n, fp, path);
+   fclose (fp);
+}
+
+static void copy_file (const char *from, const char *to)
+{
+   FILE *in = fopen (from, "rb");
+   if (!in)
+      return;
+   FILE *out = open_or_die (to, "wb");
+   char buf[1 << 16];
+   size_t k;
+   while ((k = fread (buf, 1, sizeof (buf), in)) > 0)
+      write_exact (buf, k, out, to);
+   fclose (in);
+   fclose (out);
+}
+
+static int read_count (const char *path)
+{
+   FILE *fp = fopen (path, "rt");
+   if (!fp)
+      return 0;
+   int v = read_at_int (fp, path);
+   fclose (fp);
+   return v;
+}
+
+/* Energy rows are kept until the next checkpoint, then appended to diag.dat
+ * the way wDensity_finalize does (core/diag_WDensity.c:82-104). */
+typedef struct {
+   double *rows;
+   long    n, cap;
+} diag_t;
+
+static void diag_add (diag_t *d, const double *r6)
+{
+   if (d->n == d->cap) {
+      d->cap = d->cap ? 2*d->cap : 1024;
+      d->rows = (double *) realloc (d->rows, sizeof (double)*6*d->cap);
+   }
+   memcpy (d->rows + 6*d->n, r6, sizeof (double)*6);
+   d->n++;
+}
+
+static void diag_flush (diag_t *d, int *fresh, double tau)
+{
+   FILE *fp;
+   if (*fresh) {
+      fp = open_or_die ("binData/diag.dat", "wt");
+      fprintf (fp, "variables = t, W_E, W_M, W_T_x, W_T_y, W_T_z, W_p_e_r_p, W_k_i_n, W_E_M, W_`S\n"
+                   "zone f=point\n");
+      *fresh = 0;
+   } else {
+      fp = open_or_die ("binData/diag.dat", "at");
+   }
+   for (long q = 0 ; q < d->n ; ++q) {
+      const double *r = d->rows + 6*q;
+      if (r[0] < 0.5*tau)
+         continue;
+      fprintf (fp, "%e %e %e %e %e %e %e %e %e %e\n", r[0], r[1], r[2], r[3], r[4], r[5],
+               r[4] + r[5], r[3] + r[4] + r[5], r[1] + r[2], r[1] + r[2] + r[3] + r[4] + r[5]);
+   }
+   fclose (fp);
+   d->n = 0;
+}
+
+typedef struct {
+   int sys_num;           /* next checkpoint record */
+   int map_num;           /* next file map id */
+   unsigned char head_E[HEADER_BYTES], head_H[HEADER_BYTES];
+   char prtn_src[256];
+} records_t;
+
+/* sysIO_save + plasma_save (IO_sys.c:99-124, core/plasma_IO.c:273-287). */
+static void checkpoint (mg_run_t *run, records_t *rec, const domain_t *dom, long nodes, double time)
+{
+   char path[512];
+   double *E = (double *) malloc (sizeof (double)*3*nodes);
+   double *H = (double *) malloc (sizeof (double)*3*nodes);
+   check (mg_run_get_fields (run, E, H), "download fields");
+   long long n = 0;
+   check (mg_run_marker_count (run, &n), "marker count");
+   mg_marker_t *m = (mg_marker_t *) malloc (sizeof (mg_marker_t)*(n > 0 ? n : 1));
+   check (mg_run_get_markers (run, m, n, &n), "download markers");
+
+   snprintf (path, sizeof (path), "binData/plasma_%06d_%03d.bin", rec->sys_num, 0);
+   write_markers (path, m, n);
+   write_domain (dom);
+
+   const int map_id = rec->map_num++;
+   snprintf (path, sizeof (path), "binData/fileMap_%06d.txt", map_id);
+   FILE *fp = open_or_die (path, "wt");
+   fprintf (fp, "%d cpus total.\n", 1);
+   fprintf (fp, "%d: (%d %d %d) - (%d %d %d)\n", 0, dom->dmin[0], dom->dmin[1], dom->dmin[2],
+            dom->dmax[0], dom->dmax[1], dom->dmax[2]);
+   fclose (fp);
+   fp = open_or_die ("binData/fileMap.N", "wt");
+   fprintf (fp, "@ %d filemaps total is written.\n", rec->map_num);
+   fclose (fp);
+
+   snprintf (path, sizeof (path), "binData/sys_E_%06d(%03d).bin", rec->sys_num, 0);
+   write_mesh (path, rec->head_E, E, nodes);
+   snprintf (path, sizeof (path), "binData/sys_H_%06d(%03d).bin", rec->sys_num, 0);
+   write_mesh (path, rec->head_H, H, nodes);
+   snprintf (path, sizeof (path), "binData/sys_prtn_%06d.bin", rec->sys_num);
+   copy_file (rec->prtn_src, path);
+
+   snprintf (path, sizeof (path), "binData/sys_%06d.txt", rec->sys_num);
+   fp = open_or_die (path, "wt");
+   fprintf (fp, "@ %.14e    time.\n", time);
+   fprintf (fp, "@ %d       cpus total.\n", 1);
+   fprintf (fp, "@ %d       file map id.\n", map_id);
+   fprintf (fp, "That is checkpoint (record of the full system state) #%d.\n", rec->sys_num);
+   fclose (fp);
+   rec->sys_num++;
+   fp = open_or_die ("binData/sys.N", "wt");
+   fprintf (fp, "@ %d\t  system check-point records written.\n", rec->sys_num);
+   fclose (fp);
+   free (E);
+   free (H);
+   free (m);
+}
+
+/* main_throwStopFlag / main_catchStopFlag (core/main.c:120-189): the first
+ * number asks to stop now, the second is the wall-time budget in seconds;
+ * the run stops when the elapsed time plus one more stretch of steps and a
+ * save would exceed it. */
+static int stop_requested (double t0, double per_step, int stretch, double save_time)
+{
+   FILE *fp = fopen ("tmp/stop.flag", "rt");
+   if (!fp)
+      return 0;
+   int alarm = 0, limit = 0;
+   if (fscanf (fp, "%d %d", &alarm, &limit) != 2)
+      alarm = 0, limit = 0;
+   fclose (fp);
+   if (alarm)
+      return 1;
+   return limit > 0 && now () - t0 + per_step*stretch + save_time > limit;
+}
+
+int main (int argc, char **argv)
+{
+   int precision = MG_FP64, device = 0;
+   for (int a = 1 ; a < argc ; ++a) {
+      if (!strcmp (argv[a], "--fp32"))
+         precision = MG_FP32_OFFSET;
+      else if (!strcmp (argv[a], "--device") && a + 1 < argc)
+         device = atoi (argv[++a]);
+      else
+         die ("unknown option '%s' (usage: core_b200.out [--fp32] [--device N])", argv[a]);
+   }
+   const double t_start = now ();
+
+   FILE *fp = open_or_die ("run_mandor.cfg", "rt");
+   run_cfg_t cfg;
+   cfg.total = read_at_int (fp, "run_mandor.cfg");
+   cfg.full = read_at_int (fp, "run_mandor.cfg");
+   cfg.tecplot = read_at_int (fp, "run_mandor.cfg");
+   cfg.cont = (read_at_int (fp, "run_mandor.cfg") == 1);
+   cfg.stop = read_at_int (fp, "run_mandor.cfg");
+   cfg.spectr = read_at_int (fp, "run_mandor.cfg");
+   fclose (fp);
+   if (!cfg.total || !cfg.full || !cfg.tecplot || !cfg.stop || !cfg.spectr)
+      die ("'%s' contains zero step(s)", "run_mandor.cfg");
+
+   if (!(fp = fopen ("tmp/stop.flag", "rt"))) {
+      fp = open_or_die ("tmp/stop.flag", "wt");
+      fprintf (fp, "0\n%d\n", 23*60*60 + 30*60);
+   }
+   fclose (fp);
+
+   domain_t dom = read_domain ();
+   const int records = read_count ("binData/sys.N");
+   if (records < 1)
+      die ("%s", "initial checkpoint is not prepared");
+   int point = records - 1;
+   records_t rec;
+   if (cfg.cont && point != 0) {
+      rec.sys_num = records;
+      rec.map_num = read_count ("binData/fileMap.N");
+   } else {
+      point = 0;
+      rec.sys_num = 1;
+      rec.map_num = read_count ("binData/fileMap_start.txt");
+   }
+
+   char path[512];
+   snprintf (path, sizeof (path), "binData/sys_%06d.txt", point);
+   fp = open_or_die (path, "rt");
+   double time = read_at_double (fp, path);
+   fclose (fp);
+
+   mg_params_t p;
+   memset (&p, 0, sizeof (p));
+   for (int a = 0 ; a < 3 ; ++a) {
+      if (dom.dmin[a] != 0)
+         die ("%s", "domains not starting at node 0 are not supported");
+      p.n[a] = dom.dmax[a];
+      p.h[a] = dom.h[a];
+      p.bc_min[a] = dom.bcmin[a];
+      p.bc_max[a] = dom.bcmax[a];
+   }
+   p.tau = dom.tau;
+   p.time = time;
+   p.precision = precision;
+   p.device = device;
+   const long nodes = (long) (p.n[0] + 1)*(p.n[1] + 1)*(p.n[2] + 1);
+
+   snprintf (path, sizeof (path), "binData/sys_E_%06d(%03d).bin", point, 0);
+   double *E = read_mesh (path, rec.head_E, nodes);
+   snprintf (path, sizeof (path), "binData/sys_H_%06d(%03d).bin", point, 0);
+   double *H = read_mesh (path, rec.head_H, nodes);
+   snprintf (rec.prtn_src, sizeof (rec.prtn_src), "binData/sys_prtn_%06d.bin", point);
+   long long nm = 0;
+   snprintf (path, sizeof (path), "binData/plasma_%06d_%03d.bin", point, 0);
+   mg_marker_t *m = read_markers (path, &nm);
+   p.capacity = nm;
+
+   mg_run_t *run = NULL;
+   check (mg_run_create (&p, &run), "create run");
+   check (mg_run_set_fields (run, E, H), "upload fields");
+   check (mg_run_set_markers (run, m, nm), "upload markers");
+   check (mg_run_init (run), "init");
+   free (E);
+   free (H);
+   free (m);
+   const double save_time = now () - t_start;     /* loading time estimates saving time */
+
+   printf ("core_b200.out: %lld markers, %d x %d x %d cells, %s, record %d, t = %.6e\n", nm,
+           p.n[0], p.n[1], p.n[2], precision == MG_FP64 ? "FP64" : "FP32-offset", point, time);
+   int fresh_diag = !(cfg.cont && point != 0);
+   diag_t diag = {NULL, 0, 0};
+   double rows[6*256];
+   const double t_loop = now ();
+   double last_saved = -1;
+   int stop = 0, t = 0;
+   while (t < cfg.total && !stop) {
+      /* Advance to the next checkpoint, stop-flag check or the end. */
+      int next = cfg.total;
+      const int nfull = (t/cfg.full + 1)*cfg.full;
+      const int nstop = (t/cfg.stop + 1)*cfg.stop;
+      if (nfull < next) next = nfull;
+      if (nstop < next) next = nstop;
+      if (next - t > 256) next = t + 256;
+      const int k = next - t;
+      check (mg_run_step (run, k, rows), "step");
+      for (int q = 0 ; q < k ; ++q)
+         diag_add (&diag, rows + 6*q);
+      t = next;
+      time += k*dom.tau;
+      for (int q = 0 ; q < k ; ++q) {
+         const double *r = rows + 6*q;
+         if (isnan (r[1] + r[2] + r[3] + r[4] + r[5]))
+            die ("%s", "nan detected in the energies");
+      }
+      if (t % cfg.full == 0) {
+         checkpoint (run, &rec, &dom, nodes, time);
+         diag_flush (&diag, &fresh_diag, dom.tau);
+         last_saved = time;
+      }
+      if (t % cfg.stop == 0) {
+         const double per_step = (now () - t_loop)/t;
+         stop = stop_requested (t_start, per_step, cfg.stop, save_time);
+      }
+   }
+   const double loop = now () - t_loop;
+   printf ("main: main loop have taken %f sec.\n", loop);
+   if (last_saved != time) {
+      printf ("Additional check-point to save the final state.\n");
+      checkpoint (run, &rec, &dom, nodes, time);
+   }
+   diag_flush (&diag, &fresh_diag, dom.tau);
+   free (diag.rows);
+   check (mg_run_destroy (run), "destroy run");
+   remove ("tmp/stop.flag");
+   return EXIT_SUCCESS;
+}

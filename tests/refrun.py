@@ -92,6 +92,69 @@ def read_diag(path):
     return np.array(rows)
 
 
+def mesh_header(n, name, ghost=1, vector=True):
+    """Header of a checkpoint mesh file for a one-rank run: the valid region
+    (0,0,0)-(n) and the mesh_t struct of a mesh allocated over
+    [-ghost, n+ghost] (type_mesh.h:67-84; pointers zeroed)."""
+    lo = [-ghost] * 3
+    hi = [v + ghost for v in n]
+    w = [hi[a] - lo[a] + 1 for a in range(3)]
+    node = 24 if vector else 8
+    ints = [0, 0, 0, n[0], n[1], n[2],
+            lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], 1 if vector else 0,
+            w[2], w[1] * w[2], node * w[0] * w[1] * w[2]]
+    raw = np.array(ints, "<i4").tobytes() + b"\0" * 16
+    raw += name.encode().ljust(30, b"\0") + b"\0\0"
+    assert len(raw) == MESH_HEADER_BYTES
+    return raw
+
+
+def write_checkpoint0(root, n, h, tau, bc_min, bc_max, E, H, markers, time=0.0):
+    """The record-0 file set that core.out loads (what setup.out writes):
+    domain.bin, sys.N, sys_000000.txt, file maps, E/H meshes, markers."""
+    b = os.path.join(root, "binData")
+    for d in ("binData", "output/logs", "tmp"):
+        os.makedirs(os.path.join(root, d), exist_ok=True)
+    with open(os.path.join(b, "domain.bin"), "wb") as fp:
+        fp.write(np.array(list(h) + [n[a] * h[a] for a in range(3)] + [tau], "<f8").tobytes())
+        fp.write(np.array([0, 0, 0] + list(n) + list(bc_min) + list(bc_max), "<i4").tobytes())
+    with open(os.path.join(b, "sys.N"), "w") as fp:
+        fp.write("@ 1\t  system check-point records written.\n")
+    with open(os.path.join(b, "sys_000000.txt"), "w") as fp:
+        fp.write("@ %.14e    time.\n@ 1       cpus total.\n@ 1       file map id.\n"
+                 "That is checkpoint (record of the full system state) #0.\n" % time)
+    for i in (0, 1):
+        with open(os.path.join(b, "fileMap_%06d.txt" % i), "w") as fp:
+            fp.write("1 cpus total.\n0: (0 0 0) - (%d %d %d)\n" % tuple(n))
+    with open(os.path.join(b, "fileMap_start.txt"), "w") as fp:
+        fp.write("@ 2 filemaps are generated by setup - keep them on the start of simulation.\n")
+    with open(os.path.join(b, "fileMap.N"), "w") as fp:
+        fp.write("@ 2 filemaps total is written.\n")
+    # units.bin: the 15 doubles of units_save (misc_units.c:38-58) for a
+    # 1-micron wavelength; core.out only logs them.
+    c, m_e, e = 2.99792458e10, 9.1093826e-28, 4.8032044e-10
+    lam = 1e-4
+    t = lam / c
+    om = 2 * np.pi / t
+    A = m_e * c * om / e
+    n_u = m_e * om ** 2 / (16 * np.pi ** 3 * e ** 2)
+    wp = 2 * e * np.sqrt(np.pi * n_u / m_e) * t
+    units = [lam, c, t, om, A / (2 * np.pi), 0.0, A, n_u, e * n_u,
+             om ** 2 * m_e / (4 * np.pi * e ** 2), 0.0, 1e-4 / lam, 1e-15 / t, wp, 2 * np.pi / wp]
+    with open(os.path.join(b, "units.bin"), "wb") as fp:
+        fp.write(np.array(units, "<f8").tobytes())
+    write_mesh(os.path.join(b, "sys_E_000000(000).bin"), mesh_header(n, "vec_E"), E)
+    write_mesh(os.path.join(b, "sys_H_000000(000).bin"), mesh_header(n, "vec_H"), H)
+    write_markers(os.path.join(b, "plasma_000000_000.bin"), markers)
+
+
+def write_run_cfg(root, steps, full, stop=10 ** 8):
+    with open(os.path.join(root, "run_mandor.cfg"), "w") as fp:
+        fp.write("@ %d\ttotal steps\n@ %d\tcheckpoint period\n@ -1\ttecplot\n"
+                 "@ 0\tcontinue\n@ %d\tstop-flag period\n@ -100\tspectral dumps\n"
+                 % (steps, full, stop))
+
+
 def deck_text(n, L_um, tau, bc_min, bc_max, lambda_um=1.0):
     """A minimal setup deck: units, mesh and boundary tags only."""
     lines = ["[units]", "@ %r\tlambda [microns]" % lambda_um, "",
