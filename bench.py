@@ -52,6 +52,8 @@ FALLBACK_HBM_GBS = 6650.0
 def workload(name="laser_foil"):
     if name == "weibel":
         return weibel()
+    if name.startswith("weibel_") and name[7:].isdigit():
+        return weibel(int(name[7:]))
     if name != "laser_foil":
         raise SystemExit("unknown workload %r" % name)
     n = (256, 128, 128)
@@ -74,12 +76,14 @@ def workload(name="laser_foil"):
                 bytes_per_marker=100.0)
 
 
-def weibel():
+def weibel(side=256):
     """Counter-streaming electron beams (two-stream/Weibel), precision form:
     256^3 periodic cells, h = 0.05 c/omega_p at the total density n_cr,
     Courant 0.5, beams at u_x = +-0.2 (gamma v = 0.2/sqrt(1 - 0.04)) with
-    32 markers per cell each, thermal spread 0.01, 500 steps."""
-    n = (256, 256, 256)
+    32 markers per cell each, thermal spread 0.01, 500 steps.  Workload
+    "weibel_<side>" is the same plasma on side^3 cells (smaller cases for
+    profiling)."""
+    n = (side, side, side)
     hh = 0.05 / (2 * math.pi)
     h = (hh, hh, hh)
     tau = 0.5 / math.sqrt(3 / hh ** 2)
@@ -93,7 +97,7 @@ def weibel():
              drift=(-u, 0, 0), uth=(0.01, 0.01, 0.01), seed=(1802, 9373), skip=7 * each,
              id0=1 + each),
     ]
-    return dict(name="weibel_fp32_256cubed", n=n, h=h, tau=tau, bc=(0, 0, 0), species=species,
+    return dict(name="weibel_fp32_%dcubed" % side, n=n, h=h, tau=tau, bc=(0, 0, 0), species=species,
                 laser=None, markers=2 * each, total_steps=500, precision=1, dtype="f32",
                 bytes_per_marker=60.0)
 

@@ -82,7 +82,8 @@ typedef struct {
    int       precision;   /* MG_FP64 or MG_FP32_OFFSET                 */
    int       device;      /* CUDA device ordinal                       */
    long long capacity;    /* marker capacity (0: grows on upload)      */
-   int       sort_every;  /* re-sort markers by tile every k steps (0 = default) */
+   int       sort_every;  /* precision form: re-sort markers by tile every k
+                             steps (0 = every 8; < 0 = never, untiled push) */
 } mg_params_t;
 
 /* Analytic laser source: paraxial Gaussian beam, Ey polarised, moving along

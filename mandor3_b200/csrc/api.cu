@@ -306,11 +306,15 @@ extern "C" long long mg_estimate_bytes (const mg_params_t *p, long long markers)
       return -1;
    Grid g = make_grid (p->n, p->h, p->tau, p->bc_min, p->bc_max);
    const long long elt = (p->precision == MG_FP64) ? 8 : 4;
-   long long b = 9LL*g.total*elt;
+   long long b = 12LL*g.total*elt;
    for (int a = 0 ; a < 3 ; ++a)
       b += 2LL*4*elt*(p->n[(a + 1) % 3] + 2)*(p->n[(a + 2) % 3] + 2);
-   const long long per_marker = (p->precision == MG_FP64) ? 60 : 40;
+   // FP64: SoA records; precision form: two buffer sets (the sort scatters
+   // from one into the other) and 12 bytes of sort counters per cell.
+   const long long per_marker = (p->precision == MG_FP64) ? 60 : 80;
    b += (markers + markers/8 + 1024)*per_marker;
+   if (p->precision != MG_FP64)
+      b += 12LL*(p->n[0] + MG_TILE_X)*(p->n[1] + MG_TILE_Y)*(p->n[2] + MG_TILE_Z);
    b += (long long) MG_RING*6*8 + (1 << 20);
    return b;
 }
@@ -367,6 +371,17 @@ extern "C" int mg_run_create (const mg_params_t *params, mg_run_t **out)
          if (rc == MG_OK)
             cudaMemsetAsync (*mp, 0, mb, r->stream);
       }
+   if (rc == MG_OK && f32) {
+      const int T[3] = {MG_TILE_X, MG_TILE_Y, MG_TILE_Z};
+      r->ntiles = 1;
+      for (int a = 0 ; a < 3 ; ++a) {
+         r->tiles[a] = (params->n[a] + T[a] - 1)/T[a];
+         r->ntiles *= r->tiles[a];
+      }
+      rc = mg_dev_alloc (r, (void **) &r->tile_start, sizeof (int)*(r->ntiles + 2));
+      if (rc == MG_OK)
+         cudaMemsetAsync (r->tile_start, 0, sizeof (int)*(r->ntiles + 2), r->stream);
+   }
    if (rc == MG_OK) rc = mg_dev_alloc (r, (void **) &r->dsc, sizeof (DevScalars));
    if (rc == MG_OK) rc = mg_dev_alloc (r, (void **) &r->ring, sizeof (double)*6*MG_RING);
    if (rc == MG_OK) {
@@ -431,6 +446,7 @@ extern "C" int mg_run_destroy (mg_run_t *r)
    if (r->ring) cudaFree (r->ring);
    if (r->stage) cudaFree (r->stage);
    if (r->sort_tmp) cudaFree (r->sort_tmp);
+   if (r->tile_start) cudaFree (r->tile_start);
    for (int e = 0 ; e < 4 ; ++e)
       if (r->ev[e]) cudaEventDestroy (r->ev[e]);
    if (r->stream) cudaStreamDestroy (r->stream);
@@ -659,6 +675,14 @@ extern "C" int mg_run_init (mg_run_t *r)
    CHECK_RUN (r);
    TRY (is32 (r) ? mg_fields32_init (r) : mg_fields64_init (r));
    TRY (is32 (r) ? mg_walls32 (r) : mg_walls64 (r));
+   if (is32 (r)) {
+      // Order the markers by tile before the first step; the step graph
+      // takes the tiled push only while that order is known.  sort_every < 0
+      // keeps the upload order and the untiled push.
+      mg_drop_graphs (r);
+      if (r->prm.sort_every >= 0)
+         TRY (mg_sort32 (r));
+   }
    MG_CUDA (cudaStreamSynchronize (r->stream));
    r->inited = 1;
    r->stage_no = 0;
@@ -887,12 +911,14 @@ static int build_graph (mg_run_t *r)
    return MG_OK;
 }
 
-// Precision form: markers are re-sorted by cell every sort_every steps
-// (default 8) so that warps keep sharing cells; the sort runs between graph
-// launches on the run's stream.
+// Precision form: markers are re-sorted by tile and cell every sort_every
+// steps (default 8) so that tiles stay compact and warps keep sharing cells;
+// the sort runs between graph launches on the run's stream.
 static int maybe_sort (mg_run_t *r)
 {
    if (!is32 (r))
+      return MG_OK;
+   if (r->prm.sort_every < 0)
       return MG_OK;
    const int every = r->prm.sort_every > 0 ? r->prm.sort_every : 8;
    if (r->steps_since_sort++ < every)

@@ -135,22 +135,53 @@ __global__ void k_live_scan32 (const float *qm, long long from, long long n, lon
    }
 }
 
-// ---- counting sort by cell --------------------------------------------------
-// Key: linear index of the cell in the (n0+2)(n1+2)(n2+2) grid of cells
-// -1..n; removed markers go to one extra bucket at the end and are dropped.
-__device__ __forceinline__ int sort_key (const Grid &g, int c, float qm)
+// ---- counting sort by tile and cell ----------------------------------------
+// Key: tile index (tiles of MG_TILE_X x MG_TILE_Y x MG_TILE_Z cells, x-major)
+// times the cells per tile plus the cell within the tile, so that a tile's
+// markers are contiguous and, inside it, grouped by cell.  Markers in cells
+// outside [0, n) go to one bucket after the last tile (the push handles them
+// through global memory), removed markers to one more bucket at the end.
+struct TileKey {
+   int n[3], nty, ntz, ntiles;
+};
+
+__device__ __forceinline__ int sort_key (const TileKey &t, int c, float qm)
 {
    if (qm == 0.0f)
-      return (g.n[0] + 2)*(g.n[1] + 2)*(g.n[2] + 2);
-   const int i = unpack (c, 20) + 1, j = unpack (c, 10) + 1, k = unpack (c, 0) + 1;
-   return (i*(g.n[1] + 2) + j)*(g.n[2] + 2) + k;
+      return t.ntiles*MG_TILE_CELLS + 1;
+   const int i = unpack (c, 20), j = unpack (c, 10), k = unpack (c, 0);
+   if ((unsigned) i >= (unsigned) t.n[0] || (unsigned) j >= (unsigned) t.n[1] ||
+       (unsigned) k >= (unsigned) t.n[2])
+      return t.ntiles*MG_TILE_CELLS;
+   const int tile = ((i/MG_TILE_X)*t.nty + j/MG_TILE_Y)*t.ntz + k/MG_TILE_Z;
+   const int cell = ((i % MG_TILE_X)*MG_TILE_Y + j % MG_TILE_Y)*MG_TILE_Z + k % MG_TILE_Z;
+   return tile*MG_TILE_CELLS + cell;
 }
 
-__global__ void k_hist (Grid g, Markers32 m, long long np, int *count)
+// Marker count per key, and the largest |rho| (non-negative floats order
+// like their bit patterns).  Lanes with equal keys add once per warp.
+__global__ void k_hist (TileKey t, Markers32 m, long long np, int *count, DevScalars *dsc)
 {
-   for (long long n = blockIdx.x*(long long) blockDim.x + threadIdx.x ; n < np ;
-        n += (long long) gridDim.x*blockDim.x)
-      atomicAdd (count + sort_key (g, m.cell[n], m.qm[n]), 1);
+   const int lane = threadIdx.x & 31;
+   int rmax = 0;
+   const long long stride = (long long) gridDim.x*blockDim.x;
+   for (long long base = blockIdx.x*(long long) blockDim.x + (threadIdx.x & ~31) ; base < np ; base += stride) {
+      const long long n = base + lane;
+      int key = -1 - lane;
+      if (n < np) {
+         const float qm = m.qm[n];
+         key = sort_key (t, m.cell[n], qm);
+         if (qm != 0.0f)
+            rmax = max (rmax, __float_as_int (fabsf (m.rho[n])));
+      }
+      const unsigned peers = __match_any_sync (0xffffffffu, key);
+      if (key >= 0 && lane == __ffs (peers) - 1)
+         atomicAdd (count + key, __popc (peers));
+   }
+   for (int d = 16 ; d > 0 ; d >>= 1)
+      rmax = max (rmax, __shfl_xor_sync (0xffffffffu, rmax, d));
+   if (lane == 0 && rmax > 0)
+      atomicMax ((int *) &dsc->rho_max, rmax);
 }
 
 // Three-pass exclusive scan of `count` (length len) in place.
@@ -213,33 +244,92 @@ __global__ void k_scan_apply (int *count, long long len, const long long *block_
       }
 }
 
-__global__ void k_rank (Grid g, Markers32 m, long long np, long long *offset, int *perm)
+// First marker of every tile, of the outside bucket and of the removed bucket
+// (before k_rank advances the offsets).
+__global__ void k_tile_start (const long long *offset, int ntiles, int *tile_start)
 {
-   for (long long n = blockIdx.x*(long long) blockDim.x + threadIdx.x ; n < np ;
-        n += (long long) gridDim.x*blockDim.x) {
-      const int key = sort_key (g, m.cell[n], m.qm[n]);
-      perm[n] = (int) atomicAdd ((unsigned long long *) (offset + key), 1ULL);
-   }
+   for (int t = blockIdx.x*blockDim.x + threadIdx.x ; t <= ntiles + 1 ; t += gridDim.x*blockDim.x)
+      tile_start[t] = (int) offset[t <= ntiles ? (long long) t*MG_TILE_CELLS : (long long) ntiles*MG_TILE_CELLS + 1];
 }
 
-template <typename V>
-__global__ void k_permute (const V *src, V *dst, const int *perm, long long np)
+// Moves every marker to its place in the other buffer set: the first free
+// slot of its key (lanes with equal keys take consecutive slots).
+__global__ void k_scatter (TileKey t, Markers32 m, Markers32 o, long long np, long long *offset)
 {
-   for (long long n = blockIdx.x*(long long) blockDim.x + threadIdx.x ; n < np ;
-        n += (long long) gridDim.x*blockDim.x)
-      dst[perm[n]] = src[n];
+   const int lane = threadIdx.x & 31;
+   const long long stride = (long long) gridDim.x*blockDim.x;
+   for (long long base = blockIdx.x*(long long) blockDim.x + (threadIdx.x & ~31) ; base < np ; base += stride) {
+      const long long n = base + lane;
+      int key = -1 - lane, cell = 0;
+      float qm = 0.0f;
+      if (n < np) {
+         cell = m.cell[n];
+         qm = m.qm[n];
+         key = sort_key (t, cell, qm);
+      }
+      const unsigned peers = __match_any_sync (0xffffffffu, key);
+      const int leader = __ffs (peers) - 1;
+      long long at = 0;
+      if (key >= 0 && lane == leader)
+         at = (long long) atomicAdd ((unsigned long long *) (offset + key), (unsigned long long) __popc (peers));
+      at = __shfl_sync (0xffffffffu, at, leader) + __popc (peers & ((1u << lane) - 1));
+      if (key >= 0) {
+         o.cell[at] = cell;
+         o.qm[at] = qm;
+         o.ox[at] = m.ox[n];
+         o.oy[at] = m.oy[n];
+         o.oz[at] = m.oz[n];
+         o.ux[at] = m.ux[n];
+         o.uy[at] = m.uy[n];
+         o.uz[at] = m.uz[n];
+         o.rho[at] = m.rho[n];
+         o.id[at] = m.id[n];
+      }
+   }
 }
 
 } // namespace
 
-void mg_free_markers32 (mg_run_t *r)
+static void free_set (Markers32 &m)
 {
-   void *ptrs[] = {r->m32.cell, r->m32.ox, r->m32.oy, r->m32.oz, r->m32.ux, r->m32.uy, r->m32.uz,
-                   r->m32.rho, r->m32.qm, r->m32.id};
+   void *ptrs[] = {m.cell, m.ox, m.oy, m.oz, m.ux, m.uy, m.uz, m.rho, m.qm, m.id};
    for (void *p : ptrs)
       if (p)
          cudaFree (p);
-   memset (&r->m32, 0, sizeof (r->m32));
+   memset (&m, 0, sizeof (m));
+}
+
+static int alloc_set (mg_run_t *r, Markers32 &m, long long cap)
+{
+   memset (&m, 0, sizeof (m));
+   void **d[] = {(void **) &m.cell, (void **) &m.ox, (void **) &m.oy, (void **) &m.oz,
+                 (void **) &m.ux, (void **) &m.uy, (void **) &m.uz, (void **) &m.rho,
+                 (void **) &m.qm, (void **) &m.id};
+   for (void **p : d)
+      TRY32 (mg_dev_alloc (r, p, (size_t) cap*4));
+   return MG_OK;
+}
+
+void mg_free_markers32 (mg_run_t *r)
+{
+   free_set (r->m32);
+   free_set (r->m32b);
+}
+
+namespace {
+__global__ void k_publish (DevScalars *dsc, Markers32 m)
+{
+   dsc->m32 = m;
+}
+} // namespace
+
+// Makes the current buffer set the one the step graph's kernels read (in
+// stream order, without waiting for the host).
+int mg_publish_markers32 (mg_run_t *r)
+{
+   k_publish<<<1, 1, 0, r->stream>>> (r->dsc, r->m32);
+   MG_LAUNCH_CHECK ();
+   return MG_OK;
 }
 
 int mg_ensure_capacity32 (mg_run_t *r, long long need)
@@ -253,28 +343,32 @@ int mg_ensure_capacity32 (mg_run_t *r, long long need)
    long long cap = need + need/8 + 1024;
    if (cap >= (1LL << 31) - 1)
       cap = (1LL << 31) - 2;
-   Markers32 nm;
-   memset (&nm, 0, sizeof (nm));
-   void **d[] = {(void **) &nm.cell, (void **) &nm.ox, (void **) &nm.oy, (void **) &nm.oz,
-                 (void **) &nm.ux, (void **) &nm.uy, (void **) &nm.uz, (void **) &nm.rho,
-                 (void **) &nm.qm, (void **) &nm.id};
-   for (void **p : d)
-      TRY32 (mg_dev_alloc (r, p, (size_t) cap*4));
+   Markers32 nm, nb;
+   int rc = alloc_set (r, nm, cap);
+   if (rc == MG_OK)
+      rc = alloc_set (r, nb, cap);
+   if (rc != MG_OK) {
+      free_set (nm);
+      free_set (nb);
+      return rc;
+   }
    if (r->m32.cell && r->np > 0) {
       void *src[] = {r->m32.cell, r->m32.ox, r->m32.oy, r->m32.oz, r->m32.ux, r->m32.uy, r->m32.uz,
                      r->m32.rho, r->m32.qm, r->m32.id};
+      void *dst[] = {nm.cell, nm.ox, nm.oy, nm.oz, nm.ux, nm.uy, nm.uz, nm.rho, nm.qm, nm.id};
       for (int q = 0 ; q < 10 ; ++q)
-         MG_CUDA (cudaMemcpyAsync (*d[q], src[q], r->np*4, cudaMemcpyDeviceToDevice, r->stream));
+         MG_CUDA (cudaMemcpyAsync (dst[q], src[q], r->np*4, cudaMemcpyDeviceToDevice, r->stream));
       MG_CUDA (cudaStreamSynchronize (r->stream));
    }
    if (r->m32.cell) {
-      r->dev_bytes -= (long long) r->cap*40;
+      r->dev_bytes -= (long long) r->cap*80;
       mg_free_markers32 (r);
    }
    r->m32 = nm;
+   r->m32b = nb;
    r->cap = cap;
    mg_drop_graphs (r);
-   return MG_OK;
+   return mg_publish_markers32 (r);
 }
 
 int mg_run_set_fields32 (mg_run_t *r, const double *E, const double *H)
@@ -344,6 +438,7 @@ int mg_run_set_markers32 (mg_run_t *r, const mg_marker_t *m, long long n)
       MG_LAUNCH_CHECK ();
    }
    r->np = n;
+   r->tiles_ok = 0;
    MG_CUDA (cudaMemsetAsync (&r->dsc->dead, 0, sizeof (long long), r->stream));
    MG_CUDA (cudaStreamSynchronize (r->stream));
    return MG_OK;
@@ -403,6 +498,7 @@ int mg_place64 (mg_run_t *r, const mg_place_t *spec, long long at, long long cou
 
 int mg_place32 (mg_run_t *r, const mg_place_t *spec, long long at, long long count)
 {
+   r->tiles_ok = 0;
    // Place in FP64 into staging in chunks of up to 2^26 markers (4.3 GB of
    // staging; larger chunks keep the host jump-ahead per chunk cheap), then
    // convert.
@@ -472,14 +568,25 @@ void mg_convert64to32 (mg_run_t *r, const Markers64 &v, long long c, long long a
    k_convert<<<mg_blocks_for (c, 256, 8), 256, 0, r->stream>>> (r->g, v, c, r->m32, at);
 }
 
-// Sorts live markers by cell and drops removed ones.
+// Sorts the markers by tile and cell into the other buffer set and makes
+// that set current; removed markers go to the end.
 int mg_sort32 (mg_run_t *r)
 {
-   if (r->np == 0)
+   if (r->np == 0) {
+      MG_CUDA (cudaMemsetAsync (r->tile_start, 0, sizeof (int)*(r->ntiles + 2), r->stream));
+      r->tiles_ok = 1;
+      r->steps_since_sort = 0;
       return MG_OK;
-   const long long cells = (long long) (r->g.n[0] + 2)*(r->g.n[1] + 2)*(r->g.n[2] + 2) + 1;
+   }
+   TileKey tk;
+   for (int a = 0 ; a < 3 ; ++a)
+      tk.n[a] = r->g.n[a];
+   tk.nty = r->tiles[1];
+   tk.ntz = r->tiles[2];
+   tk.ntiles = r->ntiles;
+   const long long cells = (long long) r->ntiles*MG_TILE_CELLS + 2;
    const int nb = (int) ((cells + SCAN_CHUNK - 1)/SCAN_CHUNK);
-   const size_t need = (size_t) cells*4 + (size_t) cells*8 + (size_t) nb*8 + (size_t) r->np*4 + (size_t) r->np*4 + 1024;
+   const size_t need = (size_t) cells*4 + (size_t) cells*8 + (size_t) nb*8 + 1024;
    if (r->sort_tmp_bytes < need) {
       if (r->sort_tmp) {
          cudaFree (r->sort_tmp);
@@ -492,29 +599,25 @@ int mg_sort32 (mg_run_t *r)
    char *p = (char *) r->sort_tmp;
    int *count = (int *) p;                        p += ((size_t) cells*4 + 255) & ~(size_t) 255;
    long long *offset = (long long *) p;           p += ((size_t) cells*8 + 255) & ~(size_t) 255;
-   long long *bsum = (long long *) p;             p += ((size_t) nb*8 + 255) & ~(size_t) 255;
-   int *perm = (int *) p;                         p += ((size_t) r->np*4 + 255) & ~(size_t) 255;
-   void *tmp = p;
+   long long *bsum = (long long *) p;
    MG_CUDA (cudaMemsetAsync (count, 0, (size_t) cells*4, r->stream));
+   MG_CUDA (cudaMemsetAsync (&r->dsc->rho_max, 0, sizeof (float), r->stream));
    const int T = 256;
-   k_hist<<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (r->g, r->m32, r->np, count);
+   k_hist<<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (tk, r->m32, r->np, count, r->dsc);
    k_scan_blocks<<<nb, 256, 0, r->stream>>> (count, cells, bsum);
    k_scan_sums<<<1, 32, 0, r->stream>>> (bsum, nb);
    k_scan_apply<<<nb, 256, 0, r->stream>>> (count, cells, bsum, offset);
-   k_rank<<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (r->g, r->m32, r->np, offset, perm);
+   k_tile_start<<<mg_blocks_for (r->ntiles + 2, T, 8), T, 0, r->stream>>> (offset, r->ntiles, r->tile_start);
+   k_scatter<<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (tk, r->m32, r->m32b, r->np, offset);
    MG_LAUNCH_CHECK ();
-   void **arrs[] = {(void **) &r->m32.cell, (void **) &r->m32.ox, (void **) &r->m32.oy, (void **) &r->m32.oz,
-                    (void **) &r->m32.ux, (void **) &r->m32.uy, (void **) &r->m32.uz,
-                    (void **) &r->m32.rho, (void **) &r->m32.qm, (void **) &r->m32.id};
-   for (void **a : arrs) {
-      k_permute<int><<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> ((const int *) *a, (int *) tmp, perm, r->np);
-      MG_LAUNCH_CHECK ();
-      MG_CUDA (cudaMemcpyAsync (*a, tmp, (size_t) r->np*4, cudaMemcpyDeviceToDevice, r->stream));
-   }
+   const Markers32 t = r->m32;
+   r->m32 = r->m32b;
+   r->m32b = t;
    // Removed markers now sit at the end; they stay there (the step graph
    // holds the marker count) and are dropped on download.
    r->steps_since_sort = 0;
-   return MG_OK;
+   r->tiles_ok = 1;
+   return mg_publish_markers32 (r);
 }
 
 int mg_enqueue_step32 (mg_run_t *r, int part)

@@ -20,6 +20,19 @@
 #define MG_GX 2
 #define MG_GZ_FRONT 4
 
+// Precision-form tiles: markers are counting-sorted by (tile, cell) and the
+// push stages one tile of fields and currents in shared memory at a time.
+#ifndef MG_TILE_X
+#define MG_TILE_X 8
+#endif
+#ifndef MG_TILE_Y
+#define MG_TILE_Y 8
+#endif
+#ifndef MG_TILE_Z
+#define MG_TILE_Z 4
+#endif
+#define MG_TILE_CELLS (MG_TILE_X*MG_TILE_Y*MG_TILE_Z)
+
 struct Grid {
    int    n[3];
    long   sx, sy;          // strides of i and j (k stride is 1)
@@ -55,6 +68,15 @@ static inline Grid make_grid (const int n[3], const double h[3], double tau,
    return g;
 }
 
+// FP32-offset particle arrays.
+struct Markers32 {
+   int    *cell;           // packed cell ((i+1) << 20 | (j+1) << 10 | (k+1))
+   float  *ox, *oy, *oz;   // offsets in [0,1) in units of h
+   float  *ux, *uy, *uz;
+   float  *rho, *qm;
+   int    *id;
+};
+
 // Device-side per-run scalars (one small allocation).
 struct DevScalars {
    double time;            // t = n*tau of the step being advanced
@@ -64,6 +86,10 @@ struct DevScalars {
    int    err;             // sticky error flags (1: start cell outside the
                            // ghost layers, 2: more than one cell per step)
    int    err_info[4];     // first offending marker index and cell
+   int    tile_next;       // next tile to hand out in the tiled push
+   float  rho_max;         // largest |rho| of the markers at the last sort
+   Markers32 m32;          // the current marker buffer set (precision form),
+                           // read by the kernels of the step graph
 };
 
 #define MG_RING 4096       // energy rows kept on the device between copies
@@ -75,14 +101,6 @@ struct Markers64 {
    int    *id;
 };
 
-// FP32-offset particle arrays.
-struct Markers32 {
-   int    *cell;           // linear cell index i*ny*nz + j*nz + k
-   float  *ox, *oy, *oz;   // offsets in [0,1) in units of h
-   float  *ux, *uy, *uz;
-   float  *rho, *qm;
-   int    *id;
-};
 
 struct mg_run {
    mg_params_t prm;
@@ -100,11 +118,18 @@ struct mg_run {
    // markers
    long long  np, cap;
    Markers64  m64;
-   Markers32  m32;
+   Markers32  m32;         // current buffer set (precision form)
+   Markers32  m32b;        // the other set: the sort scatters into it
    void      *sort_tmp;    // scratch for sorting / compaction
    size_t     sort_tmp_bytes;
-   int       *tile_key;
    long long  steps_since_sort;
+   int        tiles[3];    // tiles per axis (precision form)
+   int        ntiles;
+   int       *tile_start;  // ntiles + 2 marker offsets of the last sort:
+                           // tile t holds [tile_start[t], tile_start[t+1]),
+                           // then the markers outside the mesh, then the
+                           // removed ones
+   int        tiles_ok;    // tile_start describes the marker order
 
    // scalars and energy ring
    DevScalars *dsc;
@@ -192,6 +217,7 @@ int mg_walls32 (mg_run_t *r);
 int mg_enqueue_step32 (mg_run_t *r, int part);
 int mg_place32 (mg_run_t *r, const mg_place_t *spec, long long at, long long count);
 int mg_ensure_capacity32 (mg_run_t *r, long long need);
+int mg_publish_markers32 (mg_run_t *r);
 void mg_free_markers32 (mg_run_t *r);
 int mg_dev_alloc (mg_run_t *r, void **p, size_t bytes);
 int mg_ensure_stage (mg_run_t *r, size_t bytes);

@@ -146,18 +146,62 @@ __device__ __forceinline__ void deposit_piece (const Ctx32 &c, float rho, int i,
       }                                                                      \
    } while (0)
 
+// Block sums of the thermal tally and of the removed-marker count, added
+// to the run's accumulators.
+__device__ __forceinline__ void block_tally (double Wx, double Wy, double Wz, long long dead,
+                                             DevScalars *dsc)
+{
+   __shared__ double sw[3][32];
+   const int lane = threadIdx.x & 31;
+   for (int d = 16 ; d > 0 ; d >>= 1) {
+      Wx += __shfl_xor_sync (0xffffffffu, Wx, d);
+      Wy += __shfl_xor_sync (0xffffffffu, Wy, d);
+      Wz += __shfl_xor_sync (0xffffffffu, Wz, d);
+      dead += __shfl_xor_sync (0xffffffffu, dead, d);
+   }
+   const int wid = threadIdx.x >> 5;
+   if (lane == 0) {
+      sw[0][wid] = Wx;
+      sw[1][wid] = Wy;
+      sw[2][wid] = Wz;
+      if (dead)
+         atomicAdd ((unsigned long long *) &dsc->dead, (unsigned long long) dead);
+   }
+   __syncthreads ();
+   if (wid == 0) {
+      const int nw = blockDim.x >> 5;
+      Wx = lane < nw ? sw[0][lane] : 0;
+      Wy = lane < nw ? sw[1][lane] : 0;
+      Wz = lane < nw ? sw[2][lane] : 0;
+      for (int d = 16 ; d > 0 ; d >>= 1) {
+         Wx += __shfl_xor_sync (0xffffffffu, Wx, d);
+         Wy += __shfl_xor_sync (0xffffffffu, Wy, d);
+         Wz += __shfl_xor_sync (0xffffffffu, Wz, d);
+      }
+      if (lane == 0) {
+         atomicAdd (&dsc->acc[2], Wx);
+         atomicAdd (&dsc->acc[3], Wy);
+         atomicAdd (&dsc->acc[4], Wz);
+      }
+   }
+}
+
+// Markers [0, np), or [range[0], range[1]) when range is given (the markers
+// that the tiled push leaves to global memory).
 __global__ void __launch_bounds__ (256, 3)
-k_push32 (Ctx32 c, Markers32 m, long long np, DevScalars *dsc)
+k_push32 (Ctx32 c, long long np, const int *range, DevScalars *dsc)
 {
    const Grid &g = c.g;
+   const Markers32 m = dsc->m32;
    const int lane = threadIdx.x & 31;
    double Wx = 0, Wy = 0, Wz = 0;
    long long dead = 0;
    const long long warps_total = ((long long) gridDim.x*blockDim.x) >> 5;
    const long long warp0 = ((long long) blockIdx.x*blockDim.x + threadIdx.x) >> 5;
-   for (long long base = warp0*32 ; base < np ; base += warps_total*32) {
+   const long long lo = range ? range[0] : 0, hi = range ? range[1] : np;
+   for (long long base = lo + warp0*32 ; base < hi ; base += warps_total*32) {
       const long long n = base + lane;
-      bool valid = n < np;
+      bool valid = n < hi;
       float qm = 0.0f;
       if (valid) {
          qm = m.qm[n];
@@ -321,38 +365,7 @@ k_push32 (Ctx32 c, Markers32 m, long long np, DevScalars *dsc)
       }
    }
 
-   __shared__ double sw[3][8];
-   for (int d = 16 ; d > 0 ; d >>= 1) {
-      Wx += __shfl_xor_sync (0xffffffffu, Wx, d);
-      Wy += __shfl_xor_sync (0xffffffffu, Wy, d);
-      Wz += __shfl_xor_sync (0xffffffffu, Wz, d);
-      dead += __shfl_xor_sync (0xffffffffu, dead, d);
-   }
-   const int wid = threadIdx.x >> 5;
-   if (lane == 0) {
-      sw[0][wid] = Wx;
-      sw[1][wid] = Wy;
-      sw[2][wid] = Wz;
-      if (dead)
-         atomicAdd ((unsigned long long *) &dsc->dead, (unsigned long long) dead);
-   }
-   __syncthreads ();
-   if (wid == 0) {
-      const int nw = blockDim.x >> 5;
-      Wx = lane < nw ? sw[0][lane] : 0;
-      Wy = lane < nw ? sw[1][lane] : 0;
-      Wz = lane < nw ? sw[2][lane] : 0;
-      for (int d = 16 ; d > 0 ; d >>= 1) {
-         Wx += __shfl_xor_sync (0xffffffffu, Wx, d);
-         Wy += __shfl_xor_sync (0xffffffffu, Wy, d);
-         Wz += __shfl_xor_sync (0xffffffffu, Wz, d);
-      }
-      if (lane == 0) {
-         atomicAdd (&dsc->acc[2], Wx);
-         atomicAdd (&dsc->acc[3], Wy);
-         atomicAdd (&dsc->acc[4], Wz);
-      }
-   }
+   block_tally (Wx, Wy, Wz, dead, dsc);
 }
 
 // Particle walls once at load time (plasma_init, core/plasma.c:399-404).
@@ -386,7 +399,423 @@ __global__ void k_walls32 (Grid g, Markers32 m, long long np, DevScalars *dsc)
       atomicAdd ((unsigned long long *) &dsc->dead, (unsigned long long) dead);
 }
 
+// ---- tiled push --------------------------------------------------------------
+// Markers are ordered by tile and cell (mg_sort32).  One CTA takes a tile at
+// a time: it copies the E and H nodes around the tile into shared memory,
+// pushes the tile's markers with gathers from there, accumulates their
+// currents in a shared-memory copy of the tile's J nodes and adds that copy
+// to J once per chunk of markers.  A marker may have drifted up to one cell
+// outside its tile since the sort; further than that, it takes the
+// global-memory path.
+//
+// The shared copy of J is fixed point in 32-bit integers, because integer
+// shared-memory atomics are single instructions on this GPU while FP32 ones
+// are compare-and-swap loops.  One marker adds at most (13/12) |rho| to any
+// node over its whole path (|qx| = |rho v_x| <= |rho| and each weight factor
+// lies in [-1/12, 13/12]), so with a quantum of 1.125 rho_max / Q for a
+// chunk of L markers and Q = min(2^21, 2^30 / L), no node sum can leave the
+// int32 range.  Contributions round to the nearest quantum: at most
+// 2^-22 of the largest single contribution for chunks of up to 512 markers,
+// 2^-17 at the 16384-marker limit.
+#define MG_TILE_CHUNK 16384
+
+// Asynchronous 4-byte copies global -> shared (completion per thread).
+__device__ __forceinline__ void cp_async4 (void *sm, const void *gm)
+{
+   asm volatile ("cp.async.ca.shared.global [%0], [%1], 4;"
+                 :: "r" ((unsigned) __cvta_generic_to_shared (sm)), "l" (gm) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit ()
+{
+   asm volatile ("cp.async.commit_group;" ::: "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait1 ()
+{
+   asm volatile ("cp.async.wait_group 1;" ::: "memory");
+}
+
+// Starts the copy of marker n's nine pushed arrays into buffer b (the lane's
+// column of the warp's staging area); n < 0: nothing to copy.
+__device__ __forceinline__ void stage_marker (float *b, int lane, const Markers32 &m, int n)
+{
+   if (n >= 0) {
+      cp_async4 (b + 0*32 + lane, m.cell + n);
+      cp_async4 (b + 1*32 + lane, m.qm + n);
+      cp_async4 (b + 2*32 + lane, m.ox + n);
+      cp_async4 (b + 3*32 + lane, m.oy + n);
+      cp_async4 (b + 4*32 + lane, m.oz + n);
+      cp_async4 (b + 5*32 + lane, m.ux + n);
+      cp_async4 (b + 6*32 + lane, m.uy + n);
+      cp_async4 (b + 7*32 + lane, m.uz + n);
+      cp_async4 (b + 8*32 + lane, m.rho + n);
+   }
+   cp_async_commit ();
+}
+
+template <int TX, int TY, int TZ>
+struct TileDims {
+   // E, H nodes [x0-1, x0+TX+3): cells x0-1 .. x0+TX and the CIC stencil of
+   // the half-shifted components.
+   static constexpr int FX = TX + 4, FY = TY + 4, FZ = TZ + 4;
+   static constexpr int FYZ = FY*FZ, FN = FX*FYZ;
+   // J nodes [x0-2, x0+TX+3): a marker of cell x0-1 or x0+TX that moves one
+   // more cell.
+   static constexpr int JX = TX + 5, JY = TY + 5, JZ = TZ + 5;
+   static constexpr int JYZ = JY*JZ, JN = JX*JYZ;
+   // Per warp: two buffers of the nine marker arrays a push reads, 32 lanes each.
+   static constexpr int STAGE = 2*9*32;
+   static constexpr size_t BYTES = (6*FN + 3*JN + 8*STAGE)*sizeof (float);
+};
+
+template <int SX, int SY>
+__device__ __forceinline__ float cic_s (const float *F, int q, float sx, float sy, float sz)
+{
+   const float f0 = F[q], f1 = F[q + SX], f2 = F[q + SY], f3 = F[q + SX + SY];
+   const float f4 = F[q + 1], f5 = F[q + SX + 1], f6 = F[q + SY + 1], f7 = F[q + SX + SY + 1];
+   const float a00 = f0 + sx*(f1 - f0), a10 = f2 + sx*(f3 - f2);
+   const float a01 = f4 + sx*(f5 - f4), a11 = f6 + sx*(f7 - f6);
+   const float b0 = a00 + sy*(a10 - a00), b1 = a01 + sy*(a11 - a01);
+   return b0 + sz*(b1 - b0);
+}
+
+// Round w*S to the nearest integer (|w S| < 2^22): the sum with 1.5 * 2^23
+// has unit spacing, so its bit pattern minus that of 1.5 * 2^23 is the result.
+__device__ __forceinline__ int fixed (float w, float S)
+{
+   return __float_as_int (fmaf (w, S, 12582912.0f)) - 0x4B400000;
+}
+
+// Offset of weight `slot` (0..11) from the cell's node in the shared copy:
+// the same nodes and order as scatter32 (Jx at (i+1, j+a, k+b), Jy at
+// (i+a, j+1, k+b), Jz at (i+a, j+b, k+1)).
+template <class D>
+__device__ __forceinline__ int slot_offset (int slot)
+{
+   const int comp = slot >> 2, e = slot & 3, a = e & 1, b = e >> 1;
+   const int off = comp == 0 ? D::JYZ + a*D::JZ + b
+                 : comp == 1 ? D::JZ + a*D::JYZ + b
+                 :             1 + a*D::JYZ + b*D::JZ;
+   return comp*D::JN + off;
+}
+
+template <class D>
+__device__ __forceinline__ void scatter_s (int *Jt, int q, const float w[12], float S)
+{
+#pragma unroll
+   for (int s = 0 ; s < 12 ; ++s) {
+      const int comp = s >> 2, e = s & 3, a = e & 1, b = e >> 1;
+      const int off = comp*D::JN + (comp == 0 ? D::JYZ + a*D::JZ + b
+                                  : comp == 1 ? D::JZ + a*D::JYZ + b
+                                  :             1 + a*D::JYZ + b*D::JZ);
+      atomicAdd (Jt + q + off, fixed (w[s], S));
+   }
+}
+
+// Warp sum of sixteen integers per lane, transposed: afterwards lane l
+// holds the sum over all lanes of v[(l >> 1) & 15].  Each halving step sends
+// the half of the slots that the partner lane keeps: 16 shuffles in all.
+__device__ __forceinline__ int transpose_sum16 (int v[16], int lane)
+{
+#pragma unroll
+   for (int h = 8, d = 16 ; h >= 1 ; h >>= 1, d >>= 1) {
+      const bool up = lane & d;
+#pragma unroll
+      for (int s = 0 ; s < h ; ++s) {
+         const int send = up ? v[s] : v[s + h];
+         const int keep = up ? v[s + h] : v[s];
+         v[s] = keep + __shfl_xor_sync (0xffffffffu, send, d);
+      }
+   }
+   return v[0] + __shfl_xor_sync (0xffffffffu, v[0], 1);
+}
+
+template <int TX, int TY, int TZ, int ROUNDS>
+__global__ void __launch_bounds__ (256, 3)
+k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, DevScalars *dsc)
+{
+   const Markers32 m = dsc->m32;
+   using D = TileDims<TX, TY, TZ>;
+   extern __shared__ float smem[];
+   float *F = smem;                           // Ex Ey Ez Hx Hy Hz, D::FN each
+   int *Jt = (int *) (smem + 6*D::FN);        // Jx Jy Jz, D::JN each
+   float *stg = smem + 6*D::FN + 3*D::JN + (threadIdx.x >> 5)*D::STAGE;
+   __shared__ int s_tile;
+   const Grid &g = c.g;
+   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+   const int slot = (lane >> 1) & 15;
+   const int soff = slot < 12 ? slot_offset<D> (slot) : 0;
+   const bool slot_lane = !(lane & 1) && slot < 12;
+   const float rmax = 1.125f*dsc->rho_max;
+   double Wx = 0, Wy = 0, Wz = 0;
+   long long dead = 0;
+
+   for (;;) {
+      if (threadIdx.x == 0)
+         s_tile = atomicAdd (&dsc->tile_next, 1);
+      __syncthreads ();
+      const int t = s_tile;
+      if (t >= ntiles)
+         break;
+      const int mb = tile_start[t], me = tile_start[t + 1];
+      if (mb < me) {
+         const int x0 = (t/(nty*ntz))*TX, y0 = ((t/ntz) % nty)*TY, z0 = (t % ntz)*TZ;
+
+         // Stage E and H nodes [x0-1, x0+TX+3) x ... (inside the ghost layers).
+         for (int q = threadIdx.x ; q < 6*D::FN ; q += blockDim.x) {
+            const int comp = q/D::FN, rem = q - comp*D::FN;
+            const int a = rem/D::FYZ, r2 = rem - a*D::FYZ, b = r2/D::FZ, cc = r2 - b*D::FZ;
+            const int gi = x0 - 1 + a, gj = y0 - 1 + b, gk = z0 - 1 + cc;
+            float v = 0.0f;
+            if (gi <= g.n[0] + MG_GX && gj <= g.n[1] + MG_GX && gk <= g.n[2] + MG_GX) {
+               const float *src = comp == 0 ? c.E0 : comp == 1 ? c.E1 : comp == 2 ? c.E2
+                                : comp == 3 ? c.H0 : comp == 4 ? c.H1 : c.H2;
+               v = __ldg (src + g.at (gi, gj, gk));
+            }
+            F[q] = v;
+         }
+
+         for (int cb = mb ; cb < me ; cb += MG_TILE_CHUNK) {
+            const int ce = min (cb + MG_TILE_CHUNK, me);
+            const float Q = fminf (2097152.0f, 1073741824.0f/(float) (ce - cb));
+            const float S = rmax > 0.0f ? Q/rmax : 0.0f;
+            for (int q = threadIdx.x ; q < 3*D::JN ; q += blockDim.x)
+               Jt[q] = 0;
+            __syncthreads ();
+
+            // Each warp copies its next 32 markers into shared memory while
+            // it pushes the current ones.
+            stage_marker (stg, lane, m, cb + wid*32 + lane < ce ? cb + wid*32 + lane : -1);
+            int it = 0;
+            for (int base = cb + wid*32 ; base < ce ; base += nw*32, ++it) {
+               const int n = base + lane;
+               const int nn = n + nw*32;
+               stage_marker (stg + ((it + 1) & 1)*(D::STAGE/2), lane, m, nn < ce ? nn : -1);
+               cp_async_wait1 ();
+               const float *cur = stg + (it & 1)*(D::STAGE/2) + lane;
+               bool valid = n < ce;
+               float qm = 0.0f;
+               if (valid) {
+                  qm = cur[1*32];
+                  valid = (qm != 0.0f);
+               }
+               int i = 0, j = 0, k = 0, di = 0, dj = 0, dk = 0;
+               float ox = 0, oy = 0, oz = 0, dx = 0, dy = 0, dz = 0, rho = 0;
+               bool fast = false;
+               if (valid) {
+                  const int cell = __float_as_int (cur[0]);
+                  i = unpack (cell, 20);
+                  j = unpack (cell, 10);
+                  k = unpack (cell, 0);
+                  fast = (unsigned) (i - x0 + 1) <= (unsigned) (TX + 1) &&
+                         (unsigned) (j - y0 + 1) <= (unsigned) (TY + 1) &&
+                         (unsigned) (k - z0 + 1) <= (unsigned) (TZ + 1);
+                  if (!fast && (i < -1 || i > g.n[0] || j < -1 || j > g.n[1] || k < -1 || k > g.n[2])) {
+                     if (atomicOr (&dsc->err, 1) == 0) {
+                        dsc->err_info[0] = n;
+                        dsc->err_info[1] = i;
+                        dsc->err_info[2] = j;
+                        dsc->err_info[3] = k;
+                     }
+                     valid = false;
+                  }
+               }
+               if (valid) {
+                  ox = cur[2*32];
+                  oy = cur[3*32];
+                  oz = cur[4*32];
+                  const int hx = ox >= 0.5f, hy = oy >= 0.5f, hz = oz >= 0.5f;
+                  const float sx_ = hx ? ox - 0.5f : ox + 0.5f;
+                  const float sy_ = hy ? oy - 0.5f : oy + 0.5f;
+                  const float sz_ = hz ? oz - 0.5f : oz + 0.5f;
+                  float Ex, Ey, Ez, Hx, Hy, Hz;
+                  if (fast) {
+                     const int q = ((i - x0 + 1)*D::FY + (j - y0 + 1))*D::FZ + (k - z0 + 1);
+                     const int qx = hx*D::FYZ, qy = hy*D::FZ, qz = hz;
+                     Ex = cic_s<D::FYZ, D::FZ> (F, q + qx, sx_, oy, oz);
+                     Ey = cic_s<D::FYZ, D::FZ> (F + D::FN, q + qy, ox, sy_, oz);
+                     Ez = cic_s<D::FYZ, D::FZ> (F + 2*D::FN, q + qz, ox, oy, sz_);
+                     Hx = cic_s<D::FYZ, D::FZ> (F + 3*D::FN, q + qy + qz, ox, sy_, sz_);
+                     Hy = cic_s<D::FYZ, D::FZ> (F + 4*D::FN, q + qx + qz, sx_, oy, sz_);
+                     Hz = cic_s<D::FYZ, D::FZ> (F + 5*D::FN, q + qx + qy, sx_, sy_, oz);
+                  } else {
+                     const int i_ = i + hx, j_ = j + hy, k_ = k + hz;
+                     Ex = cic (c.E0, g, i_, sx_, j, oy, k, oz);
+                     Ey = cic (c.E1, g, i, ox, j_, sy_, k, oz);
+                     Ez = cic (c.E2, g, i, ox, j, oy, k_, sz_);
+                     Hx = cic (c.H0, g, i, ox, j_, sy_, k_, sz_);
+                     Hy = cic (c.H1, g, i_, sx_, j, oy, k_, sz_);
+                     Hz = cic (c.H2, g, i_, sx_, j_, sy_, k, oz);
+                  }
+
+                  rho = cur[8*32];
+                  const float tm = 0.5f*c.tau*qm;
+                  const float px = cur[5*32] + tm*Ex, py = cur[6*32] + tm*Ey, pz = cur[7*32] + tm*Ez;
+                  const float p2 = px*px + py*py + pz*pz;
+                  const float rg = rsqrtf (1.0f + p2);
+                  const float gamma = (1.0f + p2)*rg;
+                  const float W = __fdividef (p2, (gamma + 1.0f)*(p2 + 1e-19f))*rho*(float) c.vol/qm;
+                  Wx += (double) (W*px*px);
+                  Wy += (double) (W*py*py);
+                  Wz += (double) (W*pz*pz);
+                  const float tg = tm*rg;
+                  const float ax = tg*Hx, ay = tg*Hy, az = tg*Hz;
+                  const float u = px + py*az - pz*ay, v = py + pz*ax - px*az, w = pz + px*ay - py*ax;
+                  const float bxx = ax*ax, byy = ay*ay, bzz = az*az;
+                  const float bxy = ax*ay, byz = ay*az, bxz = az*ax;
+                  const float delta = __frcp_rn (1.0f + bxx + byy + bzz);
+                  float vx = tm*Ex + ((1.0f + bxx)*u + (bxy + az)*v + (bxz - ay)*w)*delta;
+                  float vy = tm*Ey + ((bxy - az)*u + (1.0f + byy)*v + (byz + ax)*w)*delta;
+                  float vz = tm*Ez + ((bxz + ay)*u + (byz - ax)*v + (1.0f + bzz)*w)*delta;
+                  const float tgi = c.tau*rsqrtf (1.0f + vx*vx + vy*vy + vz*vz);
+                  dx = vx*tgi*c.rh[0];
+                  dy = vy*tgi*c.rh[1];
+                  dz = vz*tgi*c.rh[2];
+                  float nx = ox + dx, ny = oy + dy, nz = oz + dz;
+                  di = (nx >= 1.0f) - (nx < 0.0f);
+                  dj = (ny >= 1.0f) - (ny < 0.0f);
+                  dk = (nz >= 1.0f) - (nz < 0.0f);
+                  if (fabsf (dx) >= 1.0f || fabsf (dy) >= 1.0f || fabsf (dz) >= 1.0f) {
+                     if (atomicOr (&dsc->err, 2) == 0)
+                        dsc->err_info[0] = n;
+                     valid = false;
+                  }
+                  int i2 = i + di, j2 = j + dj, k2 = k + dk;
+                  nx -= di;
+                  ny -= dj;
+                  nz -= dk;
+                  if (nx >= 1.0f) nx = 0.99999994f;
+                  if (ny >= 1.0f) ny = 0.99999994f;
+                  if (nz >= 1.0f) nz = 0.99999994f;
+                  bool gone = false;
+                  gone |= wall32 (g.bc[0][0], false, g.n[0], i2, nx, vx);
+                  gone |= wall32 (g.bc[0][1], false, g.n[1], j2, ny, vy);
+                  gone |= wall32 (g.bc[0][2], false, g.n[2], k2, nz, vz);
+                  gone |= wall32 (g.bc[1][0], true, g.n[0], i2, nx, vx);
+                  gone |= wall32 (g.bc[1][1], true, g.n[1], j2, ny, vy);
+                  gone |= wall32 (g.bc[1][2], true, g.n[2], k2, nz, vz);
+                  m.cell[n] = pack (i2, j2, k2);
+                  m.ox[n] = nx;
+                  m.oy[n] = ny;
+                  m.oz[n] = nz;
+                  m.ux[n] = vx;
+                  m.uy[n] = vy;
+                  m.uz[n] = vz;
+                  if (gone) {
+                     m.qm[n] = 0.0f;
+                     ++dead;
+                  }
+               }
+
+               // Crossing times, sorted (see k_push32).
+               float t0 = 2.0f, t1 = 2.0f, t2 = 2.0f;
+               int a0 = 0, a1 = 1, a2 = 2;
+               if (valid) {
+                  if (di) t0 = __fdividef ((di > 0 ? 1.0f : 0.0f) - ox, dx);
+                  if (dj) t1 = __fdividef ((dj > 0 ? 1.0f : 0.0f) - oy, dy);
+                  if (dk) t2 = __fdividef ((dk > 0 ? 1.0f : 0.0f) - oz, dz);
+                  CSWAP (t0, a0, t1, a1);
+                  CSWAP (t1, a1, t2, a2);
+                  CSWAP (t0, a0, t1, a1);
+               }
+               const float ta = fminf (t0, 1.0f);
+               const int jq = ((i - x0 + 2)*D::JY + (j - y0 + 2))*D::JZ + (k - z0 + 2);
+
+               // Segments after the first, lane by lane.
+               if (valid && t0 <= 1.0f) {
+                  int si = 0, sj = 0, sk = 0;
+                  float tb = t0;
+                  const int d3[3] = {di, dj, dk};
+                  const int ax3[3] = {a0, a1, a2};
+                  const float ts[4] = {t0, t1, t2, 2.0f};
+#pragma unroll
+                  for (int p = 0 ; p < 3 ; ++p) {
+                     if (ts[p] <= 1.0f) {
+                        const int a = ax3[p];
+                        si += (a == 0) ? d3[0] : 0;
+                        sj += (a == 1) ? d3[1] : 0;
+                        sk += (a == 2) ? d3[2] : 0;
+                        const float te = fminf (ts[p + 1], 1.0f);
+                        float w[12];
+                        weights32 (c, rho, ox + tb*dx - si, ox + te*dx - si, oy + tb*dy - sj,
+                                   oy + te*dy - sj, oz + tb*dz - sk, oz + te*dz - sk, w);
+                        if (fast)
+                           scatter_s<D> (Jt, jq + si*D::JYZ + sj*D::JZ + sk, w, S);
+                        else
+                           scatter32 (c, i + si, j + sj, k + sk, w);
+                        tb = te;
+                     }
+                  }
+               }
+
+               // First segment: lanes that share a cell are summed with a
+               // transposed warp sum (one shared atomic per weight), up to
+               // ROUNDS cells per warp; the remaining lanes add their own.
+               float wgt[12];
+               if (valid)
+                  weights32 (c, rho, ox, ox + ta*dx, oy, oy + ta*dy, oz, oz + ta*dz, wgt);
+               else
+                  for (int q = 0 ; q < 12 ; ++q) wgt[q] = 0.0f;
+               if (valid && !fast)
+                  scatter32 (c, i, j, k, wgt);
+               const int key = (valid && fast) ? jq : -1;
+               int fx[12];
+#pragma unroll
+               for (int q = 0 ; q < 12 ; ++q)
+                  fx[q] = key >= 0 ? fixed (wgt[q], S) : 0;
+               unsigned pend = __ballot_sync (0xffffffffu, key >= 0);
+#pragma unroll 1
+               for (int round = 0 ; pend && round < ROUNDS ; ++round) {
+                  const int k0 = __shfl_sync (0xffffffffu, key, __ffs (pend) - 1);
+                  const bool mine = (key == k0);
+                  int v[16];
+#pragma unroll
+                  for (int q = 0 ; q < 12 ; ++q)
+                     v[q] = mine ? fx[q] : 0;
+#pragma unroll
+                  for (int q = 12 ; q < 16 ; ++q)
+                     v[q] = 0;
+                  const int sum = transpose_sum16 (v, lane);
+                  if (slot_lane && sum)
+                     atomicAdd (Jt + k0 + soff, sum);
+                  pend &= ~__ballot_sync (0xffffffffu, mine);
+               }
+               if ((pend >> lane) & 1) {
+#pragma unroll
+                  for (int q = 0 ; q < 12 ; ++q)
+                     atomicAdd (Jt + key + slot_offset<D> (q), fx[q]);
+               }
+            }
+            __syncthreads ();
+
+            // Add the chunk's currents to J.
+            const float unit = S > 0.0f ? 1.0f/S : 0.0f;
+            for (int q = threadIdx.x ; q < 3*D::JN ; q += blockDim.x) {
+               const int v = Jt[q];
+               if (v == 0)
+                  continue;
+               const int comp = q/D::JN, rem = q - comp*D::JN;
+               const int a = rem/D::JYZ, r2 = rem - a*D::JYZ, b = r2/D::JZ, cc = r2 - b*D::JZ;
+               const int gi = x0 - 2 + a, gj = y0 - 2 + b, gk = z0 - 2 + cc;
+               if (gi <= g.n[0] + MG_GX && gj <= g.n[1] + MG_GX && gk <= g.n[2] + MG_GX) {
+                  float *dst = comp == 0 ? c.J0 : comp == 1 ? c.J1 : c.J2;
+                  atomicAdd (dst + g.at (gi, gj, gk), (float) v*unit);
+               }
+            }
+            __syncthreads ();
+         }
+      }
+      __syncthreads ();
+   }
+   block_tally (Wx, Wy, Wz, dead, dsc);
+}
+
 } // namespace
+
+#ifndef MG_TILE_ROUNDS
+#define MG_TILE_ROUNDS 2
+#endif
 
 int mg_push32 (mg_run_t *r)
 {
@@ -404,7 +833,32 @@ int mg_push32 (mg_run_t *r)
    }
    c.vol = r->g.h[0]*r->g.h[1]*r->g.h[2];
    const int T = 256;
-   k_push32<<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (c, r->m32, r->np, r->dsc);
+   if (!r->tiles_ok) {
+      k_push32<<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (c, r->np, nullptr, r->dsc);
+      MG_LAUNCH_CHECK ();
+      return MG_OK;
+   }
+   using D = TileDims<MG_TILE_X, MG_TILE_Y, MG_TILE_Z>;
+   auto kern = k_push32_tiles<MG_TILE_X, MG_TILE_Y, MG_TILE_Z, MG_TILE_ROUNDS>;
+   static int attr_dev = -1;
+   static int per_sm = 1, sms = 148;
+   if (attr_dev != r->device) {
+      MG_CUDA (cudaFuncSetAttribute (kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) D::BYTES));
+      MG_CUDA (cudaOccupancyMaxActiveBlocksPerMultiprocessor (&per_sm, kern, T, D::BYTES));
+      MG_CUDA (cudaDeviceGetAttribute (&sms, cudaDevAttrMultiProcessorCount, r->device));
+      if (per_sm < 1)
+         per_sm = 1;
+      attr_dev = r->device;
+   }
+   int blocks = sms*per_sm;
+   if (blocks > r->ntiles)
+      blocks = r->ntiles;
+   MG_CUDA (cudaMemsetAsync (&r->dsc->tile_next, 0, sizeof (int), r->stream));
+   kern<<<blocks, T, D::BYTES, r->stream>>> (c, r->tile_start, r->tiles[1], r->tiles[2], r->ntiles,
+                                             r->dsc);
+   MG_LAUNCH_CHECK ();
+   // Markers outside the mesh at the last sort: global-memory path.
+   k_push32<<<sms, T, 0, r->stream>>> (c, r->np, r->tile_start + r->ntiles, r->dsc);
    MG_LAUNCH_CHECK ();
    return MG_OK;
 }

@@ -117,3 +117,48 @@ def test_fp32_device_placer_matches_fp64_placement():
     for q, ax in enumerate("xyz"):
         assert np.array_equal(np.floor(a[ax] / h[q]), np.floor(b[ax] / h[q]))
         assert np.max(np.abs(a[ax] - b[ax])) < 1e-7 * h[q]
+
+
+def beams(sort_every, n=(20, 12, 28), bc=(0, 1, 0), drift=0.3, steps=20):
+    """Two counter-drifting electron beams on a grid whose sides are not
+    multiples of the tile, mirror walls on y, 6 markers per cell each."""
+    hh = 0.05 / (2 * math.pi)
+    h = (hh, 1.1 * hh, 0.9 * hh)
+    tau = 0.5 / math.sqrt(sum(1 / x ** 2 for x in h))
+    r = mg.Run(n, h, tau, bc, bc, precision=mg.FP32_OFFSET, sort_every=sort_every)
+    z = np.zeros(r.field_shape())
+    r.set_fields(z, z)
+    rho = -4 * math.pi ** 2 / 12
+    r.place_uniform((0, 0, 0), n, 6, rho, -1.0, drift=(drift, 0.0, 0.5 * drift),
+                    uth=(0.02, 0.02, 0.02), seed=(11, 22))
+    r.place_uniform((0, 0, 0), n, 6, rho, -1.0, drift=(-drift, 0.0, -0.5 * drift),
+                    uth=(0.02, 0.02, 0.02), seed=(33, 44), id0=10 ** 6)
+    r.init()
+    rows = r.step(steps)
+    return r, rows
+
+
+def test_tiled_push_matches_untiled_push():
+    # The tiled push sums currents in fixed point per tile, the untiled one
+    # in FP32 atomics: the two agree to single-precision round-off.
+    rt, a = beams(0)
+    ru, b = beams(-1)
+    scale = float(np.max(np.abs(b[:, 1:6].sum(1))))
+    np.testing.assert_allclose(a[:, 1:], b[:, 1:], rtol=1e-5, atol=1e-6 * scale)
+    Jt, Ju = rt.current(), ru.current()
+    assert np.max(np.abs(Jt - Ju)) <= 1e-4 * np.max(np.abs(Ju))
+    got, want = parity.by_id(rt.markers()), parity.by_id(ru.markers())
+    assert np.array_equal(got["id"], want["id"])
+    for ax in "xyz":
+        assert np.max(np.abs(got[ax] - want[ax])) < 1e-4 * 0.05
+
+
+def test_tiled_push_handles_markers_far_from_their_tile():
+    # Sorted once at init: after 120 steps at 0.6c most markers sit several
+    # cells away from the tile they were sorted into.
+    rt, a = beams(10 ** 6, drift=0.6, steps=120)
+    ru, b = beams(-1, drift=0.6, steps=120)
+    tot_a = a[:, 1] + a[:, 2] + a[:, 3:6].sum(1)
+    tot_b = b[:, 1] + b[:, 2] + b[:, 3:6].sum(1)
+    assert np.max(np.abs(tot_a - tot_b) / np.abs(tot_b)) < 1e-4
+    assert rt.marker_count() == ru.marker_count()
