@@ -158,25 +158,62 @@ __device__ __forceinline__ int sort_key (const TileKey &t, int c, float qm)
    return tile*MG_TILE_CELLS + cell;
 }
 
+// Counter slot of a key: eight neighbouring keys sit in eight different
+// regions of the counter array, so that nearly sorted markers do not queue
+// their atomics on one 32-byte L2 sector.  kp: keys per region.
+__device__ __forceinline__ long long spread (long long key, long long kp)
+{
+   return (key & 7)*kp + (key >> 3);
+}
+
+// Runs of equal keys in a warp (the markers arrive nearly sorted): the
+// lane's run start and, for the run's first lane, the run length.
+__device__ __forceinline__ void key_runs (int key, int lane, int &start, int &len)
+{
+   const int prev = __shfl_up_sync (0xffffffffu, key, 1);
+   const unsigned heads = __ballot_sync (0xffffffffu, lane == 0 || prev != key);
+   const unsigned le = (lane == 31) ? 0xffffffffu : ((2u << lane) - 1);
+   start = 31 - __clz (heads & le);
+   const unsigned after = heads & ~le;
+   len = (after ? __ffs (after) - 1 : 32) - lane;
+}
+
 // Marker count per key, and the largest |rho| (non-negative floats order
-// like their bit patterns).  Lanes with equal keys add once per warp.
-__global__ void k_hist (TileKey t, Markers32 m, long long np, int *count, DevScalars *dsc)
+// like their bit patterns).  One atomic per run of equal keys in a warp;
+// four warp-rows of markers per iteration keep more loads in flight.
+#define SORT_ROWS 4
+__global__ void k_hist (TileKey t, Markers32 m, long long np, int *count, long long kp, DevScalars *dsc)
 {
    const int lane = threadIdx.x & 31;
    int rmax = 0;
-   const long long stride = (long long) gridDim.x*blockDim.x;
-   for (long long base = blockIdx.x*(long long) blockDim.x + (threadIdx.x & ~31) ; base < np ; base += stride) {
-      const long long n = base + lane;
-      int key = -1 - lane;
-      if (n < np) {
-         const float qm = m.qm[n];
-         key = sort_key (t, m.cell[n], qm);
-         if (qm != 0.0f)
-            rmax = max (rmax, __float_as_int (fabsf (m.rho[n])));
+   const long long stride = (long long) gridDim.x*blockDim.x*SORT_ROWS;
+   for (long long base = (blockIdx.x*(long long) blockDim.x + (threadIdx.x & ~31))*SORT_ROWS ; base < np ;
+        base += stride) {
+      int key[SORT_ROWS];
+      // Loads first, all rows at once (indices clamped into the array).
+      float qm[SORT_ROWS], rho[SORT_ROWS];
+      int cell[SORT_ROWS];
+#pragma unroll
+      for (int q = 0 ; q < SORT_ROWS ; ++q) {
+         const long long n = min (base + 32*q + lane, np - 1);
+         qm[q] = m.qm[n];
+         cell[q] = m.cell[n];
+         rho[q] = m.rho[n];
       }
-      const unsigned peers = __match_any_sync (0xffffffffu, key);
-      if (key >= 0 && lane == __ffs (peers) - 1)
-         atomicAdd (count + key, __popc (peers));
+#pragma unroll
+      for (int q = 0 ; q < SORT_ROWS ; ++q) {
+         const bool in = base + 32*q + lane < np;
+         key[q] = in ? sort_key (t, cell[q], qm[q]) : -1;
+         if (in && qm[q] != 0.0f)
+            rmax = max (rmax, __float_as_int (fabsf (rho[q])));
+      }
+#pragma unroll
+      for (int q = 0 ; q < SORT_ROWS ; ++q) {
+         int start, len;
+         key_runs (key[q], lane, start, len);
+         if (key[q] >= 0 && start == lane)
+            atomicAdd (count + spread (key[q], kp), len);
+      }
    }
    for (int d = 16 ; d > 0 ; d >>= 1)
       rmax = max (rmax, __shfl_xor_sync (0xffffffffu, rmax, d));
@@ -186,13 +223,13 @@ __global__ void k_hist (TileKey t, Markers32 m, long long np, int *count, DevSca
 
 // Three-pass exclusive scan of `count` (length len) in place.
 #define SCAN_CHUNK 4096
-__global__ void k_scan_blocks (const int *count, long long len, long long *block_sum)
+__global__ void k_scan_blocks (const int *count, long long kp, long long len, long long *block_sum)
 {
    __shared__ long long s[256];
    const long long b0 = (long long) blockIdx.x*SCAN_CHUNK;
    long long acc = 0;
    for (int q = threadIdx.x ; q < SCAN_CHUNK ; q += blockDim.x)
-      if (b0 + q < len) acc += count[b0 + q];
+      if (b0 + q < len) acc += count[spread (b0 + q, kp)];
    s[threadIdx.x] = acc;
    __syncthreads ();
    for (int d = blockDim.x/2 ; d > 0 ; d >>= 1) {
@@ -202,19 +239,34 @@ __global__ void k_scan_blocks (const int *count, long long len, long long *block
    if (threadIdx.x == 0) block_sum[blockIdx.x] = s[0];
 }
 
+// Exclusive scan of the nb block sums in place, one block of 1024 threads
+// (thread t owns a contiguous segment).
 __global__ void k_scan_sums (long long *block_sum, int nb)
 {
-   if (threadIdx.x == 0 && blockIdx.x == 0) {
-      long long s = 0;
-      for (int q = 0 ; q < nb ; ++q) {
-         const long long v = block_sum[q];
-         block_sum[q] = s;
-         s += v;
-      }
+   __shared__ long long part[1024];
+   const int per = (nb + blockDim.x - 1)/blockDim.x;
+   const int b = threadIdx.x*per, e = min (b + per, nb);
+   long long acc = 0;
+   for (int q = b ; q < e ; ++q)
+      acc += block_sum[q];
+   part[threadIdx.x] = acc;
+   __syncthreads ();
+   for (int d = 1 ; d < (int) blockDim.x ; d <<= 1) {
+      const long long v = threadIdx.x >= (unsigned) d ? part[threadIdx.x - d] : 0;
+      __syncthreads ();
+      part[threadIdx.x] += v;
+      __syncthreads ();
+   }
+   long long run = part[threadIdx.x] - acc;
+   for (int q = b ; q < e ; ++q) {
+      const long long v = block_sum[q];
+      block_sum[q] = run;
+      run += v;
    }
 }
 
-__global__ void k_scan_apply (int *count, long long len, const long long *block_sum, long long *offset)
+__global__ void k_scan_apply (const int *count, long long kp, long long len, const long long *block_sum,
+                              long long *offset)
 {
    // One block per chunk; thread t owns SCAN_CHUNK/blockDim consecutive entries.
    __shared__ long long part[256];
@@ -223,7 +275,7 @@ __global__ void k_scan_apply (int *count, long long len, const long long *block_
    const long long my0 = b0 + (long long) threadIdx.x*per;
    long long acc = 0;
    for (int q = 0 ; q < per ; ++q)
-      if (my0 + q < len) acc += count[my0 + q];
+      if (my0 + q < len) acc += count[spread (my0 + q, kp)];
    part[threadIdx.x] = acc;
    __syncthreads ();
    if (threadIdx.x == 0) {
@@ -238,7 +290,7 @@ __global__ void k_scan_apply (int *count, long long len, const long long *block_
    long long s = part[threadIdx.x];
    for (int q = 0 ; q < per ; ++q)
       if (my0 + q < len) {
-         const long long v = count[my0 + q];
+         const long long v = count[spread (my0 + q, kp)];
          offset[my0 + q] = s;
          s += v;
       }
@@ -253,37 +305,61 @@ __global__ void k_tile_start (const long long *offset, int ntiles, int *tile_sta
 }
 
 // Moves every marker to its place in the other buffer set: the first free
-// slot of its key (lanes with equal keys take consecutive slots).
-__global__ void k_scatter (TileKey t, Markers32 m, Markers32 o, long long np, long long *offset)
+// slot of its key (a run of equal keys in a warp takes consecutive slots);
+// fill counts the slots taken per key.
+__global__ void k_scatter (TileKey t, Markers32 m, Markers32 o, long long np, const long long *offset,
+                           int *fill, long long kp)
 {
    const int lane = threadIdx.x & 31;
-   const long long stride = (long long) gridDim.x*blockDim.x;
-   for (long long base = blockIdx.x*(long long) blockDim.x + (threadIdx.x & ~31) ; base < np ; base += stride) {
-      const long long n = base + lane;
-      int key = -1 - lane, cell = 0;
-      float qm = 0.0f;
-      if (n < np) {
-         cell = m.cell[n];
-         qm = m.qm[n];
-         key = sort_key (t, cell, qm);
+   const long long stride = (long long) gridDim.x*blockDim.x*SORT_ROWS;
+   for (long long base = (blockIdx.x*(long long) blockDim.x + (threadIdx.x & ~31))*SORT_ROWS ; base < np ;
+        base += stride) {
+      // All loads first (indices clamped into the array), then the slots.
+      int key[SORT_ROWS], cell[SORT_ROWS], id[SORT_ROWS];
+      float qm[SORT_ROWS], ox[SORT_ROWS], oy[SORT_ROWS], oz[SORT_ROWS];
+      float ux[SORT_ROWS], uy[SORT_ROWS], uz[SORT_ROWS], rho[SORT_ROWS];
+      long long at[SORT_ROWS];
+#pragma unroll
+      for (int q = 0 ; q < SORT_ROWS ; ++q) {
+         const long long n = min (base + 32*q + lane, np - 1);
+         cell[q] = m.cell[n];
+         qm[q] = m.qm[n];
+         ox[q] = m.ox[n];
+         oy[q] = m.oy[n];
+         oz[q] = m.oz[n];
+         ux[q] = m.ux[n];
+         uy[q] = m.uy[n];
+         uz[q] = m.uz[n];
+         rho[q] = m.rho[n];
+         id[q] = m.id[n];
       }
-      const unsigned peers = __match_any_sync (0xffffffffu, key);
-      const int leader = __ffs (peers) - 1;
-      long long at = 0;
-      if (key >= 0 && lane == leader)
-         at = (long long) atomicAdd ((unsigned long long *) (offset + key), (unsigned long long) __popc (peers));
-      at = __shfl_sync (0xffffffffu, at, leader) + __popc (peers & ((1u << lane) - 1));
-      if (key >= 0) {
-         o.cell[at] = cell;
-         o.qm[at] = qm;
-         o.ox[at] = m.ox[n];
-         o.oy[at] = m.oy[n];
-         o.oz[at] = m.oz[n];
-         o.ux[at] = m.ux[n];
-         o.uy[at] = m.uy[n];
-         o.uz[at] = m.uz[n];
-         o.rho[at] = m.rho[n];
-         o.id[at] = m.id[n];
+#pragma unroll
+      for (int q = 0 ; q < SORT_ROWS ; ++q)
+         key[q] = base + 32*q + lane < np ? sort_key (t, cell[q], qm[q]) : -1;
+#pragma unroll
+      for (int q = 0 ; q < SORT_ROWS ; ++q) {
+         int start, len;
+         key_runs (key[q], lane, start, len);
+         at[q] = 0;
+         if (key[q] >= 0 && start == lane)
+            at[q] = offset[key[q]] + atomicAdd (fill + spread (key[q], kp), len);
+         at[q] = __shfl_sync (0xffffffffu, at[q], start) + (lane - start);
+      }
+#pragma unroll
+      for (int q = 0 ; q < SORT_ROWS ; ++q) {
+         if (key[q] >= 0) {
+            const long long a = at[q];
+            o.cell[a] = cell[q];
+            o.qm[a] = qm[q];
+            o.ox[a] = ox[q];
+            o.oy[a] = oy[q];
+            o.oz[a] = oz[q];
+            o.ux[a] = ux[q];
+            o.uy[a] = uy[q];
+            o.uz[a] = uz[q];
+            o.rho[a] = rho[q];
+            o.id[a] = id[q];
+         }
       }
    }
 }
@@ -586,7 +662,8 @@ int mg_sort32 (mg_run_t *r)
    tk.ntiles = r->ntiles;
    const long long cells = (long long) r->ntiles*MG_TILE_CELLS + 2;
    const int nb = (int) ((cells + SCAN_CHUNK - 1)/SCAN_CHUNK);
-   const size_t need = (size_t) cells*4 + (size_t) cells*8 + (size_t) nb*8 + 1024;
+   const long long kp = (cells + 7)/8;
+   const size_t need = (size_t) kp*8*4 + (size_t) cells*8 + (size_t) nb*8 + 1024;
    if (r->sort_tmp_bytes < need) {
       if (r->sort_tmp) {
          cudaFree (r->sort_tmp);
@@ -597,18 +674,20 @@ int mg_sort32 (mg_run_t *r)
       r->sort_tmp_bytes = need;
    }
    char *p = (char *) r->sort_tmp;
-   int *count = (int *) p;                        p += ((size_t) cells*4 + 255) & ~(size_t) 255;
+   int *count = (int *) p;                        p += ((size_t) kp*8*4 + 255) & ~(size_t) 255;
    long long *offset = (long long *) p;           p += ((size_t) cells*8 + 255) & ~(size_t) 255;
    long long *bsum = (long long *) p;
-   MG_CUDA (cudaMemsetAsync (count, 0, (size_t) cells*4, r->stream));
+   MG_CUDA (cudaMemsetAsync (count, 0, (size_t) kp*8*4, r->stream));
    MG_CUDA (cudaMemsetAsync (&r->dsc->rho_max, 0, sizeof (float), r->stream));
    const int T = 256;
-   k_hist<<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (tk, r->m32, r->np, count, r->dsc);
-   k_scan_blocks<<<nb, 256, 0, r->stream>>> (count, cells, bsum);
-   k_scan_sums<<<1, 32, 0, r->stream>>> (bsum, nb);
-   k_scan_apply<<<nb, 256, 0, r->stream>>> (count, cells, bsum, offset);
+   k_hist<<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (tk, r->m32, r->np, count, kp, r->dsc);
+   k_scan_blocks<<<nb, 256, 0, r->stream>>> (count, kp, cells, bsum);
+   k_scan_sums<<<1, 1024, 0, r->stream>>> (bsum, nb);
+   k_scan_apply<<<nb, 256, 0, r->stream>>> (count, kp, cells, bsum, offset);
    k_tile_start<<<mg_blocks_for (r->ntiles + 2, T, 8), T, 0, r->stream>>> (offset, r->ntiles, r->tile_start);
-   k_scatter<<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (tk, r->m32, r->m32b, r->np, offset);
+   // The counters become the per-key fill counts of the scatter.
+   MG_CUDA (cudaMemsetAsync (count, 0, (size_t) kp*8*4, r->stream));
+   k_scatter<<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (tk, r->m32, r->m32b, r->np, offset, count, kp);
    MG_LAUNCH_CHECK ();
    const Markers32 t = r->m32;
    r->m32 = r->m32b;

@@ -513,25 +513,7 @@ __device__ __forceinline__ void scatter_s (int *Jt, int q, const float w[12], fl
    }
 }
 
-// Warp sum of sixteen integers per lane, transposed: afterwards lane l
-// holds the sum over all lanes of v[(l >> 1) & 15].  Each halving step sends
-// the half of the slots that the partner lane keeps: 16 shuffles in all.
-__device__ __forceinline__ int transpose_sum16 (int v[16], int lane)
-{
-#pragma unroll
-   for (int h = 8, d = 16 ; h >= 1 ; h >>= 1, d >>= 1) {
-      const bool up = lane & d;
-#pragma unroll
-      for (int s = 0 ; s < h ; ++s) {
-         const int send = up ? v[s] : v[s + h];
-         const int keep = up ? v[s + h] : v[s];
-         v[s] = keep + __shfl_xor_sync (0xffffffffu, send, d);
-      }
-   }
-   return v[0] + __shfl_xor_sync (0xffffffffu, v[0], 1);
-}
-
-template <int TX, int TY, int TZ, int ROUNDS>
+template <int TX, int TY, int TZ, int ROUNDS, bool PER>
 __global__ void __launch_bounds__ (256, 3)
 k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, DevScalars *dsc)
 {
@@ -544,9 +526,7 @@ k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, De
    __shared__ int s_tile;
    const Grid &g = c.g;
    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-   const int slot = (lane >> 1) & 15;
-   const int soff = slot < 12 ? slot_offset<D> (slot) : 0;
-   const bool slot_lane = !(lane & 1) && slot < 12;
+   const int soff = lane < 12 ? slot_offset<D> (lane) : 0;
    const float rmax = 1.125f*dsc->rho_max;
    double Wx = 0, Wy = 0, Wz = 0;
    long long dead = 0;
@@ -689,12 +669,13 @@ k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, De
                   if (ny >= 1.0f) ny = 0.99999994f;
                   if (nz >= 1.0f) nz = 0.99999994f;
                   bool gone = false;
-                  gone |= wall32 (g.bc[0][0], false, g.n[0], i2, nx, vx);
-                  gone |= wall32 (g.bc[0][1], false, g.n[1], j2, ny, vy);
-                  gone |= wall32 (g.bc[0][2], false, g.n[2], k2, nz, vz);
-                  gone |= wall32 (g.bc[1][0], true, g.n[0], i2, nx, vx);
-                  gone |= wall32 (g.bc[1][1], true, g.n[1], j2, ny, vy);
-                  gone |= wall32 (g.bc[1][2], true, g.n[2], k2, nz, vz);
+                  // PER: every wall periodic (the walls' branches fold away).
+                  gone |= wall32 (PER ? MG_BC_PERIODIC : g.bc[0][0], false, g.n[0], i2, nx, vx);
+                  gone |= wall32 (PER ? MG_BC_PERIODIC : g.bc[0][1], false, g.n[1], j2, ny, vy);
+                  gone |= wall32 (PER ? MG_BC_PERIODIC : g.bc[0][2], false, g.n[2], k2, nz, vz);
+                  gone |= wall32 (PER ? MG_BC_PERIODIC : g.bc[1][0], true, g.n[0], i2, nx, vx);
+                  gone |= wall32 (PER ? MG_BC_PERIODIC : g.bc[1][1], true, g.n[1], j2, ny, vy);
+                  gone |= wall32 (PER ? MG_BC_PERIODIC : g.bc[1][2], true, g.n[2], k2, nz, vz);
                   m.cell[n] = pack (i2, j2, k2);
                   m.ox[n] = nx;
                   m.oy[n] = ny;
@@ -749,9 +730,10 @@ k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, De
                   }
                }
 
-               // First segment: lanes that share a cell are summed with a
-               // transposed warp sum (one shared atomic per weight), up to
-               // ROUNDS cells per warp; the remaining lanes add their own.
+               // First segment: the weights of lanes that share a cell are
+               // summed across the warp (redux.sync, one per weight) and lane q
+               // adds weight q, for up to ROUNDS cells per warp; the remaining
+               // lanes add their own.
                float wgt[12];
                if (valid)
                   weights32 (c, rho, ox, ox + ta*dx, oy, oy + ta*dy, oz, oz + ta*dz, wgt);
@@ -769,15 +751,13 @@ k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, De
                for (int round = 0 ; pend && round < ROUNDS ; ++round) {
                   const int k0 = __shfl_sync (0xffffffffu, key, __ffs (pend) - 1);
                   const bool mine = (key == k0);
-                  int v[16];
+                  int sum = 0;
 #pragma unroll
-                  for (int q = 0 ; q < 12 ; ++q)
-                     v[q] = mine ? fx[q] : 0;
-#pragma unroll
-                  for (int q = 12 ; q < 16 ; ++q)
-                     v[q] = 0;
-                  const int sum = transpose_sum16 (v, lane);
-                  if (slot_lane && sum)
+                  for (int q = 0 ; q < 12 ; ++q) {
+                     const int t = __reduce_add_sync (0xffffffffu, mine ? fx[q] : 0);
+                     sum = lane == q ? t : sum;
+                  }
+                  if (lane < 12 && sum)
                      atomicAdd (Jt + k0 + soff, sum);
                   pend &= ~__ballot_sync (0xffffffffu, mine);
                }
@@ -814,7 +794,7 @@ k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, De
 } // namespace
 
 #ifndef MG_TILE_ROUNDS
-#define MG_TILE_ROUNDS 2
+#define MG_TILE_ROUNDS 3
 #endif
 
 int mg_push32 (mg_run_t *r)
@@ -839,11 +819,17 @@ int mg_push32 (mg_run_t *r)
       return MG_OK;
    }
    using D = TileDims<MG_TILE_X, MG_TILE_Y, MG_TILE_Z>;
-   auto kern = k_push32_tiles<MG_TILE_X, MG_TILE_Y, MG_TILE_Z, MG_TILE_ROUNDS>;
+   bool per = true;
+   for (int a = 0 ; a < 3 ; ++a)
+      per = per && r->g.bc[0][a] == MG_BC_PERIODIC && r->g.bc[1][a] == MG_BC_PERIODIC;
+   auto kern = per ? k_push32_tiles<MG_TILE_X, MG_TILE_Y, MG_TILE_Z, MG_TILE_ROUNDS, true>
+                   : k_push32_tiles<MG_TILE_X, MG_TILE_Y, MG_TILE_Z, MG_TILE_ROUNDS, false>;
    static int attr_dev = -1;
    static int per_sm = 1, sms = 148;
    if (attr_dev != r->device) {
-      MG_CUDA (cudaFuncSetAttribute (kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) D::BYTES));
+      for (auto k : {k_push32_tiles<MG_TILE_X, MG_TILE_Y, MG_TILE_Z, MG_TILE_ROUNDS, true>,
+                     k_push32_tiles<MG_TILE_X, MG_TILE_Y, MG_TILE_Z, MG_TILE_ROUNDS, false>})
+         MG_CUDA (cudaFuncSetAttribute (k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) D::BYTES));
       MG_CUDA (cudaOccupancyMaxActiveBlocksPerMultiprocessor (&per_sm, kern, T, D::BYTES));
       MG_CUDA (cudaDeviceGetAttribute (&sms, cudaDevAttrMultiProcessorCount, r->device));
       if (per_sm < 1)
