@@ -182,15 +182,20 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def ncu_traffic():
-    """DRAM bytes per push launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "push64_laser_foil.md")
+def ncu_traffic(w, markers):
+    """DRAM bytes per push launch from the committed ncu summary of the
+    workload's push kernel, if any: the summary's bytes per marker (captured
+    on the same kernel, scaled by markers) or its bytes per launch."""
+    name = "push64_laser_foil.md" if w["precision"] == 0 else "push32_weibel.md"
     try:
-        text = open(path).read()
+        text = open(os.path.join(ROOT, "profiles", name)).read()
     except OSError:
         return None
+    m = re.search(r"traffic_bytes_per_marker:\s*([0-9.eE+]+)", text)
+    if m:
+        return float(m.group(1)) * markers
     m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", text)
-    return float(m.group(1)) if m else None
+    return float(m.group(1)) if m and w["name"].startswith("laser_foil") else None
 
 
 # ---------------------------------------------------------------------------
@@ -348,10 +353,11 @@ def main():
     peak, peak_kind = hbm_peak()
     algo_bytes = w["bytes_per_marker"] * n_avg
     achieved = algo_bytes / (push_ms / 1e3) / 1e9 if push_ms > 0 else None
-    roofline = {"bound": "hbm", "kernel": "k_push64" if w["precision"] == 0 else "k_push32", "achieved": achieved, "peak": peak,
+    roofline = {"bound": "hbm", "kernel": "k_push64" if w["precision"] == 0 else "k_push32_tiles",
+                "achieved": achieved, "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s",
                 "frac": achieved / peak if achieved else None,
-                "traffic": ncu_traffic(), "push_ms": push_ms, "step_ms": step_ms,
+                "traffic": ncu_traffic(w, n_avg), "push_ms": push_ms, "step_ms": step_ms,
                 "algorithmic_bytes_per_launch": algo_bytes}
 
     cpu = None
