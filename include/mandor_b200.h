@@ -84,6 +84,8 @@ typedef struct {
    long long capacity;    /* marker capacity (0: grows on upload)      */
    int       sort_every;  /* precision form: re-sort markers by tile every k
                              steps (0 = every 8; < 0 = never, untiled push) */
+   int       tile[3];     /* precision form: tile of the push in cells,
+                             {8,8,4} (also {0,0,0}), {4,4,4} or {8,8,8} */
 } mg_params_t;
 
 /* Analytic laser source: paraxial Gaussian beam, Ey polarised, moving along
@@ -175,6 +177,21 @@ int  mg_run_kernels_per_step (mg_run_t *run, int *count);
 int  mg_run_device_bytes (mg_run_t *run, long long *bytes);
 /* Estimated device bytes for a run with these parameters and markers.     */
 long long mg_estimate_bytes (const mg_params_t *params, long long markers);
+
+/* ---- batches of independent runs -----------------------------------------
+ * No counterpart in the reference (one simulation per core.out process).  A
+ * batch steps many runs of one device with ONE CUDA graph launch per step:
+ * each run's captured step graph is an independent branch of the batch
+ * graph, so small runs fill the GPU together.  Runs keep their own state,
+ * streams and energy rows; a run may belong to several batches but must not
+ * be stepped through another path while a batch step is in progress.
+ * mg_batch_step runs nsteps steps of every run; energies[i] (host, nsteps*6
+ * doubles, may be NULL) receives run i's rows.  Precision-form runs are
+ * re-sorted by tile between launches at their own sort_every.            */
+typedef struct mg_batch mg_batch_t;
+int  mg_batch_create (mg_run_t *const *runs, int nruns, mg_batch_t **out);
+int  mg_batch_step (mg_batch_t *batch, int nsteps, double *const *energies);
+int  mg_batch_destroy (mg_batch_t *batch);
 
 /* Kernel-level timing of the last mg_run_step: average device time of the
  * push kernel and of the whole step, milliseconds (CUDA events on the run's

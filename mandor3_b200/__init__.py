@@ -42,7 +42,7 @@ class Params(C.Structure):
     _fields_ = [("n", C.c_int * 3), ("h", C.c_double * 3), ("tau", C.c_double),
                 ("bc_min", C.c_int * 3), ("bc_max", C.c_int * 3), ("time", C.c_double),
                 ("precision", C.c_int), ("device", C.c_int), ("capacity", C.c_longlong),
-                ("sort_every", C.c_int)]
+                ("sort_every", C.c_int), ("tile", C.c_int * 3)]
 
 
 class Laser(C.Structure):
@@ -107,6 +107,9 @@ def load():
         "mg_run_device_bytes": [vp, C.POINTER(ll)],
         "mg_run_profile": [vp, i],
         "mg_run_last_timing": [vp, C.POINTER(d), C.POINTER(d)],
+        "mg_batch_create": [C.POINTER(vp), i, C.POINTER(vp)],
+        "mg_batch_step": [vp, i, C.POINTER(C.POINTER(d))],
+        "mg_batch_destroy": [vp],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
@@ -134,7 +137,7 @@ class Run:
     marker array, core/main.c:90-91, core/plasma.c:40-43)."""
 
     def __init__(self, n, h, tau, bc_min, bc_max, time=0.0, precision=FP64,
-                 device=0, capacity=0, sort_every=0):
+                 device=0, capacity=0, sort_every=0, tile=(0, 0, 0)):
         lib = load()
         self.n = tuple(int(v) for v in n)
         self.h = tuple(float(v) for v in h)
@@ -142,7 +145,8 @@ class Run:
         self.precision = precision
         p = Params((C.c_int * 3)(*self.n), (C.c_double * 3)(*self.h), self.tau,
                    (C.c_int * 3)(*bc_min), (C.c_int * 3)(*bc_max), float(time),
-                   int(precision), int(device), int(capacity), int(sort_every))
+                   int(precision), int(device), int(capacity), int(sort_every),
+                   (C.c_int * 3)(*tile))
         self._params = p
         ptr = C.c_void_p()
         _check(lib.mg_run_create(C.byref(p), C.byref(ptr)))
@@ -296,6 +300,39 @@ class Run:
         a, b = C.c_double(), C.c_double()
         _check(load().mg_run_last_timing(self.ptr, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+
+class Batch:
+    """Independent runs of one GPU stepped together: one CUDA graph launch
+    per step, each run's step graph a branch of it (no counterpart in the
+    reference, which runs one simulation per process)."""
+
+    def __init__(self, runs):
+        self.runs = list(runs)
+        arr = (C.c_void_p * len(self.runs))(*[r.ptr.value for r in self.runs])
+        ptr = C.c_void_p()
+        _check(load().mg_batch_create(arr, len(self.runs), C.byref(ptr)))
+        self.ptr = ptr
+
+    def step(self, nsteps):
+        """Steps every run nsteps times; returns one (nsteps, 6) array of
+        energy rows per run."""
+        rows = [np.zeros((nsteps, 6)) for _ in self.runs]
+        ptrs = (C.POINTER(C.c_double) * len(rows))(
+            *[r.ctypes.data_as(C.POINTER(C.c_double)) for r in rows])
+        _check(load().mg_batch_step(self.ptr, int(nsteps), ptrs))
+        return rows
+
+    def close(self):
+        if getattr(self, "ptr", None):
+            load().mg_batch_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def estimate_bytes(n, h, tau, bc_min, bc_max, markers, precision=FP64):

@@ -297,6 +297,15 @@ static int check_params (const mg_params_t *p)
       mg_set_error ("unknown precision form %d", p->precision);
       return MG_ERR_ARG;
    }
+   {
+      const int *t = p->tile;
+      const bool ok = (t[0] == 0 && t[1] == 0 && t[2] == 0) || (t[0] == 8 && t[1] == 8 && t[2] == 4) ||
+                      (t[0] == 4 && t[1] == 4 && t[2] == 4) || (t[0] == 8 && t[1] == 8 && t[2] == 8);
+      if (!ok) {
+         mg_set_error ("tile %dx%dx%d: the push is built for 8x8x4, 4x4x4 and 8x8x8", t[0], t[1], t[2]);
+         return MG_ERR_ARG;
+      }
+   }
    return MG_OK;
 }
 
@@ -314,7 +323,7 @@ extern "C" long long mg_estimate_bytes (const mg_params_t *p, long long markers)
    const long long per_marker = (p->precision == MG_FP64) ? 60 : 80;
    b += (markers + markers/8 + 1024)*per_marker;
    if (p->precision != MG_FP64)
-      b += 12LL*(p->n[0] + MG_TILE_X)*(p->n[1] + MG_TILE_Y)*(p->n[2] + MG_TILE_Z);
+      b += 12LL*(p->n[0] + 8)*(p->n[1] + 8)*(p->n[2] + 8);
    b += (long long) MG_RING*6*8 + (1 << 20);
    return b;
 }
@@ -372,9 +381,12 @@ extern "C" int mg_run_create (const mg_params_t *params, mg_run_t **out)
             cudaMemsetAsync (*mp, 0, mb, r->stream);
       }
    if (rc == MG_OK && f32) {
-      const int T[3] = {MG_TILE_X, MG_TILE_Y, MG_TILE_Z};
+      const bool deflt = params->tile[0] == 0 && params->tile[1] == 0 && params->tile[2] == 0;
+      const int T[3] = {deflt ? MG_TILE_X : params->tile[0], deflt ? MG_TILE_Y : params->tile[1],
+                        deflt ? MG_TILE_Z : params->tile[2]};
       r->ntiles = 1;
       for (int a = 0 ; a < 3 ; ++a) {
+         r->tdim[a] = T[a];
          r->tiles[a] = (params->n[a] + T[a] - 1)/T[a];
          r->ntiles *= r->tiles[a];
       }
@@ -1003,6 +1015,140 @@ extern "C" int mg_run_step_async (mg_run_t *r, int nsteps, double *energies_dev)
 {
    CHECK_RUN (r);
    return run_steps (r, nsteps, nullptr, energies_dev, false);
+}
+
+// ---------------------------------------------------------------------------
+// Batches: one graph launch steps every run of the batch.
+// ---------------------------------------------------------------------------
+struct mg_batch {
+   int              n;
+   mg_run_t       **runs;
+   int              device;
+   cudaStream_t     stream;
+   cudaGraph_t      graph;
+   cudaGraphExec_t  exec;
+};
+
+extern "C" int mg_batch_destroy (mg_batch_t *b)
+{
+   if (!b)
+      return MG_OK;
+   cudaSetDevice (b->device);
+   if (b->stream)
+      cudaStreamSynchronize (b->stream);
+   if (b->exec) cudaGraphExecDestroy (b->exec);
+   if (b->graph) cudaGraphDestroy (b->graph);
+   if (b->stream) cudaStreamDestroy (b->stream);
+   free (b->runs);
+   free (b);
+   return MG_OK;
+}
+
+extern "C" int mg_batch_create (mg_run_t *const *runs, int n, mg_batch_t **out)
+{
+   if (!runs || n <= 0 || !out) {
+      mg_set_error ("mg_batch_create: need at least one run");
+      return MG_ERR_ARG;
+   }
+   *out = nullptr;
+   for (int q = 0 ; q < n ; ++q) {
+      if (!runs[q]) {
+         mg_set_error ("mg_batch_create: run %d is null", q);
+         return MG_ERR_ARG;
+      }
+      if (runs[q]->device != runs[0]->device) {
+         mg_set_error ("mg_batch_create: runs on devices %d and %d", runs[0]->device, runs[q]->device);
+         return MG_ERR_ARG;
+      }
+      if (!runs[q]->inited || runs[q]->stage_no != 0) {
+         mg_set_error ("mg_batch_create: run %d is not initialised or is inside a staged step", q);
+         return MG_ERR_STATE;
+      }
+   }
+   MG_CUDA (cudaSetDevice (runs[0]->device));
+   mg_batch_t *b = (mg_batch_t *) calloc (1, sizeof (mg_batch_t));
+   b->n = n;
+   b->device = runs[0]->device;
+   b->runs = (mg_run_t **) malloc (sizeof (mg_run_t *)*n);
+   memcpy (b->runs, runs, sizeof (mg_run_t *)*n);
+   int rc = MG_OK;
+   if (cudaStreamCreateWithFlags (&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+       cudaGraphCreate (&b->graph, 0) != cudaSuccess) {
+      mg_set_error ("mg_batch_create: cannot create the stream or graph");
+      rc = MG_ERR_CUDA;
+   }
+   for (int q = 0 ; q < n && rc == MG_OK ; ++q) {
+      rc = build_graph (runs[q]);
+      cudaGraphNode_t node;
+      if (rc == MG_OK && cudaGraphAddChildGraphNode (&node, b->graph, nullptr, 0, runs[q]->gr[0]) != cudaSuccess) {
+         mg_set_error ("mg_batch_create: cannot add run %d to the batch graph", q);
+         rc = MG_ERR_CUDA;
+      }
+   }
+   if (rc == MG_OK && cudaGraphInstantiate (&b->exec, b->graph, 0) != cudaSuccess) {
+      mg_set_error ("mg_batch_create: graph instantiation failed");
+      rc = MG_ERR_CUDA;
+   }
+   if (rc != MG_OK) {
+      mg_batch_destroy (b);
+      return rc;
+   }
+   *out = b;
+   return MG_OK;
+}
+
+extern "C" int mg_batch_step (mg_batch_t *b, int nsteps, double *const *energies)
+{
+   if (!b || nsteps < 0) {
+      mg_set_error ("mg_batch_step: bad arguments");
+      return MG_ERR_ARG;
+   }
+   MG_CUDA (cudaSetDevice (b->device));
+   for (int q = 0 ; q < b->n ; ++q) {
+      mg_run_t *r = b->runs[q];
+      if (!r->graph_ok || !r->inited || r->stage_no != 0) {
+         mg_set_error ("mg_batch_step: run %d changed since the batch was built", q);
+         return MG_ERR_STATE;
+      }
+   }
+   // Everything a run enqueued before goes first.
+   for (int q = 0 ; q < b->n ; ++q) {
+      cudaEvent_t e = b->runs[q]->ev[2];
+      MG_CUDA (cudaEventRecord (e, b->runs[q]->stream));
+      MG_CUDA (cudaStreamWaitEvent (b->stream, e, 0));
+   }
+   int rc = MG_OK;
+   for (int done = 0 ; done < nsteps && rc == MG_OK ; ) {
+      const int chunk = (nsteps - done < MG_RING) ? nsteps - done : MG_RING;
+      for (int q = 0 ; q < b->n ; ++q)
+         MG_CUDA (cudaMemsetAsync (&b->runs[q]->dsc->step, 0, sizeof (int), b->stream));
+      for (int s = 0 ; s < chunk && rc == MG_OK ; ++s) {
+         // Sorts that are due go on the batch stream, between launches.
+         for (int q = 0 ; q < b->n && rc == MG_OK ; ++q) {
+            mg_run_t *r = b->runs[q];
+            cudaStream_t own = r->stream;
+            r->stream = b->stream;
+            rc = maybe_sort (r);
+            r->stream = own;
+         }
+         if (rc == MG_OK && cudaGraphLaunch (b->exec, b->stream) != cudaSuccess) {
+            mg_set_error ("mg_batch_step: graph launch failed");
+            rc = MG_ERR_CUDA;
+         }
+      }
+      for (int q = 0 ; q < b->n && rc == MG_OK && energies ; ++q)
+         if (energies[q])
+            MG_CUDA (cudaMemcpyAsync (energies[q] + 6*(size_t) done, b->runs[q]->ring, sizeof (double)*6*chunk,
+                                      cudaMemcpyDeviceToHost, b->stream));
+      MG_CUDA (cudaStreamSynchronize (b->stream));
+      done += chunk;
+   }
+   TRY (rc);
+   for (int q = 0 ; q < b->n ; ++q) {
+      b->runs[q]->time += nsteps*b->runs[q]->g.tau;
+      TRY (check_err (b->runs[q]));
+   }
+   return MG_OK;
 }
 
 extern "C" int mg_run_synchronize (mg_run_t *r)

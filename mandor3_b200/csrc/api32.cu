@@ -136,26 +136,28 @@ __global__ void k_live_scan32 (const float *qm, long long from, long long n, lon
 }
 
 // ---- counting sort by tile and cell ----------------------------------------
-// Key: tile index (tiles of MG_TILE_X x MG_TILE_Y x MG_TILE_Z cells, x-major)
+// Key: tile index (tiles of the run's tile size, power-of-two sides, x-major)
 // times the cells per tile plus the cell within the tile, so that a tile's
 // markers are contiguous and, inside it, grouped by cell.  Markers in cells
 // outside [0, n) go to one bucket after the last tile (the push handles them
 // through global memory), removed markers to one more bucket at the end.
 struct TileKey {
    int n[3], nty, ntz, ntiles;
+   int lx, ly, lz;         // log2 of the tile size per axis
+   int lc;                 // log2 of the cells per tile
 };
 
 __device__ __forceinline__ int sort_key (const TileKey &t, int c, float qm)
 {
    if (qm == 0.0f)
-      return t.ntiles*MG_TILE_CELLS + 1;
+      return (t.ntiles << t.lc) + 1;
    const int i = unpack (c, 20), j = unpack (c, 10), k = unpack (c, 0);
    if ((unsigned) i >= (unsigned) t.n[0] || (unsigned) j >= (unsigned) t.n[1] ||
        (unsigned) k >= (unsigned) t.n[2])
-      return t.ntiles*MG_TILE_CELLS;
-   const int tile = ((i/MG_TILE_X)*t.nty + j/MG_TILE_Y)*t.ntz + k/MG_TILE_Z;
-   const int cell = ((i % MG_TILE_X)*MG_TILE_Y + j % MG_TILE_Y)*MG_TILE_Z + k % MG_TILE_Z;
-   return tile*MG_TILE_CELLS + cell;
+      return t.ntiles << t.lc;
+   const int tile = ((i >> t.lx)*t.nty + (j >> t.ly))*t.ntz + (k >> t.lz);
+   const int cell = ((((i & ((1 << t.lx) - 1)) << t.ly) + (j & ((1 << t.ly) - 1))) << t.lz) + (k & ((1 << t.lz) - 1));
+   return (tile << t.lc) + cell;
 }
 
 // Counter slot of a key: eight neighbouring keys sit in eight different
@@ -298,10 +300,10 @@ __global__ void k_scan_apply (const int *count, long long kp, long long len, con
 
 // First marker of every tile, of the outside bucket and of the removed bucket
 // (before k_rank advances the offsets).
-__global__ void k_tile_start (const long long *offset, int ntiles, int *tile_start)
+__global__ void k_tile_start (const long long *offset, int ntiles, int lc, int *tile_start)
 {
    for (int t = blockIdx.x*blockDim.x + threadIdx.x ; t <= ntiles + 1 ; t += gridDim.x*blockDim.x)
-      tile_start[t] = (int) offset[t <= ntiles ? (long long) t*MG_TILE_CELLS : (long long) ntiles*MG_TILE_CELLS + 1];
+      tile_start[t] = (int) offset[t <= ntiles ? (long long) t << lc : ((long long) ntiles << lc) + 1];
 }
 
 // Moves every marker to its place in the other buffer set: the first free
@@ -660,7 +662,11 @@ int mg_sort32 (mg_run_t *r)
    tk.nty = r->tiles[1];
    tk.ntz = r->tiles[2];
    tk.ntiles = r->ntiles;
-   const long long cells = (long long) r->ntiles*MG_TILE_CELLS + 2;
+   tk.lx = __builtin_ctz (r->tdim[0]);
+   tk.ly = __builtin_ctz (r->tdim[1]);
+   tk.lz = __builtin_ctz (r->tdim[2]);
+   tk.lc = tk.lx + tk.ly + tk.lz;
+   const long long cells = ((long long) r->ntiles << tk.lc) + 2;
    const int nb = (int) ((cells + SCAN_CHUNK - 1)/SCAN_CHUNK);
    const long long kp = (cells + 7)/8;
    const size_t need = (size_t) kp*8*4 + (size_t) cells*8 + (size_t) nb*8 + 1024;
@@ -684,7 +690,7 @@ int mg_sort32 (mg_run_t *r)
    k_scan_blocks<<<nb, 256, 0, r->stream>>> (count, kp, cells, bsum);
    k_scan_sums<<<1, 1024, 0, r->stream>>> (bsum, nb);
    k_scan_apply<<<nb, 256, 0, r->stream>>> (count, kp, cells, bsum, offset);
-   k_tile_start<<<mg_blocks_for (r->ntiles + 2, T, 8), T, 0, r->stream>>> (offset, r->ntiles, r->tile_start);
+   k_tile_start<<<mg_blocks_for (r->ntiles + 2, T, 8), T, 0, r->stream>>> (offset, r->ntiles, tk.lc, r->tile_start);
    // The counters become the per-key fill counts of the scatter.
    MG_CUDA (cudaMemsetAsync (count, 0, (size_t) kp*8*4, r->stream));
    k_scatter<<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (tk, r->m32, r->m32b, r->np, offset, count, kp);

@@ -22,16 +22,10 @@
 
 // Precision-form tiles: markers are counting-sorted by (tile, cell) and the
 // push stages one tile of fields and currents in shared memory at a time.
-#ifndef MG_TILE_X
+// The default tile; a run may pick 4x4x4 or 8x8x8 instead (tdim).
 #define MG_TILE_X 8
-#endif
-#ifndef MG_TILE_Y
 #define MG_TILE_Y 8
-#endif
-#ifndef MG_TILE_Z
 #define MG_TILE_Z 4
-#endif
-#define MG_TILE_CELLS (MG_TILE_X*MG_TILE_Y*MG_TILE_Z)
 
 struct Grid {
    int    n[3];
@@ -123,7 +117,8 @@ struct mg_run {
    void      *sort_tmp;    // scratch for sorting / compaction
    size_t     sort_tmp_bytes;
    long long  steps_since_sort;
-   int        tiles[3];    // tiles per axis (precision form)
+   int        tdim[3];     // tile size in cells (precision form)
+   int        tiles[3];    // tiles per axis
    int        ntiles;
    int       *tile_start;  // ntiles + 2 marker offsets of the last sort:
                            // tile t holds [tile_start[t], tile_start[t+1]),

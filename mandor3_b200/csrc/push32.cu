@@ -797,6 +797,42 @@ k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, De
 #define MG_TILE_ROUNDS 3
 #endif
 
+#define TRY32(x)                                                             \
+   do {                                                                      \
+      int rc_ = (x);                                                         \
+      if (rc_ != MG_OK)                                                      \
+         return rc_;                                                         \
+   } while (0)
+
+// Launches the tiled push of one tile size: persistent CTAs, as many as fit
+// on the GPU (at most one per tile).
+template <int TX, int TY, int TZ>
+static int launch_tiles (mg_run_t *r, const Ctx32 &c, bool per)
+{
+   using D = TileDims<TX, TY, TZ>;
+   auto kp = k_push32_tiles<TX, TY, TZ, MG_TILE_ROUNDS, true>;
+   auto kn = k_push32_tiles<TX, TY, TZ, MG_TILE_ROUNDS, false>;
+   static int attr_dev = -1;
+   static int per_sm = 1, sms = 148;
+   if (attr_dev != r->device) {
+      MG_CUDA (cudaFuncSetAttribute (kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) D::BYTES));
+      MG_CUDA (cudaFuncSetAttribute (kn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) D::BYTES));
+      MG_CUDA (cudaOccupancyMaxActiveBlocksPerMultiprocessor (&per_sm, kn, 256, D::BYTES));
+      MG_CUDA (cudaDeviceGetAttribute (&sms, cudaDevAttrMultiProcessorCount, r->device));
+      if (per_sm < 1)
+         per_sm = 1;
+      attr_dev = r->device;
+   }
+   int blocks = sms*per_sm;
+   if (blocks > r->ntiles)
+      blocks = r->ntiles;
+   MG_CUDA (cudaMemsetAsync (&r->dsc->tile_next, 0, sizeof (int), r->stream));
+   (per ? kp : kn)<<<blocks, 256, D::BYTES, r->stream>>> (c, r->tile_start, r->tiles[1], r->tiles[2],
+                                                            r->ntiles, r->dsc);
+   MG_LAUNCH_CHECK ();
+   return MG_OK;
+}
+
 int mg_push32 (mg_run_t *r)
 {
    if (r->np == 0)
@@ -818,31 +854,18 @@ int mg_push32 (mg_run_t *r)
       MG_LAUNCH_CHECK ();
       return MG_OK;
    }
-   using D = TileDims<MG_TILE_X, MG_TILE_Y, MG_TILE_Z>;
    bool per = true;
    for (int a = 0 ; a < 3 ; ++a)
       per = per && r->g.bc[0][a] == MG_BC_PERIODIC && r->g.bc[1][a] == MG_BC_PERIODIC;
-   auto kern = per ? k_push32_tiles<MG_TILE_X, MG_TILE_Y, MG_TILE_Z, MG_TILE_ROUNDS, true>
-                   : k_push32_tiles<MG_TILE_X, MG_TILE_Y, MG_TILE_Z, MG_TILE_ROUNDS, false>;
-   static int attr_dev = -1;
-   static int per_sm = 1, sms = 148;
-   if (attr_dev != r->device) {
-      for (auto k : {k_push32_tiles<MG_TILE_X, MG_TILE_Y, MG_TILE_Z, MG_TILE_ROUNDS, true>,
-                     k_push32_tiles<MG_TILE_X, MG_TILE_Y, MG_TILE_Z, MG_TILE_ROUNDS, false>})
-         MG_CUDA (cudaFuncSetAttribute (k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) D::BYTES));
-      MG_CUDA (cudaOccupancyMaxActiveBlocksPerMultiprocessor (&per_sm, kern, T, D::BYTES));
-      MG_CUDA (cudaDeviceGetAttribute (&sms, cudaDevAttrMultiProcessorCount, r->device));
-      if (per_sm < 1)
-         per_sm = 1;
-      attr_dev = r->device;
-   }
-   int blocks = sms*per_sm;
-   if (blocks > r->ntiles)
-      blocks = r->ntiles;
-   MG_CUDA (cudaMemsetAsync (&r->dsc->tile_next, 0, sizeof (int), r->stream));
-   kern<<<blocks, T, D::BYTES, r->stream>>> (c, r->tile_start, r->tiles[1], r->tiles[2], r->ntiles,
-                                             r->dsc);
-   MG_LAUNCH_CHECK ();
+   const int *td = r->tdim;
+   if (td[0] == 4 && td[1] == 4 && td[2] == 4)
+      TRY32 ((launch_tiles<4, 4, 4> (r, c, per)));
+   else if (td[0] == 8 && td[1] == 8 && td[2] == 8)
+      TRY32 ((launch_tiles<8, 8, 8> (r, c, per)));
+   else
+      TRY32 ((launch_tiles<8, 8, 4> (r, c, per)));
+   int sms = 148;
+   MG_CUDA (cudaDeviceGetAttribute (&sms, cudaDevAttrMultiProcessorCount, r->device));
    // Markers outside the mesh at the last sort: global-memory path.
    k_push32<<<sms, T, 0, r->stream>>> (c, r->np, r->tile_start + r->ntiles, r->dsc);
    MG_LAUNCH_CHECK ();
