@@ -290,6 +290,153 @@ def run_reference_arm(args, w, world, rank):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# Many solves on one GPU: a batch of 256 runs, and a served request stream.
+# ---------------------------------------------------------------------------
+def batch_specs(count=256, steps=300, seed=1802):
+    """256 independent runs drawn from one seed: half periodic thermal
+    plasmas, half laser-foil runs; sides U{16..96} cells per axis, 4-32
+    markers per cell, foil densities U(5, 50) n_cr, a0 U(0.5, 5), foils
+    0.25 wavelength thick; precision form, `steps` steps each."""
+    from mandor3_b200 import scan, FP32_OFFSET
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(count):
+        n = tuple(int(v) for v in rng.integers(16, 97, size=3))
+        ppc = int(rng.integers(4, 33))
+        if q % 2 == 0:
+            out.append(scan.PeriodicSolve(n, ppc, 0.01 + 0.04 * rng.random(), steps,
+                                          precision=FP32_OFFSET, seed=(1802, 9373 + q)))
+        else:
+            n = (max(n[0], 24),) + n[1:]
+            out.append(scan.FoilSolve(n, max(1, ppc // 2), float(rng.uniform(0.5, 5.0)), 0.25,
+                                      float(rng.uniform(5.0, 50.0)), steps, precision=FP32_OFFSET,
+                                      seed=(1802, 9373 + q)))
+    return out
+
+
+def serve_specs(count=24, seed=9373, step_scale=1.0):
+    """Laser-foil scan solves of mixed size: grids (64, 32, 32) x U{1..4},
+    4-16 markers per cell, a0 U(1, 10), foil thickness U(0.1, 2) wavelengths,
+    density U(10, 100) n_cr, U{1000..3000} steps (times step_scale)."""
+    from mandor3_b200 import scan, FP32_OFFSET
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(count):
+        k = int(rng.integers(1, 5))
+        out.append(scan.FoilSolve((64 * k, 32 * k, 32 * k), int(rng.integers(4, 17)),
+                                  float(rng.uniform(1, 10)), float(rng.uniform(0.1, 2.0)),
+                                  float(rng.uniform(10, 100)),
+                                  max(10, int(rng.integers(1000, 3001) * step_scale)),
+                                  precision=FP32_OFFSET, seed=(1802, 9373 + q)))
+    return out
+
+
+def batch_bench(args):
+    """Throughput of 256 runs stepped by one graph launch per step, against
+    the same runs stepped one at a time (both device-resident)."""
+    import torch
+    import mandor3_b200 as mg
+    from mandor3_b200 import scan
+    specs = batch_specs(steps=args.steps or 300)
+    tuner = scan.Tuner(steps=6, sorts=(8, 16))
+    t = time.perf_counter()
+    choice = [tuner.choose(s) for s in specs]
+    tune_s = time.perf_counter() - t
+    runs = [s.build(0, tile=c[0], sort_every=c[1]) for s, c in zip(specs, choice)]
+    markers = sum(r.marker_count() for r in runs)
+    b = mg.Batch(runs)
+    b.step(args.warmup)
+    with Clocks(0) as clocks:
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        b.step(specs[0].steps)
+        torch.cuda.synchronize()
+        batch_s = time.perf_counter() - t
+    b.close()
+    for r in runs:
+        r.close()
+    # Same runs, one at a time.
+    alone_s = 0.0
+    for s, c in zip(specs, choice):
+        r = s.build(0, tile=c[0], sort_every=c[1])
+        r.step(args.warmup)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        r.step(s.steps)
+        alone_s += time.perf_counter() - t
+        r.close()
+    steps = specs[0].steps
+    value = markers * steps / batch_s
+    print(json.dumps({
+        "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": 1,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * batch_s / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "batch_256_runs", "runs": len(specs), "markers": markers,
+                   "sides": "U{16..96} per axis", "ppc": "4-32", "kinds": "half periodic thermal, half laser foil",
+                   "precision": "int cell + FP32 offset", "tuned": sorted(set(map(str, tuner.table.values()))),
+                   "tuning_seconds": tune_s},
+        "clocks": clocks.summary(),
+        "alone": {"value": markers * steps / alone_s, "seconds": alone_s},
+        "batch_over_alone": alone_s / batch_s,
+    }))
+
+
+def serve_bench(args):
+    """A Poisson stream (200 requests/s) of laser-foil scan solves served
+    with continuous batching in the precision form, against the same solves
+    run one at a time in the plain FP64 form (queued in arrival order)."""
+    import torch
+    import mandor3_b200 as mg
+    from mandor3_b200 import scan, FP64
+    specs = serve_specs(count=args.requests, step_scale=args.step_scale)
+    stream = scan.poisson_stream(specs, 200.0)
+    tuner = scan.Tuner(steps=6, sorts=(8, 16))
+    for s in specs:
+        tuner.choose(s)
+    srv = scan.Server(chunk=100, tuner=tuner)
+    with Clocks(0) as clocks:
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        res = srv.serve(stream)
+        served_s = time.perf_counter() - t
+    # Plain FP64, one solve at a time in arrival order.
+    import dataclasses
+    done, lat, fp64_s, err = 0.0, [], 0.0, []
+    for (arr, s), r in zip(stream, res):
+        plain = dataclasses.replace(s, precision=FP64)
+        rows, count, sec = scan.run_alone(plain)
+        fp64_s += sec
+        done = max(done, arr) + sec
+        lat.append(done - arr)
+        tot = lambda a: a[:, 1] + a[:, 2] + a[:, 3:6].sum(1)
+        scale = np.max(np.abs(tot(rows)))
+        err.append(float(np.max(np.abs(tot(r.rows) - tot(rows))) / scale))
+    psteps = sum(s.markers() * s.steps for s in specs)
+    print(json.dumps({
+        "metric": "scan solves/s", "value": len(specs) / served_s, "unit": "solves/s", "n_gpus": 1,
+        "steps": int(sum(s.steps for s in specs)), "warmup": 0, "ms_per_step": None,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "serve_laser_foil_scan", "requests": len(specs), "rate_per_s": 200.0,
+                   "grids": "(64,32,32) x U{1..4}", "ppc": "4-16", "a0": "U(1,10)",
+                   "thickness": "U(0.1,2) lambda", "density": "U(10,100) n_cr",
+                   "steps": "U{1000..3000} x %g" % args.step_scale, "admission": "device footprint",
+                   "budget_bytes": srv.budget, "peak_admitted_bytes": srv.peak_used,
+                   "server_host_seconds": srv.stats},
+        "clocks": clocks.summary(),
+        "served": {"seconds": served_s, "particle_steps_per_s": psteps / served_s,
+                   "latency_p50_s": scan.percentile([r.latency for r in res], 50),
+                   "latency_p99_s": scan.percentile([r.latency for r in res], 99)},
+        "plain_fp64_one_at_a_time": {"seconds": fp64_s, "solves_per_s": len(specs) / fp64_s,
+                                     "latency_p50_s": scan.percentile(lat, 50),
+                                     "latency_p99_s": scan.percentile(lat, 99)},
+        "throughput_over_plain": fp64_s / served_s,
+        "total_energy_error_vs_fp64": {"max": max(err), "median": scan.percentile(err, 50)},
+    }))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -300,9 +447,16 @@ def main():
     ap.add_argument("--ref-steps", type=int, default=12)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--requests", type=int, default=24, help="serve workload: solves in the stream")
+    ap.add_argument("--step-scale", type=float, default=1.0, help="serve workload: scale of the solves' steps")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("at least 3 warm-up steps")
+    if args.workload in ("batch", "serve"):
+        import torch
+        torch.cuda.set_device(0)
+        (batch_bench if args.workload == "batch" else serve_bench)(args)
+        return
 
     w = workload(args.workload)
     if args.steps is None:

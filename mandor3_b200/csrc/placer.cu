@@ -86,28 +86,6 @@ static void mat_step (Mat &A)
    A[96][64] = RM_MASK;           // -1 mod 2^24
 }
 
-static void mat_pow (long long e, Mat &R)
-{
-   Mat *base = (Mat *) malloc (sizeof (Mat)), *tmp = (Mat *) malloc (sizeof (Mat));
-   mat_step (*base);
-   memset (&R, 0, sizeof (Mat));
-   for (int q = 0 ; q < RM_LAG ; ++q)
-      R[q][q] = 1;
-   while (e > 0) {
-      if (e & 1) {
-         mat_mul (R, *base, *tmp);
-         memcpy (&R, tmp, sizeof (Mat));
-      }
-      e >>= 1;
-      if (e) {
-         mat_mul (*base, *base, *tmp);
-         memcpy (base, tmp, sizeof (Mat));
-      }
-   }
-   free (base);
-   free (tmp);
-}
-
 struct PlaceArgs {
    mg_place_t s;
    double h[3];
@@ -172,6 +150,30 @@ k_place (PlaceArgs a, const uint32_t *states, Markers64 m)
 
 } // namespace
 
+// Powers A^(2^j) of the one-draw matrix, j < 63, computed once per process:
+// any jump is then a product of at most 63 of them.
+static Mat *g_pow2 = nullptr;
+static std::once_flag g_pow2_once;
+
+static void pow2_table ()
+{
+   g_pow2 = (Mat *) malloc (sizeof (Mat)*63);
+   mat_step (g_pow2[0]);
+   for (int j = 1 ; j < 63 ; ++j)
+      mat_mul (g_pow2[j - 1], g_pow2[j - 1], g_pow2[j]);
+}
+
+// x <- A^e x with the cached powers (one 97x97 mat-vec per set bit of e).
+static void jump_vec (long long e, uint32_t x[RM_LAG])
+{
+   uint32_t tmp[RM_LAG];
+   for (int j = 0 ; e > 0 ; ++j, e >>= 1)
+      if (e & 1) {
+         mat_vec (g_pow2[j], x, tmp);
+         memcpy (x, tmp, sizeof (tmp));
+      }
+}
+
 // Host: generator states for `nthreads` chunks of `chunk_draws` draws
 // starting at draw `skip`.  states[t] = (F_{d_t-97} .. F_{d_t-1}).
 int mg_ranmar_states (int ij, int kl, long long skip, long long chunk_draws, int nthreads,
@@ -181,16 +183,27 @@ int mg_ranmar_states (int ij, int kl, long long skip, long long chunk_draws, int
       mg_set_error ("ranmar seeds must satisfy 0 <= ij <= 31328, 0 <= kl <= 30081 (misc_ranmar.c:81-84)");
       return MG_ERR_ARG;
    }
+   std::call_once (g_pow2_once, pow2_table);
    uint32_t s[RM_LAG], tmp[RM_LAG];
    rm_seed (ij, kl, s);
-   Mat *M = (Mat *) malloc (sizeof (Mat));
-   if (skip > 0) {
-      mat_pow (skip, *M);
-      mat_vec (*M, s, tmp);
-      memcpy (s, tmp, sizeof (s));
+   jump_vec (skip, s);
+   // One chunk's jump as a matrix: the product of the cached powers.
+   Mat *M = (Mat *) malloc (sizeof (Mat)), *T = (Mat *) malloc (sizeof (Mat));
+   if (nthreads > 1) {
+      bool first = true;
+      long long e = chunk_draws;
+      for (int j = 0 ; e > 0 ; ++j, e >>= 1) {
+         if (!(e & 1))
+            continue;
+         if (first) {
+            memcpy (M, &g_pow2[j], sizeof (Mat));
+            first = false;
+         } else {
+            mat_mul (g_pow2[j], *M, *T);
+            memcpy (M, T, sizeof (Mat));
+         }
+      }
    }
-   if (nthreads > 1)
-      mat_pow (chunk_draws, *M);
    for (int t = 0 ; t < nthreads ; ++t) {
       memcpy (states + (size_t) t*RM_LAG, s, sizeof (s));
       if (t + 1 < nthreads) {
@@ -199,6 +212,7 @@ int mg_ranmar_states (int ij, int kl, long long skip, long long chunk_draws, int
       }
    }
    free (M);
+   free (T);
    return MG_OK;
 }
 
@@ -210,9 +224,10 @@ int mg_place64 (mg_run_t *r, const mg_place_t *spec, long long at, long long cou
       a.h[q] = r->g.h[q];
    a.nmarkers = count;
    a.at = at;
-   // Threads: enough to fill the GPU, bounded so the host jump-ahead stays
-   // cheap (one 97x97 mat-vec per thread).
-   int nthreads = mg_sm_count ()*128;
+   // Generator streams: 16 per SM, which keeps the host jump-ahead (one
+   // 97x97 mat-vec per stream) at a few milliseconds; the markers are the
+   // same for any stream count.
+   int nthreads = mg_sm_count ()*16;
    if (count < nthreads) nthreads = (int) count;
    if (nthreads < 1) nthreads = 1;
    a.per_thread = (count + nthreads - 1)/nthreads;

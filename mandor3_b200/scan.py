@@ -10,7 +10,7 @@ runs.  Here many solves share the device:
   launch per step;
 * `Server` admits solves from a request stream while memory allows (each
   run's footprint from `mg_estimate_bytes`), keeps their state on the device
-  and steps every admitted run in rounds on the run's own stream, so the
+  and steps every admitted run in rounds of batched graph launches, so the
   work of solves that arrived at different times overlaps on the GPU;
   finished solves leave and free their memory for queued ones.
 
@@ -74,8 +74,7 @@ class FoilSolve:
         p = self.params()
         r = Run(p["n"], p["h"], p["tau"], p["bc_min"], p["bc_max"], precision=self.precision,
                 device=device, capacity=self.markers(), sort_every=sort_every, tile=tile)
-        z = np.zeros(r.field_shape())
-        r.set_fields(z, z)
+        # Fields start at zero (mg_run_create clears them).
         waist = 0.25 * min(n[1], n[2]) * self.h
         r.set_laser(a0=self.a0, waist=waist, x_focus=lo[0] * self.h, duration=10.0, t_start=0.0,
                     phase=0.0, plane=5, margin=3)
@@ -114,8 +113,7 @@ class PeriodicSolve:
         p = self.params()
         r = Run(p["n"], p["h"], p["tau"], p["bc_min"], p["bc_max"], precision=self.precision,
                 device=device, capacity=self.markers(), sort_every=sort_every, tile=tile)
-        z = np.zeros(r.field_shape())
-        r.set_fields(z, z)
+        # Fields start at zero (mg_run_create clears them).
         r.place_uniform((0, 0, 0), p["n"], self.ppc, -self.density * N_CR / self.ppc, -1.0,
                         uth=(self.uth,) * 3, seed=self.seed)
         r.init()
@@ -199,11 +197,13 @@ class Result:
 class Server:
     """Continuous batching of solves on one GPU.
 
-    `serve(stream)` takes (arrival seconds, spec) pairs, admits solves in
-    arrival order while their footprints fit `budget` bytes, steps every
-    admitted solve `chunk` steps per round (each on its own CUDA stream, all
-    rounds' launches issued before one wait), retires finished solves and
-    admits queued ones between rounds.  Returns the results in request order.
+    `serve(stream)` takes (arrival seconds, spec) pairs and returns the
+    results in request order.  Between rounds it admits queued solves in
+    arrival order while their footprints fit `budget` bytes and retires the
+    finished ones.  A round steps every admitted solve by the same number of
+    steps (at most `chunk`, and no more than the closest solve to its end
+    still needs) through one `Batch`: one CUDA graph launch per step for all
+    admitted solves, rebuilt whenever the set of solves changes.
     """
 
     def __init__(self, device=0, budget=None, chunk=100, tuner=None):
@@ -216,12 +216,14 @@ class Server:
             budget = int(0.85 * free)
         self.budget = budget
         self.peak_used = 0
+        # Host seconds spent admitting (building runs), rebuilding batches and
+        # stepping rounds.
+        self.stats = dict(admit_s=0.0, batch_s=0.0, step_s=0.0, rounds=0)
 
     def serve(self, stream):
-        import torch
-        dev = torch.device("cuda", self.device)
         pending = sorted(((float(t), i, s) for i, (t, s) in enumerate(stream)), key=lambda x: (x[0], x[1]))
         queue, active, results = [], [], {}
+        batch = None
         used = 0
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0
@@ -229,6 +231,7 @@ class Server:
             while pending and pending[0][0] <= now():
                 queue.append(pending.pop(0))
             # Admission in arrival order while the footprints fit.
+            changed = False
             while queue:
                 arrival, i, spec = queue[0]
                 need = footprint(spec)
@@ -237,33 +240,49 @@ class Server:
                 if used + need > self.budget:
                     break
                 queue.pop(0)
+                ta = time.perf_counter()
                 tile, every = self.tuner.choose(spec) if self.tuner else ((0, 0, 0), 0)
                 run = spec.build(self.device, tile=tile, sort_every=every)
-                rows = torch.empty((spec.steps, 6), dtype=torch.float64, device=dev)
-                active.append(dict(i=i, spec=spec, run=run, rows=rows, done=0, need=need,
+                self.stats["admit_s"] += time.perf_counter() - ta
+                active.append(dict(i=i, spec=spec, run=run, rows=[], done=0, need=need,
                                    arrival=arrival, admitted=now()))
                 used += need
                 self.peak_used = max(self.peak_used, used)
+                changed = True
             if not active:
                 if pending:
                     time.sleep(max(0.0, min(0.05, pending[0][0] - now())))
                 continue
-            for a in active:
-                k = min(self.chunk, a["spec"].steps - a["done"])
-                a["run"].step_async(k, a["rows"].data_ptr() + 8 * 6 * a["done"])
-                a["done"] += k
-            for a in active:
-                a["run"].synchronize()
+            if changed or batch is None:
+                tb = time.perf_counter()
+                if batch is not None:
+                    batch.close()
+                batch = Batch([a["run"] for a in active])
+                self.stats["batch_s"] += time.perf_counter() - tb
+            k = min([self.chunk] + [a["spec"].steps - a["done"] for a in active])
+            ts = time.perf_counter()
+            rows = batch.step(k)
+            self.stats["step_s"] += time.perf_counter() - ts
+            self.stats["rounds"] += 1
             still = []
-            for a in active:
+            for a, rw in zip(active, rows):
+                a["rows"].append(rw)
+                a["done"] += k
                 if a["done"] < a["spec"].steps:
                     still.append(a)
                     continue
                 results[a["i"]] = Result(a["i"], a["arrival"], a["admitted"], now(),
-                                         a["rows"].cpu().numpy(), a["run"].marker_count())
-                a["run"].close()
+                                         np.concatenate(a["rows"]), a["run"].marker_count())
                 used -= a["need"]
+            if len(still) != len(active):
+                batch.close()
+                batch = None
+                for a in active:
+                    if a["done"] >= a["spec"].steps:
+                        a["run"].close()
             active = still
+        if batch is not None:
+            batch.close()
         return [results[i] for i in range(len(stream))]
 
 
