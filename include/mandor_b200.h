@@ -178,6 +178,21 @@ int  mg_run_device_bytes (mg_run_t *run, long long *bytes);
 /* Estimated device bytes for a run with these parameters and markers.     */
 long long mg_estimate_bytes (const mg_params_t *params, long long markers);
 
+/* ---- Gauss-law test (core/plasma_gaussTest.c:89-149) ---------------------
+ * FP64 arithmetic in both precision forms.  mg_gauss_before stores the
+ * charge density of the markers as they are (core/main.c:376 calls
+ * gauss_before after em_energy, before plasma_move); mg_gauss_after computes
+ * it again and returns out = {max |(rho2 - rho1)/tau + div J|,
+ * max |div E - rho2|} over nodes [0, n]^3 (after em_EStep_finish,
+ * core/main.c:428).  mg_run_step_gauss runs nsteps whole steps with the test
+ * around each and writes nsteps rows {t, deltaRho_J, deltaRho_E}, the
+ * columns of output/gauss_test.dat (t: the time at the start of the step).
+ * The density is plasma_rho's (core/plasma.c:322-329, walls folded by
+ * core/plasma_rho.c:23-97; VSP filter off).                              */
+int  mg_gauss_before (mg_run_t *run);
+int  mg_gauss_after (mg_run_t *run, double out[2]);
+int  mg_run_step_gauss (mg_run_t *run, int nsteps, double *rows);
+
 /* ---- batches of independent runs -----------------------------------------
  * No counterpart in the reference (one simulation per core.out process).  A
  * batch steps many runs of one device with ONE CUDA graph launch per step:

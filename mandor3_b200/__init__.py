@@ -107,6 +107,9 @@ def load():
         "mg_run_device_bytes": [vp, C.POINTER(ll)],
         "mg_run_profile": [vp, i],
         "mg_run_last_timing": [vp, C.POINTER(d), C.POINTER(d)],
+        "mg_gauss_before": [vp],
+        "mg_gauss_after": [vp, vp],
+        "mg_run_step_gauss": [vp, i, vp],
         "mg_batch_create": [C.POINTER(vp), i, C.POINTER(vp)],
         "mg_batch_step": [vp, i, C.POINTER(C.POINTER(d))],
         "mg_batch_destroy": [vp],
@@ -271,6 +274,21 @@ class Run:
         rows = np.zeros((nsteps, 6))
         _check(load().mg_run_step(self.ptr, int(nsteps), rows.ctypes.data if nsteps else None))
         return rows
+
+    def step_gauss(self, nsteps=1):
+        """nsteps steps with the Gauss-law test around each: rows {t,
+        max |drho/dt + div J|, max |div E - rho|} (output/gauss_test.dat)."""
+        rows = np.zeros((nsteps, 3))
+        _check(load().mg_run_step_gauss(self.ptr, int(nsteps), rows.ctypes.data))
+        return rows
+
+    def gauss_before(self):
+        _check(load().mg_gauss_before(self.ptr))
+
+    def gauss_after(self):
+        out = np.zeros(2)
+        _check(load().mg_gauss_after(self.ptr, out.ctypes.data))
+        return out
 
     def step_async(self, nsteps, energies_dev=None):
         _check(load().mg_run_step_async(self.ptr, int(nsteps), energies_dev))

@@ -31,6 +31,7 @@ CUDA_UNITS = {
     "fields64.cu": ["-fmad=false"],
     "push64.cu": ["-fmad=false"],
     "placer.cu": ["-fmad=false"],
+    "gauss.cu": ["-fmad=false"],
     "api32.cu": [],
     "fields32.cu": [],
     "push32.cu": [],

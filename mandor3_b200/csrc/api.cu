@@ -459,6 +459,9 @@ extern "C" int mg_run_destroy (mg_run_t *r)
    if (r->stage) cudaFree (r->stage);
    if (r->sort_tmp) cudaFree (r->sort_tmp);
    if (r->tile_start) cudaFree (r->tile_start);
+   for (int q = 0 ; q < 2 ; ++q)
+      if (r->gauss_rho[q]) cudaFree (r->gauss_rho[q]);
+   if (r->gauss_out) cudaFree (r->gauss_out);
    for (int e = 0 ; e < 4 ; ++e)
       if (r->ev[e]) cudaEventDestroy (r->ev[e]);
    if (r->stream) cudaStreamDestroy (r->stream);
@@ -805,34 +808,67 @@ extern "C" int mg_em_EStep_finish (mg_run_t *r)
    return MG_OK;
 }
 
+// Device buffers of the Gauss-law test: two densities and the residuals.
+static int ensure_gauss (mg_run_t *r)
+{
+   if (r->gauss_rho[0])
+      return MG_OK;
+   const size_t fb = (size_t) r->g.total*sizeof (double);
+   TRY (mg_dev_alloc (r, (void **) &r->gauss_rho[0], fb));
+   TRY (mg_dev_alloc (r, (void **) &r->gauss_rho[1], fb));
+   TRY (mg_dev_alloc (r, (void **) &r->gauss_out, 2*sizeof (double)));
+   return MG_OK;
+}
+
 extern "C" int mg_plasma_rho (mg_run_t *r, double *rho)
 {
    CHECK_RUN (r);
-   if (is32 (r)) {
-      return mg_plasma_rho32 (r, rho);
+   TRY (ensure_gauss (r));
+   double *d = r->gauss_rho[1];
+   TRY (mg_gauss_rho (r, d));
+   const long vol = (long) (r->g.n[0] + 5)*(r->g.n[1] + 5)*(r->g.n[2] + 5);
+   TRY (mg_ensure_stage (r, vol*3*sizeof (double)));
+   k_fields_out<<<mg_blocks_for (vol, 256, 8), 256, 0, r->stream>>> (r->g, (double *) r->stage, d, d, d, 2);
+   MG_LAUNCH_CHECK ();
+   // Take one component of the triplets on the host.
+   double *tmp = (double *) malloc (vol*3*sizeof (double));
+   MG_CUDA (cudaMemcpyAsync (tmp, r->stage, vol*3*sizeof (double), cudaMemcpyDeviceToHost, r->stream));
+   MG_CUDA (cudaStreamSynchronize (r->stream));
+   for (long t = 0 ; t < vol ; ++t)
+      rho[t] = tmp[3*t];
+   free (tmp);
+   return MG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Gauss-law test (core/plasma_gaussTest.c:89-149).
+// ---------------------------------------------------------------------------
+extern "C" int mg_gauss_before (mg_run_t *r)
+{
+   CHECK_RUN (r);
+   TRY (ensure_gauss (r));
+   TRY (mg_gauss_rho (r, r->gauss_rho[0]));
+   MG_CUDA (cudaStreamSynchronize (r->stream));
+   return MG_OK;
+}
+
+extern "C" int mg_gauss_after (mg_run_t *r, double out[2])
+{
+   CHECK_RUN (r);
+   if (!r->gauss_rho[0]) {
+      mg_set_error ("mg_gauss_after: mg_gauss_before has not been called");
+      return MG_ERR_STATE;
    }
-   const size_t fb = (size_t) r->g.total*sizeof (double);
-   double *d = nullptr;
-   TRY (mg_dev_alloc (r, (void **) &d, fb));
-   cudaMemsetAsync (d, 0, fb, r->stream);
-   int rc = mg_rho64 (r, d);
-   if (rc == MG_OK) {
-      const long vol = (long) (r->g.n[0] + 5)*(r->g.n[1] + 5)*(r->g.n[2] + 5);
-      rc = mg_ensure_stage (r, vol*3*sizeof (double));
-      if (rc == MG_OK) {
-         k_fields_out<<<mg_blocks_for (vol, 256, 8), 256, 0, r->stream>>> (r->g, (double *) r->stage, d, d, d, 2);
-         // Take one component of the triplets on the host.
-         double *tmp = (double *) malloc (vol*3*sizeof (double));
-         cudaMemcpyAsync (tmp, r->stage, vol*3*sizeof (double), cudaMemcpyDeviceToHost, r->stream);
-         cudaStreamSynchronize (r->stream);
-         for (long t = 0 ; t < vol ; ++t)
-            rho[t] = tmp[3*t];
-         free (tmp);
-      }
+   TRY (mg_gauss_rho (r, r->gauss_rho[1]));
+   TRY (mg_gauss_residual (r, r->gauss_rho[0], r->gauss_rho[1], r->gauss_out));
+   double res[2];
+   MG_CUDA (cudaMemcpyAsync (res, r->gauss_out, sizeof (res), cudaMemcpyDeviceToHost, r->stream));
+   MG_CUDA (cudaStreamSynchronize (r->stream));
+   if (out) {
+      out[0] = res[0];
+      out[1] = res[1];
    }
-   cudaFree (d);
-   r->dev_bytes -= fb;
-   return rc;
+   return MG_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -1149,6 +1185,40 @@ extern "C" int mg_batch_step (mg_batch_t *b, int nsteps, double *const *energies
       TRY (check_err (b->runs[q]));
    }
    return MG_OK;
+}
+
+extern "C" int mg_run_step_gauss (mg_run_t *r, int nsteps, double *rows)
+{
+   CHECK_RUN (r);
+   if (!r->inited || r->stage_no != 0) {
+      mg_set_error ("mg_run_step_gauss: run not initialised or inside a staged step");
+      return MG_ERR_STATE;
+   }
+   TRY (ensure_gauss (r));
+   TRY (build_graph (r));
+   // gauss_start: the density at the start (plasma_gaussTest.c:77).
+   TRY (mg_gauss_rho (r, r->gauss_rho[1]));
+   for (int s = 0 ; s < nsteps ; ++s) {
+      double *t = r->gauss_rho[0];
+      r->gauss_rho[0] = r->gauss_rho[1];
+      r->gauss_rho[1] = t;
+      const double time = r->time;
+      TRY (maybe_sort (r));
+      MG_CUDA (cudaMemsetAsync (&r->dsc->step, 0, sizeof (int), r->stream));
+      MG_CUDA (cudaGraphLaunch (r->gexec[0], r->stream));
+      TRY (mg_gauss_rho (r, r->gauss_rho[1]));
+      TRY (mg_gauss_residual (r, r->gauss_rho[0], r->gauss_rho[1], r->gauss_out));
+      double res[2];
+      MG_CUDA (cudaMemcpyAsync (res, r->gauss_out, sizeof (res), cudaMemcpyDeviceToHost, r->stream));
+      MG_CUDA (cudaStreamSynchronize (r->stream));
+      r->time += r->g.tau;
+      if (rows) {
+         rows[3*(size_t) s] = time;
+         rows[3*(size_t) s + 1] = res[0];
+         rows[3*(size_t) s + 2] = res[1];
+      }
+   }
+   return check_err (r);
 }
 
 extern "C" int mg_run_synchronize (mg_run_t *r)

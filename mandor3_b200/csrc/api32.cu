@@ -562,14 +562,6 @@ int mg_run_get_markers32 (mg_run_t *r, mg_marker_t *out, long long cap, long lon
    return MG_OK;
 }
 
-int mg_plasma_rho32 (mg_run_t *r, double *rho)
-{
-   (void) r;
-   (void) rho;
-   mg_set_error ("mg_plasma_rho: use the FP64 form for the charge density diagnostic");
-   return MG_ERR_ARG;
-}
-
 // Placement: FP64 positions from the shared generator, then split into cell
 // and FP32 offset (placer.cu writes into a Markers64 view of staging).
 int mg_place64 (mg_run_t *r, const mg_place_t *spec, long long at, long long count);

@@ -135,6 +135,10 @@ struct mg_run {
    int         has_laser;
    mg_laser_t  laser;
 
+   // Gauss-law test: densities before/after a step, residuals
+   double     *gauss_rho[2];
+   double     *gauss_out;
+
    // staging
    void       *stage;
    size_t      stage_bytes;
@@ -193,7 +197,8 @@ int mg_fields64_zero_j (mg_run_t *r);
 int mg_fields64_h_both (mg_run_t *r);
 int mg_fields64_e_fused (mg_run_t *r);
 int mg_push64 (mg_run_t *r);
-int mg_rho64 (mg_run_t *r, double *rho_dev);
+int mg_gauss_rho (mg_run_t *r, double *rho);
+int mg_gauss_residual (mg_run_t *r, const double *rho1, const double *rho2, double *out_dev);
 int mg_end_step (mg_run_t *r);
 
 int mg_fields32_h_half (mg_run_t *r);
@@ -222,7 +227,6 @@ int mg_run_get_fields32 (mg_run_t *r, double *E, double *H);
 int mg_run_get_current32 (mg_run_t *r, double *J);
 int mg_run_set_markers32 (mg_run_t *r, const mg_marker_t *m, long long n);
 int mg_run_get_markers32 (mg_run_t *r, mg_marker_t *m, long long cap, long long *n);
-int mg_plasma_rho32 (mg_run_t *r, double *rho);
 
 // Grid sizing: a multiple of the SM count (148 on B200).
 int mg_sm_count (void);

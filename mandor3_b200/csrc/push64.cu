@@ -28,8 +28,6 @@
 
 namespace {
 
-__device__ __forceinline__ int dbl_to_int (double x) { return (int) (x + 128.0) - 128; }
-
 // MF_DBL_TO_INT (misc_PIC.h:18) without conversion instructions: for
 // y = s + 128 in [0, 2^31), t = y + 1.5*2^52 holds round(y) in the low bits
 // of its significand, t - 1.5*2^52 is that integer as a double (exact), and
@@ -497,32 +495,6 @@ k_push64 (Ctx c, Markers64 m, long long np, DevScalars *dsc)
    }
 }
 
-// CIC charge density (core/plasma_rho.c:23-60), no folding.
-__global__ void k_rho64 (Grid g, Markers64 m, long long np, double *rho)
-{
-   for (long long n = blockIdx.x*(long long) blockDim.x + threadIdx.x ; n < np ;
-        n += (long long) gridDim.x*blockDim.x) {
-      const double qm = m.qm[n];
-      if (qm == 0.0)
-         continue;
-      double sx = m.x[n]/g.h[0], sy = m.y[n]/g.h[1], sz = m.z[n]/g.h[2];
-      const int i = dbl_to_int (sx), j = dbl_to_int (sy), k = dbl_to_int (sz);
-      if (i < -1 || i > g.n[0] || j < -1 || j > g.n[1] || k < -1 || k > g.n[2])
-         continue;
-      sx -= i; sy -= j; sz -= k;
-      const long o = g.at (i, j, k), Sx = g.sx, Sy = g.sy;
-      const double v = m.rho[n];
-      atomicAdd (rho + o, (1 - sx)*(1 - sy)*(1 - sz)*v);
-      atomicAdd (rho + o + Sx, sx*(1 - sy)*(1 - sz)*v);
-      atomicAdd (rho + o + Sy, (1 - sx)*sy*(1 - sz)*v);
-      atomicAdd (rho + o + Sx + Sy, sx*sy*(1 - sz)*v);
-      atomicAdd (rho + o + 1, (1 - sx)*(1 - sy)*sz*v);
-      atomicAdd (rho + o + Sx + 1, sx*(1 - sy)*sz*v);
-      atomicAdd (rho + o + Sy + 1, (1 - sx)*sy*sz*v);
-      atomicAdd (rho + o + Sx + Sy + 1, sx*sy*sz*v);
-   }
-}
-
 // Particle walls applied once to freshly loaded markers (plasma_init,
 // core/plasma.c:399-404, on markers that all start in the shell).
 __global__ void k_walls64 (Grid g, Markers64 m, long long np, DevScalars *dsc)
@@ -602,12 +574,3 @@ int mg_push64 (mg_run_t *r)
    return MG_OK;
 }
 
-int mg_rho64 (mg_run_t *r, double *rho_dev)
-{
-   if (r->np == 0)
-      return MG_OK;
-   const int T = 256;
-   k_rho64<<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (r->g, r->m64, r->np, rho_dev);
-   MG_LAUNCH_CHECK ();
-   return MG_OK;
-}

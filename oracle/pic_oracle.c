@@ -832,26 +832,109 @@ int po_step (po_run_t *r, double out[5])
 }
 
 /* CIC charge density: core/plasma_rho.c:23-60 restated (no folding). */
+/* Charge density: CIC deposit (plasma.c:322-329 calling plasmaRho_add,
+ * plasma_rho.c:159-173, with the nested weights of mf_PIC_distribute,
+ * misc_PIC.h:164-195: node (i+a, j+b, k+c) gets wx_a*(wy_b*(wz_c*rho)), nodes in
+ * the macro's order), then the walls of plasmaRho_applyBoundary
+ * (plasma_rho.c:23-97) in the order x, y, z, lower then upper:
+ *   periodic (at the lower wall only): for the 5 layers a = -2..2,
+ *     rho[a + n] += rho[a]; rho[a] = rho[a + n];
+ *   mirror / open: with the wall node w and the outward step o,
+ *     rho[w - o] += rho[w + o]; rho[w - 2o] += rho[w + 2o]; rho[w] = 0;
+ *     rho[w + o] = -rho[w - o]; rho[w + 2o] = -rho[w - 2o];
+ * over the wall plane's nodes [-2, n+2] in the two other axes.  The VSP
+ * filter (plasma_VSP.c:32) is off at its default alpha = 1. */
+static void rho_add (double *rho, long o, long Sx, long Sy, double sx, double sy, double sz, double v)
+{
+   const double z0 = (1 - sz)*v, z1 = sz*v;
+   const double y00 = (1 - sy)*z0, y10 = sy*z0, y01 = (1 - sy)*z1, y11 = sy*z1;
+   rho[o]               += (1 - sx)*y00;
+   rho[o + Sx]          += sx*y00;
+   rho[o + Sy]          += (1 - sx)*y10;
+   rho[o + Sx + Sy]     += sx*y10;
+   rho[o + 1]           += (1 - sx)*y01;
+   rho[o + Sx + 1]      += sx*y01;
+   rho[o + Sy + 1]      += (1 - sx)*y11;
+   rho[o + Sx + Sy + 1] += sx*y11;
+}
+
 void po_rho (const po_run_t *r, double *rho)
 {
-   const int d1 = r->dim[1], d2 = r->dim[2];
-   memset (rho, 0, sizeof (double)*(long) r->dim[0]*d1*d2);
+   memset (rho, 0, sizeof (double)*(long) r->dim[0]*r->dim[1]*r->dim[2]);
    for (long n = 0 ; n < r->np ; ++n) {
       const po_marker_t *p = r->p + n;
       double sx = p->x/r->h[0], sy = p->y/r->h[1], sz = p->z/r->h[2];
       int i = dbl_to_int (sx), j = dbl_to_int (sy), k = dbl_to_int (sz);
       sx -= i; sy -= j; sz -= k;
-      long o = IX (r, i, j, k), Sx = r->s[0], Sy = r->s[1];
-      double v = p->rho;
-      rho[o]               += (1 - sx)*(1 - sy)*(1 - sz)*v;
-      rho[o + Sx]          += sx*(1 - sy)*(1 - sz)*v;
-      rho[o + Sy]          += (1 - sx)*sy*(1 - sz)*v;
-      rho[o + Sx + Sy]     += sx*sy*(1 - sz)*v;
-      rho[o + 1]           += (1 - sx)*(1 - sy)*sz*v;
-      rho[o + Sx + 1]      += sx*(1 - sy)*sz*v;
-      rho[o + Sy + 1]      += (1 - sx)*sy*sz*v;
-      rho[o + Sx + Sy + 1] += sx*sy*sz*v;
+      rho_add (rho, IX (r, i, j, k), r->s[0], r->s[1], sx, sy, sz, p->rho);
    }
+   static const int axes[3][3] = {{0, 1, 2}, {1, 0, 2}, {2, 0, 1}};
+   for (int b = 0 ; b < 6 ; ++b) {
+      const int ea = axes[b/2][0], ep = axes[b/2][1], eq = axes[b/2][2], top = b & 1;
+      const int bc = r->bc[top][ea], n = r->n[ea];
+      for (int p = -2 ; p <= r->n[ep] + 2 ; ++p)
+         for (int q = -2 ; q <= r->n[eq] + 2 ; ++q) {
+            if (bc == PO_BC_PERIODIC) {
+               if (top)
+                  continue;
+               for (int a = -2 ; a <= 2 ; ++a) {
+                  const long lo = IXA (r, ea, a, ep, p, eq, q), hi = IXA (r, ea, a + n, ep, p, eq, q);
+                  rho[hi] += rho[lo];
+                  rho[lo] = rho[hi];
+               }
+            } else {
+               const int w = top ? n : 0, o = top ? 1 : -1;
+               const long in1 = IXA (r, ea, w - o, ep, p, eq, q), out1 = IXA (r, ea, w + o, ep, p, eq, q);
+               const long in2 = IXA (r, ea, w - 2*o, ep, p, eq, q), out2 = IXA (r, ea, w + 2*o, ep, p, eq, q);
+               rho[in1] += rho[out1];
+               rho[in2] += rho[out2];
+               rho[IXA (r, ea, w, ep, p, eq, q)] = 0;
+               rho[out1] = -rho[in1];
+               rho[out2] = -rho[in2];
+            }
+         }
+   }
+}
+
+/* Gauss-law test (plasma_gaussTest.c:110-149): over nodes [0, n]^3 the
+ * largest |(rho2 - rho1)/tau + div J| and |div E - rho2|, with the run's J
+ * (after the current walls) and E (after the E step). */
+void po_gauss (const po_run_t *r, const double *rho1, const double *rho2, double out[2])
+{
+   double d0 = -1, d1 = -1;
+   const long Sx = r->s[0], Sy = r->s[1];
+   for (int i = 0 ; i <= r->n[0] ; ++i)
+      for (int j = 0 ; j <= r->n[1] ; ++j)
+         for (int k = 0 ; k <= r->n[2] ; ++k) {
+            const long o = IX (r, i, j, k);
+            const double t0 = (rho2[o] - rho1[o])/r->tau +
+                              (r->j[0][o + Sx] - r->j[0][o])/r->h[0] +
+                              (r->j[1][o + Sy] - r->j[1][o])/r->h[1] +
+                              (r->j[2][o + 1] - r->j[2][o])/r->h[2];
+            const double t1 = (r->e[0][o + Sx] - r->e[0][o])/r->h[0] +
+                              (r->e[1][o + Sy] - r->e[1][o])/r->h[1] +
+                              (r->e[2][o + 1] - r->e[2][o])/r->h[2] -
+                              rho2[o];
+            d0 = (fabs (t0) > d0) ? fabs (t0) : d0;
+            d1 = (fabs (t1) > d1) ? fabs (t1) : d1;
+         }
+   out[0] = d0;
+   out[1] = d1;
+}
+
+long po_mesh_size (const po_run_t *r)
+{
+   return (long) r->dim[0]*r->dim[1]*r->dim[2];
+}
+
+/* Copies the region [-2, n+2]^3 of an internal mesh to out (k fastest). */
+void po_region (const po_run_t *r, const double *mesh, double *out)
+{
+   long q = 0;
+   for (int i = -G ; i <= r->n[0] + G ; ++i)
+      for (int j = -G ; j <= r->n[1] + G ; ++j)
+         for (int k = -G ; k <= r->n[2] + G ; ++k)
+            out[q++] = mesh[IX (r, i, j, k)];
 }
 
 /* ------------------------------------------------------------------------

@@ -80,8 +80,15 @@ void po_em_e_step (po_run_t *r);
 void po_jbc (po_run_t *r);
 void po_em_e_finish (po_run_t *r);
 
-/* Charge density (plasma_rho.c restated), region [-2,n+2]. */
+/* Charge density (plasma.c:322-329, plasma_rho.c restated, walls folded)
+ * into an internal mesh of po_mesh_size doubles. */
 void po_rho (const po_run_t *r, double *rho);
+long po_mesh_size (const po_run_t *r);
+/* The region [-2, n+2]^3 of an internal mesh, k fastest. */
+void po_region (const po_run_t *r, const double *mesh, double *out);
+/* Gauss-law test (plasma_gaussTest.c:110-149): out = {max |(rho2-rho1)/tau
+ * + div J|, max |div E - rho2|} over nodes [0, n]^3. */
+void po_gauss (const po_run_t *r, const double *rho1, const double *rho2, double out[2]);
 
 /* Marsaglia-Zaman "ranmar" generator (misc_ranmar.c:79-146 restated). */
 typedef struct {

@@ -40,6 +40,10 @@ def _load():
     lib.po_time.argtypes = [vp]
     lib.po_em_energy.argtypes = [vp, vp, vp]
     lib.po_rho.argtypes = [vp, vp]
+    lib.po_mesh_size.restype = C.c_long
+    lib.po_mesh_size.argtypes = [vp]
+    lib.po_region.argtypes = [vp, vp, vp]
+    lib.po_gauss.argtypes = [vp, vp, vp, vp]
     lib.po_ranmar_init.argtypes = [vp, C.c_int, C.c_int]
     lib.po_ranmar.argtypes = [vp, vp, C.c_long]
     lib.po_place_count.restype = C.c_long
@@ -149,3 +153,31 @@ class OracleRun:
 
     def time(self):
         return lib().po_time(self.ptr)
+
+    def _rho_mesh(self):
+        m = np.zeros(lib().po_mesh_size(self.ptr))
+        lib().po_rho(self.ptr, m.ctypes.data)
+        return m
+
+    def rho(self):
+        """Charge density over nodes [-2, n+2]^3 (walls folded)."""
+        m = self._rho_mesh()
+        out = np.zeros((self.n[0] + 5, self.n[1] + 5, self.n[2] + 5))
+        lib().po_region(self.ptr, m.ctypes.data, out.ctypes.data)
+        return out
+
+    def step_gauss(self, k=1):
+        """k steps with the Gauss-law test around each (plasma_gaussTest.c):
+        rows {t, max |drho/dt + div J|, max |div E - rho|}, t at the start of
+        the step as the reference prints it."""
+        rows = np.zeros((k, 3))
+        rho2 = self._rho_mesh()
+        out = np.zeros(2)
+        for s in range(k):
+            rho1 = rho2
+            rows[s, 0] = self.time()
+            lib().po_step(self.ptr, np.zeros(5).ctypes.data)
+            rho2 = self._rho_mesh()
+            lib().po_gauss(self.ptr, rho1.ctypes.data, rho2.ctypes.data, out.ctypes.data)
+            rows[s, 1:] = out
+        return rows
