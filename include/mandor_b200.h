@@ -178,6 +178,29 @@ int  mg_run_device_bytes (mg_run_t *run, long long *bytes);
 /* Estimated device bytes for a run with these parameters and markers.     */
 long long mg_estimate_bytes (const mg_params_t *params, long long markers);
 
+/* ---- hard gauss-spot source (core/em_gaussSpot.c:31-156) -----------------
+ * The fields of .gaussSpot.cfg (written by setup/tag_gaussSpot.c:126-140),
+ * in its order.  After every E step (em_EStep_finish, core/em.c:216, at time
+ * t + tau) Ey and Ez on the x-plane i = (int) (x/h1 + 0.5) are set, for all
+ * j, k in [-1, n+1], to
+ *   Ey = sgn(ey) ampl sin(w t) f(t) exp(-dy_^2 - dz^2),
+ *   Ez = sgn(ez) ampl cos(w t) f(t) exp(-dy^2 - dz_^2),
+ * w = 2 pi frequency, dy = (j h2 - y)/width, dy_ = ((j - 1/2) h2 - y)/width
+ * (z alike), f = exp(-l^2) before front_offset with l = (t - front_offset)/
+ * duration, 1 on the plateau, exp(-l^2) after it with l = (t - front_offset
+ * - t_plateau)/duration.  NULL switches the source off.                    */
+typedef struct {
+   double ampl;          /* amplitude, units of E0                        */
+   double frequency;     /* omega / omega_0                               */
+   double x, y, z;       /* focal spot                                    */
+   double width;
+   double duration;
+   double front_offset;
+   double t_plateau;
+   int    ey, ez;        /* polarisation flags (their signs are used)     */
+} mg_gauss_spot_t;
+int  mg_run_set_gauss_spot (mg_run_t *run, const mg_gauss_spot_t *spot);
+
 /* ---- Gauss-law test (core/plasma_gaussTest.c:89-149) ---------------------
  * FP64 arithmetic in both precision forms.  mg_gauss_before stores the
  * charge density of the markers as they are (core/main.c:376 calls

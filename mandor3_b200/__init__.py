@@ -51,6 +51,13 @@ class Laser(C.Structure):
                 ("plane", C.c_int), ("margin", C.c_int)]
 
 
+class GaussSpot(C.Structure):
+    _fields_ = [("ampl", C.c_double), ("frequency", C.c_double), ("x", C.c_double),
+                ("y", C.c_double), ("z", C.c_double), ("width", C.c_double),
+                ("duration", C.c_double), ("front_offset", C.c_double), ("t_plateau", C.c_double),
+                ("ey", C.c_int), ("ez", C.c_int)]
+
+
 class Place(C.Structure):
     _fields_ = [("lo", C.c_int * 3), ("hi", C.c_int * 3), ("ppc", C.c_int),
                 ("rho", C.c_double), ("qDivM", C.c_double),
@@ -107,6 +114,7 @@ def load():
         "mg_run_device_bytes": [vp, C.POINTER(ll)],
         "mg_run_profile": [vp, i],
         "mg_run_last_timing": [vp, C.POINTER(d), C.POINTER(d)],
+        "mg_run_set_gauss_spot": [vp, vp],
         "mg_gauss_before": [vp],
         "mg_gauss_after": [vp, vp],
         "mg_run_step_gauss": [vp, i, vp],
@@ -220,6 +228,12 @@ class Run:
     def set_laser(self, **kw):
         self._laser = Laser(**kw)
         _check(load().mg_run_set_laser(self.ptr, C.byref(self._laser)))
+
+    def set_gauss_spot(self, **kw):
+        """Hard gauss-spot source (the fields of .gaussSpot.cfg); no
+        arguments switch it off."""
+        self._gspot = GaussSpot(**kw) if kw else None
+        _check(load().mg_run_set_gauss_spot(self.ptr, C.byref(self._gspot) if kw else None))
 
     def place_uniform(self, lo, hi, ppc, rho, qDivM, drift=(0, 0, 0), uth=(0, 0, 0),
                       seed=(1802, 9373), skip=0, id0=1):

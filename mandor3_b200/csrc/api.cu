@@ -622,6 +622,33 @@ extern "C" int mg_run_get_markers (mg_run_t *r, mg_marker_t *out, long long cap,
    return MG_OK;
 }
 
+extern "C" int mg_run_set_gauss_spot (mg_run_t *r, const mg_gauss_spot_t *s)
+{
+   CHECK_RUN (r);
+   if (!s) {
+      r->has_gspot = 0;
+   } else {
+      if (!(s->width > 0) || !(s->duration > 0)) {
+         mg_set_error ("mg_run_set_gauss_spot: width %g and duration %g must be positive", s->width, s->duration);
+         return MG_ERR_ARG;
+      }
+      GaussSpot &g = r->gspot;
+      g.ey = ((s->ey > 0) - (s->ey < 0))*s->ampl;        // em_gaussSpot.c:70-71, 121-122
+      g.ez = ((s->ez > 0) - (s->ez < 0))*s->ampl;
+      g.omega = 2*3.14159265358979323846*s->frequency;   // em_gaussSpot.c:48
+      g.y = s->y;
+      g.z = s->z;
+      g.width = s->width;
+      g.duration = s->duration;
+      g.front = s->front_offset;
+      g.plateau = s->t_plateau;
+      g.i = (int) (s->x/r->g.h[0] + 0.5);                  // em_gaussSpot.c:73
+      r->has_gspot = 1;
+   }
+   mg_drop_graphs (r);
+   return MG_OK;
+}
+
 extern "C" int mg_run_set_laser (mg_run_t *r, const mg_laser_t *l)
 {
    CHECK_RUN (r);

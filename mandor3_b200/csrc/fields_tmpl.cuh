@@ -668,6 +668,33 @@ __global__ void k_laser (Grid g, T *F, mg_laser_t l, const DevScalars *dsc,
    }
 }
 
+// Hard gauss-spot source (core/em_gaussSpot.c:129-156) at time t + tau:
+// threads over (j, k) in [-1, n+1]^2 of the plane; FP64 profile.
+template <typename T>
+__global__ void k_gauss_spot (Grid g, T *Ey, T *Ez, GaussSpot s, const DevScalars *dsc)
+{
+   const int nj = g.n[1] + 3, nk = g.n[2] + 3;
+   const long q = blockIdx.x*(long) blockDim.x + threadIdx.x;
+   if (q >= (long) nj*nk)
+      return;
+   const int j = (int) (q/nk) - 1, k = (int) (q % nk) - 1;
+   const double t = dsc->time + g.tau;
+   double f = 1;
+   if (t < s.front) {
+      const double l = (t - s.front)/s.duration;
+      f = exp (-l*l);
+   }
+   if (t > s.front + s.plateau) {
+      const double l = (t - s.front - s.plateau)/s.duration;
+      f = exp (-l*l);
+   }
+   const double dy_ = ((j - 0.5)*g.h[1] - s.y)/s.width, dy = (j*g.h[1] - s.y)/s.width;
+   const double dz = (k*g.h[2] - s.z)/s.width, dz_ = ((k - 0.5)*g.h[2] - s.z)/s.width;
+   const long o = g.at (s.i, j, k);
+   Ey[o] = (T) (s.ey*sin (s.omega*t)*f*exp (-dy_*dy_ - dz*dz));
+   Ez[o] = (T) (s.ez*cos (s.omega*t)*f*exp (-dy*dy - dz_*dz_));
+}
+
 // The field arrays of one precision form.
 template <typename T>
 struct FS {
@@ -909,7 +936,20 @@ int fields_jbc (mg_run_t *r, const FS<T> &fs)
    return MG_OK;
 }
 
-// Stage path: source at t + tau/2, then E -= tau J over [-1, n+1]^3.
+template <typename T>
+static int launch_gauss_spot (mg_run_t *r, const FS<T> &fs)
+{
+   if (!r->has_gspot || r->gspot.i < -1 || r->gspot.i > r->g.n[0] + 1)
+      return MG_OK;
+   const long nodes = (long) (r->g.n[1] + 3)*(r->g.n[2] + 3);
+   const int NT = 256, B = (int) ((nodes + NT - 1)/NT);
+   k_gauss_spot<<<B, NT, 0, r->stream>>> (r->g, fs.E[1], fs.E[2], r->gspot, r->dsc);
+   MG_LAUNCH_CHECK ();
+   return MG_OK;
+}
+
+// Stage path: source at t + tau/2, then E -= tau J over [-1, n+1]^3, then
+// the hard gauss-spot source.
 template <typename T>
 int fields_e_finish (mg_run_t *r, const FS<T> &fs)
 {
@@ -920,7 +960,7 @@ int fields_e_finish (mg_run_t *r, const FS<T> &fs)
    const int NT = 256;
    k_e_sub_j<<<mg_blocks_for (b.vol, NT, 16), NT, 0, r->stream>>> (r->g, f3 (fs.E), f3 (fs.J), b);
    MG_LAUNCH_CHECK ();
-   return MG_OK;
+   return launch_gauss_spot<T> (r, fs);
 }
 
 // Graph path: E += curl H - tau J in one pass away from the rim, E walls,
@@ -938,7 +978,7 @@ int fields_e_fused (mg_run_t *r, const FS<T> &fs)
    MG_LAUNCH_CHECK ();
    TRY_MG (launch_e_walls<T> (r, fs, 1));
    TRY_MG (launch_laser<T> (r, fs, 1, 1));
-   return MG_OK;
+   return launch_gauss_spot<T> (r, fs);
 }
 
 template <typename T>

@@ -71,6 +71,15 @@ struct Markers32 {
    int    *id;
 };
 
+// Hard gauss-spot source, parameters as the kernel uses them
+// (core/em_gaussSpot.c:64-123 conversions done).
+struct GaussSpot {
+   double ey, ez;          // signed amplitudes
+   double omega;           // 2 pi frequency
+   double y, z, width, duration, front, plateau;
+   int    i;               // x-plane
+};
+
 // Device-side per-run scalars (one small allocation).
 struct DevScalars {
    double time;            // t = n*tau of the step being advanced
@@ -134,6 +143,8 @@ struct mg_run {
    // laser
    int         has_laser;
    mg_laser_t  laser;
+   int         has_gspot;
+   GaussSpot   gspot;
 
    // Gauss-law test: densities before/after a step, residuals
    double     *gauss_rho[2];

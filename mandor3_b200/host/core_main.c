@@ -415,6 +415,19 @@ int main (int argc, char **argv)
    check (mg_run_create (&p, &run), "create run");
    check (mg_run_set_fields (run, E, H), "upload fields");
    check (mg_run_set_markers (run, m, nm), "upload markers");
+   /* Hard gauss-spot source when .gaussSpot.cfg exists (em_gaussSpot.c:42-62). */
+   FILE *gs = fopen (".gaussSpot.cfg", "rt");
+   if (gs) {
+      mg_gauss_spot_t s;
+      double *v[9] = {&s.ampl, &s.frequency, &s.x, &s.y, &s.z, &s.width, &s.duration,
+                      &s.front_offset, &s.t_plateau};
+      for (int q = 0 ; q < 9 ; ++q)
+         *v[q] = read_at_double (gs, ".gaussSpot.cfg");
+      s.ey = read_at_int (gs, ".gaussSpot.cfg");
+      s.ez = read_at_int (gs, ".gaussSpot.cfg");
+      fclose (gs);
+      check (mg_run_set_gauss_spot (run, &s), "gauss spot");
+   }
    check (mg_run_init (run), "init");
    free (E);
    free (H);

@@ -30,6 +30,8 @@ struct po_run {
    long   np;
    po_laser_t laser;
    int    has_laser;
+   po_gauss_spot_t gspot;
+   int    has_gspot;
 };
 
 static inline long IX (const po_run_t *r, int i, int j, int k)
@@ -802,11 +804,49 @@ void po_em_e_step (po_run_t *r)
 }
 
 /* em_EStep_finish (core/em.c:189-222): source at t + tau/2, E -= tau*J. */
+void po_set_gauss_spot (po_run_t *r, const po_gauss_spot_t *s)
+{
+   r->gspot = *s;
+   r->has_gspot = 1;
+}
+
+/* gaussSpot_forceE (core/em_gaussSpot.c:129-156) at time t, with the
+ * conversions of gaussSpot_init (:48, 70-73, 121-122): Ey and Ez set on the
+ * x-plane i = (int) (x/h1 + 0.5) over j, k in [-1, n+1]. */
+static void gauss_spot_e (po_run_t *r, double t)
+{
+   const po_gauss_spot_t *g = &r->gspot;
+   const double omega = 2*M_PI*g->frequency;
+   const double Ey = ((g->ey > 0) - (g->ey < 0))*g->ampl, Ez = ((g->ez > 0) - (g->ez < 0))*g->ampl;
+   const int i = g->x/r->h[0] + 0.5;
+   if (i < -1 || i > r->n[0] + 1)
+      return;
+   double timeFactor = 1;
+   if (t < g->front_offset) {
+      double l = (t - g->front_offset)/g->duration;
+      timeFactor = exp (- l*l);
+   }
+   if (t > g->front_offset + g->t_plateau) {
+      double l = (t - g->front_offset - g->t_plateau)/g->duration;
+      timeFactor = exp (- l*l);
+   }
+   for (int j = -1 ; j <= r->n[1] + 1 ; j++) {
+      const double dy_ = ((j - 0.5)*r->h[1] - g->y)/g->width, dy = (j*r->h[1] - g->y)/g->width;
+      for (int k = -1 ; k <= r->n[2] + 1 ; k++) {
+         const double dz = (k*r->h[2] - g->z)/g->width, dz_ = ((k - 0.5)*r->h[2] - g->z)/g->width;
+         r->e[1][IX (r, i, j, k)] = Ey*sin (omega*t)*timeFactor*exp (- dy_*dy_ - dz*dz);
+         r->e[2][IX (r, i, j, k)] = Ez*cos (omega*t)*timeFactor*exp (- dy*dy - dz_*dz_);
+      }
+   }
+}
+
 void po_em_e_finish (po_run_t *r)
 {
    if (r->has_laser)
       laser_e (r, r->time + 0.5*r->tau);
    e_sub_current (r);
+   if (r->has_gspot)
+      gauss_spot_e (r, r->time + r->tau);
 }
 
 /* One step in core/main.c:353-478 order. */

@@ -63,6 +63,14 @@ void po_get_markers (const po_run_t *r, po_marker_t *m);
 
 void po_set_laser (po_run_t *r, const po_laser_t *l);
 
+/* Hard gauss-spot source: the fields of .gaussSpot.cfg in its order
+ * (core/em_gaussSpot.c:46-56), frequency in omega_0. */
+typedef struct {
+   double ampl, frequency, x, y, z, width, duration, front_offset, t_plateau;
+   int    ey, ez;
+} po_gauss_spot_t;
+void po_set_gauss_spot (po_run_t *r, const po_gauss_spot_t *s);
+
 /* em_init / cap_init equivalent: ghost fill and Mur history from E. */
 void po_init (po_run_t *r);
 

@@ -4,7 +4,8 @@ Runs the reference setup.out / core.out (built from the reference sources by
 oracle/Makefile into oracle/_ref) on each case's initial state and stores the
 final markers, E, H and the diag.dat energy rows in tests/golden/<case>.npz;
 for two cases also the Gauss-law rows of core_gauss.out in
-tests/golden/gauss_<case>.npz.
+tests/golden/gauss_<case>.npz, and the fields of an empty Mur box driven by
+the hard gauss-spot source in tests/golden/gauss_spot.npz.
 
     make -C oracle ref REF=/path/to/reference
     python tests/golden/make_golden.py
@@ -64,11 +65,39 @@ def make_gauss(name):
 
 GAUSS_CASES = ("periodic_thermal", "mur_mixed")
 
+# Hard gauss-spot source in an empty Mur box (core/em_gaussSpot.c).
+SPOT_N = (20, 16, 16)
+SPOT_L_UM = (1.0, 0.8, 0.8)
+SPOT_STEPS = 40
+
+
+def spot_params(h):
+    return dict(ampl=2.0, frequency=1.0, x=6 * h[0], y=0.4, z=0.4, width=0.2, duration=0.3,
+                front_offset=0.4, t_plateau=0.1, ey=1, ez=-1)
+
+
+def make_gauss_spot():
+    rr = RefRun()
+    try:
+        dom = rr.setup(SPOT_N, SPOT_L_UM, -0.5, (2, 2, 2), (2, 2, 2))
+        h, tau = dom["h"], dom["tau"]
+        rr.set_state(np.zeros(0, dtype=oracle_port.MARKER_DTYPE))
+        rr.set_gauss_spot(**spot_params(h))
+        rr.run(SPOT_STEPS)
+        m, E, H = rr.final()
+        np.savez_compressed(os.path.join(HERE, "gauss_spot.npz"), h=h, tau=tau, E=E, H=H, diag=rr.diag())
+        print("gauss_spot: E max %.3e" % np.max(np.abs(E)))
+    finally:
+        rr.cleanup()
+
 
 if __name__ == "__main__":
     if not have_reference():
         sys.exit("reference binaries missing: make -C oracle ref REF=<reference tree>")
-    for name in (sys.argv[1:] or list(cases.CASES)):
+    for name in (sys.argv[1:] or list(cases.CASES) + ["gauss_spot"]):
+        if name == "gauss_spot":
+            make_gauss_spot()
+            continue
         make(name)
         if name in GAUSS_CASES:
             make_gauss(name)

@@ -44,6 +44,7 @@ def _load():
     lib.po_mesh_size.argtypes = [vp]
     lib.po_region.argtypes = [vp, vp, vp]
     lib.po_gauss.argtypes = [vp, vp, vp, vp]
+    lib.po_set_gauss_spot.argtypes = [vp, vp]
     lib.po_ranmar_init.argtypes = [vp, C.c_int, C.c_int]
     lib.po_ranmar.argtypes = [vp, vp, C.c_long]
     lib.po_place_count.restype = C.c_long
@@ -98,6 +99,11 @@ def ranmar(ij, kl, n):
     return out
 
 
+class PoGaussSpot(C.Structure):
+    _fields_ = [(f, C.c_double) for f in ("ampl", "frequency", "x", "y", "z", "width", "duration",
+                                          "front_offset", "t_plateau")] + [("ey", C.c_int), ("ez", C.c_int)]
+
+
 class OracleRun:
     def __init__(self, n, h, tau, bc_min, bc_max, time=0.0):
         self.n = tuple(int(v) for v in n)
@@ -141,6 +147,10 @@ class OracleRun:
     def set_laser(self, **kw):
         self._laser = Laser(**kw)
         lib().po_set_laser(self.ptr, C.byref(self._laser))
+
+    def set_gauss_spot(self, **kw):
+        self._gspot = PoGaussSpot(**kw)
+        lib().po_set_gauss_spot(self.ptr, C.byref(self._gspot))
 
     def init(self):
         lib().po_init(self.ptr)

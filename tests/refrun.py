@@ -201,6 +201,15 @@ class RefRun:
                 _, hdr, _ = read_mesh(f)
                 write_mesh(f, hdr, arr)
 
+    def set_gauss_spot(self, ampl, frequency, x, y, z, width, duration, front_offset, t_plateau, ey, ez):
+        """.gaussSpot.cfg as setup/tag_gaussSpot.c:126-140 writes it (the
+        order core/em_gaussSpot.c:46-56 reads)."""
+        vals = [ampl, frequency, x, y, z, width, duration, front_offset, t_plateau]
+        with open(self.path(".gaussSpot.cfg"), "w") as fp:
+            for v in vals:
+                fp.write("@ %.17e\tparameter\n" % v)
+            fp.write("@ %d\tEy\n@ %d\tEz\n" % (ey, ez))
+
     def run(self, steps, exe="core.out", timeout=3600):
         with open(self.path("run_mandor.cfg"), "w") as fp:
             fp.write("@ %d\ttotal steps\n@ %d\tcheckpoint period\n@ -1\ttecplot\n"

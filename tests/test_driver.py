@@ -159,3 +159,27 @@ def test_driver_stops_on_request():
                    [cases.H_LAMBDA] * 3))) - 4) < 1e-6
     finally:
         shutil.rmtree(root, ignore_errors=True)
+
+
+@pytest.mark.gpu
+def test_driver_applies_the_gauss_spot_config():
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import make_golden
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "gauss_spot.npz"))
+    h, tau = tuple(g["h"]), float(g["tau"])
+    root = tempfile.mkdtemp(prefix="mg_drv_")
+    try:
+        n = make_golden.SPOT_N
+        z = np.zeros((n[0] + 1, n[1] + 1, n[2] + 1, 3))
+        refrun.write_checkpoint0(root, n, h, tau, (2, 2, 2), (2, 2, 2), z, z,
+                                 np.zeros(0, refrun.MARKER_DTYPE))
+        refrun.write_run_cfg(root, make_golden.SPOT_STEPS, 10 ** 6)
+        refrun.RefRun(root).set_gauss_spot(**make_golden.spot_params(h))
+        out = subprocess.run([DRIVER], cwd=root, stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
+                             timeout=600)
+        assert out.returncode == 0, out.stdout.decode()
+        m, E, H = read_record(root, 1)
+        assert parity.rel_err(E, g["E"]) < 1e-12 and parity.rel_err(H, g["H"]) < 1e-12
+    finally:
+        shutil.rmtree(root, ignore_errors=True)

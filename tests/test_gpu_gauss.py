@@ -72,3 +72,32 @@ def test_stage_hooks_give_the_same_rows():
     out = r.gauss_after()
     assert abs(out[0] - ref[0, 1]) <= 1e-6 * ref[0, 1]
     assert abs(out[1] - ref[0, 2]) <= 1e-6 * ref[0, 2]
+
+
+@pytest.mark.parametrize("precision,tol", [(mg.FP64, 1e-12), (mg.FP32_OFFSET, 1e-5)])
+@pytest.mark.parametrize("staged", [False, True])
+def test_gauss_spot_matches_the_reference(precision, tol, staged):
+    import sys, os
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import make_golden
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "gauss_spot.npz"))
+    h, tau = tuple(g["h"]), float(g["tau"])
+    r = mg.Run(make_golden.SPOT_N, h, tau, (2, 2, 2), (2, 2, 2), precision=precision)
+    z = np.zeros(r.field_shape())
+    r.set_fields(z, z)
+    r.set_gauss_spot(**make_golden.spot_params(h))
+    r.init()
+    if staged:
+        for _ in range(make_golden.SPOT_STEPS):
+            r.em_HHalfStep()
+            r.em_energy()
+            r.plasma_move()
+            r.em_HStep()
+            r.em_EStep_start()
+            r.jbc_finish()
+            r.em_EStep_finish()
+    else:
+        r.step(make_golden.SPOT_STEPS)
+    E, H = r.fields()
+    assert parity.rel_err(E, g["E"]) < tol
+    assert parity.rel_err(H, g["H"]) < tol
