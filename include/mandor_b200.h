@@ -178,6 +178,51 @@ int  mg_run_device_bytes (mg_run_t *run, long long *bytes);
 /* Estimated device bytes for a run with these parameters and markers.     */
 long long mg_estimate_bytes (const mg_params_t *params, long long markers);
 
+/* ---- the reference's placers (setup.out tags) on the device --------------
+ * Markers are appended in setup.out's order with ids id0, id0+1, ... (the
+ * ids setup/plasma.c:93-123 writes); positions, momenta and weights are
+ * bit-identical to setup.out's.  Call mg_run_init afterwards.
+ *
+ * mg_run_place_maxwell: [plasma] (setup/tag_plasma.c:45-152, no filters)
+ * then [DF:Maxwell] (setup/tag_maxwell.c:36-168): in every cell (I-major) the
+ * lattice points ((i + 1/2)/nx) h1 + I h1, ... of nx*ny*nz per cell, `layers`
+ * markers on each (an even number); momenta from the quiet-start pattern
+ * (Hammersley radix-2/3/5 quartets, setup/setup_denavit.c, mapped through the
+ * inverse of the integral of exp(-x^2), setup/setup_distrMapper.c, or uniform
+ * spacing with exp(-x^2) weights), mirrored pairs, weights normalised to
+ * rho = omega_pe2 4 pi^2 / qDivM / markers-per-cell, optionally the thermal
+ * energy tuned (tune_energy).                                              */
+typedef struct {
+   int    nx, ny, nz, layers;
+   double omega_pe2;      /* (omega_pe/omega_0)^2                         */
+   double qDivM;
+   double ux, uy, uz;     /* thermal momenta per axis                      */
+   int    tune_energy, uniform_weight;
+   int    id0;
+} mg_maxwell_t;
+int  mg_run_place_maxwell (mg_run_t *run, const mg_maxwell_t *spec);
+
+/* mg_run_place_foil: [DF:foil] (setup/tag_foil.c:60-230): lattice points of
+ * nx*ny*nz per cell in the cells [5, n-5) of every axis whose lower wall is
+ * not periodic ([0, n) otherwise) where alpha = (shift - (r - r0).l)/width
+ * + 1/2 lies in [m, 1 - m], m = 1e-10 (h1+h2+h3)/(3 width); rho =
+ * (n1 + (n2 - n1) alpha)/(nx ny nz) (profile 0) or n1 (n2/n1)^alpha/(nx ny nz)
+ * (profile 1), with n1, n2 converted as the deck gives them (< 0: critical
+ * densities, > 0: cm^-3) for charge q and wavelength lambda_cm
+ * (misc_units.c:95-120); u = 0, qDivM = q/M.  Lengths in wavelengths.     */
+typedef struct {
+   double x0, y0, z0;     /* foil centre                                   */
+   double lx, ly, lz;     /* normal (normalised here)                      */
+   double width, shift;
+   int    profile;        /* 0 linear, 1 exponential                       */
+   double n1, n2;
+   double q, M;           /* charge in |e|, mass in m_e                    */
+   int    nx, ny, nz;
+   double lambda_cm;      /* wavelength, cm ([units] tag x 1e-4)           */
+   int    id0;
+} mg_foil_t;
+int  mg_run_place_foil (mg_run_t *run, const mg_foil_t *spec);
+
 /* ---- hard gauss-spot source (core/em_gaussSpot.c:31-156) -----------------
  * The fields of .gaussSpot.cfg (written by setup/tag_gaussSpot.c:126-140),
  * in its order.  After every E step (em_EStep_finish, core/em.c:216, at time

@@ -58,6 +58,21 @@ class GaussSpot(C.Structure):
                 ("ey", C.c_int), ("ez", C.c_int)]
 
 
+class Maxwell(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("layers", C.c_int),
+                ("omega_pe2", C.c_double), ("qDivM", C.c_double), ("ux", C.c_double),
+                ("uy", C.c_double), ("uz", C.c_double), ("tune_energy", C.c_int),
+                ("uniform_weight", C.c_int), ("id0", C.c_int)]
+
+
+class Foil(C.Structure):
+    _fields_ = [("x0", C.c_double), ("y0", C.c_double), ("z0", C.c_double), ("lx", C.c_double),
+                ("ly", C.c_double), ("lz", C.c_double), ("width", C.c_double), ("shift", C.c_double),
+                ("profile", C.c_int), ("n1", C.c_double), ("n2", C.c_double), ("q", C.c_double),
+                ("M", C.c_double), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("lambda_cm", C.c_double), ("id0", C.c_int)]
+
+
 class Place(C.Structure):
     _fields_ = [("lo", C.c_int * 3), ("hi", C.c_int * 3), ("ppc", C.c_int),
                 ("rho", C.c_double), ("qDivM", C.c_double),
@@ -115,6 +130,8 @@ def load():
         "mg_run_profile": [vp, i],
         "mg_run_last_timing": [vp, C.POINTER(d), C.POINTER(d)],
         "mg_run_set_gauss_spot": [vp, vp],
+        "mg_run_place_maxwell": [vp, vp],
+        "mg_run_place_foil": [vp, vp],
         "mg_gauss_before": [vp],
         "mg_gauss_after": [vp, vp],
         "mg_run_step_gauss": [vp, i, vp],
@@ -228,6 +245,18 @@ class Run:
     def set_laser(self, **kw):
         self._laser = Laser(**kw)
         _check(load().mg_run_set_laser(self.ptr, C.byref(self._laser)))
+
+    def place_maxwell(self, nx, ny, nz, layers, omega_pe2, qDivM, ux, uy, uz, tune_energy=0,
+                      uniform_weight=1, id0=1):
+        """[plasma] + [DF:Maxwell] of setup.out on the device (quiet start)."""
+        s = Maxwell(nx, ny, nz, layers, omega_pe2, qDivM, ux, uy, uz, tune_energy, uniform_weight, id0)
+        _check(load().mg_run_place_maxwell(self.ptr, C.byref(s)))
+
+    def place_foil(self, x0, y0, z0, lx, ly, lz, width, n1, n2, q, M, nx, ny, nz, shift=0.0,
+                   profile=0, lambda_cm=1e-4, id0=1):
+        """[DF:foil] of setup.out on the device."""
+        s = Foil(x0, y0, z0, lx, ly, lz, width, shift, profile, n1, n2, q, M, nx, ny, nz, lambda_cm, id0)
+        _check(load().mg_run_place_foil(self.ptr, C.byref(s)))
 
     def set_gauss_spot(self, **kw):
         """Hard gauss-spot source (the fields of .gaussSpot.cfg); no

@@ -32,6 +32,7 @@ CUDA_UNITS = {
     "push64.cu": ["-fmad=false"],
     "placer.cu": ["-fmad=false"],
     "gauss.cu": ["-fmad=false"],
+    "tags.cu": ["-fmad=false"],
     "api32.cu": [],
     "fields32.cu": [],
     "push32.cu": [],

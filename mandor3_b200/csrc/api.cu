@@ -1307,6 +1307,11 @@ int mg_place64 (mg_run_t *r, const mg_place_t *spec, long long at, long long cou
 int mg_place32 (mg_run_t *r, const mg_place_t *spec, long long at, long long count);
 int mg_ensure_capacity32 (mg_run_t *r, long long need);
 
+int mg_ensure_capacity64 (mg_run_t *r, long long need)
+{
+   return ensure_capacity (r, need);
+}
+
 extern "C" int mg_run_place_uniform (mg_run_t *r, const mg_place_t *s)
 {
    CHECK_RUN (r);

@@ -91,12 +91,72 @@ def make_gauss_spot():
         rr.cleanup()
 
 
+# The reference placers (see make_placers).
+FOIL = dict(n=(24, 8, 8), L_um=(1.2, 0.4, 0.4), bc=(2, 0, 0),
+            spec=dict(x0=0.6, y0=0.2, z0=0.2, lx=1.0, ly=0.2, lz=0.0, width=0.2, shift=0.01,
+                      profile=1, n1=-20.0, n2=-60.0, q=-1.0, M=1.0, nx=2, ny=2, nz=2))
+
+
+def placer_deck(cfg):
+    """A setup deck with one [DF:foil] tag (setup/tag_foil.c:60-100 order)."""
+    from refrun import deck_text
+    s = cfg["spec"]
+    text = deck_text(cfg["n"], cfg["L_um"], -0.5, cfg["bc"], cfg["bc"])
+    text += ("\n[DF:foil]\n@ %.17g\tx0\n@ %.17g\ty0\n@ %.17g\tz0\n@ %.17g\tlx\n@ %.17g\tly\n"
+             "@ %.17g\tlz\n@ %.17g\twidth\n> %.17g\tshift\n@ %s\tprofile\n@ %.17g\tn1\n"
+             "@ %.17g\tn2\n@ %.17g\tq\n@ %.17g\tM\n@ %d\tnx\n@ %d\tny\n@ %d\tnz\n"
+             % (s["x0"], s["y0"], s["z0"], s["lx"], s["ly"], s["lz"], s["width"], s["shift"],
+                "linear" if s["profile"] == 0 else "exponential", s["n1"], s["n2"], s["q"], s["M"],
+                s["nx"], s["ny"], s["nz"]))
+    return text
+
+
+MAXWELL_SPECS = [dict(nx=2, ny=2, nz=1, layers=4, omega_pe2=1.5, qDivM=-1.0, ux=0.05, uy=0.1, uz=0.02,
+                      tune_energy=1, uniform_weight=1),
+                 dict(nx=1, ny=2, nz=3, layers=2, omega_pe2=0.7, qDivM=-1.0, ux=0.03, uy=0.03, uz=0.06,
+                      tune_energy=0, uniform_weight=0)]
+
+
+def make_placers():
+    """[DF:foil] through setup.out; the Maxwell quiet-start pattern through
+    oracle/_ref/maxwell_pattern.out (the reference's sampler and mapper):
+    setup.out's own [plasma] + [DF:Maxwell] path cannot serve, because
+    tag_plasma.c:109 (`cell[p].vx = p++`) reads and increments p without a
+    sequence point, and under GCC the pattern index lands in the next marker."""
+    import subprocess
+    from refrun import read_markers, read_domain, REF_DIR
+    rr = RefRun()
+    try:
+        with open(rr.path("deck.input"), "w") as fp:
+            fp.write(placer_deck(FOIL))
+        rr._run("setup.out", "deck.input", "create")
+        dom = read_domain(rr.path("binData", "domain.bin"))
+        m = read_markers(rr.path("binData", "plasma_000000_000.bin"))
+        np.savez_compressed(os.path.join(HERE, "place_foil.npz"), h=dom["h"], tau=dom["tau"],
+                            markers=m.tobytes())
+        print("place_foil: %d markers" % len(m))
+    finally:
+        rr.cleanup()
+    pats = []
+    for s in MAXWELL_SPECS:
+        args = [str(s[k]) for k in ("nx", "ny", "nz", "layers", "omega_pe2", "qDivM", "ux", "uy", "uz",
+                                    "tune_energy", "uniform_weight")]
+        out = subprocess.run([os.path.join(REF_DIR, "maxwell_pattern.out")] + args, stdout=subprocess.PIPE,
+                             check=True).stdout.decode()
+        pats.append(np.array([[float(v) for v in line.split()] for line in out.splitlines()]))
+    np.savez_compressed(os.path.join(HERE, "place_maxwell.npz"), **{"pattern%d" % q: p for q, p in enumerate(pats)})
+    print("place_maxwell: patterns of %s markers" % [len(p) for p in pats])
+
+
 if __name__ == "__main__":
     if not have_reference():
         sys.exit("reference binaries missing: make -C oracle ref REF=<reference tree>")
-    for name in (sys.argv[1:] or list(cases.CASES) + ["gauss_spot"]):
+    for name in (sys.argv[1:] or list(cases.CASES) + ["gauss_spot", "placers"]):
         if name == "gauss_spot":
             make_gauss_spot()
+            continue
+        if name == "placers":
+            make_placers()
             continue
         make(name)
         if name in GAUSS_CASES:
