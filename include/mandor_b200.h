@@ -178,6 +178,17 @@ int  mg_run_device_bytes (mg_run_t *run, long long *bytes);
 /* Estimated device bytes for a run with these parameters and markers.     */
 long long mg_estimate_bytes (const mg_params_t *params, long long markers);
 
+/* ---- tecplot dumps (IO_tecplot.c:108-266) --------------------------------
+ * Node-centred fields over [0, n]^3, AoS (n+1)^3 x 3 doubles, as tecIO_saveVec
+ * interpolates them: E and J as 0.5 (F[p] + F[p + d_c]) per component c, H as
+ * the average of its 4 nodes in the two other axes.  core.out writes E and H
+ * after plasma_move (E^n and H^n: call mg_tecplot_fields after
+ * mg_plasma_move) and J after the E step (mg_tecplot_currents after
+ * mg_em_EStep_finish); core_b200.out does both at the tecplot period of
+ * run_mandor.cfg.                                                          */
+int  mg_tecplot_fields (mg_run_t *run, double *E, double *H);
+int  mg_tecplot_currents (mg_run_t *run, double *J);
+
 /* ---- the reference's placers (setup.out tags) on the device --------------
  * Markers are appended in setup.out's order with ids id0, id0+1, ... (the
  * ids setup/plasma.c:93-123 writes); positions, momenta and weights are

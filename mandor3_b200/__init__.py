@@ -130,6 +130,8 @@ def load():
         "mg_run_profile": [vp, i],
         "mg_run_last_timing": [vp, C.POINTER(d), C.POINTER(d)],
         "mg_run_set_gauss_spot": [vp, vp],
+        "mg_tecplot_fields": [vp, vp, vp],
+        "mg_tecplot_currents": [vp, vp],
         "mg_run_place_maxwell": [vp, vp],
         "mg_run_place_foil": [vp, vp],
         "mg_gauss_before": [vp],
@@ -245,6 +247,17 @@ class Run:
     def set_laser(self, **kw):
         self._laser = Laser(**kw)
         _check(load().mg_run_set_laser(self.ptr, C.byref(self._laser)))
+
+    def tecplot_fields(self):
+        """Node-centred E and H (IO_tecplot.c interpolation) over [0, n]^3."""
+        E, H = np.zeros(self.field_shape()), np.zeros(self.field_shape())
+        _check(load().mg_tecplot_fields(self.ptr, E.ctypes.data, H.ctypes.data))
+        return E, H
+
+    def tecplot_current(self):
+        J = np.zeros(self.field_shape())
+        _check(load().mg_tecplot_currents(self.ptr, J.ctypes.data))
+        return J
 
     def place_maxwell(self, nx, ny, nz, layers, omega_pe2, qDivM, ux, uy, uz, tune_energy=0,
                       uniform_weight=1, id0=1):

@@ -33,6 +33,7 @@ CUDA_UNITS = {
     "placer.cu": ["-fmad=false"],
     "gauss.cu": ["-fmad=false"],
     "tags.cu": ["-fmad=false"],
+    "tecplot.cu": ["-fmad=false"],
     "api32.cu": [],
     "fields32.cu": [],
     "push32.cu": [],

@@ -261,9 +261,50 @@ static void diag_flush (diag_t *d, int *fresh, double tau)
 typedef struct {
    int sys_num;           /* next checkpoint record */
    int map_num;           /* next file map id */
+   int tec_num;           /* next tecplot record */
    unsigned char head_E[HEADER_BYTES], head_H[HEADER_BYTES];
    char prtn_src[256];
 } records_t;
+
+/* fileMap_save (IO_fileMap.c:129-157) for one rank: the map record, then
+ * fileMap.N; returns the record's id. */
+static int save_filemap (records_t *rec, const domain_t *dom)
+{
+   char path[512];
+   const int map_id = rec->map_num++;
+   snprintf (path, sizeof (path), "binData/fileMap_%06d.txt", map_id);
+   FILE *fp = open_or_die (path, "wt");
+   fprintf (fp, "%d cpus total.\n", 1);
+   fprintf (fp, "%d: (%d %d %d) - (%d %d %d)\n", 0, dom->dmin[0], dom->dmin[1], dom->dmin[2],
+            dom->dmax[0], dom->dmax[1], dom->dmax[2]);
+   fclose (fp);
+   fp = open_or_die ("binData/fileMap.N", "wt");
+   fprintf (fp, "@ %d filemaps total is written.\n", rec->map_num);
+   fclose (fp);
+   return map_id;
+}
+
+/* Region (0,0,0)-(n) and the mesh_t fields (type_mesh.h:67-84) of a mesh
+ * allocated over [-ghost, n+ghost], pointers zeroed: the header mesh_save and
+ * tecIO_saveVec write (type_mesh.c:285-313). */
+static void mesh_head (const int n[3], const char *name, int ghost, int vector,
+                       unsigned char out[HEADER_BYTES])
+{
+   int v[16] = {0, 0, 0, n[0], n[1], n[2]};
+   int w[3];
+   for (int a = 0 ; a < 3 ; ++a) {
+      v[6 + 2*a] = -ghost;
+      v[7 + 2*a] = n[a] + ghost;
+      w[a] = n[a] + 2*ghost + 1;
+   }
+   v[12] = vector ? 1 : 0;
+   v[13] = w[2];
+   v[14] = w[1]*w[2];
+   v[15] = (vector ? 24 : 8)*w[0]*w[1]*w[2];
+   memset (out, 0, HEADER_BYTES);
+   memcpy (out, v, sizeof (v));
+   strncpy ((char *) out + sizeof (v) + 16, name, 29);
+}
 
 /* sysIO_save + plasma_save (IO_sys.c:99-124, core/plasma_IO.c:273-287). */
 static void checkpoint (mg_run_t *run, records_t *rec, const domain_t *dom, long nodes, double time)
@@ -281,16 +322,8 @@ static void checkpoint (mg_run_t *run, records_t *rec, const domain_t *dom, long
    write_markers (path, m, n);
    write_domain (dom);
 
-   const int map_id = rec->map_num++;
-   snprintf (path, sizeof (path), "binData/fileMap_%06d.txt", map_id);
-   FILE *fp = open_or_die (path, "wt");
-   fprintf (fp, "%d cpus total.\n", 1);
-   fprintf (fp, "%d: (%d %d %d) - (%d %d %d)\n", 0, dom->dmin[0], dom->dmin[1], dom->dmin[2],
-            dom->dmax[0], dom->dmax[1], dom->dmax[2]);
-   fclose (fp);
-   fp = open_or_die ("binData/fileMap.N", "wt");
-   fprintf (fp, "@ %d filemaps total is written.\n", rec->map_num);
-   fclose (fp);
+   const int map_id = save_filemap (rec, dom);
+   FILE *fp;
 
    snprintf (path, sizeof (path), "binData/sys_E_%06d(%03d).bin", rec->sys_num, 0);
    write_mesh (path, rec->head_E, E, nodes);
@@ -333,6 +366,72 @@ static int stop_requested (double t0, double per_step, int stretch, double save_
    return limit > 0 && now () - t0 + per_step*stretch + save_time > limit;
 }
 
+/* One step with the tecplot dump (core/main.c:384-391, 430-434): the staged
+ * step, with E^n, H^n and the density of the moved markers written after
+ * plasma_move (tecIO_saveFields, IO_tecplot.c:220-245) and J after the E step
+ * (tecIO_saveCurrents, IO_tecplot.c:250-266).  row: the step's energy row. */
+static void tecplot_step (mg_run_t *run, records_t *rec, const domain_t *dom, long nodes, double time,
+                          double row[6])
+{
+   char path[512];
+   const int n[3] = {dom->dmax[0], dom->dmax[1], dom->dmax[2]};
+   unsigned char head[HEADER_BYTES];
+   double *a = (double *) malloc (sizeof (double)*3*nodes), *b = (double *) malloc (sizeof (double)*3*nodes);
+   const long full = (long) (n[0] + 5)*(n[1] + 5)*(n[2] + 5);
+   double *rho = (double *) malloc (sizeof (double)*full);
+
+   check (mg_em_HHalfStep (run), "H half step");
+   check (mg_em_energy (run, &row[1], &row[2]), "field energy");
+   check (mg_plasma_move (run), "plasma move");
+   check (mg_plasma_temperature (run, &row[3], &row[4], &row[5]), "temperature");
+   row[0] = time;
+   check (mg_plasma_rho (run, rho), "charge density");
+   check (mg_tecplot_fields (run, a, b), "tecplot fields");
+   write_domain (dom);                                        /* parameter_save */
+   const int map_id = save_filemap (rec, dom);
+   snprintf (path, sizeof (path), "binData/tec_E_%06d(%03d).bin", rec->tec_num, 0);
+   write_mesh (path, rec->head_E, a, nodes);
+   snprintf (path, sizeof (path), "binData/tec_H_%06d(%03d).bin", rec->tec_num, 0);
+   write_mesh (path, rec->head_H, b, nodes);
+   snprintf (path, sizeof (path), "binData/tec_%06d.txt", rec->tec_num);
+   FILE *fp = open_or_die (path, "wb");
+   const int cpus = 1;
+   write_exact (&time, sizeof (double), fp, path);
+   write_exact (&cpus, sizeof (int), fp, path);
+   write_exact (&map_id, sizeof (int), fp, path);
+   fclose (fp);
+   snprintf (path, sizeof (path), "binData/tec_prtn_%06d.bin", rec->tec_num);
+   copy_file (rec->prtn_src, path);
+
+   check (mg_em_HStep (run), "H step");
+   check (mg_em_EStep_start (run), "E step");
+   check (mg_jbc_finish (run), "current walls");
+   check (mg_em_EStep_finish (run), "E step finish");
+   check (mg_tecplot_currents (run, a), "tecplot currents");
+   mesh_head (n, "vec_J", 2, 1, head);
+   snprintf (path, sizeof (path), "binData/tec_J_%06d(%03d).bin", rec->tec_num, 0);
+   write_mesh (path, head, a, nodes);
+   /* rho over [0, n]^3 out of [-2, n+2]^3 */
+   long q = 0;
+   for (int i = 0 ; i <= n[0] ; ++i)
+      for (int j = 0 ; j <= n[1] ; ++j)
+         for (int k = 0 ; k <= n[2] ; ++k)
+            b[q++] = rho[((long) (i + 2)*(n[1] + 5) + (j + 2))*(n[2] + 5) + (k + 2)];
+   mesh_head (n, "rho", 2, 0, head);
+   snprintf (path, sizeof (path), "binData/tec_rho_%06d(%03d).bin", rec->tec_num, 0);
+   fp = open_or_die (path, "wb");
+   write_exact (head, HEADER_BYTES, fp, path);
+   write_exact (b, sizeof (double)*nodes, fp, path);
+   fclose (fp);
+   rec->tec_num++;
+   fp = open_or_die ("binData/tecplot.N", "wt");
+   fprintf (fp, "@ %d  tecplots' records written.\n", rec->tec_num);
+   fclose (fp);
+   free (a);
+   free (b);
+   free (rho);
+}
+
 int main (int argc, char **argv)
 {
    int precision = MG_FP64, device = 0;
@@ -373,10 +472,15 @@ int main (int argc, char **argv)
    if (cfg.cont && point != 0) {
       rec.sys_num = records;
       rec.map_num = read_count ("binData/fileMap.N");
+      FILE *tn = fopen ("binData/tecplot.N", "rt");       /* tecIO_setRecordNum (-1) */
+      rec.tec_num = tn ? read_at_int (tn, "binData/tecplot.N") : 0;
+      if (tn)
+         fclose (tn);
    } else {
       point = 0;
       rec.sys_num = 1;
       rec.map_num = read_count ("binData/fileMap_start.txt");
+      rec.tec_num = 1;                                  /* after setup's record 0 */
    }
 
    char path[512];
@@ -450,8 +554,19 @@ int main (int argc, char **argv)
       if (nfull < next) next = nfull;
       if (nstop < next) next = nstop;
       if (next - t > 256) next = t + 256;
-      const int k = next - t;
-      check (mg_run_step (run, k, rows), "step");
+      /* core/main.c:384: a tecplot dump on every step t (counted from 1) with
+       * t % chPoint_tecplot == 0. */
+      if (cfg.tecplot > 0) {
+         const int ntec = (t/cfg.tecplot + 1)*cfg.tecplot;
+         if (ntec - 1 > t && ntec - 1 < next) next = ntec - 1;
+      }
+      int k = next - t;
+      if (cfg.tecplot > 0 && (t + 1) % cfg.tecplot == 0) {
+         tecplot_step (run, &rec, &dom, nodes, time, rows);
+         k = 1;
+         next = t + 1;
+      } else
+         check (mg_run_step (run, k, rows), "step");
       for (int q = 0 ; q < k ; ++q)
          diag_add (&diag, rows + 6*q);
       t = next;

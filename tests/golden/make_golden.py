@@ -148,10 +148,57 @@ def make_placers():
     print("place_maxwell: patterns of %s markers" % [len(p) for p in pats])
 
 
+# Tecplot dumps: the reference core.out on the drop-in driver's case with a
+# tecplot period of 4 steps (12 steps: records 1..3).
+TEC_PERIOD = 4
+
+
+def read_tecplot(root, num):
+    """The arrays of tecplot record num: E, H, J, rho over [0, n]^3 and the
+    binary record header {time, cpus, file map id}."""
+    from refrun import read_mesh, MESH_HEADER_BYTES
+    b = os.path.join(root, "binData")
+    out = {}
+    for f in ("E", "H", "J"):
+        _, hdr, a = read_mesh(os.path.join(b, "tec_%s_%06d(000).bin" % (f, num)))
+        out[f] = a
+    raw = open(os.path.join(b, "tec_rho_%06d(000).bin" % num), "rb").read()
+    out["rho"] = np.frombuffer(raw[MESH_HEADER_BYTES:], "<f8")
+    info = open(os.path.join(b, "tec_%06d.txt" % num), "rb").read()
+    out["time"] = np.frombuffer(info[:8], "<f8")[0]
+    out["ids"] = np.frombuffer(info[8:16], "<i4")
+    return out
+
+
+def make_tecplot():
+    import tempfile, shutil, refrun
+    import test_driver
+    root = tempfile.mkdtemp(prefix="mg_tec_")
+    try:
+        rr = RefRun(root)
+        test_driver.prepare(root)
+        with open(os.path.join(root, "run_mandor.cfg"), "w") as fp:
+            fp.write("@ %d\ttotal\n@ %d\tfull\n@ %d\ttecplot\n@ 0\tcontinue\n@ %d\tstop\n@ -100\tspectr\n"
+                     % (test_driver.CASE["steps"], 10 ** 6, TEC_PERIOD, 10 ** 6))
+        rr._run("core.out")
+        arrays = {}
+        for num in (1, 2, 3):
+            t = read_tecplot(root, num)
+            for k, v in t.items():
+                arrays["%s%d" % (k, num)] = v
+        np.savez_compressed(os.path.join(HERE, "tecplot.npz"), **arrays)
+        print("tecplot: records 1-3")
+    finally:
+        shutil.rmtree(root, ignore_errors=True)
+
+
 if __name__ == "__main__":
     if not have_reference():
         sys.exit("reference binaries missing: make -C oracle ref REF=<reference tree>")
-    for name in (sys.argv[1:] or list(cases.CASES) + ["gauss_spot", "placers"]):
+    for name in (sys.argv[1:] or list(cases.CASES) + ["gauss_spot", "placers", "tecplot"]):
+        if name == "tecplot":
+            make_tecplot()
+            continue
         if name == "gauss_spot":
             make_gauss_spot()
             continue

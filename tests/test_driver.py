@@ -183,3 +183,29 @@ def test_driver_applies_the_gauss_spot_config():
         assert parity.rel_err(E, g["E"]) < 1e-12 and parity.rel_err(H, g["H"]) < 1e-12
     finally:
         shutil.rmtree(root, ignore_errors=True)
+
+
+@pytest.mark.gpu
+def test_driver_writes_the_reference_tecplot_records():
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import make_golden
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "tecplot.npz"))
+    root = tempfile.mkdtemp(prefix="mg_drv_")
+    try:
+        prepare(root)
+        with open(os.path.join(root, "run_mandor.cfg"), "w") as fp:
+            fp.write("@ %d\ttotal\n@ %d\tfull\n@ %d\ttecplot\n@ 0\tcontinue\n@ %d\tstop\n@ -100\tspectr\n"
+                     % (CASE["steps"], 10 ** 6, make_golden.TEC_PERIOD, 10 ** 6))
+        out = subprocess.run([DRIVER], cwd=root, stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
+                             timeout=600)
+        assert out.returncode == 0, out.stdout.decode()
+        assert open(os.path.join(root, "binData", "tecplot.N")).read().startswith("@ 4")
+        for num in (1, 2, 3):
+            t = make_golden.read_tecplot(root, num)
+            for f in ("E", "H", "J", "rho"):
+                assert parity.rel_err(t[f], g["%s%d" % (f, num)]) < 1e-12, (f, num)
+            assert abs(t["time"] - g["time%d" % num]) <= 1e-15
+            assert np.array_equal(t["ids"], g["ids%d" % num])
+    finally:
+        shutil.rmtree(root, ignore_errors=True)
