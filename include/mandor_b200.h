@@ -189,6 +189,17 @@ long long mg_estimate_bytes (const mg_params_t *params, long long markers);
 int  mg_tecplot_fields (mg_run_t *run, double *E, double *H);
 int  mg_tecplot_currents (mg_run_t *run, double *J);
 
+/* ---- probes (core/diag_probe.c:409-446) ----------------------------------
+ * mg_run_set_probes: probe nodes ijk[3*q..3*q+2] in [0, n) (n = 0 removes
+ * them).  Every step then records, right after the H half step (where
+ * core/main.c:373 calls probe_postData), one row {t, Ex, Ey, Ez, Hx, Hy, Hz}
+ * per probe of E^n and H^n interpolated to the node like the tecplot
+ * dumps.  mg_run_probe_samples copies the rows of the steps of the last
+ * mg_run_step call (nsteps <= 4096, rows step-major, nsteps x nprobes x 7) or,
+ * after a staged step, its one row.                                       */
+int  mg_run_set_probes (mg_run_t *run, const int *ijk, int nprobes);
+int  mg_run_probe_samples (mg_run_t *run, int nsteps, double *out);
+
 /* ---- the reference's placers (setup.out tags) on the device --------------
  * Markers are appended in setup.out's order with ids id0, id0+1, ... (the
  * ids setup/plasma.c:93-123 writes); positions, momenta and weights are

@@ -130,6 +130,8 @@ def load():
         "mg_run_profile": [vp, i],
         "mg_run_last_timing": [vp, C.POINTER(d), C.POINTER(d)],
         "mg_run_set_gauss_spot": [vp, vp],
+        "mg_run_set_probes": [vp, vp, i],
+        "mg_run_probe_samples": [vp, i, vp],
         "mg_tecplot_fields": [vp, vp, vp],
         "mg_tecplot_currents": [vp, vp],
         "mg_run_place_maxwell": [vp, vp],
@@ -247,6 +249,18 @@ class Run:
     def set_laser(self, **kw):
         self._laser = Laser(**kw)
         _check(load().mg_run_set_laser(self.ptr, C.byref(self._laser)))
+
+    def set_probes(self, ijk):
+        """Probe nodes (q, 3) ints; every step records E^n and H^n there."""
+        a = np.ascontiguousarray(np.asarray(ijk, dtype="<i4").reshape(-1, 3))
+        self.nprobes = len(a)
+        _check(load().mg_run_set_probes(self.ptr, a.ctypes.data if len(a) else None, len(a)))
+
+    def probe_samples(self, nsteps):
+        """(nsteps, nprobes, 7) rows {t, Ex, Ey, Ez, Hx, Hy, Hz} of the last step call."""
+        out = np.zeros((nsteps, getattr(self, "nprobes", 0), 7))
+        _check(load().mg_run_probe_samples(self.ptr, int(nsteps), out.ctypes.data))
+        return out
 
     def tecplot_fields(self):
         """Node-centred E and H (IO_tecplot.c interpolation) over [0, n]^3."""

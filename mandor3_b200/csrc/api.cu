@@ -459,6 +459,9 @@ extern "C" int mg_run_destroy (mg_run_t *r)
    if (r->stage) cudaFree (r->stage);
    if (r->sort_tmp) cudaFree (r->sort_tmp);
    if (r->tile_start) cudaFree (r->tile_start);
+   if (r->probe_ijk) cudaFree (r->probe_ijk);
+   if (r->probe_ring) cudaFree (r->probe_ring);
+   if (r->probe_ptrs) cudaFree (r->probe_ptrs);
    for (int q = 0 ; q < 2 ; ++q)
       if (r->gauss_rho[q]) cudaFree (r->gauss_rho[q]);
    if (r->gauss_out) cudaFree (r->gauss_out);
@@ -736,6 +739,12 @@ extern "C" int mg_em_HHalfStep (mg_run_t *r)
    CHECK_RUN (r);
    TRY (expect_stage (r, 0, __func__));
    TRY (is32 (r) ? mg_fields32_h_half (r) : mg_fields64_h_half (r));
+   // Probe samples of this step into row 0 (core/main.c:373 samples after
+   // em_energy; nothing in between changes E or H^n).
+   if (r->nprobes > 0) {
+      MG_CUDA (cudaMemsetAsync (&r->dsc->step, 0, sizeof (int), r->stream));
+      TRY (mg_probes_enqueue (r));
+   }
    r->stage_no = 1;
    return MG_OK;
 }
@@ -907,6 +916,7 @@ int mg_enqueue_step64 (mg_run_t *r, int part)
 {
    if (part < 0 || part == 0) {
       TRY (mg_fields64_h_both (r));
+      TRY (mg_probes_enqueue (r));
       TRY (mg_fields64_zero_j (r));
    }
    if (part < 0 || part == 1)

@@ -146,6 +146,12 @@ struct mg_run {
    int         has_gspot;
    GaussSpot   gspot;
 
+   // probes: nodes, per-step sample ring (MG_RING rows of nprobes x 7)
+   int         nprobes;
+   int        *probe_ijk;
+   double     *probe_ring;
+   void      **probe_ptrs;   // E and H^n component arrays (device copy)
+
    // Gauss-law test: densities before/after a step, residuals
    double     *gauss_rho[2];
    double     *gauss_out;
@@ -209,6 +215,7 @@ int mg_fields64_h_both (mg_run_t *r);
 int mg_fields64_e_fused (mg_run_t *r);
 int mg_push64 (mg_run_t *r);
 int mg_gauss_rho (mg_run_t *r, double *rho);
+int mg_probes_enqueue (mg_run_t *r);
 int mg_gauss_residual (mg_run_t *r, const double *rho1, const double *rho2, double *out_dev);
 int mg_end_step (mg_run_t *r);
 

@@ -16,9 +16,15 @@
  *   binData/plasma_%06d_000.bin  core/plasma_IO.c:273-287
  *   binData/diag.dat           core/diag_WDensity.c:30-157
  *   tmp/stop.flag              core/main.c:120-189
+ *   binData/tec_*, tecplot.N   IO_tecplot.c:108-266
+ *   run_probes.cfg, binData/probe_*.bin, output/probe_locations.dat
+ *                              core/diag_probe.c:48-446, probe.h
+ *   tmp/spectrDump_%d_0, binData/spectr.N
+ *                              spectr_dump.c:15-109, type_CFile.c:112-370
  *
  *   core_b200.out [--fp32] [--device N]
  */
+#include <dirent.h>
 #include <errno.h>
 #include <math.h>
 #include <stdio.h>
@@ -262,6 +268,7 @@ typedef struct {
    int sys_num;           /* next checkpoint record */
    int map_num;           /* next file map id */
    int tec_num;           /* next tecplot record */
+   int spectr_num;        /* next spectral dump */
    unsigned char head_E[HEADER_BYTES], head_H[HEADER_BYTES];
    char prtn_src[256];
 } records_t;
@@ -366,12 +373,319 @@ static int stop_requested (double t0, double per_step, int stretch, double save_
    return limit > 0 && now () - t0 + per_step*stretch + save_time > limit;
 }
 
-/* One step with the tecplot dump (core/main.c:384-391, 430-434): the staged
- * step, with E^n, H^n and the density of the moved markers written after
- * plasma_move (tecIO_saveFields, IO_tecplot.c:220-245) and J after the E step
- * (tecIO_saveCurrents, IO_tecplot.c:250-266).  row: the step's energy row. */
-static void tecplot_step (mg_run_t *run, records_t *rec, const domain_t *dom, long nodes, double time,
-                          double row[6])
+/* ---- probes (core/diag_probe.c) ------------------------------------------ */
+
+typedef struct {
+   int     n;          /* probes after de-duplication, nodes in ijk */
+   int    *ijk;
+   int     nact;       /* probes with every index in [0, n): these are sampled */
+   int    *act;
+   FILE  **fp;
+   double *rows;       /* samples of one step call: steps x nact x 7 */
+} probes_t;
+
+static int dbl_to_int (double x) { return (int) (x + 128.0) - 128; }     /* misc_PIC.h:18 */
+
+/* probe_addDraft (core/diag_probe.c:150-163). */
+static void probe_add (probes_t *p, double x, double y, double z, double micron, const domain_t *d)
+{
+   p->ijk = (int *) realloc (p->ijk, sizeof (int)*3*(p->n + 1));
+   int *q = p->ijk + 3*p->n++;
+   q[0] = dbl_to_int (x*micron/d->h[0]);
+   q[1] = dbl_to_int (y*micron/d->h[1]);
+   q[2] = dbl_to_int (z*micron/d->h[2]);
+}
+
+/* cfg_readWord (misc_cfgReader.c:141-162): a line that starts with '@', its
+ * first word after the '@', '>' and blanks. */
+static void cfg_word (FILE *fp, char *word, size_t cap)
+{
+   char line[1024];
+   if (!fgets (line, sizeof (line), fp) || line[0] != '@')
+      die ("%s", "run_probes.cfg: parameter is absent");
+   const char *w = line;
+   while (*w == ' ' || *w == '@' || *w == '>')
+      ++w;
+   size_t l = 0;
+   while (w[l] > ' ' && l + 1 < cap)
+      ++l;
+   memcpy (word, w, l);
+   word[l] = 0;
+}
+
+/* cfg_readOptDouble / cfg_readOptInt (misc_cfgReader.c:88-111): '>' then the
+ * number, the rest of the line skipped. */
+static double cfg_opt_double (FILE *fp)
+{
+   double v = 0;
+   char rest[1024];
+   if (fgetc (fp) != '>' || fscanf (fp, "%le", &v) != 1)
+      die ("%s", "run_probes.cfg: missing optional double parameter");
+   if (!fgets (rest, sizeof (rest), fp))
+      rest[0] = 0;
+   return v;
+}
+
+static int cfg_opt_int (FILE *fp)
+{
+   int v = 0;
+   char rest[1024];
+   if (fgetc (fp) != '>' || fscanf (fp, "%d", &v) != 1)
+      die ("%s", "run_probes.cfg: missing optional int parameter");
+   if (!fgets (rest, sizeof (rest), fp))
+      rest[0] = 0;
+   return v;
+}
+
+/* One micron in code units: the 12th of the 15 doubles of binData/units.bin
+ * (units_save / units_load, misc_units.c:39-88). */
+static double micron_units (void)
+{
+   FILE *fp = open_or_die ("binData/units.bin", "rb");
+   double u[12];
+   read_exact (u, sizeof (u), fp, "binData/units.bin");
+   fclose (fp);
+   return u[11];
+}
+
+/* probe_allocate + probe_touch (core/diag_probe.c:48-100, 121-395) for one
+ * rank: old probe files removed unless the run continues, run_probes.cfg
+ * read (point / line / rectangle / volume groups up to 'end'), repeated
+ * nodes removed, output/probe_locations.dat and binData/probe_globals.bin
+ * written and the files of the probes inside the domain opened. */
+static void probes_open (probes_t *p, const domain_t *d, int cont)
+{
+   memset (p, 0, sizeof (*p));
+   if (!cont) {
+      DIR *dir = opendir ("./binData");
+      if (!dir)
+         die ("%s", "cannot open 'binData' folder");
+      struct dirent *e;
+      while ((e = readdir (dir))) {
+         const size_t l = strlen (e->d_name);
+         if (strncmp (e->d_name, "probe_", 6) || l < 4 || strncmp (e->d_name + l - 4, ".bin", 4))
+            continue;
+         char name[600];
+         snprintf (name, sizeof (name), "binData/%s", e->d_name);
+         remove (name);
+      }
+      closedir (dir);
+   }
+   FILE *fp = fopen ("run_probes.cfg", "rt");
+   const double micron = micron_units ();
+   while (fp) {
+      char word[200];
+      cfg_word (fp, word, sizeof (word));
+      if (!strcmp (word, "end")) {
+         fclose (fp);
+         fp = NULL;
+      } else if (!strcmp (word, "point")) {
+         const double x = cfg_opt_double (fp), y = cfg_opt_double (fp), z = cfg_opt_double (fp);
+         probe_add (p, x, y, z, micron, d);
+      } else if (!strcmp (word, "line")) {
+         double x1 = cfg_opt_double (fp), y1 = cfg_opt_double (fp), z1 = cfg_opt_double (fp);
+         double x2 = cfg_opt_double (fp), y2 = cfg_opt_double (fp), z2 = cfg_opt_double (fp);
+         const int N = 2 + abs (cfg_opt_int (fp));
+         const double dx = (x2 - x1)/(N - 1), dy = (y2 - y1)/(N - 1), dz = (z2 - z1)/(N - 1);
+         for (int i = 0 ; i < N ; ++i, x1 += dx, y1 += dy, z1 += dz)
+            probe_add (p, x1, y1, z1, micron, d);
+      } else if (!strcmp (word, "rectangle") || !strcmp (word, "volume")) {
+         const int sides = strcmp (word, "volume") ? 2 : 3;
+         double o[3], e[3][3];
+         int N[3] = {1, 1, 1};
+         for (int a = 0 ; a < 3 ; ++a)
+            o[a] = cfg_opt_double (fp);
+         for (int s = 0 ; s < sides ; ++s)
+            for (int a = 0 ; a < 3 ; ++a)
+               e[s][a] = cfg_opt_double (fp);
+         for (int s = 0 ; s < sides ; ++s) {
+            N[s] = 2 + abs (cfg_opt_int (fp));
+            for (int a = 0 ; a < 3 ; ++a)
+               e[s][a] = (e[s][a] - o[a])/(N[s] - 1);
+         }
+         for (int a = 0 ; a < N[0] ; ++a)
+            for (int b = 0 ; b < N[1] ; ++b)
+               for (int c = 0 ; c < N[2] ; ++c) {
+                  double v[3];
+                  for (int q = 0 ; q < 3 ; ++q)
+                     v[q] = sides == 2 ? o[q] + a*e[0][q] + b*e[1][q]
+                                       : o[q] + a*e[0][q] + b*e[1][q] + c*e[2][q];
+                  probe_add (p, v[0], v[1], v[2], micron, d);
+               }
+      } else {
+         die ("bad probe group '%s' (use 'point', 'line', 'rectangle', or 'volume')", word);
+      }
+   }
+   /* Repeated nodes: the last probe takes the place of the repeat, which is
+    * then tested again (core/diag_probe.c:343-350). */
+   for (int p1 = 0 ; p1 < p->n ; ++p1)
+      for (int p2 = p1 + 1 ; p2 < p->n ; ++p2)
+         if (!memcmp (p->ijk + 3*p1, p->ijk + 3*p2, 3*sizeof (int))) {
+            --p->n;
+            memmove (p->ijk + 3*p2, p->ijk + 3*p->n, 3*sizeof (int));
+            --p2;
+         }
+
+   fp = open_or_die ("output/probe_locations.dat", "wt");
+   fprintf (fp, "variables = \"x [<greek>m</greek>m]\", \"y [<greek>m</greek>m]\", "
+                "\"z [<greek>m</greek>m]\"\nzone t=\"domain\", f= point\n");
+   for (int i = 0 ; i < 2 ; ++i)
+      for (int j = 0 ; j < 2 ; ++j)
+         for (int k = 0 ; k < 2 ; ++k)
+            fprintf (fp, "%e %e %e\n", (d->dmin[0]*i + d->dmax[0]*(1 - i))*d->h[0]/micron,
+                     (d->dmin[1]*j + d->dmax[1]*(1 - j))*d->h[1]/micron,
+                     (d->dmin[2]*k + d->dmax[2]*(1 - k))*d->h[2]/micron);
+   fprintf (fp, "zone t=\"probes\", f= point\n");
+   for (int q = 0 ; q < p->n ; ++q)
+      fprintf (fp, "%e %e %e\n", p->ijk[3*q]*d->h[0]/micron, p->ijk[3*q + 1]*d->h[1]/micron,
+               p->ijk[3*q + 2]*d->h[2]/micron);
+   fclose (fp);
+
+   /* probeGlobals_t {tau, h1, h2, h3, min[3], max[3]} (probe.h) */
+   double globals[10] = {d->tau, d->h[0], d->h[1], d->h[2]};
+   for (int a = 0 ; a < 3 ; ++a) {
+      globals[4 + a] = d->dmin[a]*d->h[a];
+      globals[7 + a] = d->dmax[a]*d->h[a];
+   }
+   fp = open_or_die ("binData/probe_globals.bin", "wb");
+   write_exact (globals, sizeof (globals), fp, "binData/probe_globals.bin");
+   fclose (fp);
+
+   p->act = (int *) malloc (sizeof (int)*3*(p->n > 0 ? p->n : 1));
+   p->fp = (FILE **) malloc (sizeof (FILE *)*(p->n > 0 ? p->n : 1));
+   for (int q = 0 ; q < p->n ; ++q) {
+      const int *c = p->ijk + 3*q;
+      int inside = 1;
+      for (int a = 0 ; a < 3 ; ++a)
+         inside &= c[a] >= d->dmin[a] && c[a] < d->dmax[a];
+      if (!inside)
+         continue;
+      char name[200];
+      snprintf (name, sizeof (name), "binData/probe_%d_%d_%d.bin", c[0], c[1], c[2]);
+      FILE *f = fopen (name, "rb");
+      if (!f) {
+         /* probeHeader_t {char magic[8] = "probes", int i, j, k} */
+         unsigned char head[20] = "probes";
+         memcpy (head + 8, c, 3*sizeof (int));
+         f = open_or_die (name, "wb");
+         write_exact (head, sizeof (head), f, name);
+      } else {
+         fclose (f);
+         f = open_or_die (name, "ab");
+      }
+      memcpy (p->act + 3*p->nact, c, 3*sizeof (int));
+      p->fp[p->nact++] = f;
+   }
+   p->rows = (double *) malloc (sizeof (double)*7*256*(p->nact > 0 ? p->nact : 1));
+}
+
+/* probe_postData (core/diag_probe.c:409-429): one probeSample_t {time, Ex,
+ * Ey, Ez, Hx, Hy, Hz} per step and probe, from the device's sample ring. */
+static void probes_write (mg_run_t *run, probes_t *p, int steps)
+{
+   if (p->nact == 0 || steps == 0)
+      return;
+   check (mg_run_probe_samples (run, steps, p->rows), "probe samples");
+   for (int s = 0 ; s < steps ; ++s)
+      for (int q = 0 ; q < p->nact ; ++q)
+         write_exact (p->rows + 7*((long) s*p->nact + q), 7*sizeof (double), p->fp[q], "probe file");
+}
+
+static void probes_close (probes_t *p)
+{
+   for (int q = 0 ; q < p->nact ; ++q)
+      fclose (p->fp[q]);
+   free (p->ijk);
+   free (p->act);
+   free (p->fp);
+   free (p->rows);
+}
+
+/* ---- spectral dumps (spectr_dump.c:66-109) -------------------------------- */
+
+static long chunk_open (FILE *fp, const char *name)
+{
+   const long pos = ftell (fp);
+   const long long size = -1;
+   const int deleted = 0, l = (int) strlen (name);
+   write_exact (&size, sizeof (size), fp, "spectral dump");
+   write_exact (&deleted, sizeof (int), fp, "spectral dump");
+   write_exact (&l, sizeof (int), fp, "spectral dump");
+   fputc ('\n', fp);
+   write_exact (name, l, fp, "spectral dump");
+   fputc ('\n', fp);
+   return pos;
+}
+
+/* The chunk's size, header included, into its first 8 bytes
+ * (CF_closeChunk, type_CFile.c:357-370). */
+static void chunk_close (FILE *fp, long pos)
+{
+   const long long size = ftell (fp) - pos;
+   fseek (fp, pos, SEEK_SET);
+   write_exact (&size, sizeof (size), fp, "spectral dump");
+   fseek (fp, 0, SEEK_END);
+}
+
+/* tmp/spectrDump_<num>_0: chunk file with the global parameters, the dumped
+ * region [0, n-1]^3 and the raw E^n and H^n components over it; then
+ * binData/spectr.N.  E, H: nodes [0, n]^3, 3 doubles a node. */
+static void spectr_dump (records_t *rec, const domain_t *d, double time, const double *E, const double *H)
+{
+   char path[512];
+   snprintf (path, sizeof (path), "tmp/spectrDump_%d_%d", rec->spectr_num, 0);
+   FILE *fp = open_or_die (path, "wb");
+   fputs ("============\n Chunk file\n============\n", fp);
+   long c = chunk_open (fp, "global parameters");
+   fprintf (fp, "%d\t  cpus total.\n", 1);
+   fprintf (fp, "%d\t  i-min.\n", d->dmin[0]);
+   fprintf (fp, "%d\t  j-min.\n", d->dmin[1]);
+   fprintf (fp, "%d\t  k-min.\n", d->dmin[2]);
+   fprintf (fp, "%d\t  i-max.\n", d->dmax[0]);
+   fprintf (fp, "%d\t  j-max.\n", d->dmax[1]);
+   fprintf (fp, "%d\t  k-max.\n", d->dmax[2]);
+   fprintf (fp, "%.14e\t  time.\n", time);
+   fprintf (fp, "%e\t  h1.\n", d->h[0]);
+   fprintf (fp, "%e\t  h2.\n", d->h[1]);
+   fprintf (fp, "%e\t  h3.\n", d->h[2]);
+   chunk_close (fp, c);
+   /* reg_t {min[3], max[3], cpu, barcode, wrap[3]} after mf_mesh_initUnroll
+    * (type_mesh2.h:29-37): region [0, n-1]^3, strides of its own array. */
+   const int n[3] = {d->dmax[0], d->dmax[1], d->dmax[2]};
+   const int reg[11] = {0, 0, 0, n[0] - 1, n[1] - 1, n[2] - 1, 0, 0, n[1]*n[2], n[2], 1};
+   c = chunk_open (fp, "cpu region");
+   write_exact (reg, sizeof (reg), fp, path);
+   chunk_close (fp, c);
+   const long nk = n[2] + 1, nj = n[1] + 1;
+   double *line = (double *) malloc (sizeof (double)*n[2]);
+   for (int f = 0 ; f < 6 ; ++f) {
+      const char names[6][4] = {"E.x", "E.y", "E.z", "H.x", "H.y", "H.z"};
+      const double *src = f < 3 ? E : H;
+      c = chunk_open (fp, names[f]);
+      for (int i = 0 ; i < n[0] ; ++i)
+         for (int j = 0 ; j < n[1] ; ++j) {
+            for (int k = 0 ; k < n[2] ; ++k)
+               line[k] = src[3*(((long) i*nj + j)*nk + k) + f % 3];
+            write_exact (line, sizeof (double)*n[2], fp, path);
+         }
+      chunk_close (fp, c);
+   }
+   free (line);
+   fclose (fp);
+   rec->spectr_num++;
+   fp = open_or_die ("binData/spectr.N", "wt");
+   fprintf (fp, "@ %d  spectr dumps written.\n", rec->spectr_num);
+   fclose (fp);
+}
+
+/* One step with a tecplot dump, a spectral dump or both (core/main.c:384-402,
+ * 430-434): the staged step, with the probe samples after the field energy;
+ * E^n, H^n and the density of the moved markers written after plasma_move
+ * (tecIO_saveFields, IO_tecplot.c:220-245), then the spectral dump of E^n and
+ * H^n, and J after the E step (tecIO_saveCurrents, IO_tecplot.c:250-266).
+ * row: the step's energy row. */
+static void staged_step (mg_run_t *run, records_t *rec, const domain_t *dom, long nodes, double time,
+                         double row[6], int tec, int spectr, probes_t *probes)
 {
    char path[512];
    const int n[3] = {dom->dmax[0], dom->dmax[1], dom->dmax[2]};
@@ -382,9 +696,24 @@ static void tecplot_step (mg_run_t *run, records_t *rec, const domain_t *dom, lo
 
    check (mg_em_HHalfStep (run), "H half step");
    check (mg_em_energy (run, &row[1], &row[2]), "field energy");
+   probes_write (run, probes, 1);
    check (mg_plasma_move (run), "plasma move");
    check (mg_plasma_temperature (run, &row[3], &row[4], &row[5]), "temperature");
    row[0] = time;
+   if (spectr && !tec) {
+      check (mg_run_get_fields (run, a, b), "download fields");
+      spectr_dump (rec, dom, time, a, b);
+   }
+   if (!tec) {
+      check (mg_em_HStep (run), "H step");
+      check (mg_em_EStep_start (run), "E step");
+      check (mg_jbc_finish (run), "current walls");
+      check (mg_em_EStep_finish (run), "E step finish");
+      free (a);
+      free (b);
+      free (rho);
+      return;
+   }
    check (mg_plasma_rho (run, rho), "charge density");
    check (mg_tecplot_fields (run, a, b), "tecplot fields");
    write_domain (dom);                                        /* parameter_save */
@@ -402,6 +731,10 @@ static void tecplot_step (mg_run_t *run, records_t *rec, const domain_t *dom, lo
    fclose (fp);
    snprintf (path, sizeof (path), "binData/tec_prtn_%06d.bin", rec->tec_num);
    copy_file (rec->prtn_src, path);
+   if (spectr) {
+      check (mg_run_get_fields (run, a, b), "download fields");
+      spectr_dump (rec, dom, time, a, b);
+   }
 
    check (mg_em_HStep (run), "H step");
    check (mg_em_EStep_start (run), "E step");
@@ -476,11 +809,13 @@ int main (int argc, char **argv)
       rec.tec_num = tn ? read_at_int (tn, "binData/tecplot.N") : 0;
       if (tn)
          fclose (tn);
+      rec.spectr_num = read_count ("binData/spectr.N");   /* spectr_continueDump */
    } else {
       point = 0;
       rec.sys_num = 1;
       rec.map_num = read_count ("binData/fileMap_start.txt");
       rec.tec_num = 1;                                  /* after setup's record 0 */
+      rec.spectr_num = 0;
    }
 
    char path[512];
@@ -532,6 +867,10 @@ int main (int argc, char **argv)
       fclose (gs);
       check (mg_run_set_gauss_spot (run, &s), "gauss spot");
    }
+   probes_t probes;
+   probes_open (&probes, &dom, cfg.cont && point > 0);
+   if (probes.nact > 0)
+      check (mg_run_set_probes (run, probes.act, probes.nact), "probes");
    check (mg_run_init (run), "init");
    free (E);
    free (H);
@@ -556,17 +895,24 @@ int main (int argc, char **argv)
       if (next - t > 256) next = t + 256;
       /* core/main.c:384: a tecplot dump on every step t (counted from 1) with
        * t % chPoint_tecplot == 0. */
-      if (cfg.tecplot > 0) {
-         const int ntec = (t/cfg.tecplot + 1)*cfg.tecplot;
-         if (ntec - 1 > t && ntec - 1 < next) next = ntec - 1;
-      }
+      /* The same for the spectral dumps (core/main.c:395). */
+      const int every[2] = {cfg.tecplot, cfg.spectr};
+      for (int q = 0 ; q < 2 ; ++q)
+         if (every[q] > 0) {
+            const int nd = (t/every[q] + 1)*every[q];
+            if (nd - 1 > t && nd - 1 < next) next = nd - 1;
+         }
       int k = next - t;
-      if (cfg.tecplot > 0 && (t + 1) % cfg.tecplot == 0) {
-         tecplot_step (run, &rec, &dom, nodes, time, rows);
+      const int tec = cfg.tecplot > 0 && (t + 1) % cfg.tecplot == 0;
+      const int spectr = cfg.spectr > 0 && (t + 1) % cfg.spectr == 0;
+      if (tec || spectr) {
+         staged_step (run, &rec, &dom, nodes, time, rows, tec, spectr, &probes);
          k = 1;
          next = t + 1;
-      } else
+      } else {
          check (mg_run_step (run, k, rows), "step");
+         probes_write (run, &probes, k);
+      }
       for (int q = 0 ; q < k ; ++q)
          diag_add (&diag, rows + 6*q);
       t = next;
@@ -595,6 +941,7 @@ int main (int argc, char **argv)
    diag_flush (&diag, &fresh_diag, dom.tau);
    free (diag.rows);
    check (mg_run_destroy (run), "destroy run");
+   probes_close (&probes);
    remove ("tmp/stop.flag");
    return EXIT_SUCCESS;
 }

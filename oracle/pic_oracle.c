@@ -871,6 +871,65 @@ int po_step (po_run_t *r, double out[5])
    return 0;
 }
 
+/* probe_postData (core/diag_probe.c:409-429): E^n and H^n at the node, E
+ * averaged over its two edges along the component, H over the four faces
+ * around the node's edge; the time is the step's t = n tau. */
+static void probes (const po_run_t *r, const int *ijk, int n, double *o)
+{
+   const long Sx = r->s[0], Sy = r->s[1];
+   for (int q = 0 ; q < n ; ++q, o += 7) {
+      const long p = IX (r, ijk[3*q], ijk[3*q + 1], ijk[3*q + 2]);
+      const double *const *E = (const double *const *) r->e, *const *H = (const double *const *) r->b;
+      o[0] = r->time;
+      o[1] = 0.5*(E[0][p] + E[0][p + Sx]);
+      o[2] = 0.5*(E[1][p] + E[1][p + Sy]);
+      o[3] = 0.5*(E[2][p] + E[2][p + 1]);
+      o[4] = 0.25*(H[0][p] + H[0][p + Sy] + H[0][p + 1] + H[0][p + Sy + 1]);
+      o[5] = 0.25*(H[1][p] + H[1][p + Sx] + H[1][p + 1] + H[1][p + Sx + 1]);
+      o[6] = 0.25*(H[2][p] + H[2][p + Sx] + H[2][p + Sy] + H[2][p + Sx + Sy]);
+   }
+}
+
+/* E^n and H^n of the coming step over [0, n]^3 (what spectr_dump writes,
+ * core/main.c:395-402): H^n from a half step on a copy of H^(n-1/2). */
+void po_fields_n (po_run_t *r, double *E, double *H)
+{
+   const long size = po_mesh_size (r);
+   double *keep[3];
+   for (int c = 0 ; c < 3 ; ++c) {
+      keep[c] = (double *) malloc (sizeof (double)*size);
+      memcpy (keep[c], r->b[c], sizeof (double)*size);
+   }
+   po_em_h_half (r);
+   po_get_fields (r, E, H);
+   for (int c = 0 ; c < 3 ; ++c) {
+      memcpy (r->b[c], keep[c], sizeof (double)*size);
+      free (keep[c]);
+   }
+}
+
+int po_step_probes (po_run_t *r, const int *ijk, int n, double *samples, double out[5])
+{
+   double we, wm, wt[3];
+   po_em_h_half (r);
+   po_em_energy (r, &we, &wm);
+   probes (r, ijk, n, samples);
+   po_plasma_move (r, wt);
+   po_em_h_step (r);
+   po_em_e_step (r);
+   po_jbc (r);
+   po_em_e_finish (r);
+   r->time += r->tau;
+   if (out) {
+      out[0] = we;
+      out[1] = wm;
+      out[2] = wt[0];
+      out[3] = wt[1];
+      out[4] = wt[2];
+   }
+   return 0;
+}
+
 /* CIC charge density: core/plasma_rho.c:23-60 restated (no folding). */
 /* Charge density: CIC deposit (plasma.c:322-329 calling plasmaRho_add,
  * plasma_rho.c:159-173, with the nested weights of mf_PIC_distribute,

@@ -77,6 +77,11 @@ void po_init (po_run_t *r);
 /* One full time step; out[5] = {W_E, W_M, W_Tx, W_Ty, W_Tz} at t = n*tau
  * (wDensity_addPoint arguments).  Returns 0. */
 int  po_step (po_run_t *r, double out[5]);
+/* po_step with the probe samples of core/diag_probe.c:409-429 taken after the
+ * field energy: 7 doubles {t, Ex, Ey, Ez, Hx, Hy, Hz} per node of ijk. */
+int  po_step_probes (po_run_t *r, const int *ijk, int n, double *samples, double out[5]);
+/* E^n and H^n of the coming step over [0, n]^3, the run's state unchanged. */
+void po_fields_n (po_run_t *r, double *E, double *H);
 double po_time (const po_run_t *r);
 
 /* Stage-level entry points (same order as core/main.c's loop). */

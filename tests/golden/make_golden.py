@@ -5,7 +5,9 @@ oracle/Makefile into oracle/_ref) on each case's initial state and stores the
 final markers, E, H and the diag.dat energy rows in tests/golden/<case>.npz;
 for two cases also the Gauss-law rows of core_gauss.out in
 tests/golden/gauss_<case>.npz, and the fields of an empty Mur box driven by
-the hard gauss-spot source in tests/golden/gauss_spot.npz.
+the hard gauss-spot source in tests/golden/gauss_spot.npz; the reference
+placers, tecplot dumps, probes and spectral dumps in place_*.npz,
+tecplot.npz and probes.npz.
 
     make -C oracle ref REF=/path/to/reference
     python tests/golden/make_golden.py
@@ -192,10 +194,79 @@ def make_tecplot():
         shutil.rmtree(root, ignore_errors=True)
 
 
+# Probes and spectral dumps: the reference core.out on the drop-in driver's
+# case with a probe deck (points, a repeat, one outside the domain, a line, a
+# rectangle and a volume), spectral dumps every 5 steps and a tecplot dump at
+# step 10 (steps 5 and 10: one dump alone, one beside a tecplot dump).
+# Probe positions in cells (x h, the case's h is one value on all axes).
+PROBE_GROUPS = [
+    ("point", (5.3, 4.2, 7.6)),
+    ("point", (5.6, 4.4, 7.9)),               # the same node again
+    ("point", (12.2, 4.2, 7.6)),              # i = n: outside
+    ("line", (0.2, 0.3, 0.1, 11.5, 9.6, 13.7), (3,)),
+    ("rectangle", (1.2, 2.1, 3.3, 10.4, 2.1, 3.3, 1.2, 8.7, 3.3), (1, 0)),
+    ("volume", (2.5, 1.5, 0.5, 9.5, 1.5, 0.5, 2.5, 7.5, 0.5, 2.5, 1.5, 12.5), (0, 0, 0)),
+]
+
+
+def probe_deck(h):
+    lines = []
+    for g in PROBE_GROUPS:
+        lines.append("@ %s\t\tprobe group" % g[0])
+        for q, v in enumerate(g[1]):
+            lines.append("> %.9f\t\tcoordinate [micron]" % (v * h[q % 3]))
+        for v in (g[2] if len(g) > 2 else ()):
+            lines.append("> %d\t\tadditional points" % v)
+    lines.append("@ end\t\tterminator")
+    return "\n".join(lines) + "\n"
+SPECTR_PERIOD = 5
+PROBE_TEC_PERIOD = 10
+
+
+def probe_run_cfg(steps):
+    return ("@ %d\ttotal\n@ %d\tfull\n@ %d\ttecplot\n@ 0\tcontinue\n@ %d\tstop\n@ %d\tspectr\n"
+            % (steps, 10 ** 6, PROBE_TEC_PERIOD, 10 ** 6, SPECTR_PERIOD))
+
+
+def probe_files(root):
+    """The probe and spectral-dump files of a run directory: name -> bytes."""
+    out = {}
+    for d in ("binData", "tmp", "output"):
+        for f in sorted(os.listdir(os.path.join(root, d))):
+            if (f.startswith("probe_") and f.endswith(".bin")) or f.startswith("spectrDump_") \
+                    or f in ("spectr.N", "probe_locations.dat"):
+                out[d + "/" + f] = open(os.path.join(root, d, f), "rb").read()
+    return out
+
+
+def make_probes():
+    import tempfile, shutil
+    import test_driver
+    root = tempfile.mkdtemp(prefix="mg_probe_")
+    try:
+        rr = RefRun(root)
+        test_driver.prepare(root)
+        with open(os.path.join(root, "run_mandor.cfg"), "w") as fp:
+            fp.write(probe_run_cfg(test_driver.CASE["steps"]))
+        n, L_um = cases.geometry(test_driver.CASE)
+        with open(os.path.join(root, "run_probes.cfg"), "w") as fp:
+            fp.write(probe_deck([L_um[a] / n[a] for a in range(3)]))
+        rr._run("core.out")
+        files = probe_files(root)
+        np.savez_compressed(os.path.join(HERE, "probes.npz"),
+                            **{k: np.frombuffer(v, np.uint8) for k, v in files.items()})
+        print("probes: %d files" % len(files))
+    finally:
+        shutil.rmtree(root, ignore_errors=True)
+
+
 if __name__ == "__main__":
     if not have_reference():
         sys.exit("reference binaries missing: make -C oracle ref REF=<reference tree>")
-    for name in (sys.argv[1:] or list(cases.CASES) + ["gauss_spot", "placers", "tecplot"]):
+    for name in (sys.argv[1:] or list(cases.CASES) + ["gauss_spot", "placers", "tecplot", "probes"]):
+        if name == "probes":
+            make_probes()
+            continue
         if name == "tecplot":
             make_tecplot()
             continue

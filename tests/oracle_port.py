@@ -36,6 +36,8 @@ def _load():
     lib.po_set_laser.argtypes = [vp, vp]
     lib.po_init.argtypes = [vp]
     lib.po_step.argtypes = [vp, vp]
+    lib.po_step_probes.argtypes = [vp, vp, C.c_int, vp, vp]
+    lib.po_fields_n.argtypes = [vp, vp, vp]
     lib.po_time.restype = C.c_double
     lib.po_time.argtypes = [vp]
     lib.po_em_energy.argtypes = [vp, vp, vp]
@@ -160,6 +162,23 @@ class OracleRun:
         for s in range(k):
             lib().po_step(self.ptr, rows[s].ctypes.data)
         return rows
+
+    def step_probes(self, ijk, k=1):
+        """k steps with the probe samples of each (core/diag_probe.c:409-429):
+        (k, nprobes, 7) rows {t, Ex, Ey, Ez, Hx, Hy, Hz} of E^n and H^n."""
+        a = np.ascontiguousarray(np.asarray(ijk, dtype=np.int32).reshape(-1, 3))
+        out = np.zeros((k, len(a), 7))
+        for s in range(k):
+            lib().po_step_probes(self.ptr, a.ctypes.data, len(a), out[s].ctypes.data,
+                                 np.zeros(5).ctypes.data)
+        return out
+
+    def fields_n(self):
+        """E^n and H^n of the coming step over [0, n]^3 (state unchanged)."""
+        E = np.zeros(self.shape())
+        H = np.zeros(self.shape())
+        lib().po_fields_n(self.ptr, E.ctypes.data, H.ctypes.data)
+        return E, H
 
     def time(self):
         return lib().po_time(self.ptr)

@@ -92,6 +92,37 @@ def read_diag(path):
     return np.array(rows)
 
 
+PROBE_SAMPLE = np.dtype([(k, "<f8") for k in ("t", "Ex", "Ey", "Ez", "Hx", "Hy", "Hz")])
+
+
+def read_probe(raw):
+    """A probe file (core/diag_probe.c:86-98, probe.h): probeHeader_t
+    {char magic[8] = "probes", int i, j, k} then probeSample_t rows."""
+    raw = bytes(raw)
+    assert raw[:8] == b"probes\0\0", raw[:8]
+    ijk = tuple(int(v) for v in np.frombuffer(raw[8:20], "<i4"))
+    return ijk, np.frombuffer(raw[20:], "<f8").reshape(-1, 7)
+
+
+def read_chunks(raw):
+    """A chunk file (type_CFile.c:112-370): the magic, then chunks of
+    {INT64 size with header, int deleted, int name length, '\\n', name,
+    '\\n', data}; returns [(name, deleted, data bytes)]."""
+    raw = bytes(raw)
+    magic = b"============\n Chunk file\n============\n"
+    assert raw.startswith(magic)
+    out, pos = [], len(magic)
+    while pos < len(raw):
+        size = int(np.frombuffer(raw[pos:pos + 8], "<i8")[0])
+        deleted, l = (int(v) for v in np.frombuffer(raw[pos + 8:pos + 16], "<i4"))
+        assert raw[pos + 16:pos + 17] == b"\n" and raw[pos + 17 + l:pos + 18 + l] == b"\n"
+        name = raw[pos + 17:pos + 17 + l].decode()
+        out.append((name, deleted, raw[pos + 18 + l:pos + size]))
+        pos += size
+    assert pos == len(raw)
+    return out
+
+
 def mesh_header(n, name, ghost=1, vector=True):
     """Header of a checkpoint mesh file for a one-rank run: the valid region
     (0,0,0)-(n) and the mesh_t struct of a mesh allocated over
