@@ -32,6 +32,14 @@ struct po_run {
    int    has_laser;
    po_gauss_spot_t gspot;
    int    has_gspot;
+   /* TF/SF interface */
+   int    has_tfsf, tfsf_on, tfsf_frame;
+   po_tfsf_t tfsf;
+   struct { int min[3], max[3], comp, ep, eq, used; double sf; long vol, at; } face[24];
+   long   frame_size;
+   double *frames;                  /* play: recorded frames */
+   long   nrec;                     /* record: frames written */
+   double *rec;
 };
 
 static inline long IX (const po_run_t *r, int i, int j, int k)
@@ -93,6 +101,8 @@ void po_destroy (po_run_t *r)
       for (int a = 0 ; a < 3 ; ++a)
          free (r->mur[t][a]);
    free (r->p);
+   free (r->frames);
+   free (r->rec);
    free (r);
 }
 
@@ -787,10 +797,14 @@ void po_em_h_half (po_run_t *r)
    h_bc (r);
 }
 
+static void tfsf_h (po_run_t *r);
+static void tfsf_e (po_run_t *r);
+
 /* em_HStep (core/em.c:115-131): H^n -> H^(n+1/2) plus source at t = n*tau. */
 void po_em_h_step (po_run_t *r)
 {
    h_advance (r, 0.5);
+   tfsf_h (r);
    if (r->has_laser)
       laser_h (r, r->time);
    h_bc (r);
@@ -803,7 +817,6 @@ void po_em_e_step (po_run_t *r)
    e_bc (r);
 }
 
-/* em_EStep_finish (core/em.c:189-222): source at t + tau/2, E -= tau*J. */
 void po_set_gauss_spot (po_run_t *r, const po_gauss_spot_t *s)
 {
    r->gspot = *s;
@@ -840,19 +853,192 @@ static void gauss_spot_e (po_run_t *r, double t)
    }
 }
 
+/* em_EStep_finish (core/em.c:189-222): TF/SF, source at t + tau/2,
+ * E -= tau*J, hard gauss spot at t + tau, frame count. */
 void po_em_e_finish (po_run_t *r)
 {
+   tfsf_e (r);
    if (r->has_laser)
       laser_e (r, r->time + 0.5*r->tau);
    e_sub_current (r);
    if (r->has_gspot)
       gauss_spot_e (r, r->time + r->tau);
+   r->tfsf_frame++;                                            /* :849-853 */
+}
+
+/* ------------------------------------------------------------------------
+ * TF/SF interface (core/em_TFSF.c:480-851).
+ * ---------------------------------------------------------------------- */
+
+/* TFSF_init (:480-558) face geometry; record mode cuts the faces to the
+ * domain (TFSF_turnRec :239-252: E faces to [0, n-1], H faces to [1, n]),
+ * play mode drops the open faces (TFSF_openFaces :296-323) and requires the
+ * rest 5 cells inside the walls (TFSF_turnPlay :341-357). */
+int po_set_tfsf (po_run_t *r, const po_tfsf_t *t, const double *frames)
+{
+   r->tfsf = *t;
+   r->frame_size = 0;
+   const int *side[2] = {t->lo, t->hi};
+   for (int a = 0 ; a < 3 ; ++a) {
+      const int ep = (a + 1) % 3, eq = (a + 2) % 3;
+      for (int top = 0 ; top < 2 ; ++top)
+         for (int comp = 0 ; comp < 2 ; ++comp) {
+            const int f = 4*a + 2*top + comp;
+            for (int fh = 0 ; fh < 2 ; ++fh) {
+               const int q = f + 12*fh;
+               for (int b = 0 ; b < 3 ; ++b) {
+                  r->face[q].min[b] = t->lo[b];
+                  r->face[q].max[b] = t->hi[b];
+               }
+               r->face[q].min[a] = r->face[q].max[a] = side[top][a];
+               const int ce = (a + 1 + comp) % 3;
+               r->face[q].min[ce] += 1;
+               if (fh) {
+                  r->face[q].min[a] += top;
+                  r->face[q].max[a] += top;
+               }
+               r->face[q].comp = fh ? 3 - ce - a : ce;
+               r->face[q].ep = ep;
+               r->face[q].eq = eq;
+               r->face[q].sf = (1 - 2*top)*(1 - 2*comp)*(r->tau/r->h[a]);
+               if (t->mode == PO_TFSF_REC)
+                  for (int b = 0 ; b < 3 ; ++b) {
+                     const int lo = fh ? 1 : 0, hi = fh ? r->n[b] : r->n[b] - 1;
+                     if (r->face[q].min[b] < lo) r->face[q].min[b] = lo;
+                     if (r->face[q].max[b] > hi) r->face[q].max[b] = hi;
+                  }
+               long v = 1;
+               for (int b = 0 ; b < 3 ; ++b)
+                  v *= (r->face[q].max[b] >= r->face[q].min[b]) ? r->face[q].max[b] - r->face[q].min[b] + 1 : 0;
+               r->face[q].vol = v;
+               /* An open face keeps its slot in the frame layout of the
+                * recorded files; only its use is dropped. */
+               r->face[q].used = v > 0 && !(t->mode != PO_TFSF_REC && t->open[top][a]);
+               if (r->face[q].used && t->mode != PO_TFSF_REC)
+                  for (int b = 0 ; b < 3 ; ++b)
+                     if (r->face[q].min[b] < 5 || r->face[q].max[b] > r->n[b] - 5)
+                        return -1;
+            }
+         }
+   }
+   for (int q = 0 ; q < 24 ; ++q) {
+      r->face[q].at = r->frame_size;
+      r->frame_size += r->face[q].vol;
+   }
+   free (r->frames);
+   r->frames = NULL;
+   if (t->mode != PO_TFSF_REC) {
+      r->frames = (double *) malloc (sizeof (double)*(size_t) r->frame_size*(t->frames > 0 ? t->frames : 1));
+      memcpy (r->frames, frames, sizeof (double)*(size_t) r->frame_size*t->frames);
+   }
+   r->tfsf_frame = (int) (r->time/r->tau + 0.1);              /* :455 */
+   r->tfsf_on = 1;
+   r->has_tfsf = 1;
+   r->nrec = 0;
+   return 0;
+}
+
+long po_tfsf_faces (const po_run_t *r, int *regions)
+{
+   for (int q = 0 ; q < 24 && regions ; ++q)
+      for (int b = 0 ; b < 3 ; ++b) {
+         regions[6*q + b] = r->face[q].min[b];
+         regions[6*q + 3 + b] = r->face[q].max[b];
+      }
+   return r->frame_size;
+}
+
+long po_tfsf_recorded (const po_run_t *r, double *out)
+{
+   if (out && r->nrec)
+      memcpy (out, r->rec, sizeof (double)*(size_t) r->nrec*r->frame_size);
+   return r->nrec;
+}
+
+static int tfsf_playing (const po_run_t *r)
+{
+   return r->has_tfsf && r->tfsf_on && r->tfsf.mode != PO_TFSF_REC;
+}
+
+/* Start of a step (em_HHalfStep, core/em.c:85-105).  Record: TFSF_writeMesh
+ * (:565-594) of E^n and H^(n-1/2).  Play: the cap caching of the half step
+ * already calls TFSF_postEStep on the boundary slabs (core/em_caps.c:602-608),
+ * which switches the interface off for good once frame n + 1 is the last
+ * (:831-834) -- before this step's H and E faces are touched. */
+static void tfsf_record (po_run_t *r)
+{
+   if (tfsf_playing (r) && r->tfsf_frame + 1 >= r->tfsf.frames - 1)
+      r->tfsf_on = 0;
+   if (!r->has_tfsf || r->tfsf.mode != PO_TFSF_REC)
+      return;
+   r->rec = (double *) realloc (r->rec, sizeof (double)*(size_t) (r->nrec + 1)*r->frame_size);
+   double *o = r->rec + r->nrec*r->frame_size;
+   for (int q = 0 ; q < 24 ; ++q) {
+      if (!r->face[q].used)
+         continue;
+      const double *F = q < 12 ? r->e[r->face[q].comp] : r->b[r->face[q].comp];
+      const int ep = r->face[q].ep, eq = r->face[q].eq;
+      int c[3] = {r->face[q].min[0], r->face[q].min[1], r->face[q].min[2]};
+      for (c[ep] = r->face[q].min[ep] ; c[ep] <= r->face[q].max[ep] ; ++c[ep])
+         for (c[eq] = r->face[q].min[eq] ; c[eq] <= r->face[q].max[eq] ; ++c[eq])
+            *o++ = F[IX (r, c[0], c[1], c[2])]*r->face[q].sf;
+   }
+   r->nrec++;
+}
+
+/* TFSF_addSource / TFSF_subSource (:669-781) of frame fr's recorded values
+ * of the other field onto faces [q0, q0 + 12). */
+static void tfsf_apply (po_run_t *r, int q0, int fr, double sign)
+{
+   for (int q = q0 ; q < q0 + 12 ; ++q) {
+      if (!r->face[q].used)
+         continue;
+      double *F = q < 12 ? r->e[r->face[q].comp] : r->b[r->face[q].comp];
+      const double *src = r->frames + (long) fr*r->frame_size + r->face[(q + 12) % 24].at;
+      const int ep = r->face[q].ep, eq = r->face[q].eq;
+      int c[3] = {r->face[q].min[0], r->face[q].min[1], r->face[q].min[2]};
+      for (c[ep] = r->face[q].min[ep] ; c[ep] <= r->face[q].max[ep] ; ++c[ep])
+         for (c[eq] = r->face[q].min[eq] ; c[eq] <= r->face[q].max[eq] ; ++c[eq], ++src) {
+            if (sign > 0)
+               F[IX (r, c[0], c[1], c[2])] += *src;
+            else
+               F[IX (r, c[0], c[1], c[2])] -= *src;
+         }
+   }
+}
+
+/* TFSF_postHStep (:805-819): H faces get the recorded E of frame n
+ * (backward: T - n). */
+static void tfsf_h (po_run_t *r)
+{
+   const int tf = r->tfsf_frame, last = r->tfsf.frames;
+   if (!tfsf_playing (r) || tf >= last - 1)
+      return;
+   tfsf_apply (r, 12, r->tfsf.mode == PO_TFSF_PLAY ? tf : last - 1 - tf, 1.0);
+}
+
+/* TFSF_postEStep (:825-844): E faces get the recorded H of frame n + 1
+ * (backward: T - n, subtracted). */
+static void tfsf_e (po_run_t *r)
+{
+   const int tf = r->tfsf_frame, last = r->tfsf.frames;
+   if (!tfsf_playing (r))
+      return;
+   if (tf + 1 >= last - 1) {
+      r->tfsf_on = 0;
+      return;
+   }
+   if (r->tfsf.mode == PO_TFSF_PLAY)
+      tfsf_apply (r, 0, tf + 1, 1.0);
+   else
+      tfsf_apply (r, 0, last - 1 - tf, -1.0);
 }
 
 /* One step in core/main.c:353-478 order. */
 int po_step (po_run_t *r, double out[5])
 {
    double we, wm, wt[3];
+   tfsf_record (r);
    po_em_h_half (r);
    po_em_energy (r, &we, &wm);
    po_plasma_move (r, wt);
@@ -911,6 +1097,7 @@ void po_fields_n (po_run_t *r, double *E, double *H)
 int po_step_probes (po_run_t *r, const int *ijk, int n, double *samples, double out[5])
 {
    double we, wm, wt[3];
+   tfsf_record (r);
    po_em_h_half (r);
    po_em_energy (r, &we, &wm);
    probes (r, ijk, n, samples);

@@ -71,6 +71,29 @@ typedef struct {
 } po_gauss_spot_t;
 void po_set_gauss_spot (po_run_t *r, const po_gauss_spot_t *s);
 
+/* TF/SF interface (core/em_TFSF.c).  24 faces: E faces f = 0..11 in the
+ * reference's order (Ey_xMin, Ez_xMin, Ey_xMax, Ez_xMax, Ez_yMin, Ex_yMin,
+ * ..., Ey_zMax), then the H faces (Hz_xMin, Hy_xMin, ...).  A frame holds
+ * the recorded values of the 12 E faces then of the 12 H faces, each over
+ * its face region with the first tangential axis ep = (a+1)%3 slowest and
+ * eq = (a+2)%3 fastest, as the recording files store them (values already
+ * times the face's source factor). */
+enum { PO_TFSF_PLAY = 0, PO_TFSF_REC = 1, PO_TFSF_BACK = 2 };
+typedef struct {
+   int lo[3], hi[3];       /* interface bounding box (TFSF.cfg)               */
+   int mode;               /* PO_TFSF_*                                        */
+   int open[2][3];         /* play: faces removed, [min/max][axis]            */
+   int frames;             /* play: frames recorded (lastFrameTime.bin)       */
+} po_tfsf_t;
+/* Play: frames[frames x frame size]; record: frames NULL.  Returns 0, or -1
+ * when a played face is closer than 5 cells to a wall. */
+int  po_set_tfsf (po_run_t *r, const po_tfsf_t *t, const double *frames);
+/* Face regions (24 x {min[3], max[3]}; volume <= 0: face unused) and the
+ * doubles per frame. */
+long po_tfsf_faces (const po_run_t *r, int *regions);
+/* Frames recorded so far (record mode), copied to out when out != NULL. */
+long po_tfsf_recorded (const po_run_t *r, double *out);
+
 /* em_init / cap_init equivalent: ghost fill and Mur history from E. */
 void po_init (po_run_t *r);
 

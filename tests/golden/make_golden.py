@@ -6,8 +6,8 @@ final markers, E, H and the diag.dat energy rows in tests/golden/<case>.npz;
 for two cases also the Gauss-law rows of core_gauss.out in
 tests/golden/gauss_<case>.npz, and the fields of an empty Mur box driven by
 the hard gauss-spot source in tests/golden/gauss_spot.npz; the reference
-placers, tecplot dumps, probes and spectral dumps in place_*.npz,
-tecplot.npz and probes.npz.
+placers, tecplot dumps, probes and spectral dumps, and TF/SF record and
+play runs in place_*.npz, tecplot.npz, probes.npz and tfsf.npz.
 
     make -C oracle ref REF=/path/to/reference
     python tests/golden/make_golden.py
@@ -21,6 +21,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
 
 import cases  # noqa: E402
+import refrun  # noqa: E402
 import oracle_port  # noqa: E402
 from refrun import RefRun, have_reference  # noqa: E402
 
@@ -260,12 +261,86 @@ def make_probes():
         shutil.rmtree(root, ignore_errors=True)
 
 
+# TF/SF interface (core/em_TFSF.c): a record run (hard gauss spot inside
+# the interface box of an empty Mur box), the reference TFSFdefrag on its
+# streams, then play runs forward (with a warm electron cloud across the
+# faces) and backward (empty) on the merged streams.
+TFSF_N = (18, 14, 14)
+TFSF_L_UM = (0.9, 0.7, 0.7)
+TFSF_BOX = (5, 12, 5, 8, 5, 8)
+TFSF_STEPS = 16
+
+
+def tfsf_spot(h):
+    sp = spot_params(h)
+    sp.update(x=8 * h[0], y=0.325, z=0.325)
+    return sp
+
+
+def tfsf_plasma(h):
+    return oracle_port.place(lo=(3, 3, 3), hi=(15, 11, 11), ppc=2, rho=-0.5, qDivM=-1.0, h=h,
+                             uth=(0.1, 0.1, 0.1), seed=(1802, 9373))
+
+
+def tfsf_files(d, suffix):
+    return {k: open(os.path.join(d, "%s_%s.bin" % (k, suffix)), "rb").read()
+            for k in refrun.TFSF_FACES}
+
+
+def make_tfsf():
+    import shutil, glob
+    rec, plays = RefRun(), []
+    out = {}
+    try:
+        dom = rec.setup(TFSF_N, TFSF_L_UM, -0.5, (2, 2, 2), (2, 2, 2))
+        h = dom["h"]
+        rec.set_state(np.zeros(0, dtype=oracle_port.MARKER_DTYPE))
+        rec.set_gauss_spot(**tfsf_spot(h))
+        rec.set_tfsf(TFSF_BOX, 1)
+        rec.run(TFSF_STEPS)
+        d = rec.path(".EM_sources", "TFSF")
+        for k, v in tfsf_files(d, "000").items():
+            out["rec/" + k] = v
+        for f in ("consistencyCheck.dat", "TFSF_defrag.map", "lastFrameTime.bin"):
+            out["rec/" + f] = open(os.path.join(d, f), "rb").read()
+        rec.defrag()
+        for k, v in tfsf_files(d, "99999").items():
+            out["merged/" + k] = v
+        out["merged/lastFrameTime.bin"] = open(os.path.join(d, "lastFrameTime.bin"), "rb").read()
+        for mode, plasma in ((0, True), (2, False)):
+            play = RefRun()
+            plays.append(play)
+            play.setup(TFSF_N, TFSF_L_UM, -0.5, (2, 2, 2), (2, 2, 2))
+            play.set_state(tfsf_plasma(h) if plasma else np.zeros(0, dtype=oracle_port.MARKER_DTYPE))
+            pd = play.path(".EM_sources", "TFSF")
+            for f in glob.glob(os.path.join(d, "*_99999.bin")) + [os.path.join(d, "consistencyCheck.dat"),
+                                                                 os.path.join(d, "lastFrameTime.bin")]:
+                shutil.copy(f, pd)
+            play.set_tfsf(TFSF_BOX, mode)
+            play.run(TFSF_STEPS)
+            m, E, H = play.final()
+            out["play%d/E" % mode] = E.tobytes()
+            if plasma:
+                out["play%d/H" % mode] = H.tobytes()
+                out["play%d/diag" % mode] = play.diag().tobytes()
+        np.savez_compressed(os.path.join(HERE, "tfsf.npz"), h=np.array(h), tau=dom["tau"],
+                            **{k: np.frombuffer(v, np.uint8) for k, v in out.items()})
+        print("tfsf: %d entries" % len(out))
+    finally:
+        rec.cleanup()
+        for p in plays:
+            p.cleanup()
+
+
 if __name__ == "__main__":
     if not have_reference():
         sys.exit("reference binaries missing: make -C oracle ref REF=<reference tree>")
-    for name in (sys.argv[1:] or list(cases.CASES) + ["gauss_spot", "placers", "tecplot", "probes"]):
+    for name in (sys.argv[1:] or list(cases.CASES) + ["gauss_spot", "placers", "tecplot", "probes", "tfsf"]):
         if name == "probes":
             make_probes()
+            continue
+        if name == "tfsf":
+            make_tfsf()
             continue
         if name == "tecplot":
             make_tecplot()

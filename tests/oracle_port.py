@@ -38,6 +38,12 @@ def _load():
     lib.po_step.argtypes = [vp, vp]
     lib.po_step_probes.argtypes = [vp, vp, C.c_int, vp, vp]
     lib.po_fields_n.argtypes = [vp, vp, vp]
+    lib.po_set_tfsf.restype = C.c_int
+    lib.po_set_tfsf.argtypes = [vp, vp, vp]
+    lib.po_tfsf_faces.restype = C.c_long
+    lib.po_tfsf_faces.argtypes = [vp, vp]
+    lib.po_tfsf_recorded.restype = C.c_long
+    lib.po_tfsf_recorded.argtypes = [vp, vp]
     lib.po_time.restype = C.c_double
     lib.po_time.argtypes = [vp]
     lib.po_em_energy.argtypes = [vp, vp, vp]
@@ -80,6 +86,15 @@ class Place(C.Structure):
                 ("drift", C.c_double * 3), ("uth", C.c_double * 3),
                 ("seed_ij", C.c_int), ("seed_kl", C.c_int), ("skip", C.c_long),
                 ("id0", C.c_int)]
+
+
+TFSF_PLAY, TFSF_REC, TFSF_BACK = 0, 1, 2
+
+
+class Tfsf(C.Structure):
+    """po_tfsf_t (oracle/pic_oracle.h)."""
+    _fields_ = [("lo", C.c_int * 3), ("hi", C.c_int * 3), ("mode", C.c_int),
+                ("open", (C.c_int * 3) * 2), ("frames", C.c_int)]
 
 
 def place(lo, hi, ppc, rho, qDivM, h, drift=(0, 0, 0), uth=(0, 0, 0),
@@ -179,6 +194,29 @@ class OracleRun:
         H = np.zeros(self.shape())
         lib().po_fields_n(self.ptr, E.ctypes.data, H.ctypes.data)
         return E, H
+
+    def set_tfsf(self, lo, hi, mode, open=((0, 0, 0), (0, 0, 0)), frames=0, **kw):
+        """TF/SF interface; play modes take the recorded frames (k, size)."""
+        t = Tfsf((C.c_int * 3)(*lo), (C.c_int * 3)(*hi), mode,
+                 ((C.c_int * 3) * 2)(*[(C.c_int * 3)(*o) for o in open]), frames)
+        data = kw.get("frames_data")
+        self._tfsf_frames = np.ascontiguousarray(data, dtype="<f8") if data is not None else None
+        ptr = self._tfsf_frames.ctypes.data if self._tfsf_frames is not None else None
+        if lib().po_set_tfsf(self.ptr, C.byref(t), ptr) != 0:
+            raise ValueError("TF/SF face closer than 5 cells to a wall")
+
+    def tfsf_faces(self):
+        """(24, 6) face regions {min, max} in the recorded stream order."""
+        out = np.zeros((24, 6), np.int32)
+        lib().po_tfsf_faces(self.ptr, out.ctypes.data)
+        return out
+
+    def tfsf_recorded(self):
+        n = lib().po_tfsf_recorded(self.ptr, None)
+        size = lib().po_tfsf_faces(self.ptr, None)
+        out = np.zeros((n, size))
+        lib().po_tfsf_recorded(self.ptr, out.ctypes.data)
+        return out
 
     def time(self):
         return lib().po_time(self.ptr)

@@ -104,6 +104,24 @@ def read_probe(raw):
     return ijk, np.frombuffer(raw[20:], "<f8").reshape(-1, 7)
 
 
+TFSF_E_FACES = ("Ey_xMin", "Ez_xMin", "Ey_xMax", "Ez_xMax", "Ez_yMin", "Ex_yMin",
+                "Ez_yMax", "Ex_yMax", "Ex_zMin", "Ey_zMin", "Ex_zMax", "Ey_zMax")
+TFSF_H_FACES = ("Hz_xMin", "Hy_xMin", "Hz_xMax", "Hy_xMax", "Hx_yMin", "Hz_yMin",
+                "Hx_yMax", "Hz_yMax", "Hy_zMin", "Hx_zMin", "Hy_zMax", "Hx_zMax")
+TFSF_FACES = TFSF_E_FACES + TFSF_H_FACES      # core/em_TFSF.c:86-119
+
+
+def read_tfsf_stream(raw):
+    """A TF/SF face stream (core/em_TFSF.c:256-268, 565-594): reg_t header
+    {min[3], max[3], cpu, barcode, wrap[3]} then frames of the region's
+    values, the face's first tangential axis slowest.  Returns (header ints,
+    frames (k, volume))."""
+    raw = bytes(raw)
+    head = np.frombuffer(raw[:44], "<i4")
+    vol = int(np.prod(head[3:6] - head[0:3] + 1))
+    return head, np.frombuffer(raw[44:], "<f8").reshape(-1, vol)
+
+
 def read_chunks(raw):
     """A chunk file (type_CFile.c:112-370): the magic, then chunks of
     {INT64 size with header, int deleted, int name length, '\\n', name,
@@ -240,6 +258,28 @@ class RefRun:
             for v in vals:
                 fp.write("@ %.17e\tparameter\n" % v)
             fp.write("@ %d\tEy\n@ %d\tEz\n" % (ey, ez))
+
+    def set_tfsf(self, box, mode, open_faces=None):
+        """.EM_sources/TFSF/TFSF.cfg as setup/tag_TFSF.c:164-171 writes it
+        (the order core/em_TFSF.c:157-166 reads), and openFaces.cfg
+        (setup/tag_TFSFFaces.c) when faces are opened."""
+        d = self.path(".EM_sources", "TFSF")
+        with open(os.path.join(d, "TFSF.cfg"), "w") as fp:
+            for v in box:
+                fp.write("@ %5d       TFSF interface bounding box.\n" % v)
+            fp.write("@ %5d       Interface regime.\n" % mode)
+        if open_faces is not None:
+            with open(os.path.join(d, "openFaces.cfg"), "w") as fp:
+                for axis in range(3):
+                    for top in range(2):
+                        fp.write("@ %d\topen face flag\n" % open_faces[top][axis])
+
+    def defrag(self):
+        """The reference's TFSFdefrag on the recorded streams, no filter."""
+        with open(self.path(".EM_sources", "TFSF", "filter.cfg"), "w") as fp:
+            fp.write("@ % 5d       I0.\n@ % 5d       I1.\n@ % 5d       Shift frames.\n"
+                     % (-10 ** 6, 10 ** 6, 0))
+        self._run("TFSFdefrag.out")
 
     def run(self, steps, exe="core.out", timeout=3600):
         with open(self.path("run_mandor.cfg"), "w") as fp:
