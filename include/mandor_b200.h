@@ -189,6 +189,40 @@ long long mg_estimate_bytes (const mg_params_t *params, long long markers);
 int  mg_tecplot_fields (mg_run_t *run, double *E, double *H);
 int  mg_tecplot_currents (mg_run_t *run, double *J);
 
+/* ---- TF/SF interface (core/em_TFSF.c) -------------------------------------
+ * Replaces TFSF_init / TFSF_preHStep / TFSF_postHStep / TFSF_postEStep /
+ * TFSF_completeFrame (core/em_TFSF.c:480-853, called from core/em.c:92,
+ * 125, 200, 218).  24 faces: the E faces Ey_xMin, Ez_xMin, Ey_xMax, Ez_xMax,
+ * Ez_yMin, Ex_yMin, Ez_yMax, Ex_yMax, Ex_zMin, Ey_zMin, Ex_zMax, Ey_zMax, then
+ * the H faces Hz_xMin, Hy_xMin, ..., Hx_zMax (core/em_TFSF.c:86-119).  A
+ * frame is the values of the 12 E faces then of the 12 H faces, each over
+ * its region (mg_run_tfsf_faces) with the face's first tangential axis
+ * (a+1)%3 slowest: the layout of the recorded streams after their reg_t
+ * header.
+ *   record: every step stores E^n and H^(n-1/2) times the face's source
+ *           factor at its start; mg_run_tfsf_recorded copies the frames of
+ *           the last mg_run_step call (<= 4096 steps) or staged step.
+ *   play:   frames come from the merged streams (*_99999.bin); the step
+ *           with frame counter n (int (t/tau + 0.1) at mg_run_set_tfsf, +1
+ *           per step) reads frame n and n + 1 forward, T - 1 - n backward,
+ *           and plays while n + 1 < T - 1 (T = frames).  They must be on
+ *           the device, in a ring of `ring` slots, before the step runs
+ *           (mg_run_tfsf_put_frames); a missing frame fails the step with
+ *           MG_ERR_STATE.  Played faces must stay 5 cells inside the walls.
+ * mg_run_set_tfsf (run, NULL) removes the interface.                        */
+enum { MG_TFSF_PLAY_FORWARD = 0, MG_TFSF_RECORD = 1, MG_TFSF_PLAY_BACKWARD = 2 };
+typedef struct {
+   int lo[3], hi[3];       /* interface bounding box (TFSF.cfg)               */
+   int mode;               /* MG_TFSF_*                                        */
+   int open[2][3];         /* play: faces removed, [min/max][axis]            */
+   int frames;             /* play: frames recorded (lastFrameTime.bin)       */
+   int ring;               /* play: device frame slots (>= 2)                 */
+} mg_tfsf_t;
+int  mg_run_set_tfsf (mg_run_t *run, const mg_tfsf_t *cfg);
+int  mg_run_tfsf_faces (mg_run_t *run, int regions[24*6], long long *frame_doubles);
+int  mg_run_tfsf_put_frames (mg_run_t *run, int first, int count, const double *frames);
+int  mg_run_tfsf_recorded (mg_run_t *run, int nsteps, double *frames);
+
 /* ---- probes (core/diag_probe.c:409-446) ----------------------------------
  * mg_run_set_probes: probe nodes ijk[3*q..3*q+2] in [0, n) (n = 0 removes
  * them).  Every step then records, right after the H half step (where

@@ -58,6 +58,15 @@ class GaussSpot(C.Structure):
                 ("ey", C.c_int), ("ez", C.c_int)]
 
 
+TFSF_PLAY_FORWARD, TFSF_RECORD, TFSF_PLAY_BACKWARD = 0, 1, 2
+
+
+class Tfsf(C.Structure):
+    """mg_tfsf_t: TF/SF interface box, mode, open faces, frames, ring slots."""
+    _fields_ = [("lo", C.c_int * 3), ("hi", C.c_int * 3), ("mode", C.c_int),
+                ("open", (C.c_int * 3) * 2), ("frames", C.c_int), ("ring", C.c_int)]
+
+
 class Maxwell(C.Structure):
     _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("layers", C.c_int),
                 ("omega_pe2", C.c_double), ("qDivM", C.c_double), ("ux", C.c_double),
@@ -130,6 +139,10 @@ def load():
         "mg_run_profile": [vp, i],
         "mg_run_last_timing": [vp, C.POINTER(d), C.POINTER(d)],
         "mg_run_set_gauss_spot": [vp, vp],
+        "mg_run_set_tfsf": [vp, vp],
+        "mg_run_tfsf_faces": [vp, vp, vp],
+        "mg_run_tfsf_put_frames": [vp, i, i, vp],
+        "mg_run_tfsf_recorded": [vp, i, vp],
         "mg_run_set_probes": [vp, vp, i],
         "mg_run_probe_samples": [vp, i, vp],
         "mg_tecplot_fields": [vp, vp, vp],
@@ -290,6 +303,35 @@ class Run:
         arguments switch it off."""
         self._gspot = GaussSpot(**kw) if kw else None
         _check(load().mg_run_set_gauss_spot(self.ptr, C.byref(self._gspot) if kw else None))
+
+    def set_tfsf(self, lo=None, hi=None, mode=TFSF_PLAY_FORWARD, open=((0, 0, 0), (0, 0, 0)), frames=0,
+                 ring=2):
+        """TF/SF interface (mg_run_set_tfsf); no box removes it."""
+        if lo is None:
+            _check(load().mg_run_set_tfsf(self.ptr, None))
+            return
+        t = Tfsf((C.c_int * 3)(*lo), (C.c_int * 3)(*hi), mode,
+                 ((C.c_int * 3) * 2)(*[(C.c_int * 3)(*o) for o in open]), frames, ring)
+        _check(load().mg_run_set_tfsf(self.ptr, C.byref(t)))
+
+    def tfsf_faces(self):
+        """((24, 6) face regions {min, max}, doubles per frame)."""
+        regions = np.zeros((24, 6), np.int32)
+        size = C.c_longlong(0)
+        _check(load().mg_run_tfsf_faces(self.ptr, regions.ctypes.data, C.byref(size)))
+        return regions, size.value
+
+    def tfsf_put_frames(self, first, frames):
+        """Frames first, first + 1, ... ((k, frame size) doubles) to the device ring."""
+        a = np.ascontiguousarray(frames, dtype="<f8")
+        _check(load().mg_run_tfsf_put_frames(self.ptr, int(first), len(a), a.ctypes.data))
+
+    def tfsf_recorded(self, nsteps):
+        """(nsteps, frame size) recorded frames of the last step call."""
+        _, size = self.tfsf_faces()
+        out = np.zeros((nsteps, size))
+        _check(load().mg_run_tfsf_recorded(self.ptr, int(nsteps), out.ctypes.data))
+        return out
 
     def place_uniform(self, lo, hi, ppc, rho, qDivM, drift=(0, 0, 0), uth=(0, 0, 0),
                       seed=(1802, 9373), skip=0, id0=1):

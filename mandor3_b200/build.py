@@ -34,6 +34,7 @@ CUDA_UNITS = {
     "gauss.cu": ["-fmad=false"],
     "tags.cu": ["-fmad=false"],
     "tecplot.cu": ["-fmad=false"],
+    "tfsf.cu": ["-fmad=false"],
     "api32.cu": [],
     "fields32.cu": [],
     "push32.cu": [],

@@ -179,6 +179,7 @@ __global__ void k_end_step (DevScalars *dsc, double *ring, double volume, double
       dsc->acc[q] = 0;
    dsc->time += tau;
    dsc->step += 1;
+   dsc->tfsf_frame += 1;          // TFSF_completeFrame (core/em_TFSF.c:849-853)
 }
 
 } // namespace
@@ -462,6 +463,7 @@ extern "C" int mg_run_destroy (mg_run_t *r)
    if (r->probe_ijk) cudaFree (r->probe_ijk);
    if (r->probe_ring) cudaFree (r->probe_ring);
    if (r->probe_ptrs) cudaFree (r->probe_ptrs);
+   mg_tfsf_free (r);
    for (int q = 0 ; q < 2 ; ++q)
       if (r->gauss_rho[q]) cudaFree (r->gauss_rho[q]);
    if (r->gauss_out) cudaFree (r->gauss_out);
@@ -738,13 +740,14 @@ extern "C" int mg_em_HHalfStep (mg_run_t *r)
 {
    CHECK_RUN (r);
    TRY (expect_stage (r, 0, __func__));
-   TRY (is32 (r) ? mg_fields32_h_half (r) : mg_fields64_h_half (r));
-   // Probe samples of this step into row 0 (core/main.c:373 samples after
-   // em_energy; nothing in between changes E or H^n).
-   if (r->nprobes > 0) {
+   // A stage-by-stage step keeps its probe samples and TF/SF record in row 0.
+   if (r->nprobes > 0 || mg_tfsf_recording (r))
       MG_CUDA (cudaMemsetAsync (&r->dsc->step, 0, sizeof (int), r->stream));
-      TRY (mg_probes_enqueue (r));
-   }
+   TRY (mg_tfsf_record (r));
+   TRY (is32 (r) ? mg_fields32_h_half (r) : mg_fields64_h_half (r));
+   // Probe samples (core/main.c:373 samples after em_energy; nothing in
+   // between changes E or H^n).
+   TRY (mg_probes_enqueue (r));
    r->stage_no = 1;
    return MG_OK;
 }
@@ -769,6 +772,10 @@ static int check_err (mg_run_t *r)
    int info[5];
    MG_CUDA (cudaMemcpyAsync (info, &r->dsc->err, sizeof (int)*5, cudaMemcpyDeviceToHost, r->stream));
    MG_CUDA (cudaStreamSynchronize (r->stream));
+   if (info[0] & 4) {
+      mg_set_error ("TF/SF frame %d is not on the device (mg_run_tfsf_put_frames)", info[1]);
+      return MG_ERR_STATE;
+   }
    if (info[0]) {
       mg_set_error ("marker %d left the mesh or moved more than one cell per step "
                     "(flags %d, cell %d %d %d); the step is invalid", info[1], info[0], info[2], info[3], info[4]);
@@ -915,6 +922,7 @@ extern "C" int mg_gauss_after (mg_run_t *r, double out[2])
 int mg_enqueue_step64 (mg_run_t *r, int part)
 {
    if (part < 0 || part == 0) {
+      TRY (mg_tfsf_record (r));
       TRY (mg_fields64_h_both (r));
       TRY (mg_probes_enqueue (r));
       TRY (mg_fields64_zero_j (r));

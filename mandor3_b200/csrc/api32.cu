@@ -700,6 +700,7 @@ int mg_sort32 (mg_run_t *r)
 int mg_enqueue_step32 (mg_run_t *r, int part)
 {
    if (part < 0 || part == 0) {
+      TRY32 (mg_tfsf_record (r));
       TRY32 (mg_fields32_h_both (r));
       TRY32 (mg_probes_enqueue (r));
       TRY32 (mg_fields32_zero_j (r));

@@ -879,6 +879,7 @@ int fields_energy (mg_run_t *r, const FS<T> &fs)
 template <typename T>
 int fields_h_step (mg_run_t *r, const FS<T> &fs)
 {
+   TRY_MG (mg_tfsf_h (r));
    TRY_MG (launch_laser<T> (r, fs, 0));
    const Grid &g = r->g;
    for (int ea = 0 ; ea < 3 ; ++ea) {
@@ -905,6 +906,7 @@ int fields_h_both (mg_run_t *r, const FS<T> &fs)
       g, f3 (fs.E), f3 (fs.H), f3 (fs.Hn), b, (T) (0.5*g.tau/g.h[0]), (T) (0.5*g.tau/g.h[1]), (T) (0.5*g.tau/g.h[2]),
       energy_pick (g), r->dsc);
    MG_LAUNCH_CHECK ();
+   TRY_MG (mg_tfsf_h (r));
    TRY_MG (launch_laser<T> (r, fs, 0));
    return launch_h_walls<T> (r, fs, 1);
 }
@@ -948,11 +950,12 @@ static int launch_gauss_spot (mg_run_t *r, const FS<T> &fs)
    return MG_OK;
 }
 
-// Stage path: source at t + tau/2, then E -= tau J over [-1, n+1]^3, then
-// the hard gauss-spot source.
+// Stage path: TF/SF faces, source at t + tau/2, then E -= tau J over
+// [-1, n+1]^3, then the hard gauss-spot source (core/em.c:189-222).
 template <typename T>
 int fields_e_finish (mg_run_t *r, const FS<T> &fs)
 {
+   TRY_MG (mg_tfsf_e (r));
    TRY_MG (launch_laser<T> (r, fs, 1));
    const int lo[3] = {-1, -1, -1};
    const int hi[3] = {r->g.n[0] + 1, r->g.n[1] + 1, r->g.n[2] + 1};
@@ -966,9 +969,15 @@ int fields_e_finish (mg_run_t *r, const FS<T> &fs)
 // Graph path: E += curl H - tau J in one pass away from the rim, E walls,
 // source, then -tau J on the rim.  Bit-identical to the stage path: every
 // node sees the same operations in the same order.  Needs the J walls done.
+// A playing TF/SF interface adds to E between the curl and -tau J on its
+// faces, so with one the graph takes the stage path's two passes.
 template <typename T>
 int fields_e_fused (mg_run_t *r, const FS<T> &fs)
 {
+   if (mg_tfsf_playing (r)) {
+      TRY_MG (fields_e_step<T> (r, fs));
+      return fields_e_finish<T> (r, fs);
+   }
    const Grid &g = r->g;
    Box b = e_box (g);
    Rim rm = rim (r);

@@ -90,6 +90,7 @@ struct DevScalars {
                            // ghost layers, 2: more than one cell per step)
    int    err_info[4];     // first offending marker index and cell
    int    tile_next;       // next tile to hand out in the tiled push
+   int    tfsf_frame;      // TF/SF frame counter (steps since t = 0)
    float  rho_max;         // largest |rho| of the markers at the last sort
    Markers32 m32;          // the current marker buffer set (precision form),
                            // read by the kernels of the step graph
@@ -145,6 +146,9 @@ struct mg_run {
    mg_laser_t  laser;
    int         has_gspot;
    GaussSpot   gspot;
+
+   // TF/SF interface (tfsf.cu), null when off
+   struct mg_tfsf_state *tfsf;
 
    // probes: nodes, per-step sample ring (MG_RING rows of nprobes x 7)
    int         nprobes;
@@ -216,6 +220,12 @@ int mg_fields64_e_fused (mg_run_t *r);
 int mg_push64 (mg_run_t *r);
 int mg_gauss_rho (mg_run_t *r, double *rho);
 int mg_probes_enqueue (mg_run_t *r);
+int mg_tfsf_h (mg_run_t *r);
+int mg_tfsf_e (mg_run_t *r);
+int mg_tfsf_record (mg_run_t *r);
+bool mg_tfsf_playing (const mg_run_t *r);
+bool mg_tfsf_recording (const mg_run_t *r);
+void mg_tfsf_free (mg_run_t *r);
 int mg_gauss_residual (mg_run_t *r, const double *rho1, const double *rho2, double *out_dev);
 int mg_end_step (mg_run_t *r);
 

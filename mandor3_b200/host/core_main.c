@@ -21,6 +21,9 @@
  *                              core/diag_probe.c:48-446, probe.h
  *   tmp/spectrDump_%d_0, binData/spectr.N
  *                              spectr_dump.c:15-109, type_CFile.c:112-370
+ *   .EM_sources/TFSF/TFSF.cfg, openFaces.cfg, consistencyCheck.dat,
+ *   lastFrameTime.bin, TFSF_defrag.map, <face>_000.bin / <face>_99999.bin
+ *                              core/em_TFSF.c:143-460, 565-594, 855-891
  *
  *   core_b200.out [--fp32] [--device N]
  */
@@ -31,6 +34,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <time.h>
+#include <unistd.h>
 
 #include "mandor_b200.h"
 
@@ -601,6 +605,227 @@ static void probes_close (probes_t *p)
    free (p->rows);
 }
 
+/* ---- TF/SF interface (core/em_TFSF.c) ------------------------------------- */
+
+static const char *const TFSF_NAME[24] = {                 /* core/em_TFSF.c:86-119 */
+   "Ey_xMin", "Ez_xMin", "Ey_xMax", "Ez_xMax", "Ez_yMin", "Ex_yMin",
+   "Ez_yMax", "Ex_yMax", "Ex_zMin", "Ey_zMin", "Ex_zMax", "Ey_zMax",
+   "Hz_xMin", "Hy_xMin", "Hz_xMax", "Hy_xMax", "Hx_yMin", "Hz_yMin",
+   "Hx_yMax", "Hz_yMax", "Hy_zMin", "Hx_zMin", "Hy_zMax", "Hx_zMax"};
+
+typedef struct {
+   int       on;
+   mg_tfsf_t cfg;
+   int       region[24][6];     /* regions in the frame layout */
+   long long size;              /* doubles per frame */
+   int       frame;             /* frame counter of the next step */
+   int       written;           /* record: frames written by this run */
+   FILE     *fp[24];            /* record: the face streams */
+   double   *buf;               /* 257 frames */
+} tfsf_t;
+
+static long long region_volume (const int r[6])
+{
+   long long v = 1;
+   for (int a = 0 ; a < 3 ; ++a)
+      v *= (r[3 + a] >= r[a]) ? r[3 + a] - r[a] + 1 : 0;
+   return v;
+}
+
+static void tfsf_path (char *out, size_t cap, int f, int cpu)
+{
+   snprintf (out, cap, ".EM_sources/TFSF/%s_%03d.bin", TFSF_NAME[f], cpu);   /* :143-148 */
+}
+
+/* TFSF_init for one rank: reads TFSF.cfg (and in play openFaces.cfg,
+ * consistencyCheck.dat, lastFrameTime.bin), configures the run; record mode
+ * opens the face streams and writes consistencyCheck.dat and the merge map
+ * (TFSF_turnRec :229-283, TFSF_defragInit :199-224). */
+static void tfsf_open (tfsf_t *t, mg_run_t *run, const domain_t *d, double time)
+{
+   memset (t, 0, sizeof (*t));
+   if (!access (".EM_sources/TFSF/TFSF_defrag.map", F_OK))
+      die ("%s", "input data is not compiled (use 'TFSFdefrag')");
+   FILE *fp = fopen (".EM_sources/TFSF/TFSF.cfg", "rt");
+   if (!fp)
+      return;
+   const char *cfg = ".EM_sources/TFSF/TFSF.cfg";
+   for (int a = 0 ; a < 3 ; ++a) {
+      t->cfg.lo[a] = read_at_int (fp, cfg);
+      t->cfg.hi[a] = read_at_int (fp, cfg);
+   }
+   t->cfg.mode = read_at_int (fp, cfg);
+   fclose (fp);
+   if (t->cfg.mode != MG_TFSF_PLAY_FORWARD && t->cfg.mode != MG_TFSF_RECORD &&
+       t->cfg.mode != MG_TFSF_PLAY_BACKWARD)
+      return;                                   /* inactive */
+   t->on = 1;
+   if (t->cfg.mode == MG_TFSF_RECORD) {
+      check (mg_run_set_tfsf (run, &t->cfg), "TF/SF interface");
+      check (mg_run_tfsf_faces (run, (int *) t->region, &t->size), "TF/SF faces");
+      for (int f = 0 ; f < 24 ; ++f) {
+         if (region_volume (t->region[f]) <= 0)
+            continue;
+         char name[200];
+         tfsf_path (name, sizeof (name), f, 0);
+         t->fp[f] = open_or_die (name, "wb");
+         /* reg_t {min[3], max[3], cpu, barcode = mode, wrap[3]} */
+         const int head[11] = {t->region[f][0], t->region[f][1], t->region[f][2], t->region[f][3],
+                               t->region[f][4], t->region[f][5], 0, t->cfg.mode, 0, 0, 0};
+         write_exact (head, sizeof (head), t->fp[f], name);
+      }
+      fp = open_or_die (".EM_sources/TFSF/consistencyCheck.dat", "wt");
+      fprintf (fp, "@ %d\tInterface size in X direction (nodes)\n", t->cfg.hi[0] - t->cfg.lo[0]);
+      fprintf (fp, "@ %d\tInterface size in Y direction (nodes)\n", t->cfg.hi[1] - t->cfg.lo[1]);
+      fprintf (fp, "@ %d\tInterface size in Z direction (nodes)\n", t->cfg.hi[2] - t->cfg.lo[2]);
+      fprintf (fp, "@ %.12e\tTime step\n", d->tau);
+      fprintf (fp, "@ %.12e\tSpatial step along X\n", d->h[0]);
+      fprintf (fp, "@ %.12e\tSpatial step along Y\n", d->h[1]);
+      fprintf (fp, "@ %.12e\tSpatial step along Z\n", d->h[2]);
+      fclose (fp);
+      /* The merge map: each face's full region (TFSF_init :505-553), its
+       * unrolling axes, the merged stream and this rank's stream. */
+      fp = open_or_die (".EM_sources/TFSF/TFSF_defrag.map", "at");
+      const int *side[2] = {t->cfg.lo, t->cfg.hi};
+      for (int f = 0 ; f < 24 ; ++f) {
+         const int fe = f % 12, a = fe/4, top = (fe/2) % 2, comp = fe % 2, ce = (a + 1 + comp) % 3;
+         int lo[3], hi[3];
+         for (int b = 0 ; b < 3 ; ++b) {
+            lo[b] = t->cfg.lo[b];
+            hi[b] = t->cfg.hi[b];
+         }
+         lo[a] = hi[a] = side[top][a];
+         lo[ce] += 1;
+         if (f >= 12) {
+            lo[a] += top;
+            hi[a] += top;
+         }
+         char name[200];
+         fprintf (fp, "[%d %d] [%d %d] [%d %d]\n", lo[0], hi[0], lo[1], hi[1], lo[2], hi[2]);
+         fprintf (fp, "ep = %d, eq = %d\n", (a + 1) % 3, (a + 2) % 3);
+         tfsf_path (name, sizeof (name), f, 99999);
+         fprintf (fp, "%s\n", name);
+         if (t->fp[f]) {
+            tfsf_path (name, sizeof (name), f, 0);
+            fprintf (fp, "%s\n", name);
+         }
+         fprintf (fp, "---\n");
+      }
+      fclose (fp);
+   } else {
+      fp = fopen (".EM_sources/TFSF/openFaces.cfg", "rt");
+      if (fp) {
+         for (int a = 0 ; a < 3 ; ++a)
+            for (int top = 0 ; top < 2 ; ++top)
+               t->cfg.open[top][a] = read_at_int (fp, ".EM_sources/TFSF/openFaces.cfg");
+         fclose (fp);
+      }
+      const char *cc = ".EM_sources/TFSF/consistencyCheck.dat";
+      fp = fopen (cc, "rt");
+      if (!fp)
+         die ("%s", "there are no recorded data");
+      for (int a = 0 ; a < 3 ; ++a)
+         if (read_at_int (fp, cc) != t->cfg.hi[a] - t->cfg.lo[a])
+            die ("inconsistent size along axis '%s'", a == 0 ? "X" : a == 1 ? "Y" : "Z");
+      const double old_tau = read_at_double (fp, cc);
+      if (!(fabs (1 - old_tau/d->tau) < 1e-11))
+         die ("%s", "inconsistent time step");
+      for (int a = 0 ; a < 3 ; ++a)
+         if (!(fabs (1 - read_at_double (fp, cc)/d->h[a]) < 1e-11))
+            die ("inconsistent spatial step along %s", a == 0 ? "X" : a == 1 ? "Y" : "Z");
+      fclose (fp);
+      fp = open_or_die (".EM_sources/TFSF/lastFrameTime.bin", "rb");
+      read_exact (&t->cfg.frames, sizeof (int), fp, ".EM_sources/TFSF/lastFrameTime.bin");
+      fclose (fp);
+      t->cfg.ring = 512;
+      check (mg_run_set_tfsf (run, &t->cfg), "TF/SF interface");
+      check (mg_run_tfsf_faces (run, (int *) t->region, &t->size), "TF/SF faces");
+      /* the merged streams stay open for the frames of each step call */
+      for (int f = 0 ; f < 24 ; ++f) {
+         char name[200];
+         tfsf_path (name, sizeof (name), f, 99999);
+         t->fp[f] = fopen (name, "rb");
+         const int fe = f % 12, a = fe/4, top = (fe/2) % 2;
+         if (!t->fp[f] && !t->cfg.open[top][a])
+            die ("cannot open '%s'", name);
+      }
+   }
+   t->frame = (int) (time/d->tau + 0.1);
+   t->buf = (double *) malloc (sizeof (double)*(size_t) (t->size > 0 ? t->size : 1)*257);
+}
+
+/* Play: the frames steps frame .. frame + k - 1 read (TFSF_cacheFrame,
+ * :785-806), from the merged streams to the device ring. */
+static void tfsf_before (tfsf_t *t, mg_run_t *run, int k)
+{
+   if (!t->on || t->cfg.mode == MG_TFSF_RECORD || t->size == 0)
+      return;
+   const int last = t->cfg.frames;
+   int lo, hi;
+   if (t->cfg.mode == MG_TFSF_PLAY_FORWARD) {
+      lo = t->frame;
+      hi = t->frame + k;
+   } else {
+      lo = last - 1 - (t->frame + k - 1);
+      hi = last - 1 - t->frame;
+   }
+   if (lo < 0) lo = 0;
+   if (hi > last - 1) hi = last - 1;
+   if (hi < lo)
+      return;
+   for (int fr = lo ; fr <= hi ; ++fr) {
+      double *o = t->buf + (size_t) (fr - lo)*t->size;
+      for (int f = 0 ; f < 24 ; ++f) {
+         const long long v = region_volume (t->region[f]);
+         if (!t->fp[f]) {
+            memset (o, 0, sizeof (double)*v);
+         } else {
+            fseek (t->fp[f], 44 + (long) fr*v*(long) sizeof (double), SEEK_SET);
+            if (fread (o, sizeof (double), v, t->fp[f]) != (size_t) v)
+               die ("TF/SF stream '%s' ends before the frames the run plays", TFSF_NAME[f]);
+         }
+         o += v;
+      }
+   }
+   check (mg_run_tfsf_put_frames (run, lo, hi - lo + 1, t->buf), "TF/SF frames");
+}
+
+/* Record: the frames of the last k steps to the face streams. */
+static void tfsf_after (tfsf_t *t, mg_run_t *run, int k)
+{
+   if (!t->on)
+      return;
+   t->frame += k;
+   if (t->cfg.mode != MG_TFSF_RECORD || t->size == 0)
+      return;
+   check (mg_run_tfsf_recorded (run, k, t->buf), "TF/SF record");
+   for (int s = 0 ; s < k ; ++s) {
+      const double *o = t->buf + (size_t) s*t->size;
+      for (int f = 0 ; f < 24 ; ++f) {
+         const long long v = region_volume (t->region[f]);
+         if (t->fp[f])
+            write_exact (o, sizeof (double)*v, t->fp[f], TFSF_NAME[f]);
+         o += v;
+      }
+   }
+   t->written += k;
+}
+
+/* TFSF_shutDown (:862-891): streams closed, record mode writes the frame
+ * count. */
+static void tfsf_close (tfsf_t *t)
+{
+   for (int f = 0 ; f < 24 ; ++f)
+      if (t->fp[f])
+         fclose (t->fp[f]);
+   if (t->on && t->cfg.mode == MG_TFSF_RECORD) {
+      FILE *fp = open_or_die (".EM_sources/TFSF/lastFrameTime.bin", "wb");
+      write_exact (&t->written, sizeof (int), fp, ".EM_sources/TFSF/lastFrameTime.bin");
+      fclose (fp);
+   }
+   free (t->buf);
+}
+
 /* ---- spectral dumps (spectr_dump.c:66-109) -------------------------------- */
 
 static long chunk_open (FILE *fp, const char *name)
@@ -685,8 +910,9 @@ static void spectr_dump (records_t *rec, const domain_t *d, double time, const d
  * H^n, and J after the E step (tecIO_saveCurrents, IO_tecplot.c:250-266).
  * row: the step's energy row. */
 static void staged_step (mg_run_t *run, records_t *rec, const domain_t *dom, long nodes, double time,
-                         double row[6], int tec, int spectr, probes_t *probes)
+                         double row[6], int tec, int spectr, probes_t *probes, tfsf_t *tfsf)
 {
+   tfsf_before (tfsf, run, 1);
    char path[512];
    const int n[3] = {dom->dmax[0], dom->dmax[1], dom->dmax[2]};
    unsigned char head[HEADER_BYTES];
@@ -709,6 +935,7 @@ static void staged_step (mg_run_t *run, records_t *rec, const domain_t *dom, lon
       check (mg_em_EStep_start (run), "E step");
       check (mg_jbc_finish (run), "current walls");
       check (mg_em_EStep_finish (run), "E step finish");
+      tfsf_after (tfsf, run, 1);
       free (a);
       free (b);
       free (rho);
@@ -740,6 +967,7 @@ static void staged_step (mg_run_t *run, records_t *rec, const domain_t *dom, lon
    check (mg_em_EStep_start (run), "E step");
    check (mg_jbc_finish (run), "current walls");
    check (mg_em_EStep_finish (run), "E step finish");
+   tfsf_after (tfsf, run, 1);
    check (mg_tecplot_currents (run, a), "tecplot currents");
    mesh_head (n, "vec_J", 2, 1, head);
    snprintf (path, sizeof (path), "binData/tec_J_%06d(%03d).bin", rec->tec_num, 0);
@@ -867,6 +1095,8 @@ int main (int argc, char **argv)
       fclose (gs);
       check (mg_run_set_gauss_spot (run, &s), "gauss spot");
    }
+   tfsf_t tfsf;
+   tfsf_open (&tfsf, run, &dom, time);
    probes_t probes;
    probes_open (&probes, &dom, cfg.cont && point > 0);
    if (probes.nact > 0)
@@ -906,12 +1136,14 @@ int main (int argc, char **argv)
       const int tec = cfg.tecplot > 0 && (t + 1) % cfg.tecplot == 0;
       const int spectr = cfg.spectr > 0 && (t + 1) % cfg.spectr == 0;
       if (tec || spectr) {
-         staged_step (run, &rec, &dom, nodes, time, rows, tec, spectr, &probes);
+         staged_step (run, &rec, &dom, nodes, time, rows, tec, spectr, &probes, &tfsf);
          k = 1;
          next = t + 1;
       } else {
+         tfsf_before (&tfsf, run, k);
          check (mg_run_step (run, k, rows), "step");
          probes_write (run, &probes, k);
+         tfsf_after (&tfsf, run, k);
       }
       for (int q = 0 ; q < k ; ++q)
          diag_add (&diag, rows + 6*q);
@@ -942,6 +1174,7 @@ int main (int argc, char **argv)
    free (diag.rows);
    check (mg_run_destroy (run), "destroy run");
    probes_close (&probes);
+   tfsf_close (&tfsf);
    remove ("tmp/stop.flag");
    return EXIT_SUCCESS;
 }
