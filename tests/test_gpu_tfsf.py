@@ -4,6 +4,7 @@ import numpy as np
 import pytest
 
 import parity
+import refrun
 import test_tfsf
 from test_tfsf import BC, GOLD, box_cfg, make_golden, merged_frames, raw, streams
 
