@@ -279,6 +279,37 @@ typedef struct {
 } mg_foil_t;
 int  mg_run_place_foil (mg_run_t *run, const mg_foil_t *spec);
 
+/* mg_run_place_two_stream: [DF:two-stream] (setup/tag_twoStream.c:23-103):
+ * n[0] n[1] n[2] lattice nodes ((i + 1/2) L_x/n_x, ...) each with a marker
+ * of u = +V and one of u = -V (in that order), V = gamma sqrt(3)/(2|k|)
+ * along k = 2 pi (m_x/L_x, m_y/L_y, m_z/L_z), rho = gamma^2/qDivM
+ * L_x L_y L_z/(h1 h2 h3 n_x n_y n_z); L: the domain lengths of
+ * binData/domain.bin; ids id0, id0 + 1, ...                               */
+typedef struct {
+   double gamma, qDivM;   /* growth rate, q/M (|q/M| <= 1)                 */
+   int    n[3], m[3];     /* markers per beam along each axis; mode numbers */
+   double L[3];
+   int    id0;
+} mg_two_stream_t;
+int  mg_run_place_two_stream (mg_run_t *run, const mg_two_stream_t *spec);
+
+/* mg_run_df_uniform: [DF:uniform] (setup/tag_DF_uniform.c:36-70) on the
+ * placed markers [first, first + count) (before mg_run_init): u = u0 +
+ * (rand ()/RAND_MAX - 1/2) du per axis with the GNU C library's rand () from
+ * its default seed, three draws per marker (x, y, z), after draws_before
+ * draws taken by earlier tags; rho = rho_deck rho_crit/ppc (rho_crit = e
+ * n_cr/rho0 for wavelength lambda_cm), q/M as given.
+ * mg_run_shift_velocity: [velocity shift] 'last' (setup/tag_vShift.c:29-49):
+ * u += dv on [first, first + count).                                       */
+typedef struct {
+   double rho, qDivM, ux, uy, uz, dux, duy, duz;   /* the tag's values, its order */
+   int    ppc;            /* particles per cell of the markers' [plasma] tag */
+   double lambda_cm;
+   long long draws_before;
+} mg_df_uniform_t;
+int  mg_run_df_uniform (mg_run_t *run, long long first, long long count, const mg_df_uniform_t *df);
+int  mg_run_shift_velocity (mg_run_t *run, long long first, long long count, const double dv[3]);
+
 /* ---- hard gauss-spot source (core/em_gaussSpot.c:31-156) -----------------
  * The fields of .gaussSpot.cfg (written by setup/tag_gaussSpot.c:126-140),
  * in its order.  After every E step (em_EStep_finish, core/em.c:216, at time

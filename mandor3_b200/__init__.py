@@ -67,6 +67,17 @@ class Tfsf(C.Structure):
                 ("open", (C.c_int * 3) * 2), ("frames", C.c_int), ("ring", C.c_int)]
 
 
+class TwoStream(C.Structure):
+    _fields_ = [("gamma", C.c_double), ("qDivM", C.c_double), ("n", C.c_int * 3), ("m", C.c_int * 3),
+                ("L", C.c_double * 3), ("id0", C.c_int)]
+
+
+class DfUniform(C.Structure):
+    _fields_ = [("rho", C.c_double), ("qDivM", C.c_double), ("ux", C.c_double), ("uy", C.c_double),
+                ("uz", C.c_double), ("dux", C.c_double), ("duy", C.c_double), ("duz", C.c_double),
+                ("ppc", C.c_int), ("lambda_cm", C.c_double), ("draws_before", C.c_longlong)]
+
+
 class Maxwell(C.Structure):
     _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("layers", C.c_int),
                 ("omega_pe2", C.c_double), ("qDivM", C.c_double), ("ux", C.c_double),
@@ -140,6 +151,9 @@ def load():
         "mg_run_last_timing": [vp, C.POINTER(d), C.POINTER(d)],
         "mg_run_set_gauss_spot": [vp, vp],
         "mg_run_set_tfsf": [vp, vp],
+        "mg_run_place_two_stream": [vp, vp],
+        "mg_run_df_uniform": [vp, C.c_longlong, C.c_longlong, vp],
+        "mg_run_shift_velocity": [vp, C.c_longlong, C.c_longlong, vp],
         "mg_run_tfsf_faces": [vp, vp, vp],
         "mg_run_tfsf_put_frames": [vp, i, i, vp],
         "mg_run_tfsf_recorded": [vp, i, vp],
@@ -303,6 +317,20 @@ class Run:
         arguments switch it off."""
         self._gspot = GaussSpot(**kw) if kw else None
         _check(load().mg_run_set_gauss_spot(self.ptr, C.byref(self._gspot) if kw else None))
+
+    def place_two_stream(self, gamma, qDivM, n, m, L, id0=1):
+        """[DF:two-stream] markers (mg_run_place_two_stream)."""
+        s = TwoStream(gamma, qDivM, (C.c_int * 3)(*n), (C.c_int * 3)(*m), (C.c_double * 3)(*L), id0)
+        _check(load().mg_run_place_two_stream(self.ptr, C.byref(s)))
+
+    def df_uniform(self, first, count, rho, qDivM, u, du, ppc, lambda_cm, draws_before=0):
+        """[DF:uniform] on placed markers [first, first + count)."""
+        s = DfUniform(rho, qDivM, u[0], u[1], u[2], du[0], du[1], du[2], ppc, lambda_cm, draws_before)
+        _check(load().mg_run_df_uniform(self.ptr, int(first), int(count), C.byref(s)))
+
+    def shift_velocity(self, first, count, dv):
+        """[velocity shift]: u += dv on placed markers [first, first + count)."""
+        _check(load().mg_run_shift_velocity(self.ptr, int(first), int(count), (C.c_double * 3)(*dv)))
 
     def set_tfsf(self, lo=None, hi=None, mode=TFSF_PLAY_FORWARD, open=((0, 0, 0), (0, 0, 0)), frames=0,
                  ring=2):

@@ -16,6 +16,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <vector>
+
 #include "mg_internal.cuh"
 
 #define TRY_T(x)                                                             \
@@ -553,4 +555,307 @@ extern "C" int mg_run_place_foil (mg_run_t *r, const mg_foil_t *s)
    cudaFree (count);
    cudaFree (first);
    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// [DF:uniform] (setup/tag_DF_uniform.c:36-70): velocities of markers already
+// placed, u = u0 + (rand ()/RAND_MAX - 1/2) du per axis, drawn from the C
+// library's rand () (three draws per marker, x then y then z).
+//
+// rand () of the GNU C library with the default seed is the additive
+// feedback generator published in its random(3) sources: r_0 = 1,
+// r_i = 16807 r_(i-1) mod (2^31 - 1) for i < 31, r_i = r_(i-31) for
+// i = 31..33, r_i = r_(i-3) + r_(i-31) mod 2^32 after that, and draw k is
+// r_(k+344) >> 1.  The recurrence is linear over the integers mod 2^32, so
+// the 31-value window at any draw is a power of its 31 x 31 step matrix
+// applied to the window at draw 0; each thread starts from its own window
+// and steps its draws in order.
+// ---------------------------------------------------------------------------
+namespace {
+
+typedef unsigned int u32;
+const int LAG = 31;
+
+struct Mat31 { u32 a[LAG][LAG]; };
+
+Mat31 mat_mul (const Mat31 &x, const Mat31 &y)
+{
+   Mat31 z;
+   for (int i = 0 ; i < LAG ; ++i)
+      for (int j = 0 ; j < LAG ; ++j) {
+         u32 s = 0;
+         for (int k = 0 ; k < LAG ; ++k)
+            s += x.a[i][k]*y.a[k][j];
+         z.a[i][j] = s;
+      }
+   return z;
+}
+
+void mat_vec (const Mat31 &m, const u32 *v, u32 *out)
+{
+   u32 t[LAG];
+   for (int i = 0 ; i < LAG ; ++i) {
+      u32 s = 0;
+      for (int k = 0 ; k < LAG ; ++k)
+         s += m.a[i][k]*v[k];
+      t[i] = s;
+   }
+   memcpy (out, t, sizeof (t));
+}
+
+// One draw on a window (r_(i-31), ..., r_(i-1)) -> (r_(i-30), ..., r_i).
+Mat31 step_matrix ()
+{
+   Mat31 m;
+   memset (&m, 0, sizeof (m));
+   for (int k = 0 ; k < LAG - 1 ; ++k)
+      m.a[k][k + 1] = 1;
+   m.a[LAG - 1][LAG - 3] = 1;
+   m.a[LAG - 1][0] = 1;
+   return m;
+}
+
+Mat31 mat_pow (long long e)
+{
+   Mat31 r, b = step_matrix ();
+   memset (&r, 0, sizeof (r));
+   for (int i = 0 ; i < LAG ; ++i)
+      r.a[i][i] = 1;
+   for ( ; e > 0 ; e >>= 1) {
+      if (e & 1)
+         r = mat_mul (r, b);
+      b = mat_mul (b, b);
+   }
+   return r;
+}
+
+// The window before draw 0: r_313 .. r_343.
+void rand_window0 (u32 *w)
+{
+   u32 r[344];
+   long long s = 1;
+   r[0] = 1;
+   for (int i = 1 ; i < 31 ; ++i) {
+      s = (16807*s) % 2147483647;
+      r[i] = (u32) s;
+   }
+   for (int i = 31 ; i < 34 ; ++i)
+      r[i] = r[i - 31];
+   for (int i = 34 ; i < 344 ; ++i)
+      r[i] = r[i - 3] + r[i - 31];
+   memcpy (w, r + 344 - LAG, sizeof (u32)*LAG);
+}
+
+struct DfUniform {
+   double u[3], du[3];
+   float rho, qm;
+};
+
+template <typename U>
+__global__ void k_df_uniform (U *ux, U *uy, U *uz, float *rho, float *qm, long long first, long long count,
+                              long long per, int threads, const u32 *windows, DfUniform d)
+{
+   const int t = blockIdx.x*blockDim.x + threadIdx.x;
+   if (t >= threads)
+      return;
+   u32 w[LAG];
+   for (int k = 0 ; k < LAG ; ++k)
+      w[k] = windows[(long long) t*LAG + k];
+   int j = 0;
+   const long long b = (long long) t*per, e = (b + per < count) ? b + per : count;
+   for (long long q = b ; q < e ; ++q) {
+      double v[3];
+      for (int a = 0 ; a < 3 ; ++a) {
+         const u32 x = w[(j + LAG - 3) % LAG] + w[j];
+         w[j] = x;
+         j = (j + 1) % LAG;
+         const double f = (double) (int) (x >> 1)/(double) 2147483647;
+         v[a] = d.u[a] + (f - 0.5)*d.du[a];
+      }
+      const long long o = first + q;
+      ux[o] = (U) v[0];
+      uy[o] = (U) v[1];
+      uz[o] = (U) v[2];
+      rho[o] = d.rho;
+      qm[o] = d.qm;
+   }
+}
+
+template <typename U>
+__global__ void k_shift (U *ux, U *uy, U *uz, long long first, long long count, double dx, double dy, double dz)
+{
+   for (long long q = blockIdx.x*(long long) blockDim.x + threadIdx.x ; q < count ;
+        q += (long long) gridDim.x*blockDim.x) {
+      const long long o = first + q;
+      ux[o] = (U) ((double) ux[o] + dx);
+      uy[o] = (U) ((double) uy[o] + dy);
+      uz[o] = (U) ((double) uz[o] + dz);
+   }
+}
+
+struct TwoStream {
+   int n[3];
+   double d[3], v[3];
+   float rho, qm;
+   int id0;
+};
+
+__global__ void k_two_stream (TwoStream s, Markers64 m, long long at, long long first, long long count)
+{
+   for (long long qq = blockIdx.x*(long long) blockDim.x + threadIdx.x ; qq < count ;
+        qq += (long long) gridDim.x*blockDim.x) {
+      const long long q = first + qq, node = q/2;
+      const int k = (int) (node % s.n[2]), j = (int) ((node/s.n[2]) % s.n[1]);
+      const int i = (int) (node/((long long) s.n[2]*s.n[1]));
+      const long long o = at + qq;
+      m.x[o] = (i + 0.5)*s.d[0];
+      m.y[o] = (j + 0.5)*s.d[1];
+      m.z[o] = (k + 0.5)*s.d[2];
+      m.ux[o] = (q & 1) ? - s.v[0] : s.v[0];
+      m.uy[o] = (q & 1) ? - s.v[1] : s.v[1];
+      m.uz[o] = (q & 1) ? - s.v[2] : s.v[2];
+      m.rho[o] = s.rho;
+      m.qm[o] = s.qm;
+      m.id[o] = s.id0 + (int) q;
+   }
+}
+
+int check_range (const mg_run_t *r, long long first, long long count, const char *fn)
+{
+   if (first < 0 || count < 0 || first + count > r->np) {
+      mg_set_error ("%s: markers [%lld, %lld) outside the %lld placed", fn, first, first + count, r->np);
+      return MG_ERR_ARG;
+   }
+   if (r->inited) {
+      mg_set_error ("%s: markers are reordered by mg_run_init; apply tags before it", fn);
+      return MG_ERR_STATE;
+   }
+   return MG_OK;
+}
+
+} // namespace
+
+extern "C" int mg_run_df_uniform (mg_run_t *r, long long first, long long count, const mg_df_uniform_t *s)
+{
+   if (!r || !s) {
+      mg_set_error ("mg_run_df_uniform: null argument");
+      return MG_ERR_ARG;
+   }
+   TRY_T (check_range (r, first, count, "mg_run_df_uniform"));
+   if (!(s->rho*s->qDivM > 0) || s->ppc <= 0 || !(s->lambda_cm > 0) || s->draws_before < 0) {
+      mg_set_error ("mg_run_df_uniform: sign of rho differs from sign of q/M, or bad ppc, wavelength or draws");
+      return MG_ERR_ARG;
+   }
+   if (count == 0)
+      return MG_OK;
+   MG_CUDA (cudaSetDevice (r->device));
+   const Units u = units_for (s->lambda_cm);
+   const double rho_crit = CGS_E*u.ncr/u.rho0;                     // tag_DF_uniform.c:38
+   double rho = s->rho;
+   rho *= rho_crit/s->ppc;                                           // :54
+   DfUniform d;
+   d.u[0] = s->ux; d.u[1] = s->uy; d.u[2] = s->uz;
+   d.du[0] = s->dux; d.du[1] = s->duy; d.du[2] = s->duz;
+   d.rho = (float) rho;
+   d.qm = (float) s->qDivM;
+   // Threads, each with a run of consecutive markers and its start window.
+   const long long per = (count + 148*128 - 1)/(148*128) > 64 ? (count + 148*128 - 1)/(148*128) : 64;
+   const int threads = (int) ((count + per - 1)/per);
+   std::vector<u32> win ((size_t) threads*LAG);
+   u32 w[LAG];
+   rand_window0 (w);
+   mat_vec (mat_pow (s->draws_before), w, w);
+   const Mat31 jump = mat_pow (3*per);
+   for (int t = 0 ; t < threads ; ++t) {
+      memcpy (&win[(size_t) t*LAG], w, sizeof (w));
+      if (t + 1 < threads)
+         mat_vec (jump, w, w);
+   }
+   u32 *dw = nullptr;
+   if (cudaMalloc (&dw, sizeof (u32)*win.size ()) != cudaSuccess) {
+      mg_set_error ("mg_run_df_uniform: device allocation failed");
+      return MG_ERR_OOM;
+   }
+   int rc = MG_OK;
+   if (cudaMemcpy (dw, win.data (), sizeof (u32)*win.size (), cudaMemcpyHostToDevice) != cudaSuccess)
+      rc = MG_ERR_CUDA;
+   if (rc == MG_OK) {
+      const int B = (threads + 127)/128;
+      if (r->prm.precision == MG_FP64)
+         k_df_uniform<double><<<B, 128, 0, r->stream>>> (r->m64.ux, r->m64.uy, r->m64.uz, r->m64.rho, r->m64.qm,
+                                                        first, count, per, threads, dw, d);
+      else
+         k_df_uniform<float><<<B, 128, 0, r->stream>>> (r->m32.ux, r->m32.uy, r->m32.uz, r->m32.rho, r->m32.qm,
+                                                       first, count, per, threads, dw, d);
+      if (cudaGetLastError () != cudaSuccess || cudaStreamSynchronize (r->stream) != cudaSuccess) {
+         mg_set_error ("mg_run_df_uniform: kernel failed");
+         rc = MG_ERR_CUDA;
+      }
+   }
+   cudaFree (dw);
+   return rc;
+}
+
+extern "C" int mg_run_shift_velocity (mg_run_t *r, long long first, long long count, const double dv[3])
+{
+   if (!r || !dv) {
+      mg_set_error ("mg_run_shift_velocity: null argument");
+      return MG_ERR_ARG;
+   }
+   TRY_T (check_range (r, first, count, "mg_run_shift_velocity"));
+   if (count == 0)
+      return MG_OK;
+   MG_CUDA (cudaSetDevice (r->device));
+   const int B = mg_blocks_for (count, 256, 8);
+   if (r->prm.precision == MG_FP64)
+      k_shift<double><<<B, 256, 0, r->stream>>> (r->m64.ux, r->m64.uy, r->m64.uz, first, count, dv[0], dv[1], dv[2]);
+   else
+      k_shift<float><<<B, 256, 0, r->stream>>> (r->m32.ux, r->m32.uy, r->m32.uz, first, count, dv[0], dv[1], dv[2]);
+   MG_LAUNCH_CHECK ();
+   MG_CUDA (cudaStreamSynchronize (r->stream));
+   return MG_OK;
+}
+
+extern "C" int mg_run_place_two_stream (mg_run_t *r, const mg_two_stream_t *s)
+{
+   if (!r || !s) {
+      mg_set_error ("mg_run_place_two_stream: null argument");
+      return MG_ERR_ARG;
+   }
+   if (s->n[0] <= 0 || s->n[1] <= 0 || s->n[2] <= 0 || !(s->gamma > 0) || !(fabs (s->qDivM) <= 1) ||
+       s->qDivM == 0 || (s->m[0] == 0 && s->m[1] == 0 && s->m[2] == 0) ||
+       !(s->L[0] > 0 && s->L[1] > 0 && s->L[2] > 0)) {
+      mg_set_error ("mg_run_place_two_stream: bad input parameters");
+      return MG_ERR_ARG;
+   }
+   MG_CUDA (cudaSetDevice (r->device));
+   // setup/tag_twoStream.c:23-103 in its order.
+   const int Nbeam = s->n[0]*s->n[1]*s->n[2];
+   double rho = s->gamma*s->gamma/s->qDivM;
+   const double kx = 2*PI*s->m[0]/s->L[0], ky = 2*PI*s->m[1]/s->L[1], kz = 2*PI*s->m[2]/s->L[2];
+   const double kAbs = sqrt (kx*kx + ky*ky + kz*kz);
+   const double V = s->gamma*sqrt (3.0)/(2*kAbs);
+   TwoStream t;
+   t.v[0] = V*kx/kAbs;
+   t.v[1] = V*ky/kAbs;
+   t.v[2] = V*kz/kAbs;
+   rho *= s->L[0]*s->L[1]*s->L[2]/(r->g.h[0]*r->g.h[1]*r->g.h[2]*Nbeam);
+   for (int a = 0 ; a < 3 ; ++a) {
+      t.n[a] = s->n[a];
+      t.d[a] = s->L[a]/(double) s->n[a];
+   }
+   t.rho = (float) rho;
+   t.qm = (float) s->qDivM;
+   t.id0 = s->id0;
+   const long long total = 2LL*Nbeam;
+   for (long long done = 0 ; done < total ; ) {
+      const long long c = (total - done < STAGE_MARKERS) ? total - done : STAGE_MARKERS;
+      Markers64 v;
+      long long at = 0;
+      TRY_T (target (r, c, v, at));
+      k_two_stream<<<mg_blocks_for (c, 256, 8), 256, 0, r->stream>>> (t, v, at, done, c);
+      TRY_T (commit (r, v, c));
+      done += c;
+   }
+   return MG_OK;
 }

@@ -332,15 +332,72 @@ def make_tfsf():
             p.cleanup()
 
 
+# Setup tags on the device (row f-4): [DF:two-stream] alone and followed by
+# [velocity shift] through setup.out, and [DF:uniform] through the harness
+# oracle/_ref/df_uniform.out (the reference tag on 1000 markers, with and
+# without earlier rand () draws).
+TS = dict(n=(8, 6, 10), L_um=(0.8, 0.6, 1.0), gamma=0.1, qDivM=-1.0, N=(4, 3, 5), m=(1, 2, 1),
+          dv=(0.01, -0.02, 0.003))
+DF_CASES = [dict(rho=-1.0, qDivM=-1.0, u=(0.01, 0.0, -0.02), du=(2.0, 1.0, 0.5), skip=0, lam=1.0),
+            dict(rho=2.5, qDivM=1.0 / 1836, u=(0.0, 0.3, 0.0), du=(0.1, 0.2, 0.3), skip=7, lam=0.8)]
+DF_MARKERS = 1000
+DF_PPC = 4                      # fixed in oracle/df_uniform_main.c
+
+
+def two_stream_deck(shift):
+    from refrun import deck_text
+    text = deck_text(TS["n"], TS["L_um"], -0.5, (0, 0, 0), (0, 0, 0))
+    text += ("\n[DF:two-stream]\n@ %.17g\tgamma\n@ %.17g\tq/M\n@ %d\tNx\n@ %d\tNy\n@ %d\tNz\n"
+             "@ %d\tmx\n@ %d\tmy\n@ %d\tmz\n" % ((TS["gamma"], TS["qDivM"]) + TS["N"] + TS["m"]))
+    if shift:
+        text += ("\n[velocity shift]\n@ %.17g\tdvx\n@ %.17g\tdvy\n@ %.17g\tdvz\n@ last\tcomponent\n"
+                 % TS["dv"])
+    return text
+
+
+def df_deck(c):
+    return "".join("@ %.17g\tvalue\n" % v for v in (c["rho"], c["qDivM"]) + c["u"] + c["du"])
+
+
+def make_setup_tags():
+    import subprocess, tempfile
+    out = {}
+    for shift in (0, 1):
+        rr = RefRun()
+        try:
+            with open(rr.path("deck.input"), "w") as fp:
+                fp.write(two_stream_deck(shift))
+            rr._run("setup.out", "deck.input", "create")
+            m = refrun.read_markers(rr.path("binData", "plasma_000000_000.bin"))
+            out["two_stream%d" % shift] = np.frombuffer(m.tobytes(), np.uint8)
+            out["domain"] = np.array(list(refrun.read_domain(rr.path("binData", "domain.bin"))["h"]) +
+                                     list(refrun.read_domain(rr.path("binData", "domain.bin"))["L"]))
+        finally:
+            rr.cleanup()
+    for q, c in enumerate(DF_CASES):
+        with tempfile.NamedTemporaryFile("w", suffix=".cfg", delete=False) as fp:
+            fp.write(df_deck(c))
+        res = subprocess.run([os.path.join(refrun.REF_DIR, "df_uniform.out"), repr(c["lam"]), str(DF_MARKERS),
+                              str(c["skip"]), fp.name], stdout=subprocess.PIPE, check=True)
+        os.remove(fp.name)
+        out["df%d" % q] = np.loadtxt(res.stdout.decode().splitlines()[-DF_MARKERS:])
+    np.savez_compressed(os.path.join(HERE, "setup_tags.npz"), **out)
+    print("setup tags: %s" % sorted(out))
+
+
 if __name__ == "__main__":
     if not have_reference():
         sys.exit("reference binaries missing: make -C oracle ref REF=<reference tree>")
-    for name in (sys.argv[1:] or list(cases.CASES) + ["gauss_spot", "placers", "tecplot", "probes", "tfsf"]):
+    for name in (sys.argv[1:] or list(cases.CASES) + ["gauss_spot", "placers", "tecplot", "probes", "tfsf",
+                                                 "setup_tags"]):
         if name == "probes":
             make_probes()
             continue
         if name == "tfsf":
             make_tfsf()
+            continue
+        if name == "setup_tags":
+            make_setup_tags()
             continue
         if name == "tecplot":
             make_tecplot()
