@@ -336,7 +336,7 @@ def make_tfsf():
 # [velocity shift] through setup.out, and [DF:uniform] through the harness
 # oracle/_ref/df_uniform.out (the reference tag on 1000 markers, with and
 # without earlier rand () draws).
-TS = dict(n=(8, 6, 10), L_um=(0.8, 0.6, 1.0), gamma=0.1, qDivM=-1.0, N=(4, 3, 5), m=(1, 2, 1),
+TS = dict(n=(8, 8, 10), L_um=(0.8, 0.8, 1.0), gamma=0.1, qDivM=-1.0, N=(4, 3, 5), m=(1, 2, 1),
           dv=(0.01, -0.02, 0.003))
 DF_CASES = [dict(rho=-1.0, qDivM=-1.0, u=(0.01, 0.0, -0.02), du=(2.0, 1.0, 0.5), skip=0, lam=1.0),
             dict(rho=2.5, qDivM=1.0 / 1836, u=(0.0, 0.3, 0.0), du=(0.1, 0.2, 0.3), skip=7, lam=0.8)]

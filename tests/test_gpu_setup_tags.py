@@ -67,13 +67,14 @@ def test_df_uniform_matches_the_reference_tag(precision):
 
 
 def test_df_uniform_at_scale_follows_the_c_library():
-    """300 000 markers after 12 345 earlier draws, threads starting from
-    jumped-ahead windows: every draw equals the C library's."""
+    """About 300 000 markers after 12 345 earlier draws, threads starting
+    from jumped-ahead windows: every draw equals the C library's."""
     c = dict(rho=-1.0, qDivM=-1.0, u=(0.0, 0.1, 0.2), du=(1.0, 2.0, 3.0))
-    n, skip = 300000, 12345
-    r, _ = run(mg.FP64, n)
-    r.place_uniform((0, 0, 0), make_golden.TS["n"], 625, 1.0, 1.0)
-    assert r.marker_count() == n
+    skip = 12345
+    r, _ = run(mg.FP64, 470 * 640)
+    r.place_uniform((0, 0, 0), make_golden.TS["n"], 470, 1.0, 1.0)
+    n = r.marker_count()
+    assert n == 470 * 640
     r.df_uniform(0, n, c["rho"], c["qDivM"], c["u"], c["du"], make_golden.DF_PPC, 1e-4, draws_before=skip)
     got = r.markers()
     u, rho = df_uniform(c, n, libc_rand(3 * n, skip))
