@@ -160,26 +160,6 @@ __device__ __forceinline__ int sort_key (const TileKey &t, int c, float qm)
    return (tile << t.lc) + cell;
 }
 
-// Counter slot of a key: eight neighbouring keys sit in eight different
-// regions of the counter array, so that nearly sorted markers do not queue
-// their atomics on one 32-byte L2 sector.  kp: keys per region.
-__device__ __forceinline__ long long spread (long long key, long long kp)
-{
-   return (key & 7)*kp + (key >> 3);
-}
-
-// Runs of equal keys in a warp (the markers arrive nearly sorted): the
-// lane's run start and, for the run's first lane, the run length.
-__device__ __forceinline__ void key_runs (int key, int lane, int &start, int &len)
-{
-   const int prev = __shfl_up_sync (0xffffffffu, key, 1);
-   const unsigned heads = __ballot_sync (0xffffffffu, lane == 0 || prev != key);
-   const unsigned le = (lane == 31) ? 0xffffffffu : ((2u << lane) - 1);
-   start = 31 - __clz (heads & le);
-   const unsigned after = heads & ~le;
-   len = (after ? __ffs (after) - 1 : 32) - lane;
-}
-
 // Marker count per key, and the largest |rho| (non-negative floats order
 // like their bit patterns).  One atomic per run of equal keys in a warp;
 // four warp-rows of markers per iteration keep more loads in flight.
@@ -224,7 +204,6 @@ __global__ void k_hist (TileKey t, Markers32 m, long long np, int *count, long l
 }
 
 // Three-pass exclusive scan of `count` (length len) in place.
-#define SCAN_CHUNK 4096
 __global__ void k_scan_blocks (const int *count, long long kp, long long len, long long *block_sum)
 {
    __shared__ long long s[256];
@@ -640,6 +619,19 @@ void mg_convert64to32 (mg_run_t *r, const Markers64 &v, long long c, long long a
 
 // Sorts the markers by tile and cell into the other buffer set and makes
 // that set current; removed markers go to the end.
+// Exclusive scan of the len counters (spread layout, kp keys per region)
+// into offset; bsum: (len + SCAN_CHUNK - 1)/SCAN_CHUNK scratch entries.
+int mg_scan_counts (mg_run_t *r, const int *count, long long kp, long long len, long long *offset,
+                    long long *bsum)
+{
+   const int nb = (int) ((len + SCAN_CHUNK - 1)/SCAN_CHUNK);
+   k_scan_blocks<<<nb, 256, 0, r->stream>>> (count, kp, len, bsum);
+   k_scan_sums<<<1, 1024, 0, r->stream>>> (bsum, nb);
+   k_scan_apply<<<nb, 256, 0, r->stream>>> (count, kp, len, bsum, offset);
+   MG_LAUNCH_CHECK ();
+   return MG_OK;
+}
+
 int mg_sort32 (mg_run_t *r)
 {
    if (r->np == 0) {

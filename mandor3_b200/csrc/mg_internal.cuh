@@ -220,6 +220,30 @@ int mg_fields64_e_fused (mg_run_t *r);
 int mg_push64 (mg_run_t *r);
 int mg_gauss_rho (mg_run_t *r, double *rho);
 int mg_probes_enqueue (mg_run_t *r);
+int mg_sort64 (mg_run_t *r);
+#define SCAN_CHUNK 4096
+int mg_scan_counts (mg_run_t *r, const int *count, long long kp, long long len, long long *offset,
+                    long long *bsum);
+
+// Counter slot of a sort key: eight neighbouring keys sit in eight different
+// regions of the counter array, so that nearly sorted markers do not queue
+// their atomics on one 32-byte L2 sector.  kp: keys per region.
+static __device__ __forceinline__ long long spread (long long key, long long kp)
+{
+   return (key & 7)*kp + (key >> 3);
+}
+
+// Runs of equal keys in a warp (markers arrive nearly sorted): the lane's
+// run start and, for the run's first lane, the run length.
+static __device__ __forceinline__ void key_runs (int key, int lane, int &start, int &len)
+{
+   const int prev = __shfl_up_sync (0xffffffffu, key, 1);
+   const unsigned heads = __ballot_sync (0xffffffffu, lane == 0 || prev != key);
+   const unsigned le = (lane == 31) ? 0xffffffffu : ((2u << lane) - 1);
+   start = 31 - __clz (heads & le);
+   const unsigned after = heads & ~le;
+   len = (after ? __ffs (after) - 1 : 32) - lane;
+}
 int mg_tfsf_h (mg_run_t *r);
 int mg_tfsf_e (mg_run_t *r);
 int mg_tfsf_record (mg_run_t *r);

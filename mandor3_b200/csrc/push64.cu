@@ -574,3 +574,165 @@ int mg_push64 (mg_run_t *r)
    return MG_OK;
 }
 
+
+// ---- cell sort of the FP64 markers -------------------------------------------
+// Every sort_every steps (default 16) the markers are put in cell order
+// (i, then j, then k), so that the markers of a warp share the 48 field
+// values of their gather in L1 and their current atomics aggregate.  A
+// counting sort: keys (the push's own cell index, removed markers last),
+// counts, scan, scatter into scratch arrays, copy back -- the step graph
+// keeps its marker pointers.  The push's arithmetic per marker is unchanged;
+// only the order of the current sums on J changes.
+namespace {
+
+struct Key64 {
+   int n[3];
+   double h[3], rh[3];
+   int cells;              // (n0+2)(n1+2)(n2+2): cells [-1, n]; then outside, removed
+};
+
+__device__ __forceinline__ int key64 (const Key64 &t, double x, double y, double z, float qm)
+{
+   if (qm == 0.0f)
+      return t.cells + 1;
+   double f;
+   const int i = cell_of (div_by (x, t.h[0], t.rh[0]), f);
+   const int j = cell_of (div_by (y, t.h[1], t.rh[1]), f);
+   const int k = cell_of (div_by (z, t.h[2], t.rh[2]), f);
+   if (i < -1 || i > t.n[0] || j < -1 || j > t.n[1] || k < -1 || k > t.n[2])
+      return t.cells;
+   return ((i + 1)*(t.n[1] + 2) + (j + 1))*(t.n[2] + 2) + (k + 1);
+}
+
+#define SORT64_ROWS 4
+__global__ void k_hist64 (Key64 t, Markers64 m, long long np, int *count, long long kp)
+{
+   const int lane = threadIdx.x & 31;
+   const long long stride = (long long) gridDim.x*blockDim.x*SORT64_ROWS;
+   for (long long base = (blockIdx.x*(long long) blockDim.x + (threadIdx.x & ~31))*SORT64_ROWS ; base < np ;
+        base += stride) {
+      double x[SORT64_ROWS], y[SORT64_ROWS], z[SORT64_ROWS];
+      float qm[SORT64_ROWS];
+#pragma unroll
+      for (int q = 0 ; q < SORT64_ROWS ; ++q) {
+         const long long n = min (base + 32*q + lane, np - 1);
+         x[q] = m.x[n];
+         y[q] = m.y[n];
+         z[q] = m.z[n];
+         qm[q] = m.qm[n];
+      }
+#pragma unroll
+      for (int q = 0 ; q < SORT64_ROWS ; ++q) {
+         const int key = base + 32*q + lane < np ? key64 (t, x[q], y[q], z[q], qm[q]) : -1;
+         int start, len;
+         key_runs (key, lane, start, len);
+         if (key >= 0 && start == lane)
+            atomicAdd (count + spread (key, kp), len);
+      }
+   }
+}
+
+__global__ void k_scatter64 (Key64 t, Markers64 m, Markers64 o, long long np, const long long *offset,
+                             int *fill, long long kp)
+{
+   const int lane = threadIdx.x & 31;
+   const long long stride = (long long) gridDim.x*blockDim.x*SORT64_ROWS;
+   for (long long base = (blockIdx.x*(long long) blockDim.x + (threadIdx.x & ~31))*SORT64_ROWS ; base < np ;
+        base += stride) {
+      double x[SORT64_ROWS], y[SORT64_ROWS], z[SORT64_ROWS], ux[SORT64_ROWS], uy[SORT64_ROWS], uz[SORT64_ROWS];
+      float rho[SORT64_ROWS], qm[SORT64_ROWS];
+      int id[SORT64_ROWS], key[SORT64_ROWS];
+      long long at[SORT64_ROWS];
+#pragma unroll
+      for (int q = 0 ; q < SORT64_ROWS ; ++q) {
+         const long long n = min (base + 32*q + lane, np - 1);
+         x[q] = m.x[n]; y[q] = m.y[n]; z[q] = m.z[n];
+         ux[q] = m.ux[n]; uy[q] = m.uy[n]; uz[q] = m.uz[n];
+         rho[q] = m.rho[n]; qm[q] = m.qm[n]; id[q] = m.id[n];
+      }
+#pragma unroll
+      for (int q = 0 ; q < SORT64_ROWS ; ++q) {
+         key[q] = base + 32*q + lane < np ? key64 (t, x[q], y[q], z[q], qm[q]) : -1;
+         int start, len;
+         key_runs (key[q], lane, start, len);
+         at[q] = 0;
+         if (key[q] >= 0 && start == lane)
+            at[q] = offset[key[q]] + atomicAdd (fill + spread (key[q], kp), len);
+         at[q] = __shfl_sync (0xffffffffu, at[q], start) + (lane - start);
+      }
+#pragma unroll
+      for (int q = 0 ; q < SORT64_ROWS ; ++q)
+         if (key[q] >= 0) {
+            const long long a = at[q];
+            o.x[a] = x[q]; o.y[a] = y[q]; o.z[a] = z[q];
+            o.ux[a] = ux[q]; o.uy[a] = uy[q]; o.uz[a] = uz[q];
+            o.rho[a] = rho[q]; o.qm[a] = qm[q]; o.id[a] = id[q];
+         }
+   }
+}
+
+} // namespace
+
+int mg_sort64 (mg_run_t *r)
+{
+   r->steps_since_sort = 0;
+   if (r->np == 0)
+      return MG_OK;
+   Key64 t;
+   for (int a = 0 ; a < 3 ; ++a) {
+      t.n[a] = r->g.n[a];
+      t.h[a] = r->g.h[a];
+      t.rh[a] = 1.0/r->g.h[a];
+   }
+   const long long cells = (long long) (t.n[0] + 2)*(t.n[1] + 2)*(t.n[2] + 2);
+   if (cells + 2 >= (1LL << 31)) {
+      mg_set_error ("mg_sort64: %lld cells exceed the sort's key range", cells);
+      return MG_ERR_ARG;
+   }
+   t.cells = (int) cells;
+   const long long len = cells + 2, kp = (len + 7)/8;
+   const long long nb = (len + SCAN_CHUNK - 1)/SCAN_CHUNK;
+   const size_t a_count = ((size_t) kp*8*4 + 255) & ~(size_t) 255;
+   const size_t a_off = ((size_t) len*8 + 255) & ~(size_t) 255;
+   const size_t a_bsum = ((size_t) nb*8 + 255) & ~(size_t) 255;
+   const size_t a_mark = (size_t) r->np*(6*8 + 3*4) + 9*256;
+   const size_t need = a_count + a_off + a_bsum + a_mark;
+   if (r->sort_tmp_bytes < need) {
+      if (r->sort_tmp) {
+         cudaFree (r->sort_tmp);
+         r->dev_bytes -= r->sort_tmp_bytes;
+         r->sort_tmp = nullptr;
+         r->sort_tmp_bytes = 0;
+      }
+      const int rc = mg_dev_alloc (r, &r->sort_tmp, need);
+      if (rc != MG_OK)
+         return rc;
+      r->sort_tmp_bytes = need;
+   }
+   char *p = (char *) r->sort_tmp;
+   int *count = (int *) p;                 p += a_count;
+   long long *offset = (long long *) p;    p += a_off;
+   long long *bsum = (long long *) p;      p += a_bsum;
+   Markers64 o;
+   auto take = [&] (size_t bytes) { char *q = p; p += (bytes + 255) & ~(size_t) 255; return q; };
+   o.x = (double *) take (r->np*8); o.y = (double *) take (r->np*8); o.z = (double *) take (r->np*8);
+   o.ux = (double *) take (r->np*8); o.uy = (double *) take (r->np*8); o.uz = (double *) take (r->np*8);
+   o.rho = (float *) take (r->np*4); o.qm = (float *) take (r->np*4); o.id = (int *) take (r->np*4);
+   const int T = 256;
+   MG_CUDA (cudaMemsetAsync (count, 0, (size_t) kp*8*4, r->stream));
+   k_hist64<<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (t, r->m64, r->np, count, kp);
+   MG_LAUNCH_CHECK ();
+   const int rc = mg_scan_counts (r, count, kp, len, offset, bsum);
+   if (rc != MG_OK)
+      return rc;
+   MG_CUDA (cudaMemsetAsync (count, 0, (size_t) kp*8*4, r->stream));
+   k_scatter64<<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (t, r->m64, o, r->np, offset, count, kp);
+   MG_LAUNCH_CHECK ();
+   const Markers64 &m = r->m64;
+   void *dst[9] = {m.x, m.y, m.z, m.ux, m.uy, m.uz, m.rho, m.qm, m.id};
+   const void *src[9] = {o.x, o.y, o.z, o.ux, o.uy, o.uz, o.rho, o.qm, o.id};
+   for (int q = 0 ; q < 9 ; ++q)
+      MG_CUDA (cudaMemcpyAsync (dst[q], src[q], (size_t) r->np*(q < 6 ? 8 : 4), cudaMemcpyDeviceToDevice,
+                                r->stream));
+   return MG_OK;
+}
