@@ -218,12 +218,16 @@ struct Wall {
    long s_a, s_p, s_q;     // strides along the three axes
 };
 
+// Transverse axes of a wall with the one of smallest stride as eq, the
+// fastest thread index (z for the x and y walls, y for the z walls), so
+// that a warp's nodes are contiguous in memory where they can be.  The
+// wall operations treat the two tangential components alike.
 static Wall make_wall (const Grid &g, int ea)
 {
    Wall w;
    w.ea = ea;
-   w.ep = (ea + 1) % 3;
-   w.eq = (ea + 2) % 3;
+   w.ep = ea == 0 ? 1 : 0;
+   w.eq = ea == 2 ? 1 : 2;
    w.np_ = g.n[w.ep] + 2;
    w.nq_ = g.n[w.eq] + 2;
    const long s[3] = {g.sx, g.sy, 1};
@@ -489,7 +493,7 @@ __global__ void k_e_walls (Grid g, F3T<T> E, F3T<T> J, Wall w, int op_min, int o
    if (w.ea == 2)
       own = true;
    else if (w.ea == 1)
-      own = !p_rim;                 // ep = z
+      own = !q_rim;                 // eq = z
    else
       own = !p_rim && !q_rim;       // ep = y, eq = z
    if (!own)
