@@ -215,63 +215,14 @@ int mg_ensure_stage (mg_run_t *r, size_t bytes)
    return MG_OK;
 }
 
-static void free_set64 (Markers64 &m)
+static void free_markers (mg_run_t *r)
 {
-   void *ptrs[] = {m.x, m.y, m.z, m.ux, m.uy, m.uz, m.rho, m.qm, m.id};
+   void *ptrs[] = {r->m64.x, r->m64.y, r->m64.z, r->m64.ux, r->m64.uy, r->m64.uz,
+                   r->m64.rho, r->m64.qm, r->m64.id};
    for (void *p : ptrs)
       if (p)
          cudaFree (p);
-   memset (&m, 0, sizeof (m));
-}
-
-static size_t marker_bytes64 (long long cap);
-
-// Frees both buffer sets of the plain form.
-static void free_markers (mg_run_t *r)
-{
-   free_set64 (r->m64);
-   if (r->m64b.x)
-      r->dev_bytes -= marker_bytes64 (r->cap);
-   free_set64 (r->m64b);
-}
-
-namespace {
-__global__ void k_publish64 (DevScalars *dsc, Markers64 m)
-{
-   dsc->m64 = m;
-}
-} // namespace
-
-// Makes the current plain-form set the one the step graph's push reads.
-int mg_publish_markers64 (mg_run_t *r)
-{
-   k_publish64<<<1, 1, 0, r->stream>>> (r->dsc, r->m64);
-   MG_LAUNCH_CHECK ();
-   return MG_OK;
-}
-
-// The sort's second set of `cap` markers, allocated at the first sort.
-int mg_alloc_markers64b (mg_run_t *r)
-{
-   if (r->m64b.x)
-      return MG_OK;
-   Markers64 nm;
-   memset (&nm, 0, sizeof (nm));
-   void **d[] = {(void **) &nm.x, (void **) &nm.y, (void **) &nm.z, (void **) &nm.ux,
-                 (void **) &nm.uy, (void **) &nm.uz};
-   int rc = MG_OK;
-   for (void **p : d)
-      if (rc == MG_OK)
-         rc = mg_dev_alloc (r, p, (size_t) r->cap*8);
-   if (rc == MG_OK) rc = mg_dev_alloc (r, (void **) &nm.rho, (size_t) r->cap*4);
-   if (rc == MG_OK) rc = mg_dev_alloc (r, (void **) &nm.qm, (size_t) r->cap*4);
-   if (rc == MG_OK) rc = mg_dev_alloc (r, (void **) &nm.id, (size_t) r->cap*4);
-   if (rc != MG_OK) {
-      free_set64 (nm);
-      return rc;
-   }
-   r->m64b = nm;
-   return MG_OK;
+   memset (&r->m64, 0, sizeof (r->m64));
 }
 
 static size_t marker_bytes64 (long long cap) { return (size_t) cap*(6*8 + 4 + 4 + 4); }
@@ -312,7 +263,7 @@ static int ensure_capacity (mg_run_t *r, long long need)
    r->cap = cap;
    // The captured graphs hold the old pointers.
    mg_drop_graphs (r);
-   return mg_publish_markers64 (r);
+   return MG_OK;
 }
 
 static int check_params (const mg_params_t *p)

@@ -80,13 +80,6 @@ struct GaussSpot {
    int    i;               // x-plane
 };
 
-// FP64 particle arrays (structure of arrays).
-struct Markers64 {
-   double *x, *y, *z, *ux, *uy, *uz;
-   float  *rho, *qm;
-   int    *id;
-};
-
 // Device-side per-run scalars (one small allocation).
 struct DevScalars {
    double time;            // t = n*tau of the step being advanced
@@ -101,10 +94,16 @@ struct DevScalars {
    float  rho_max;         // largest |rho| of the markers at the last sort
    Markers32 m32;          // the current marker buffer set (precision form),
                            // read by the kernels of the step graph
-   Markers64 m64;          // the same for the plain form
 };
 
 #define MG_RING 4096       // energy rows kept on the device between copies
+
+// FP64 particle arrays (structure of arrays).
+struct Markers64 {
+   double *x, *y, *z, *ux, *uy, *uz;
+   float  *rho, *qm;
+   int    *id;
+};
 
 
 struct mg_run {
@@ -147,8 +146,6 @@ struct mg_run {
    mg_laser_t  laser;
    int         has_gspot;
    GaussSpot   gspot;
-
-   Markers64   m64b;       // plain form: the sort's second buffer set (lazy)
 
    // TF/SF interface (tfsf.cu), null when off
    struct mg_tfsf_state *tfsf;
@@ -224,7 +221,6 @@ int mg_push64 (mg_run_t *r);
 int mg_gauss_rho (mg_run_t *r, double *rho);
 int mg_probes_enqueue (mg_run_t *r);
 int mg_sort64 (mg_run_t *r);
-int mg_publish_markers64 (mg_run_t *r);
 #define SCAN_CHUNK 4096
 int mg_scan_counts (mg_run_t *r, const int *count, long long kp, long long len, long long *offset,
                     long long *bsum);

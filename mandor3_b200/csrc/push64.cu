@@ -297,9 +297,8 @@ __device__ __forceinline__ bool wall (int bc, bool top, double &x, double &v, do
 
 template <int MINB>
 __global__ void __launch_bounds__ (256, MINB)
-k_push64 (Ctx c, long long np, DevScalars *dsc)
+k_push64 (Ctx c, Markers64 m, long long np, DevScalars *dsc)
 {
-   const Markers64 m = dsc->m64;
    const Grid &g = c.g;
    const double h1 = g.h[0], h2 = g.h[1], h3 = g.h[2], tau = g.tau;
    const double L0 = g.n[0]*h1, L1 = g.n[1]*h2, L2 = g.n[2]*h3;
@@ -570,7 +569,7 @@ int mg_push64 (mg_run_t *r)
    // Three blocks of 256 per SM (80 registers, a few spilled): the extra
    // warps hide the gather latency better than a spill-free 128-register
    // build with two blocks (measured about 10% faster on the laser-foil run).
-   k_push64<3><<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (c, r->np, r->dsc);
+   k_push64<3><<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (c, r->m64, r->np, r->dsc);
    MG_LAUNCH_CHECK ();
    return MG_OK;
 }
@@ -581,10 +580,9 @@ int mg_push64 (mg_run_t *r)
 // (i, then j, then k), so that the markers of a warp share the 48 field
 // values of their gather in L1 and their current atomics aggregate.  A
 // counting sort: keys (the push's own cell index, removed markers last),
-// counts, scan, scatter into the second buffer set, which becomes the
-// current one (the step graph's push reads the set from the device
-// scalars).  The push's arithmetic per marker is unchanged; only the order
-// of the current sums on J changes.
+// counts, scan, scatter into scratch arrays, copy back -- the step graph
+// keeps its marker pointers.  The push's arithmetic per marker is unchanged;
+// only the order of the current sums on J changes.
 namespace {
 
 struct Key64 {
@@ -675,8 +673,6 @@ __global__ void k_scatter64 (Key64 t, Markers64 m, Markers64 o, long long np, co
 
 } // namespace
 
-int mg_alloc_markers64b (mg_run_t *r);
-
 int mg_sort64 (mg_run_t *r)
 {
    r->steps_since_sort = 0;
@@ -699,12 +695,8 @@ int mg_sort64 (mg_run_t *r)
    const size_t a_count = ((size_t) kp*8*4 + 255) & ~(size_t) 255;
    const size_t a_off = ((size_t) len*8 + 255) & ~(size_t) 255;
    const size_t a_bsum = ((size_t) nb*8 + 255) & ~(size_t) 255;
-   const size_t need = a_count + a_off + a_bsum;
-   {
-      const int rc = mg_alloc_markers64b (r);
-      if (rc != MG_OK)
-         return rc;
-   }
+   const size_t a_mark = (size_t) r->np*(6*8 + 3*4) + 9*256;
+   const size_t need = a_count + a_off + a_bsum + a_mark;
    if (r->sort_tmp_bytes < need) {
       if (r->sort_tmp) {
          cudaFree (r->sort_tmp);
@@ -720,8 +712,12 @@ int mg_sort64 (mg_run_t *r)
    char *p = (char *) r->sort_tmp;
    int *count = (int *) p;                 p += a_count;
    long long *offset = (long long *) p;    p += a_off;
-   long long *bsum = (long long *) p;
-   const Markers64 o = r->m64b;
+   long long *bsum = (long long *) p;      p += a_bsum;
+   Markers64 o;
+   auto take = [&] (size_t bytes) { char *q = p; p += (bytes + 255) & ~(size_t) 255; return q; };
+   o.x = (double *) take (r->np*8); o.y = (double *) take (r->np*8); o.z = (double *) take (r->np*8);
+   o.ux = (double *) take (r->np*8); o.uy = (double *) take (r->np*8); o.uz = (double *) take (r->np*8);
+   o.rho = (float *) take (r->np*4); o.qm = (float *) take (r->np*4); o.id = (int *) take (r->np*4);
    const int T = 256;
    MG_CUDA (cudaMemsetAsync (count, 0, (size_t) kp*8*4, r->stream));
    k_hist64<<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (t, r->m64, r->np, count, kp);
@@ -732,7 +728,11 @@ int mg_sort64 (mg_run_t *r)
    MG_CUDA (cudaMemsetAsync (count, 0, (size_t) kp*8*4, r->stream));
    k_scatter64<<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (t, r->m64, o, r->np, offset, count, kp);
    MG_LAUNCH_CHECK ();
-   r->m64b = r->m64;
-   r->m64 = o;
-   return mg_publish_markers64 (r);
+   const Markers64 &m = r->m64;
+   void *dst[9] = {m.x, m.y, m.z, m.ux, m.uy, m.uz, m.rho, m.qm, m.id};
+   const void *src[9] = {o.x, o.y, o.z, o.ux, o.uy, o.uz, o.rho, o.qm, o.id};
+   for (int q = 0 ; q < 9 ; ++q)
+      MG_CUDA (cudaMemcpyAsync (dst[q], src[q], (size_t) r->np*(q < 6 ? 8 : 4), cudaMemcpyDeviceToDevice,
+                                r->stream));
+   return MG_OK;
 }
