@@ -730,7 +730,7 @@ extern "C" int mg_run_init (mg_run_t *r)
       if (r->prm.sort_every >= 0)
          TRY (mg_sort32 (r));
    } else if (r->prm.sort_every >= 0) {
-      TRY (mg_sort64 (r));        // block order for the gather's locality
+      TRY (mg_sort64 (r));        // cell order for the gather's locality
    }
    MG_CUDA (cudaStreamSynchronize (r->stream));
    r->inited = 1;
@@ -1009,13 +1009,13 @@ static int build_graph (mg_run_t *r)
 // Precision form: markers are re-sorted by tile and cell every sort_every
 // steps (default 8) so that tiles stay compact and warps keep sharing cells;
 // the sort runs between graph launches on the run's stream.
-// The plain form is put in cell-block order every sort_every steps (default
-// 8) for the gather's locality (mg_sort64).
+// The plain form is put in cell order every sort_every steps (default 16)
+// for the gather's locality (mg_sort64).
 static int maybe_sort (mg_run_t *r)
 {
    if (r->prm.sort_every < 0)
       return MG_OK;
-   const int every = r->prm.sort_every > 0 ? r->prm.sort_every : 8;
+   const int every = r->prm.sort_every > 0 ? r->prm.sort_every : (is32 (r) ? 8 : 16);
    if (r->steps_since_sort++ < every)
       return MG_OK;
    return is32 (r) ? mg_sort32 (r) : mg_sort64 (r);

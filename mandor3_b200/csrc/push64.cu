@@ -576,22 +576,19 @@ int mg_push64 (mg_run_t *r)
 
 
 // ---- cell sort of the FP64 markers -------------------------------------------
-// Every sort_every steps (default 8) the markers are put in order of 2^3-cell
-// blocks, so that the markers of a warp share the field values of their
-// gather in L1 and their current atomics aggregate.  A
+// Every sort_every steps (default 16) the markers are put in cell order
+// (i, then j, then k), so that the markers of a warp share the 48 field
+// values of their gather in L1 and their current atomics aggregate.  A
 // counting sort: keys (the push's own cell index, removed markers last),
 // counts, scan, scatter into scratch arrays, copy back -- the step graph
 // keeps its marker pointers.  The push's arithmetic per marker is unchanged;
 // only the order of the current sums on J changes.
 namespace {
 
-// Keys: blocks of 2 x 2 x 2 cells over cells [-1, n] (a warp's markers then
-// gather from one 3 x 3 x 3 node neighbourhood), x-major; then the markers
-// outside, then the removed ones.
 struct Key64 {
-   int n[3], b[3];         // cells and blocks per axis
+   int n[3];
    double h[3], rh[3];
-   int cells;              // blocks in all
+   int cells;              // (n0+2)(n1+2)(n2+2): cells [-1, n]; then outside, removed
 };
 
 __device__ __forceinline__ int key64 (const Key64 &t, double x, double y, double z, float qm)
@@ -604,7 +601,7 @@ __device__ __forceinline__ int key64 (const Key64 &t, double x, double y, double
    const int k = cell_of (div_by (z, t.h[2], t.rh[2]), f);
    if (i < -1 || i > t.n[0] || j < -1 || j > t.n[1] || k < -1 || k > t.n[2])
       return t.cells;
-   return (((i + 1) >> 1)*t.b[1] + ((j + 1) >> 1))*t.b[2] + ((k + 1) >> 1);
+   return ((i + 1)*(t.n[1] + 2) + (j + 1))*(t.n[2] + 2) + (k + 1);
 }
 
 #define SORT64_ROWS 4
@@ -684,11 +681,10 @@ int mg_sort64 (mg_run_t *r)
    Key64 t;
    for (int a = 0 ; a < 3 ; ++a) {
       t.n[a] = r->g.n[a];
-      t.b[a] = (r->g.n[a] + 3)/2;
       t.h[a] = r->g.h[a];
       t.rh[a] = 1.0/r->g.h[a];
    }
-   const long long cells = (long long) t.b[0]*t.b[1]*t.b[2];
+   const long long cells = (long long) (t.n[0] + 2)*(t.n[1] + 2)*(t.n[2] + 2);
    if (cells + 2 >= (1LL << 31)) {
       mg_set_error ("mg_sort64: %lld cells exceed the sort's key range", cells);
       return MG_ERR_ARG;
