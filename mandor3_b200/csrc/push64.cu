@@ -265,6 +265,19 @@ __device__ __forceinline__ double warp_sum (double v)
    return v;
 }
 
+// Segmented inclusive sum over lanes: lanes [seg_start, lane] of the run of
+// equal keys that contains this lane.
+__device__ __forceinline__ double seg_scan (double v, int lane, int seg_start)
+{
+#pragma unroll
+   for (int d = 1 ; d < 32 ; d <<= 1) {
+      const double t = __shfl_up_sync (0xffffffffu, v, d);
+      if (lane - d >= seg_start)
+         v += t;
+   }
+   return v;
+}
+
 // One wall of core/plasma_walls.c:27-104; returns true if the marker goes.
 // Once removed, later walls leave it alone (it is dropped by the caller).
 __device__ __forceinline__ bool wall (int bc, bool top, double &x, double &v, double L, double h)
@@ -282,23 +295,10 @@ __device__ __forceinline__ bool wall (int bc, bool top, double &x, double &v, do
    return (!top && x <= h) || (top && x >= L - h);
 }
 
-// Address of weight q (0..11) of the cell at offset o, in scatter12's order.
-__device__ __forceinline__ double *slot12 (const Ctx &c, long long o, int q)
-{
-   const long sx = c.g.sx, sy = c.g.sy;
-   const int a = q & 1, b = (q >> 1) & 1;
-   switch (q >> 2) {
-   case 0:  return c.J0 + o + sx + a*sy + b;
-   case 1:  return c.J1 + o + sy + a*sx + b;
-   default: return c.J2 + o + 1 + a*sx + b*sy;
-   }
-}
-
 template <int MINB>
 __global__ void __launch_bounds__ (256, MINB)
 k_push64 (Ctx c, Markers64 m, long long np, DevScalars *dsc)
 {
-   __shared__ double s_w[8][12*32];           // per warp: weight-major, lane-minor
    const Grid &g = c.g;
    const double h1 = g.h[0], h2 = g.h[1], h3 = g.h[2], tau = g.tau;
    const double L0 = g.n[0]*h1, L1 = g.n[1]*h2, L2 = g.n[2]*h3;
@@ -442,44 +442,25 @@ k_push64 (Ctx c, Markers64 m, long long np, DevScalars *dsc)
       else if (valid && nseg >= 2)
          multicell_rest (c, i, j, k, i2, j2, k2, x1, y1, z1, x2, y2, z2, rho);
 
-      // First segment: summed per start cell across the warp.  Markers come
-      // in cell order, so a warp holds a few runs of equal cells: every lane
-      // puts its 12 weights in the warp's shared-memory table, then for each
-      // run lane q < 12 adds up weight q over the run's lanes and issues the
-      // one atomic of that weight.
+      // First segment: warp-aggregated by start cell.
       double wgt[12];
       if (valid)
          segment_weights (c, fi, fj, fk, x1, xa, y1, ya, z1, za, rho, wgt);
       else
          for (int q = 0 ; q < 12 ; ++q) wgt[q] = 0;
-      const long long key = valid ? g.at (i, j, k) : -1;
+      const long long key = valid ? g.at (i, j, k) : -1 - lane;
       const long long prev = __shfl_up_sync (0xffffffffu, key, 1);
-      const unsigned heads = __ballot_sync (0xffffffffu, lane == 0 || prev != key);
-      double *tab = s_w[threadIdx.x >> 5];
+      const long long next = __shfl_down_sync (0xffffffffu, key, 1);
+      const bool head = (lane == 0) || (prev != key);
+      const bool tail = (lane == 31) || (next != key);
+      const unsigned heads = __ballot_sync (0xffffffffu, head);
+      const unsigned le = (lane == 31) ? 0xffffffffu : ((1u << (lane + 1)) - 1);
+      const int seg_start = 31 - __clz (heads & le);
 #pragma unroll
       for (int q = 0 ; q < 12 ; ++q)
-         tab[q*32 + lane] = wgt[q];
-      __syncwarp ();
-      unsigned left = heads;
-      while (left) {
-         const int s0 = __ffs (left) - 1;
-         left &= left - 1;
-         const int s1 = left ? __ffs (left) - 1 : 32;
-         const long long o = __shfl_sync (0xffffffffu, key, s0);
-         if (o >= 0 && lane < 12) {
-            const double *col = tab + lane*32;
-            double a = col[s0], b = 0.0;
-            int l = s0 + 1;
-            for ( ; l + 1 < s1 ; l += 2) {
-               a += col[l];
-               b += col[l + 1];
-            }
-            if (l < s1)
-               a += col[l];
-            atomicAdd (slot12 (c, o, lane), a + b);
-         }
-      }
-      __syncwarp ();
+         wgt[q] = seg_scan (wgt[q], lane, seg_start);
+      if (valid && tail)
+         scatter12 (c, i, j, k, wgt);
    }
 
    // Thermal energy tally: block reduction, one atomic per block.
