@@ -167,7 +167,6 @@ __global__ void k_live_scan (const float *qm, long long from, long long n, long 
 // accumulators cleared, time advanced (parameter_setTime, core/main.c:435).
 __global__ void k_end_step (DevScalars *dsc, double *ring, double volume, double tau)
 {
-   mg_pdl ();
    const int s = dsc->step % MG_RING;
    double *row = ring + 6*s;
    row[0] = dsc->time;
@@ -846,7 +845,7 @@ extern "C" int mg_em_EStep_finish (mg_run_t *r)
    TRY (expect_stage (r, 6, __func__));
    TRY (is32 (r) ? mg_fields32_e_finish (r) : mg_fields64_e_finish (r));
    // Time advances at the end of the step (core/main.c:435).
-   MG_CUDA (mg_launch (k_end_step, 1, 1, 0, r->stream, r->dsc, r->ring, r->g.h[0]*r->g.h[1]*r->g.h[2], r->g.tau));
+   k_end_step<<<1, 1, 0, r->stream>>> (r->dsc, r->ring, r->g.h[0]*r->g.h[1]*r->g.h[2], r->g.tau);
    MG_LAUNCH_CHECK ();
    MG_CUDA (cudaStreamSynchronize (r->stream));
    r->time += r->g.tau;
@@ -935,7 +934,7 @@ int mg_enqueue_step64 (mg_run_t *r, int part)
    if (part < 0 || part == 2) {
       TRY (mg_fields64_jbc (r));
       TRY (mg_fields64_e_fused (r));
-      MG_CUDA (mg_launch (k_end_step, 1, 1, 0, r->stream, r->dsc, r->ring, r->g.h[0]*r->g.h[1]*r->g.h[2], r->g.tau));
+      k_end_step<<<1, 1, 0, r->stream>>> (r->dsc, r->ring, r->g.h[0]*r->g.h[1]*r->g.h[2], r->g.tau);
       MG_LAUNCH_CHECK ();
    }
    return MG_OK;
@@ -945,7 +944,7 @@ int mg_enqueue_step32 (mg_run_t *r, int part);
 
 int mg_end_step (mg_run_t *r)
 {
-   MG_CUDA (mg_launch (k_end_step, 1, 1, 0, r->stream, r->dsc, r->ring, r->g.h[0]*r->g.h[1]*r->g.h[2], r->g.tau));
+   k_end_step<<<1, 1, 0, r->stream>>> (r->dsc, r->ring, r->g.h[0]*r->g.h[1]*r->g.h[2], r->g.tau);
    MG_LAUNCH_CHECK ();
    return MG_OK;
 }

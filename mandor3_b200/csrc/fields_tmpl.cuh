@@ -89,7 +89,6 @@ __global__ void __launch_bounds__ (256)
 k_h_fused (Grid g, F3T<T> E, F3T<T> H, F3T<T> Hn, Box b, T c1, T c2, T c3,
            EnergyPick ep, DevScalars *dsc)
 {
-   mg_pdl ();
    __shared__ double sw[2][8];
    const T *Ex = E.c[0], *Ey = E.c[1], *Ez = E.c[2];
    const long sx = g.sx, sy = g.sy;
@@ -151,7 +150,6 @@ k_h_fused (Grid g, F3T<T> E, F3T<T> H, F3T<T> Hn, Box b, T c1, T c2, T c3,
 template <typename T>
 __global__ void k_e_advance (Grid g, F3T<T> E, F3T<T> H, Box b, T c1, T c2, T c3)
 {
-   mg_pdl ();
    T *Ex = E.c[0], *Ey = E.c[1], *Ez = E.c[2];
    const T *Hx = H.c[0], *Hy = H.c[1], *Hz = H.c[2];
    const long sx = g.sx, sy = g.sy;
@@ -188,7 +186,6 @@ template <typename T>
 __global__ void __launch_bounds__ (256)
 k_e_fused (Grid g, F3T<T> E, F3T<T> H, F3T<T> J, Box b, T c1, T c2, T c3, Rim rm)
 {
-   mg_pdl ();
    T *Ex = E.c[0], *Ey = E.c[1], *Ez = E.c[2];
    const T *Hx = H.c[0], *Hy = H.c[1], *Hz = H.c[2];
    const long sx = g.sx, sy = g.sy;
@@ -378,7 +375,6 @@ __global__ void k_mur_init (Grid g, F3T<T> E, Wall w, int top, T *mur)
 template <typename T>
 __global__ void k_h_walls (Grid g, F3T<T> H, F3T<T> Hn, Wall w, int op_min, int op_max, int both)
 {
-   mg_pdl ();
    long o;
    int p, q;
    if (!wall_node (g, w, 0, o, p, q))
@@ -478,7 +474,6 @@ template <typename T>
 __global__ void k_e_walls (Grid g, F3T<T> E, F3T<T> J, Wall w, int op_min, int op_max, T *mur_min,
                            T *mur_max, T alpha, int sub_j)
 {
-   mg_pdl ();
    const long t = blockIdx.x*(long) blockDim.x + threadIdx.x;
    const int np1 = w.np_ + 1, nq1 = w.nq_ + 1;          // [-1, n+1]
    if (t >= (long) np1*nq1)
@@ -600,7 +595,6 @@ __device__ __forceinline__ void j_fold (const Grid &g, F3T<T> &J, int ea, int to
 template <typename T>
 __global__ void k_j_walls (Grid g, F3T<T> J, int ea)
 {
-   mg_pdl ();
    const int ep = (ea == 0) ? 1 : 0, eq = (ea == 2) ? 1 : 2;
    const int np_ = g.n[ep] + 5, nq_ = g.n[eq] + 5;
    const long t = blockIdx.x*(long) blockDim.x + threadIdx.x;
@@ -619,7 +613,6 @@ __global__ void k_j_walls (Grid g, F3T<T> J, int ea)
 template <typename T>
 __global__ void k_e_sub_j (Grid g, F3T<T> E, F3T<T> J, Box b)
 {
-   mg_pdl ();
    const T tau = (T) g.tau;
    for (long t = blockIdx.x*(long) blockDim.x + threadIdx.x ; t < b.vol ; t += (long) gridDim.x*blockDim.x) {
       int i, j, k;
@@ -658,7 +651,6 @@ template <typename T>
 __global__ void k_laser (Grid g, T *F, mg_laser_t l, const DevScalars *dsc,
                          int is_e, F3T<T> E, F3T<T> J, int sub_j)
 {
-   mg_pdl ();
    const int nj = g.n[1] - 2*l.margin + 1, nk = g.n[2] - 2*l.margin + 1;
    const long t = blockIdx.x*(long) blockDim.x + threadIdx.x;
    if (nj <= 0 || nk <= 0 || t >= (long) nj*nk)
@@ -685,7 +677,6 @@ __global__ void k_laser (Grid g, T *F, mg_laser_t l, const DevScalars *dsc,
 template <typename T>
 __global__ void k_gauss_spot (Grid g, T *Ey, T *Ez, GaussSpot s, const DevScalars *dsc)
 {
-   mg_pdl ();
    const int nj = g.n[1] + 3, nk = g.n[2] + 3;
    const long q = blockIdx.x*(long) blockDim.x + threadIdx.x;
    if (q >= (long) nj*nk)
@@ -747,7 +738,7 @@ static int launch_h_walls (mg_run_t *r, const FS<T> &fs, int both)
       const int NT = 256, B = (int) ((nodes + NT - 1)/NT);
       int op0, op1;
       wall_ops (g, ea, op0, op1);
-      MG_CUDA (mg_launch (k_h_walls<T>, B, NT, 0, r->stream, g, f3 (fs.H), f3 (fs.Hn), w, op0, op1, both));
+      k_h_walls<<<B, NT, 0, r->stream>>> (g, f3 (fs.H), f3 (fs.Hn), w, op0, op1, both);
       MG_LAUNCH_CHECK ();
    }
    return MG_OK;
@@ -763,7 +754,7 @@ static int launch_hn_walls (mg_run_t *r, const FS<T> &fs)
       const int NT = 256, B = (int) ((nodes + NT - 1)/NT);
       int op0, op1;
       wall_ops (g, ea, op0, op1);
-      MG_CUDA (mg_launch (k_h_walls<T>, B, NT, 0, r->stream, g, f3 (fs.Hn), f3 (fs.Hn), w, op0, op1, 0));
+      k_h_walls<<<B, NT, 0, r->stream>>> (g, f3 (fs.Hn), f3 (fs.Hn), w, op0, op1, 0);
       MG_LAUNCH_CHECK ();
    }
    return MG_OK;
@@ -781,8 +772,8 @@ static int launch_e_walls (mg_run_t *r, const FS<T> &fs, int sub_j)
       const T alpha = (T) ((g.tau - g.h[ea])/(g.tau + g.h[ea]));
       int op0, op1;
       wall_ops (g, ea, op0, op1);
-      MG_CUDA (mg_launch (k_e_walls<T>, B, NT, 0, r->stream, g, f3 (fs.E), f3 (fs.J), w, op0, op1, fs.mur[0][ea],
-                                         fs.mur[1][ea], alpha, sub_j));
+      k_e_walls<<<B, NT, 0, r->stream>>> (g, f3 (fs.E), f3 (fs.J), w, op0, op1, fs.mur[0][ea],
+                                         fs.mur[1][ea], alpha, sub_j);
       MG_LAUNCH_CHECK ();
    }
    return MG_OK;
@@ -798,8 +789,8 @@ static int launch_laser (mg_run_t *r, const FS<T> &fs, int is_e, int sub_j = 0)
    if (nj <= 0 || nk <= 0)
       return MG_OK;
    const int NT = 256, B = (int) ((nj*nk + NT - 1)/NT);
-   MG_CUDA (mg_launch (k_laser<T>, B, NT, 0, r->stream, r->g, is_e ? fs.E[1] : fs.H[2], l, r->dsc, is_e,
-                                    f3 (fs.E), f3 (fs.J), sub_j));
+   k_laser<<<B, NT, 0, r->stream>>> (r->g, is_e ? fs.E[1] : fs.H[2], l, r->dsc, is_e,
+                                    f3 (fs.E), f3 (fs.J), sub_j);
    MG_LAUNCH_CHECK ();
    return MG_OK;
 }
@@ -874,8 +865,9 @@ int fields_h_half (mg_run_t *r, const FS<T> &fs)
    Box b = h_box (g);
    const int NT = 256;
    MG_CUDA (cudaMemsetAsync (r->dsc->acc, 0, 2*sizeof (double), r->stream));
-   MG_CUDA (mg_launch (k_h_fused<T>, mg_blocks_for (b.vol, NT, 8), NT, 0, r->stream, g, f3 (fs.E), f3 (fs.H), f3 (fs.Hn), b, (T) (0.5*g.tau/g.h[0]), (T) (0.5*g.tau/g.h[1]), (T) (0.5*g.tau/g.h[2]),
-      energy_pick (g), r->dsc));
+   k_h_fused<<<mg_blocks_for (b.vol, NT, 8), NT, 0, r->stream>>> (
+      g, f3 (fs.E), f3 (fs.H), f3 (fs.Hn), b, (T) (0.5*g.tau/g.h[0]), (T) (0.5*g.tau/g.h[1]), (T) (0.5*g.tau/g.h[2]),
+      energy_pick (g), r->dsc);
    MG_LAUNCH_CHECK ();
    return launch_hn_walls<T> (r, fs);
 }
@@ -900,7 +892,7 @@ int fields_h_step (mg_run_t *r, const FS<T> &fs)
       const int NT = 256, B = (int) ((nodes + NT - 1)/NT);
       int op0, op1;
       wall_ops (g, ea, op0, op1);
-      MG_CUDA (mg_launch (k_h_walls<T>, B, NT, 0, r->stream, g, f3 (fs.H), f3 (fs.H), w, op0, op1, 0));
+      k_h_walls<<<B, NT, 0, r->stream>>> (g, f3 (fs.H), f3 (fs.H), w, op0, op1, 0);
       MG_LAUNCH_CHECK ();
    }
    return MG_OK;
@@ -914,8 +906,9 @@ int fields_h_both (mg_run_t *r, const FS<T> &fs)
    Box b = h_box (g);
    const int NT = 256;
    MG_CUDA (cudaMemsetAsync (r->dsc->acc, 0, 2*sizeof (double), r->stream));
-   MG_CUDA (mg_launch (k_h_fused<T>, mg_blocks_for (b.vol, NT, 8), NT, 0, r->stream, g, f3 (fs.E), f3 (fs.H), f3 (fs.Hn), b, (T) (0.5*g.tau/g.h[0]), (T) (0.5*g.tau/g.h[1]), (T) (0.5*g.tau/g.h[2]),
-      energy_pick (g), r->dsc));
+   k_h_fused<<<mg_blocks_for (b.vol, NT, 8), NT, 0, r->stream>>> (
+      g, f3 (fs.E), f3 (fs.H), f3 (fs.Hn), b, (T) (0.5*g.tau/g.h[0]), (T) (0.5*g.tau/g.h[1]), (T) (0.5*g.tau/g.h[2]),
+      energy_pick (g), r->dsc);
    MG_LAUNCH_CHECK ();
    TRY_MG (mg_tfsf_h (r));
    TRY_MG (launch_laser<T> (r, fs, 0));
@@ -929,7 +922,8 @@ int fields_e_step (mg_run_t *r, const FS<T> &fs)
    const Grid &g = r->g;
    Box b = e_box (g);
    const int NT = 256;
-   MG_CUDA (mg_launch (k_e_advance<T>, mg_blocks_for (b.vol, NT, 16), NT, 0, r->stream, g, f3 (fs.E), f3 (fs.H), b, (T) (g.tau/g.h[0]), (T) (g.tau/g.h[1]), (T) (g.tau/g.h[2])));
+   k_e_advance<<<mg_blocks_for (b.vol, NT, 16), NT, 0, r->stream>>> (
+      g, f3 (fs.E), f3 (fs.H), b, (T) (g.tau/g.h[0]), (T) (g.tau/g.h[1]), (T) (g.tau/g.h[2]));
    MG_LAUNCH_CHECK ();
    return launch_e_walls<T> (r, fs, 0);
 }
@@ -942,7 +936,7 @@ int fields_jbc (mg_run_t *r, const FS<T> &fs)
       const int ep = (ea == 0) ? 1 : 0, eq = (ea == 2) ? 1 : 2;
       const long nodes = (long) (g.n[ep] + 5)*(g.n[eq] + 5);
       const int NT = 256, B = (int) ((nodes + NT - 1)/NT);
-      MG_CUDA (mg_launch (k_j_walls<T>, B, NT, 0, r->stream, g, f3 (fs.J), ea));
+      k_j_walls<<<B, NT, 0, r->stream>>> (g, f3 (fs.J), ea);
       MG_LAUNCH_CHECK ();
    }
    return MG_OK;
@@ -955,7 +949,7 @@ static int launch_gauss_spot (mg_run_t *r, const FS<T> &fs)
       return MG_OK;
    const long nodes = (long) (r->g.n[1] + 3)*(r->g.n[2] + 3);
    const int NT = 256, B = (int) ((nodes + NT - 1)/NT);
-   MG_CUDA (mg_launch (k_gauss_spot<T>, B, NT, 0, r->stream, r->g, fs.E[1], fs.E[2], r->gspot, r->dsc));
+   k_gauss_spot<<<B, NT, 0, r->stream>>> (r->g, fs.E[1], fs.E[2], r->gspot, r->dsc);
    MG_LAUNCH_CHECK ();
    return MG_OK;
 }
@@ -971,7 +965,7 @@ int fields_e_finish (mg_run_t *r, const FS<T> &fs)
    const int hi[3] = {r->g.n[0] + 1, r->g.n[1] + 1, r->g.n[2] + 1};
    Box b = make_box (lo, hi);
    const int NT = 256;
-   MG_CUDA (mg_launch (k_e_sub_j<T>, mg_blocks_for (b.vol, NT, 16), NT, 0, r->stream, r->g, f3 (fs.E), f3 (fs.J), b));
+   k_e_sub_j<<<mg_blocks_for (b.vol, NT, 16), NT, 0, r->stream>>> (r->g, f3 (fs.E), f3 (fs.J), b);
    MG_LAUNCH_CHECK ();
    return launch_gauss_spot<T> (r, fs);
 }
@@ -992,7 +986,8 @@ int fields_e_fused (mg_run_t *r, const FS<T> &fs)
    Box b = e_box (g);
    Rim rm = rim (r);
    const int NT = 256;
-   MG_CUDA (mg_launch (k_e_fused<T>, mg_blocks_for (b.vol, NT, 8), NT, 0, r->stream, g, f3 (fs.E), f3 (fs.H), f3 (fs.J), b, (T) (g.tau/g.h[0]), (T) (g.tau/g.h[1]), (T) (g.tau/g.h[2]), rm));
+   k_e_fused<<<mg_blocks_for (b.vol, NT, 8), NT, 0, r->stream>>> (
+      g, f3 (fs.E), f3 (fs.H), f3 (fs.J), b, (T) (g.tau/g.h[0]), (T) (g.tau/g.h[1]), (T) (g.tau/g.h[2]), rm);
    MG_LAUNCH_CHECK ();
    TRY_MG (launch_e_walls<T> (r, fs, 1));
    TRY_MG (launch_laser<T> (r, fs, 1, 1));

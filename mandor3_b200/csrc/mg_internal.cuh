@@ -271,34 +271,6 @@ int mg_place32 (mg_run_t *r, const mg_place_t *spec, long long at, long long cou
 int mg_ensure_capacity32 (mg_run_t *r, long long need);
 int mg_publish_markers32 (mg_run_t *r);
 void mg_free_markers32 (mg_run_t *r);
-// Programmatic dependent launch.  The kernels of a step start with mg_pdl:
-// it waits until the kernel before them has finished and its writes are
-// visible, then lets the kernel after them be scheduled while they run, so
-// that launch latency overlaps work.  mg_launch launches with the attribute
-// that allows this; launched the ordinary way, both instructions do nothing.
-static __device__ __forceinline__ void mg_pdl ()
-{
-   asm volatile ("griddepcontrol.wait;" ::: "memory");
-   asm volatile ("griddepcontrol.launch_dependents;" ::: "memory");
-}
-
-template <typename... P, typename... A>
-static inline cudaError_t mg_launch (void (*k) (P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
-                                     A &&... a)
-{
-   cudaLaunchConfig_t cfg = {};
-   cfg.gridDim = grid;
-   cfg.blockDim = block;
-   cfg.dynamicSmemBytes = smem;
-   cfg.stream = s;
-   cudaLaunchAttribute at;
-   at.id = cudaLaunchAttributeProgrammaticStreamSerialization;
-   at.val.programmaticStreamSerializationAllowed = 1;
-   cfg.attrs = &at;
-   cfg.numAttrs = 1;
-   return cudaLaunchKernelEx (&cfg, k, static_cast<A &&> (a)...);
-}
-
 int mg_dev_alloc (mg_run_t *r, void **p, size_t bytes);
 int mg_ensure_stage (mg_run_t *r, size_t bytes);
 void mg_drop_graphs (mg_run_t *r);

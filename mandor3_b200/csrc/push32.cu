@@ -191,7 +191,6 @@ __device__ __forceinline__ void block_tally (double Wx, double Wy, double Wz, lo
 __global__ void __launch_bounds__ (256, 3)
 k_push32 (Ctx32 c, long long np, const int *range, DevScalars *dsc)
 {
-   mg_pdl ();
    const Grid &g = c.g;
    const Markers32 m = dsc->m32;
    const int lane = threadIdx.x & 31;
@@ -518,7 +517,6 @@ template <int TX, int TY, int TZ, int ROUNDS, bool PER>
 __global__ void __launch_bounds__ (256, 3)
 k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, DevScalars *dsc)
 {
-   mg_pdl ();
    const Markers32 m = dsc->m32;
    using D = TileDims<TX, TY, TZ>;
    extern __shared__ float smem[];
@@ -829,8 +827,8 @@ static int launch_tiles (mg_run_t *r, const Ctx32 &c, bool per)
    if (blocks > r->ntiles)
       blocks = r->ntiles;
    MG_CUDA (cudaMemsetAsync (&r->dsc->tile_next, 0, sizeof (int), r->stream));
-   MG_CUDA (mg_launch ((per ? kp : kn), blocks, 256, D::BYTES, r->stream, c, r->tile_start, r->tiles[1], r->tiles[2],
-                                                            r->ntiles, r->dsc));
+   (per ? kp : kn)<<<blocks, 256, D::BYTES, r->stream>>> (c, r->tile_start, r->tiles[1], r->tiles[2],
+                                                            r->ntiles, r->dsc);
    MG_LAUNCH_CHECK ();
    return MG_OK;
 }
@@ -852,7 +850,7 @@ int mg_push32 (mg_run_t *r)
    c.vol = r->g.h[0]*r->g.h[1]*r->g.h[2];
    const int T = 256;
    if (!r->tiles_ok) {
-      MG_CUDA (mg_launch (k_push32, mg_blocks_for (r->np, T, 8), T, 0, r->stream, c, r->np, nullptr, r->dsc));
+      k_push32<<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (c, r->np, nullptr, r->dsc);
       MG_LAUNCH_CHECK ();
       return MG_OK;
    }
@@ -869,7 +867,7 @@ int mg_push32 (mg_run_t *r)
    int sms = 148;
    MG_CUDA (cudaDeviceGetAttribute (&sms, cudaDevAttrMultiProcessorCount, r->device));
    // Markers outside the mesh at the last sort: global-memory path.
-   MG_CUDA (mg_launch (k_push32, sms, T, 0, r->stream, c, r->np, r->tile_start + r->ntiles, r->dsc));
+   k_push32<<<sms, T, 0, r->stream>>> (c, r->np, r->tile_start + r->ntiles, r->dsc);
    MG_LAUNCH_CHECK ();
    return MG_OK;
 }

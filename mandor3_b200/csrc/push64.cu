@@ -299,7 +299,6 @@ template <int MINB>
 __global__ void __launch_bounds__ (256, MINB)
 k_push64 (Ctx c, Markers64 m, long long np, DevScalars *dsc)
 {
-   mg_pdl ();
    const Grid &g = c.g;
    const double h1 = g.h[0], h2 = g.h[1], h3 = g.h[2], tau = g.tau;
    const double L0 = g.n[0]*h1, L1 = g.n[1]*h2, L2 = g.n[2]*h3;
@@ -570,7 +569,7 @@ int mg_push64 (mg_run_t *r)
    // Three blocks of 256 per SM (80 registers, a few spilled): the extra
    // warps hide the gather latency better than a spill-free 128-register
    // build with two blocks (measured about 10% faster on the laser-foil run).
-   MG_CUDA (mg_launch (k_push64<3>, mg_blocks_for (r->np, T, 8), T, 0, r->stream, c, r->m64, r->np, r->dsc));
+   k_push64<3><<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (c, r->m64, r->np, r->dsc);
    MG_LAUNCH_CHECK ();
    return MG_OK;
 }

@@ -60,7 +60,6 @@ template <typename T>
 __global__ void k_probes (Grid g, T *const *E, T *const *H, const int *ijk, int n, const DevScalars *dsc,
                           double *ring)
 {
-   mg_pdl ();
    const int q = blockIdx.x*blockDim.x + threadIdx.x;
    if (q >= n)
       return;
@@ -86,13 +85,13 @@ int mg_probes_enqueue (mg_run_t *r)
       return MG_OK;
    const int NT = 128, B = (r->nprobes + NT - 1)/NT;
    if (r->prm.precision == MG_FP64)
-      MG_CUDA (mg_launch (k_probes<double>, B, NT, 0, r->stream, r->g, (double *const *) r->probe_ptrs,
+      k_probes<double><<<B, NT, 0, r->stream>>> (r->g, (double *const *) r->probe_ptrs,
                                                  (double *const *) r->probe_ptrs + 3, r->probe_ijk,
-                                                 r->nprobes, r->dsc, r->probe_ring));
+                                                 r->nprobes, r->dsc, r->probe_ring);
    else
-      MG_CUDA (mg_launch (k_probes<float>, B, NT, 0, r->stream, r->g, (float *const *) r->probe_ptrs,
+      k_probes<float><<<B, NT, 0, r->stream>>> (r->g, (float *const *) r->probe_ptrs,
                                                 (float *const *) r->probe_ptrs + 3, r->probe_ijk,
-                                                r->nprobes, r->dsc, r->probe_ring));
+                                                r->nprobes, r->dsc, r->probe_ring);
    MG_LAUNCH_CHECK ();
    return MG_OK;
 }

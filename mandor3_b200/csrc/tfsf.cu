@@ -78,7 +78,6 @@ __global__ void k_tfsf_add (Fields6<T> F, const long long *off, const int *comp,
                             const double *ring, const int *slot_frame, int slots, long long frame_size,
                             int is_e, int mode, int last, DevScalars *dsc)
 {
-   mg_pdl ();
    const int t = blockIdx.x*blockDim.x + threadIdx.x;
    if (t >= n)
       return;
@@ -113,7 +112,6 @@ template <typename T>
 __global__ void k_tfsf_rec (Fields6<T> F, const long long *off, const int *comp, const double *sf, long long n,
                             double *ring, const DevScalars *dsc)
 {
-   mg_pdl ();
    const long long t = blockIdx.x*(long long) blockDim.x + threadIdx.x;
    if (t >= n)
       return;
@@ -400,11 +398,13 @@ static int add (mg_run_t *r, int fh)
    const mg_tfsf_state *s = r->tfsf;
    const int NT = 128, B = (s->add_n[fh] + NT - 1)/NT;
    if (is32 (r))
-      MG_CUDA (mg_launch (k_tfsf_add<float>, B, NT, 0, r->stream, fields6<float> (r->E32, r->H32), s->add_off[fh], s->add_comp[fh], s->add_src[fh], s->add_n[fh], s->ring,
-         s->slot_frame, s->cfg.ring, s->frame_size, fh == 0, s->cfg.mode, s->cfg.frames, r->dsc));
+      k_tfsf_add<float><<<B, NT, 0, r->stream>>> (
+         fields6<float> (r->E32, r->H32), s->add_off[fh], s->add_comp[fh], s->add_src[fh], s->add_n[fh], s->ring,
+         s->slot_frame, s->cfg.ring, s->frame_size, fh == 0, s->cfg.mode, s->cfg.frames, r->dsc);
    else
-      MG_CUDA (mg_launch (k_tfsf_add<double>, B, NT, 0, r->stream, fields6<double> (r->E, r->H), s->add_off[fh], s->add_comp[fh], s->add_src[fh], s->add_n[fh], s->ring,
-         s->slot_frame, s->cfg.ring, s->frame_size, fh == 0, s->cfg.mode, s->cfg.frames, r->dsc));
+      k_tfsf_add<double><<<B, NT, 0, r->stream>>> (
+         fields6<double> (r->E, r->H), s->add_off[fh], s->add_comp[fh], s->add_src[fh], s->add_n[fh], s->ring,
+         s->slot_frame, s->cfg.ring, s->frame_size, fh == 0, s->cfg.mode, s->cfg.frames, r->dsc);
    MG_LAUNCH_CHECK ();
    return MG_OK;
 }
@@ -425,11 +425,11 @@ int mg_tfsf_record (mg_run_t *r)
    const int NT = 256;
    const int B = (int) ((s->frame_size + NT - 1)/NT);
    if (is32 (r))
-      MG_CUDA (mg_launch (k_tfsf_rec<float>, B, NT, 0, r->stream, fields6<float> (r->E32, r->H32), s->rec_off, s->rec_comp,
-                                                  s->rec_sf, s->frame_size, s->rec_ring, r->dsc));
+      k_tfsf_rec<float><<<B, NT, 0, r->stream>>> (fields6<float> (r->E32, r->H32), s->rec_off, s->rec_comp,
+                                                  s->rec_sf, s->frame_size, s->rec_ring, r->dsc);
    else
-      MG_CUDA (mg_launch (k_tfsf_rec<double>, B, NT, 0, r->stream, fields6<double> (r->E, r->H), s->rec_off, s->rec_comp,
-                                                   s->rec_sf, s->frame_size, s->rec_ring, r->dsc));
+      k_tfsf_rec<double><<<B, NT, 0, r->stream>>> (fields6<double> (r->E, r->H), s->rec_off, s->rec_comp,
+                                                   s->rec_sf, s->frame_size, s->rec_ring, r->dsc);
    MG_LAUNCH_CHECK ();
    return MG_OK;
 }
