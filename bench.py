@@ -449,6 +449,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--requests", type=int, default=24, help="serve workload: solves in the stream")
     ap.add_argument("--step-scale", type=float, default=1.0, help="serve workload: scale of the solves' steps")
+    ap.add_argument("--compare-fp64", type=int, default=0, metavar="K",
+                    help="precision-form workloads: also run K steps in both forms from t = 0 and report the "
+                         "energy-history error of each quantity against the FP64 form")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("at least 3 warm-up steps")
@@ -514,6 +517,10 @@ def main():
                 "traffic": ncu_traffic(w, n_avg), "push_ms": push_ms, "step_ms": step_ms,
                 "algorithmic_bytes_per_launch": algo_bytes}
 
+    compare = None
+    if args.compare_fp64 > 0 and w["precision"] != 0:
+        compare = compare_fp64(w, device, args.compare_fp64)
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         res = reference_sample(w, args.ref_steps)
@@ -532,7 +539,29 @@ def main():
             "clocks": clocks.summary(), "e2e": e2e,
             "gpu_launches": launches_per_step * args.steps, "roofline": roofline,
             "cpu_baseline": cpu}
+    if compare:
+        line["fp64_comparison"] = compare
     print(json.dumps(line), flush=True)
+
+
+def compare_fp64(w, device, steps):
+    """The workload's energy history over `steps` steps from t = 0 in the
+    precision form and in the plain FP64 form (same markers: the same
+    placer draws), one run after the other; per quantity, the largest
+    difference over the history relative to the FP64 quantity's largest
+    magnitude."""
+    hist = {}
+    for prec in (w["precision"], 0):
+        r = make_run(dict(w, precision=prec), device)
+        hist[prec] = r.step(steps)
+        r.close()
+    a, b = hist[w["precision"]], hist[0]
+    def err(qa, qb):
+        return float(np.max(np.abs(qa - qb)) / max(np.max(np.abs(qb)), 1e-300))
+    tot = lambda h: h[:, 1] + h[:, 2] + h[:, 3:6].sum(1)
+    return {"steps": steps, "W_E": err(a[:, 1], b[:, 1]), "W_M": err(a[:, 2], b[:, 2]),
+            "W_T": err(a[:, 3:6].sum(1), b[:, 3:6].sum(1)), "W_total": err(tot(a), tot(b)),
+            "note": "max over the history of |precision form - FP64| / max |FP64| per quantity"}
 
 
 def config_of(w, world):
