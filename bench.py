@@ -455,6 +455,9 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("at least 3 warm-up steps")
+    if args.workload in ("yee", "yee_fp32"):
+        yee_bench(args)
+        return
     if args.workload in ("batch", "serve"):
         import torch
         torch.cuda.set_device(0)
@@ -542,6 +545,55 @@ def main():
     if compare:
         line["fp64_comparison"] = compare
     print(json.dumps(line), flush=True)
+
+
+def yee_bench(args):
+    """Field-only Yee solver: a 256^3 box with Mur walls on all faces and an
+    initial Gaussian E pulse, no markers; cell-updates/s and the fraction of
+    the measured HBM bandwidth for 96 B (FP64) / 48 B (FP32) per cell update
+    (read E, H; write E, H)."""
+    import torch
+    import mandor3_b200 as mg
+    fp32 = args.workload == "yee_fp32"
+    n = (256, 256, 256)
+    h = (0.05, 0.05, 0.05)
+    tau = 0.5 / math.sqrt(sum(1.0 / v ** 2 for v in h))
+    r = mg.Run(n, h, tau, (2, 2, 2), (2, 2, 2), precision=mg.FP32_OFFSET if fp32 else mg.FP64)
+    x = np.arange(n[0] + 1)[:, None, None, None]
+    E = np.zeros(r.field_shape())
+    E[..., 1] = np.exp(-((x - 128) * h[0] / 1.0) ** 2)[..., 0]
+    r.set_fields(E, np.zeros(r.field_shape()))
+    r.init()
+    steps = args.steps or 200
+    r.step(max(args.warmup, 3))
+    stream = torch.cuda.ExternalStream(r.stream(), device=0)
+    torch.cuda.synchronize()
+    with Clocks(0) as clocks:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r.step_async(steps)
+        e1.record(stream)
+        r.synchronize()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    cells = n[0] * n[1] * n[2]
+    bpc = 48.0 if fp32 else 96.0
+    peak, peak_kind = hbm_peak()
+    achieved = cells * bpc / (ms / 1e3) / 1e9
+    r.close()
+    print(json.dumps({
+        "metric": "Yee cell-updates/s", "value": cells / (ms / 1e3), "unit": "cell-updates/s", "n_gpus": 1,
+        "steps": steps, "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if fp32 else "f64", "data": "synthetic",
+        "config": {"workload": "yee_%s_256cubed" % ("fp32" if fp32 else "fp64"), "grid": list(n),
+                   "bc": "mur x6", "markers": 0, "l2": "inputs larger than L2 (fields %.1f GB)"
+                   % (12 * (n[0] + 5) ** 3 * (4 if fp32 else 8) / 1e9)},
+        "clocks": clocks.summary(),
+        "roofline": {"bound": "hbm", "kernel": "whole step (k_h_fused, k_e_fused, walls)",
+                     "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "algorithmic_bytes_per_step": cells * bpc}}), flush=True)
 
 
 def compare_fp64(w, device, steps):
