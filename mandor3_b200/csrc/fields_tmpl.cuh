@@ -373,19 +373,12 @@ __global__ void k_mur_init (Grid g, F3T<T> E, Wall w, int top, T *mur)
 // upper wall (they touch disjoint nodes for n >= 3).  H walls act on both
 // H arrays (H at n and at n+1/2).
 template <typename T>
-__global__ void k_h_walls (Grid g, F3T<T> H, F3T<T> Hn, Wall w, int op_min, int op_max, int both,
-                           int sides)
+__global__ void k_h_walls (Grid g, F3T<T> H, F3T<T> Hn, Wall w, int op_min, int op_max, int both)
 {
-   // sides = 2: lower and upper walls in separate threads (first and second
-   // half of the grid); they touch disjoint nodes.
-   const long t0 = blockIdx.x*(long) blockDim.x + threadIdx.x;
-   const long plane = (long) w.np_*w.nq_;
-   if (t0 >= sides*plane)
+   long o;
+   int p, q;
+   if (!wall_node (g, w, 0, o, p, q))
       return;
-   const int side = sides == 2 ? (int) (t0/plane) : -1;
-   const long tt = t0 - (side > 0 ? plane : 0);
-   const int p = (int) (tt / w.nq_), q = (int) (tt % w.nq_);
-   const long o = g.origin + p*w.s_p + q*w.s_q;
    const int N = g.n[w.ea];
    const long s = w.s_a;
    for (int arr = 0 ; arr < (both ? 2 : 1) ; ++arr) {
@@ -406,21 +399,17 @@ __global__ void k_h_walls (Grid g, F3T<T> H, F3T<T> Hn, Wall w, int op_min, int 
          }
          continue;
       }
-      if (side <= 0) {
-         const T p1 = Hp[o + s], q1 = Hq[o + s];
-         Hp[o] = p1;
-         Hq[o] = q1;
-         if (op_min == OP_MIRROR_MIN)
-            Ha[o] = 0;
-      }
-      if (side != 0) {
-         const long t = o + N*s;
-         const T pN = Hp[t], qN = Hq[t];
-         Hp[t + s] = pN;
-         Hq[t + s] = qN;
-         if (op_max == OP_MIRROR_MAX)
-            Ha[t] = 0;
-      }
+      const T p1 = Hp[o + s], q1 = Hq[o + s];
+      const long t = o + N*s;
+      const T pN = Hp[t], qN = Hq[t];
+      Hp[o] = p1;
+      Hq[o] = q1;
+      if (op_min == OP_MIRROR_MIN)
+         Ha[o] = 0;
+      Hp[t + s] = pN;
+      Hq[t + s] = qN;
+      if (op_max == OP_MIRROR_MAX)
+         Ha[t] = 0;
    }
 }
 
@@ -481,32 +470,19 @@ __device__ __forceinline__ void e_wall_op (const Grid &g, F3T<T> &E, const Wall 
 // later wall reads or writes such a node, so its -tau J comes after every
 // wall operation on it, as in core/em.c:189-222.  Threads cover transverse
 // indices [-1, n+1]; the wall operations act on [0, n+1].
-//
-// sides = 2 (no periodic wall on the axis): the lower and the upper wall of a
-// line are separate threads (first and second half of the grid), each with
-// its wall operation and the -tau J of its three rim nodes, {-1, 0, 1} or
-// {n-1, n, n+1}; the two touch disjoint nodes for n >= 8, and a Mur wall
-// reads its inner node before its own thread subtracts that node's current.
-// sides = 1 (periodic axis): one thread does both walls, then all six nodes,
-// since the periodic copy reads the lower nodes and writes the upper ones.
 template <typename T>
 __global__ void k_e_walls (Grid g, F3T<T> E, F3T<T> J, Wall w, int op_min, int op_max, T *mur_min,
-                           T *mur_max, T alpha, int sub_j, int sides)
+                           T *mur_max, T alpha, int sub_j)
 {
-   const long t0 = blockIdx.x*(long) blockDim.x + threadIdx.x;
+   const long t = blockIdx.x*(long) blockDim.x + threadIdx.x;
    const int np1 = w.np_ + 1, nq1 = w.nq_ + 1;          // [-1, n+1]
-   const long line = (long) np1*nq1;
-   if (t0 >= sides*line)
+   if (t >= (long) np1*nq1)
       return;
-   const int side = sides == 2 ? (int) (t0/line) : -1;     // 0 lower, 1 upper, -1 both
-   const long t = t0 - (side > 0 ? line : 0);
    const int p = (int) (t / nq1) - 1, q = (int) (t % nq1) - 1;
    const long o = g.origin + p*w.s_p + q*w.s_q;
    if (p >= 0 && q >= 0) {
-      if (side <= 0)
-         e_wall_op (g, E, w, op_min, o, p, q, mur_min, alpha);
-      if (side != 0)
-         e_wall_op (g, E, w, op_max, o, p, q, mur_max, alpha);
+      e_wall_op (g, E, w, op_min, o, p, q, mur_min, alpha);
+      e_wall_op (g, E, w, op_max, o, p, q, mur_max, alpha);
    }
    if (!sub_j)
       return;
@@ -524,12 +500,9 @@ __global__ void k_e_walls (Grid g, F3T<T> E, F3T<T> J, Wall w, int op_min, int o
       return;
    const T tau = (T) g.tau;
    const int vs[6] = {-1, 0, 1, N - 1, N, N + 1};
-   const int u0 = side == 1 ? 3 : 0, u1 = side == 0 ? 3 : 6;
    T e[6][3], jv[6][3];
 #pragma unroll
    for (int u = 0 ; u < 6 ; ++u) {
-      if (u < u0 || u >= u1)
-         continue;
       const long x = o + vs[u]*w.s_a;
 #pragma unroll
       for (int c = 0 ; c < 3 ; ++c) {
@@ -539,8 +512,6 @@ __global__ void k_e_walls (Grid g, F3T<T> E, F3T<T> J, Wall w, int op_min, int o
    }
 #pragma unroll
    for (int u = 0 ; u < 6 ; ++u) {
-      if (u < u0 || u >= u1)
-         continue;
       const long x = o + vs[u]*w.s_a;
 #pragma unroll
       for (int c = 0 ; c < 3 ; ++c)
@@ -621,27 +592,19 @@ __device__ __forceinline__ void j_fold (const Grid &g, F3T<T> &J, int ea, int to
    }
 }
 
-// sides = 2 (no periodic wall on the axis): the lower and upper folds of a
-// line in separate threads (first and second half of the grid); they touch
-// the nodes [-2, 2] and [n-2, n+2] along the axis, disjoint for n >= 8.
 template <typename T>
-__global__ void k_j_walls (Grid g, F3T<T> J, int ea, int sides)
+__global__ void k_j_walls (Grid g, F3T<T> J, int ea)
 {
    const int ep = (ea == 0) ? 1 : 0, eq = (ea == 2) ? 1 : 2;
    const int np_ = g.n[ep] + 5, nq_ = g.n[eq] + 5;
-   const long plane = (long) np_*nq_;
-   const long t0 = blockIdx.x*(long) blockDim.x + threadIdx.x;
-   if (t0 >= sides*plane)
+   const long t = blockIdx.x*(long) blockDim.x + threadIdx.x;
+   if (t >= (long) np_*nq_)
       return;
-   const int side = sides == 2 ? (int) (t0/plane) : -1;
-   const long t = t0 - (side > 0 ? plane : 0);
    const long s[3] = {g.sx, g.sy, 1};
    const int p = (int) (t / nq_) - 2, q = (int) (t % nq_) - 2;
    const long base = g.origin + p*s[ep] + q*s[eq];
-   if (side <= 0)
-      j_fold (g, J, ea, 0, g.bc[0][ea], base, s);
-   if (side != 0)
-      j_fold (g, J, ea, 1, g.bc[1][ea], base, s);
+   j_fold (g, J, ea, 0, g.bc[0][ea], base, s);
+   j_fold (g, J, ea, 1, g.bc[1][ea], base, s);
 }
 
 
@@ -771,12 +734,11 @@ static int launch_h_walls (mg_run_t *r, const FS<T> &fs, int both)
    const Grid &g = r->g;
    for (int ea = 0 ; ea < 3 ; ++ea) {
       Wall w = make_wall (g, ea);
+      const long nodes = (long) w.np_*w.nq_;
+      const int NT = 256, B = (int) ((nodes + NT - 1)/NT);
       int op0, op1;
       wall_ops (g, ea, op0, op1);
-      const int sides = op0 == OP_PERIODIC ? 1 : 2;
-      const long nodes = (long) sides*w.np_*w.nq_;
-      const int NT = 256, B = (int) ((nodes + NT - 1)/NT);
-      k_h_walls<<<B, NT, 0, r->stream>>> (g, f3 (fs.H), f3 (fs.Hn), w, op0, op1, both, sides);
+      k_h_walls<<<B, NT, 0, r->stream>>> (g, f3 (fs.H), f3 (fs.Hn), w, op0, op1, both);
       MG_LAUNCH_CHECK ();
    }
    return MG_OK;
@@ -788,12 +750,11 @@ static int launch_hn_walls (mg_run_t *r, const FS<T> &fs)
    const Grid &g = r->g;
    for (int ea = 0 ; ea < 3 ; ++ea) {
       Wall w = make_wall (g, ea);
+      const long nodes = (long) w.np_*w.nq_;
+      const int NT = 256, B = (int) ((nodes + NT - 1)/NT);
       int op0, op1;
       wall_ops (g, ea, op0, op1);
-      const int sides = op0 == OP_PERIODIC ? 1 : 2;
-      const long nodes = (long) sides*w.np_*w.nq_;
-      const int NT = 256, B = (int) ((nodes + NT - 1)/NT);
-      k_h_walls<<<B, NT, 0, r->stream>>> (g, f3 (fs.Hn), f3 (fs.Hn), w, op0, op1, 0, sides);
+      k_h_walls<<<B, NT, 0, r->stream>>> (g, f3 (fs.Hn), f3 (fs.Hn), w, op0, op1, 0);
       MG_LAUNCH_CHECK ();
    }
    return MG_OK;
@@ -806,14 +767,13 @@ static int launch_e_walls (mg_run_t *r, const FS<T> &fs, int sub_j)
    const Grid &g = r->g;
    for (int ea = 0 ; ea < 3 ; ++ea) {
       Wall w = make_wall (g, ea);
+      const long nodes = (long) (w.np_ + 1)*(w.nq_ + 1);
+      const int NT = 128, B = (int) ((nodes + NT - 1)/NT);
       const T alpha = (T) ((g.tau - g.h[ea])/(g.tau + g.h[ea]));
       int op0, op1;
       wall_ops (g, ea, op0, op1);
-      const int sides = op0 == OP_PERIODIC ? 1 : 2;
-      const long nodes = (long) sides*(w.np_ + 1)*(w.nq_ + 1);
-      const int NT = 128, B = (int) ((nodes + NT - 1)/NT);
       k_e_walls<<<B, NT, 0, r->stream>>> (g, f3 (fs.E), f3 (fs.J), w, op0, op1, fs.mur[0][ea],
-                                         fs.mur[1][ea], alpha, sub_j, sides);
+                                         fs.mur[1][ea], alpha, sub_j);
       MG_LAUNCH_CHECK ();
    }
    return MG_OK;
@@ -928,12 +888,11 @@ int fields_h_step (mg_run_t *r, const FS<T> &fs)
    const Grid &g = r->g;
    for (int ea = 0 ; ea < 3 ; ++ea) {
       Wall w = make_wall (g, ea);
+      const long nodes = (long) w.np_*w.nq_;
+      const int NT = 256, B = (int) ((nodes + NT - 1)/NT);
       int op0, op1;
       wall_ops (g, ea, op0, op1);
-      const int sides = op0 == OP_PERIODIC ? 1 : 2;
-      const long nodes = (long) sides*w.np_*w.nq_;
-      const int NT = 256, B = (int) ((nodes + NT - 1)/NT);
-      k_h_walls<<<B, NT, 0, r->stream>>> (g, f3 (fs.H), f3 (fs.H), w, op0, op1, 0, sides);
+      k_h_walls<<<B, NT, 0, r->stream>>> (g, f3 (fs.H), f3 (fs.H), w, op0, op1, 0);
       MG_LAUNCH_CHECK ();
    }
    return MG_OK;
@@ -975,10 +934,9 @@ int fields_jbc (mg_run_t *r, const FS<T> &fs)
    const Grid &g = r->g;
    for (int ea = 0 ; ea < 3 ; ++ea) {
       const int ep = (ea == 0) ? 1 : 0, eq = (ea == 2) ? 1 : 2;
-      const int sides = g.bc[0][ea] == MG_BC_PERIODIC ? 1 : 2;
-      const long nodes = (long) sides*(g.n[ep] + 5)*(g.n[eq] + 5);
+      const long nodes = (long) (g.n[ep] + 5)*(g.n[eq] + 5);
       const int NT = 256, B = (int) ((nodes + NT - 1)/NT);
-      k_j_walls<<<B, NT, 0, r->stream>>> (g, f3 (fs.J), ea, sides);
+      k_j_walls<<<B, NT, 0, r->stream>>> (g, f3 (fs.J), ea);
       MG_LAUNCH_CHECK ();
    }
    return MG_OK;
