@@ -604,7 +604,7 @@ __device__ __forceinline__ int key64 (const Key64 &t, double x, double y, double
    return ((i + 1)*(t.n[1] + 2) + (j + 1))*(t.n[2] + 2) + (k + 1);
 }
 
-#define SORT64_ROWS 4
+#define SORT64_ROWS 8
 __global__ void k_hist64 (Key64 t, Markers64 m, long long np, int *count, long long kp)
 {
    const int lane = threadIdx.x & 31;
