@@ -228,7 +228,10 @@ def reference_sample(w, steps):
 
 
 # ---------------------------------------------------------------------------
-def dist_setup():
+def dist_setup(backend="nccl"):
+    """One process per GPU (replicas: each rank runs its own copy of the
+    workload, no data-path collective); the process group only carries the
+    timing reductions.  backend "gloo" runs the same logic on CPU."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -236,29 +239,39 @@ def dist_setup():
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return world, rank, local
+
+
+def _reduce(v, world, op):
+    import torch
+    import torch.distributed as dist
+    on_gpu = dist.get_backend() == "nccl"
+    t = torch.tensor([float(v)], device="cuda" if on_gpu else "cpu", dtype=torch.float64)
+    dist.all_reduce(t, op=op)
+    return float(t.item())
 
 
 def dist_max(v, world):
     if world == 1:
         return v
-    import torch
     import torch.distributed as dist
-    t = torch.tensor([float(v)], device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return _reduce(v, world, dist.ReduceOp.MAX)
+
+
+def replica_value(units, ms, world):
+    """Whole-job throughput of replicas: the units all ranks processed over
+    the slowest rank's time (ms)."""
+    return dist_sum(units, world) / (dist_max(ms, world) / 1e3)
 
 
 def dist_sum(v, world):
     if world == 1:
         return v
-    import torch
     import torch.distributed as dist
-    t = torch.tensor([float(v)], device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(v, world, dist.ReduceOp.SUM)
 
 
 def barrier(world):
@@ -502,8 +515,7 @@ def main():
     r.close()
     n_avg = 0.5 * (n_before + n_after)
     ms_max = dist_max(ms, world)
-    total_ps = dist_sum(n_avg * args.steps, world)
-    value = total_ps / (ms_max / 1e3)
+    value = replica_value(n_avg * args.steps, ms, world)
 
     # End to end through the C ABI from pinned host buffers.
     e2e = None
