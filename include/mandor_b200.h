@@ -191,6 +191,22 @@ long long mg_estimate_bytes (const mg_params_t *params, long long markers);
 int  mg_tecplot_fields (mg_run_t *run, double *E, double *H);
 int  mg_tecplot_currents (mg_run_t *run, double *J);
 
+/* ---- asynchronous checkpoints -----------------------------------------------
+ * mg_run_snapshot: the state mg_run_get_fields and mg_run_get_markers would
+ * return (E, H over the checkpoint region; the live markers, compacted;
+ * *n their count) is copied into device buffers of the run at the current
+ * step boundary and then to E, H, m (NULL: skipped) on a stream of its own;
+ * the call returns once the device copy is taken, and the run may keep
+ * stepping.  The host buffers must not be read before mg_run_snapshot_wait
+ * (the next snapshot, and mg_run_destroy, wait too).  Pinned buffers from
+ * mg_host_alloc let the copy overlap the steps.  Replaces the synchronous
+ * sysIO_save / plasma_save reads of core/main.c:445-460 with no change to
+ * the files written.  No counterpart in the reference.                      */
+int   mg_run_snapshot (mg_run_t *run, double *E, double *H, mg_marker_t *m, long long cap, long long *n);
+int   mg_run_snapshot_wait (mg_run_t *run);
+void *mg_host_alloc (size_t bytes);
+void  mg_host_free (void *p);
+
 /* ---- TF/SF interface (core/em_TFSF.c) -------------------------------------
  * Replaces TFSF_init / TFSF_preHStep / TFSF_postHStep / TFSF_postEStep /
  * TFSF_completeFrame (core/em_TFSF.c:480-853, called from core/em.c:92,

@@ -151,6 +151,8 @@ def load():
         "mg_run_last_timing": [vp, C.POINTER(d), C.POINTER(d)],
         "mg_run_set_gauss_spot": [vp, vp],
         "mg_run_set_tfsf": [vp, vp],
+        "mg_run_snapshot": [vp, vp, vp, vp, C.c_longlong, vp],
+        "mg_run_snapshot_wait": [vp],
         "mg_run_place_two_stream": [vp, vp],
         "mg_run_df_uniform": [vp, C.c_longlong, C.c_longlong, vp],
         "mg_run_shift_velocity": [vp, C.c_longlong, C.c_longlong, vp],
@@ -317,6 +319,21 @@ class Run:
         arguments switch it off."""
         self._gspot = GaussSpot(**kw) if kw else None
         _check(load().mg_run_set_gauss_spot(self.ptr, C.byref(self._gspot) if kw else None))
+
+    def snapshot(self):
+        """Starts an asynchronous copy of the checkpoint state (mg_run_snapshot);
+        returns a function that waits for it and gives (E, H, markers)."""
+        E = np.zeros(self.field_shape())
+        H = np.zeros(self.field_shape())
+        cap = max(self.marker_count(), 1)
+        m = np.zeros(cap, MARKER_DTYPE)
+        n = C.c_longlong()
+        _check(load().mg_run_snapshot(self.ptr, E.ctypes.data, H.ctypes.data, m.ctypes.data, cap,
+                                      C.byref(n)))
+        def wait():
+            _check(load().mg_run_snapshot_wait(self.ptr))
+            return E, H, m[:n.value]
+        return wait
 
     def place_two_stream(self, gamma, qDivM, n, m, L, id0=1):
         """[DF:two-stream] markers (mg_run_place_two_stream)."""

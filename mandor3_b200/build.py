@@ -80,7 +80,7 @@ def build(force=False, verbose=False):
     main_src = os.path.join(HOST, "core_main.c")
     if os.path.exists(main_src) and (force or _newer(main_src, DRIVER, [LIB])):
         _run(["gcc", "-O2", "-std=gnu99", "-Wall", "-I" + INCLUDE, "-I" + HOST, main_src,
-              "-o", DRIVER, "-L" + PKG, "-lmandor_b200", "-Wl,-rpath,$ORIGIN", "-lm"], verbose)
+              "-o", DRIVER, "-L" + PKG, "-lmandor_b200", "-Wl,-rpath,$ORIGIN", "-lm", "-lpthread"], verbose)
     return LIB
 
 

@@ -424,6 +424,8 @@ extern "C" int mg_run_create (const mg_params_t *params, mg_run_t **out)
    return MG_OK;
 }
 
+static void free_snapshot (mg_run_t *r);
+
 extern "C" int mg_run_destroy (mg_run_t *r)
 {
    if (!r)
@@ -464,6 +466,7 @@ extern "C" int mg_run_destroy (mg_run_t *r)
    if (r->probe_ring) cudaFree (r->probe_ring);
    if (r->probe_ptrs) cudaFree (r->probe_ptrs);
    mg_tfsf_free (r);
+   free_snapshot (r);
    for (int q = 0 ; q < 2 ; ++q)
       if (r->gauss_rho[q]) cudaFree (r->gauss_rho[q]);
    if (r->gauss_out) cudaFree (r->gauss_out);
@@ -501,28 +504,37 @@ extern "C" int mg_run_set_fields (mg_run_t *r, const double *E, const double *H)
    return MG_OK;
 }
 
-extern "C" int mg_run_get_fields (mg_run_t *r, double *E, double *H)
+// E and H over the checkpoint region into E, H (host memory, or device
+// memory when dev: converted in place, no copy, nothing waited for).
+int mg_fields_out (mg_run_t *r, double *E, double *H, bool dev)
 {
-   CHECK_RUN (r);
-   if (r->prm.precision != MG_FP64) {
-      return mg_run_get_fields32 (r, E, H);
-   }
+   if (r->prm.precision != MG_FP64)
+      return mg_fields_out32 (r, E, H, dev);
    const long vol = (long) (r->g.n[0] + 1)*(r->g.n[1] + 1)*(r->g.n[2] + 1);
    const size_t bytes = (size_t) vol*3*sizeof (double);
-   TRY (mg_ensure_stage (r, bytes));
+   if (!dev)
+      TRY (mg_ensure_stage (r, bytes));
    double *dst[2] = {E, H};
    // Between mg_em_HHalfStep and mg_em_HStep the reference's H is H^n.
    double **src[2] = {r->E, (r->stage_no >= 1 && r->stage_no <= 3) ? r->Hn : r->H};
    for (int f = 0 ; f < 2 ; ++f) {
       if (!dst[f])
          continue;
-      k_fields_out<<<mg_blocks_for (vol, 256, 8), 256, 0, r->stream>>> (r->g, (double *) r->stage,
+      k_fields_out<<<mg_blocks_for (vol, 256, 8), 256, 0, r->stream>>> (r->g, dev ? dst[f] : (double *) r->stage,
                                                                         src[f][0], src[f][1], src[f][2], 0);
       MG_LAUNCH_CHECK ();
-      MG_CUDA (cudaMemcpyAsync (dst[f], r->stage, bytes, cudaMemcpyDeviceToHost, r->stream));
-      MG_CUDA (cudaStreamSynchronize (r->stream));
+      if (!dev) {
+         MG_CUDA (cudaMemcpyAsync (dst[f], r->stage, bytes, cudaMemcpyDeviceToHost, r->stream));
+         MG_CUDA (cudaStreamSynchronize (r->stream));
+      }
    }
    return MG_OK;
+}
+
+extern "C" int mg_run_get_fields (mg_run_t *r, double *E, double *H)
+{
+   CHECK_RUN (r);
+   return mg_fields_out (r, E, H, false);
 }
 
 extern "C" int mg_run_get_current (mg_run_t *r, double *J)
@@ -586,9 +598,15 @@ extern "C" int mg_run_marker_count (mg_run_t *r, long long *n)
 extern "C" int mg_run_get_markers (mg_run_t *r, mg_marker_t *out, long long cap, long long *n)
 {
    CHECK_RUN (r);
-   if (r->prm.precision != MG_FP64) {
-      return mg_run_get_markers32 (r, out, cap, n);
-   }
+   return mg_markers_out (r, out, cap, n, false);
+}
+
+// The live markers, compacted, into out (host memory, or device memory when
+// dev).
+int mg_markers_out (mg_run_t *r, mg_marker_t *out, long long cap, long long *n, bool dev)
+{
+   if (r->prm.precision != MG_FP64)
+      return mg_markers_out32 (r, out, cap, n, dev);
    long long live = 0;
    TRY (mg_run_marker_count (r, &live));
    if (n)
@@ -618,13 +636,119 @@ extern "C" int mg_run_get_markers (mg_run_t *r, mg_marker_t *out, long long cap,
          mg_set_error ("mg_run_get_markers: live count changed during download");
          return MG_ERR_STATE;
       }
-      MG_CUDA (cudaMemcpyAsync (out + written, dst, got*sizeof (mg_marker_t), cudaMemcpyDeviceToHost, r->stream));
+      MG_CUDA (cudaMemcpyAsync (out + written, dst, got*sizeof (mg_marker_t),
+                                dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, r->stream));
       MG_CUDA (cudaStreamSynchronize (r->stream));
       written += got;
    }
    if (n)
       *n = written;
    return MG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Asynchronous snapshot: the checkpoint state (fields over [0, n]^3 and the
+// live markers, compacted) is converted into device buffers of the run on
+// its own stream -- a step boundary -- and copied to the caller's host
+// buffers on a second stream, so that later steps run while it travels.
+// ---------------------------------------------------------------------------
+static void free_snapshot (mg_run_t *r)
+{
+   if (r->snap_pending && r->snap_done)
+      cudaEventSynchronize (r->snap_done);
+   r->snap_pending = 0;
+   if (r->snap_E) cudaFree (r->snap_E);
+   if (r->snap_H) cudaFree (r->snap_H);
+   if (r->snap_m) cudaFree (r->snap_m);
+   r->snap_E = r->snap_H = nullptr;
+   r->snap_m = nullptr;
+   r->snap_cap = 0;
+   if (r->snap_ready) cudaEventDestroy (r->snap_ready);
+   if (r->snap_done) cudaEventDestroy (r->snap_done);
+   if (r->snap_stream) cudaStreamDestroy (r->snap_stream);
+   r->snap_ready = r->snap_done = nullptr;
+   r->snap_stream = nullptr;
+}
+
+extern "C" int mg_run_snapshot_wait (mg_run_t *r)
+{
+   CHECK_RUN (r);
+   if (!r->snap_pending)
+      return MG_OK;
+   MG_CUDA (cudaEventSynchronize (r->snap_done));
+   r->snap_pending = 0;
+   return MG_OK;
+}
+
+extern "C" int mg_run_snapshot (mg_run_t *r, double *E, double *H, mg_marker_t *m, long long cap,
+                                long long *n)
+{
+   CHECK_RUN (r);
+   TRY (mg_run_snapshot_wait (r));
+   if (r->stage_no != 0) {
+      mg_set_error ("mg_run_snapshot: a stage-by-stage step is in progress");
+      return MG_ERR_STATE;
+   }
+   long long live = 0;
+   TRY (mg_run_marker_count (r, &live));
+   if (m && cap < live) {
+      mg_set_error ("mg_run_snapshot: buffer holds %lld markers, %lld live", cap, live);
+      return MG_ERR_CAPACITY;
+   }
+   const long vol = (long) (r->g.n[0] + 1)*(r->g.n[1] + 1)*(r->g.n[2] + 1);
+   const size_t fbytes = (size_t) vol*3*sizeof (double);
+   if (!r->snap_stream) {
+      MG_CUDA (cudaStreamCreateWithFlags (&r->snap_stream, cudaStreamNonBlocking));
+      MG_CUDA (cudaEventCreateWithFlags (&r->snap_ready, cudaEventDisableTiming));
+      MG_CUDA (cudaEventCreateWithFlags (&r->snap_done, cudaEventDisableTiming));
+   }
+   if (!r->snap_E) {
+      TRY (mg_dev_alloc (r, (void **) &r->snap_E, fbytes));
+      TRY (mg_dev_alloc (r, (void **) &r->snap_H, fbytes));
+   }
+   if (m && live > r->snap_cap) {
+      if (r->snap_m) {
+         cudaFree (r->snap_m);
+         r->dev_bytes -= (long long) r->snap_cap*sizeof (mg_marker_t);
+         r->snap_m = nullptr;
+         r->snap_cap = 0;
+      }
+      const long long c = live + live/8 + 1024;
+      TRY (mg_dev_alloc (r, (void **) &r->snap_m, (size_t) c*sizeof (mg_marker_t)));
+      r->snap_cap = c;
+   }
+   TRY (mg_fields_out (r, E ? r->snap_E : nullptr, H ? r->snap_H : nullptr, true));
+   long long got = 0;
+   if (m)
+      TRY (mg_markers_out (r, r->snap_m, r->snap_cap, &got, true));
+   MG_CUDA (cudaEventRecord (r->snap_ready, r->stream));
+   MG_CUDA (cudaStreamWaitEvent (r->snap_stream, r->snap_ready, 0));
+   if (E) MG_CUDA (cudaMemcpyAsync (E, r->snap_E, fbytes, cudaMemcpyDeviceToHost, r->snap_stream));
+   if (H) MG_CUDA (cudaMemcpyAsync (H, r->snap_H, fbytes, cudaMemcpyDeviceToHost, r->snap_stream));
+   if (m && got > 0)
+      MG_CUDA (cudaMemcpyAsync (m, r->snap_m, (size_t) got*sizeof (mg_marker_t), cudaMemcpyDeviceToHost,
+                                r->snap_stream));
+   MG_CUDA (cudaEventRecord (r->snap_done, r->snap_stream));
+   r->snap_pending = 1;
+   if (n)
+      *n = got;
+   return MG_OK;
+}
+
+extern "C" void *mg_host_alloc (size_t bytes)
+{
+   void *p = nullptr;
+   if (cudaMallocHost (&p, bytes ? bytes : 1) != cudaSuccess) {
+      mg_set_error ("mg_host_alloc: %zu bytes of pinned memory not available", bytes);
+      return nullptr;
+   }
+   return p;
+}
+
+extern "C" void mg_host_free (void *p)
+{
+   if (p)
+      cudaFreeHost (p);
 }
 
 extern "C" int mg_run_set_gauss_spot (mg_run_t *r, const mg_gauss_spot_t *s)

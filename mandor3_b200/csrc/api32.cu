@@ -449,21 +449,24 @@ int mg_run_set_fields32 (mg_run_t *r, const double *E, const double *H)
    return MG_OK;
 }
 
-int mg_run_get_fields32 (mg_run_t *r, double *E, double *H)
+int mg_fields_out32 (mg_run_t *r, double *E, double *H, bool dev)
 {
    const long vol = (long) (r->g.n[0] + 1)*(r->g.n[1] + 1)*(r->g.n[2] + 1);
    const size_t bytes = (size_t) vol*3*sizeof (double);
-   TRY32 (mg_ensure_stage (r, bytes));
+   if (!dev)
+      TRY32 (mg_ensure_stage (r, bytes));
    double *dst[2] = {E, H};
    float **src[2] = {r->E32, (r->stage_no >= 1 && r->stage_no <= 3) ? r->Hn32 : r->H32};
    for (int f = 0 ; f < 2 ; ++f) {
       if (!dst[f])
          continue;
       k_fields_out32<<<mg_blocks_for (vol, 256, 8), 256, 0, r->stream>>> (
-         r->g, (double *) r->stage, src[f][0], src[f][1], src[f][2], 0);
+         r->g, dev ? dst[f] : (double *) r->stage, src[f][0], src[f][1], src[f][2], 0);
       MG_LAUNCH_CHECK ();
-      MG_CUDA (cudaMemcpyAsync (dst[f], r->stage, bytes, cudaMemcpyDeviceToHost, r->stream));
-      MG_CUDA (cudaStreamSynchronize (r->stream));
+      if (!dev) {
+         MG_CUDA (cudaMemcpyAsync (dst[f], r->stage, bytes, cudaMemcpyDeviceToHost, r->stream));
+         MG_CUDA (cudaStreamSynchronize (r->stream));
+      }
    }
    return MG_OK;
 }
@@ -502,7 +505,7 @@ int mg_run_set_markers32 (mg_run_t *r, const mg_marker_t *m, long long n)
    return MG_OK;
 }
 
-int mg_run_get_markers32 (mg_run_t *r, mg_marker_t *out, long long cap, long long *n)
+int mg_markers_out32 (mg_run_t *r, mg_marker_t *out, long long cap, long long *n, bool dev)
 {
    long long live = 0;
    TRY32 (mg_run_marker_count (r, &live));
@@ -533,7 +536,8 @@ int mg_run_get_markers32 (mg_run_t *r, mg_marker_t *out, long long cap, long lon
          mg_set_error ("mg_run_get_markers: live count changed during download");
          return MG_ERR_STATE;
       }
-      MG_CUDA (cudaMemcpyAsync (out + written, dst, got*sizeof (mg_marker_t), cudaMemcpyDeviceToHost, r->stream));
+      MG_CUDA (cudaMemcpyAsync (out + written, dst, got*sizeof (mg_marker_t),
+                                dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, r->stream));
       MG_CUDA (cudaStreamSynchronize (r->stream));
       written += got;
    }

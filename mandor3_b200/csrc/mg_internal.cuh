@@ -147,6 +147,15 @@ struct mg_run {
    int         has_gspot;
    GaussSpot   gspot;
 
+   // asynchronous snapshot (mg_run_snapshot): device copy of the
+   // checkpoint state, copied to the caller's buffers on its own stream
+   double     *snap_E, *snap_H;
+   mg_marker_t *snap_m;
+   long long   snap_cap;
+   cudaStream_t snap_stream;
+   cudaEvent_t snap_ready, snap_done;
+   int         snap_pending;
+
    // TF/SF interface (tfsf.cu), null when off
    struct mg_tfsf_state *tfsf;
 
@@ -275,10 +284,12 @@ int mg_dev_alloc (mg_run_t *r, void **p, size_t bytes);
 int mg_ensure_stage (mg_run_t *r, size_t bytes);
 void mg_drop_graphs (mg_run_t *r);
 int mg_run_set_fields32 (mg_run_t *r, const double *E, const double *H);
-int mg_run_get_fields32 (mg_run_t *r, double *E, double *H);
+int mg_fields_out32 (mg_run_t *r, double *E, double *H, bool dev);
+int mg_fields_out (mg_run_t *r, double *E, double *H, bool dev);
+int mg_markers_out (mg_run_t *r, mg_marker_t *out, long long cap, long long *n, bool dev);
 int mg_run_get_current32 (mg_run_t *r, double *J);
 int mg_run_set_markers32 (mg_run_t *r, const mg_marker_t *m, long long n);
-int mg_run_get_markers32 (mg_run_t *r, mg_marker_t *m, long long cap, long long *n);
+int mg_markers_out32 (mg_run_t *r, mg_marker_t *m, long long cap, long long *n, bool dev);
 
 // Grid sizing: a multiple of the SM count (148 on B200).
 int mg_sm_count (void);

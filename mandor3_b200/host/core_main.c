@@ -30,6 +30,7 @@
 #include <dirent.h>
 #include <errno.h>
 #include <math.h>
+#include <pthread.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -317,46 +318,102 @@ static void mesh_head (const int n[3], const char *name, int ghost, int vector,
    strncpy ((char *) out + sizeof (v) + 16, name, 29);
 }
 
-/* sysIO_save + plasma_save (IO_sys.c:99-124, core/plasma_IO.c:273-287). */
-static void checkpoint (mg_run_t *run, records_t *rec, const domain_t *dom, long nodes, double time)
+/* sysIO_save + plasma_save (IO_sys.c:99-124, core/plasma_IO.c:273-287),
+ * asynchronously: the run's state is snapshot on the device at the step
+ * boundary (mg_run_snapshot), then a writer thread waits for its copy into
+ * pinned host buffers and writes the record while the main loop steps on.
+ * The small shared files (domain.bin, the file map) are written here, in
+ * order with the tecplot records; the record's own files follow in the
+ * thread, sys_%06d.txt and sys.N last, so sys.N never names an incomplete
+ * record.  One record is in flight at a time. */
+typedef struct {
+   pthread_t   th;
+   int         active;
+   mg_run_t   *run;
+   double     *E, *H;
+   mg_marker_t *m;
+   long long   cap, n;
+   long        nodes;
+   int         sys_num, map_id;
+   double      time;
+   unsigned char head_E[HEADER_BYTES], head_H[HEADER_BYTES];
+   char        prtn_src[256];
+} ckpt_t;
+
+static void *ckpt_write (void *arg)
 {
+   ckpt_t *c = (ckpt_t *) arg;
    char path[512];
-   double *E = (double *) malloc (sizeof (double)*3*nodes);
-   double *H = (double *) malloc (sizeof (double)*3*nodes);
-   check (mg_run_get_fields (run, E, H), "download fields");
-   long long n = 0;
-   check (mg_run_marker_count (run, &n), "marker count");
-   mg_marker_t *m = (mg_marker_t *) malloc (sizeof (mg_marker_t)*(n > 0 ? n : 1));
-   check (mg_run_get_markers (run, m, n, &n), "download markers");
-
-   snprintf (path, sizeof (path), "binData/plasma_%06d_%03d.bin", rec->sys_num, 0);
-   write_markers (path, m, n);
-   write_domain (dom);
-
-   const int map_id = save_filemap (rec, dom);
-   FILE *fp;
-
-   snprintf (path, sizeof (path), "binData/sys_E_%06d(%03d).bin", rec->sys_num, 0);
-   write_mesh (path, rec->head_E, E, nodes);
-   snprintf (path, sizeof (path), "binData/sys_H_%06d(%03d).bin", rec->sys_num, 0);
-   write_mesh (path, rec->head_H, H, nodes);
-   snprintf (path, sizeof (path), "binData/sys_prtn_%06d.bin", rec->sys_num);
-   copy_file (rec->prtn_src, path);
-
-   snprintf (path, sizeof (path), "binData/sys_%06d.txt", rec->sys_num);
-   fp = open_or_die (path, "wt");
-   fprintf (fp, "@ %.14e    time.\n", time);
+   check (mg_run_snapshot_wait (c->run), "checkpoint copy");
+   snprintf (path, sizeof (path), "binData/plasma_%06d_%03d.bin", c->sys_num, 0);
+   write_markers (path, c->m, c->n);
+   snprintf (path, sizeof (path), "binData/sys_E_%06d(%03d).bin", c->sys_num, 0);
+   write_mesh (path, c->head_E, c->E, c->nodes);
+   snprintf (path, sizeof (path), "binData/sys_H_%06d(%03d).bin", c->sys_num, 0);
+   write_mesh (path, c->head_H, c->H, c->nodes);
+   snprintf (path, sizeof (path), "binData/sys_prtn_%06d.bin", c->sys_num);
+   copy_file (c->prtn_src, path);
+   snprintf (path, sizeof (path), "binData/sys_%06d.txt", c->sys_num);
+   FILE *fp = open_or_die (path, "wt");
+   fprintf (fp, "@ %.14e    time.\n", c->time);
    fprintf (fp, "@ %d       cpus total.\n", 1);
-   fprintf (fp, "@ %d       file map id.\n", map_id);
-   fprintf (fp, "That is checkpoint (record of the full system state) #%d.\n", rec->sys_num);
+   fprintf (fp, "@ %d       file map id.\n", c->map_id);
+   fprintf (fp, "That is checkpoint (record of the full system state) #%d.\n", c->sys_num);
    fclose (fp);
-   rec->sys_num++;
    fp = open_or_die ("binData/sys.N", "wt");
-   fprintf (fp, "@ %d\t  system check-point records written.\n", rec->sys_num);
+   fprintf (fp, "@ %d\t  system check-point records written.\n", c->sys_num + 1);
    fclose (fp);
-   free (E);
-   free (H);
-   free (m);
+   return NULL;
+}
+
+static void ckpt_join (ckpt_t *c)
+{
+   if (c->active) {
+      pthread_join (c->th, NULL);
+      c->active = 0;
+   }
+}
+
+static void checkpoint (ckpt_t *c, mg_run_t *run, records_t *rec, const domain_t *dom, long nodes,
+                        double time)
+{
+   ckpt_join (c);
+   long long live = 0;
+   check (mg_run_marker_count (run, &live), "marker count");
+   if (!c->E) {
+      c->E = (double *) mg_host_alloc (sizeof (double)*3*nodes);
+      c->H = (double *) mg_host_alloc (sizeof (double)*3*nodes);
+      if (!c->E || !c->H)
+         die ("%s", "no pinned host memory for the checkpoint buffers");
+   }
+   if (live > c->cap) {
+      mg_host_free (c->m);
+      c->cap = live + 1;
+      c->m = (mg_marker_t *) mg_host_alloc (sizeof (mg_marker_t)*c->cap);
+      if (!c->m)
+         die ("%s", "no pinned host memory for the checkpoint markers");
+   }
+   check (mg_run_snapshot (run, c->E, c->H, c->m, c->cap, &c->n), "checkpoint snapshot");
+   write_domain (dom);
+   c->map_id = save_filemap (rec, dom);
+   c->run = run;
+   c->nodes = nodes;
+   c->sys_num = rec->sys_num++;
+   c->time = time;
+   memcpy (c->head_E, rec->head_E, HEADER_BYTES);
+   memcpy (c->head_H, rec->head_H, HEADER_BYTES);
+   memcpy (c->prtn_src, rec->prtn_src, sizeof (c->prtn_src));
+   if (pthread_create (&c->th, NULL, ckpt_write, c) != 0)
+      die ("%s", "cannot start the checkpoint writer");
+   c->active = 1;
+}
+
+static void ckpt_free (ckpt_t *c)
+{
+   ckpt_join (c);
+   mg_host_free (c->E);
+   mg_host_free (c->H);
+   mg_host_free (c->m);
 }
 
 /* main_throwStopFlag / main_catchStopFlag (core/main.c:120-189): the first
@@ -1114,6 +1171,8 @@ int main (int argc, char **argv)
    double rows[6*256];
    const double t_loop = now ();
    double last_saved = -1;
+   ckpt_t ckpt;
+   memset (&ckpt, 0, sizeof (ckpt));
    int stop = 0, t = 0;
    while (t < cfg.total && !stop) {
       /* Advance to the next checkpoint, stop-flag check or the end. */
@@ -1155,7 +1214,7 @@ int main (int argc, char **argv)
             die ("%s", "nan detected in the energies");
       }
       if (t % cfg.full == 0) {
-         checkpoint (run, &rec, &dom, nodes, time);
+         checkpoint (&ckpt, run, &rec, &dom, nodes, time);
          diag_flush (&diag, &fresh_diag, dom.tau);
          last_saved = time;
       }
@@ -1168,8 +1227,9 @@ int main (int argc, char **argv)
    printf ("main: main loop have taken %f sec.\n", loop);
    if (last_saved != time) {
       printf ("Additional check-point to save the final state.\n");
-      checkpoint (run, &rec, &dom, nodes, time);
+      checkpoint (&ckpt, run, &rec, &dom, nodes, time);
    }
+   ckpt_free (&ckpt);
    diag_flush (&diag, &fresh_diag, dom.tau);
    free (diag.rows);
    check (mg_run_destroy (run), "destroy run");

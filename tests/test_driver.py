@@ -209,3 +209,30 @@ def test_driver_writes_the_reference_tecplot_records():
             assert np.array_equal(t["ids"], g["ids%d" % num])
     finally:
         shutil.rmtree(root, ignore_errors=True)
+
+
+@pytest.mark.gpu
+def test_snapshot_is_the_state_at_its_step():
+    """mg_run_snapshot: the copy equals mg_run_get_fields / get_markers at the
+    step it was taken, however many steps run before it is read."""
+    import mandor3_b200 as mg
+    root = tempfile.mkdtemp(prefix="mg_drv_")
+    try:
+        n, h, tau, m0, E0, H0 = prepare(root)
+    finally:
+        shutil.rmtree(root, ignore_errors=True)
+    for prec in (mg.FP64, mg.FP32_OFFSET):
+        r = mg.Run(n, h, tau, CASE["bc_min"], CASE["bc_max"], precision=prec)
+        r.set_fields(E0, H0)
+        r.set_markers(m0)
+        r.init()
+        r.step(3)
+        E, H = r.fields()
+        m = r.markers()
+        wait = r.snapshot()
+        r.step(5)
+        Es, Hs, ms = wait()
+        assert np.array_equal(Es, E) and np.array_equal(Hs, H)
+        assert np.array_equal(np.sort(ms, order="id"), np.sort(m, order="id"))
+        assert not np.array_equal(r.fields()[0], E)
+        r.close()
