@@ -328,6 +328,30 @@ typedef struct {
 int  mg_run_df_uniform (mg_run_t *run, long long first, long long count, const mg_df_uniform_t *df);
 int  mg_run_shift_velocity (mg_run_t *run, long long first, long long count, const double dv[3]);
 
+/* ---- focused-laser soft sources (scpic/em_mirror.c, scpic/em_sources.c) ----
+ * Replaces init_sources / add_H_sources / add_E_sources (scpic/em_sources.c,
+ * called from core/em.c:126, 208).  A mirror as setup.out's [focused laser]
+ * tag leaves it in .EM_sources/laser/mirror_NN: its nine "@" doubles in the
+ * file's order (amplitude: < 0 e E/(m w c), > 0 intensity [W/cm^2]; f-number;
+ * focus x, y, z [micron]; duration [fs]; arrival at the focus [fs]; phase;
+ * radius ratio), the direction (> 0: +x), and its E and H profiles over the
+ * x-plane nodes j, k in [5, n - 5] ((n1-9)(n2-9) records of {y_cos, y_sin,
+ * z_cos, z_sin}, j-major); r0 and t0 are units (mc_r0) and units (mc_t0)
+ * (binData/units.bin doubles 0 and 2).  After the H step (after TF/SF) the
+ * H plane i = 5 (backward n0 - 4) gets Hy += a (z_cos cos p + z_sin sin p),
+ * Hz += a (y_cos cos p + y_sin sin p) of the E profile at t, after the E
+ * step the E plane i = 4 (backward n0 - 4) the same of the H profile at
+ * t + tau/2, with a = exp (-(2 t'/dt)^2) tau/h1, p = 2 pi t' + phi0 and
+ * t' = t - T0 + delay, all converted as scpic/em_mirror.c:292-332 does.   */
+typedef struct {
+   double values[9];
+   int    direction;
+   double r0, t0;
+   const double *E, *H;
+} mg_mirror_t;
+int  mg_run_add_mirror (mg_run_t *run, const mg_mirror_t *mirror);
+int  mg_run_clear_mirrors (mg_run_t *run);
+
 /* ---- hard gauss-spot source (core/em_gaussSpot.c:31-156) -----------------
  * The fields of .gaussSpot.cfg (written by setup/tag_gaussSpot.c:126-140),
  * in its order.  After every E step (em_EStep_finish, core/em.c:216, at time

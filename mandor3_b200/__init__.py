@@ -67,6 +67,12 @@ class Tfsf(C.Structure):
                 ("open", (C.c_int * 3) * 2), ("frames", C.c_int), ("ring", C.c_int)]
 
 
+class Mirror(C.Structure):
+    """mg_mirror_t: a focused-laser mirror file's values, direction, units and profiles."""
+    _fields_ = [("values", C.c_double * 9), ("direction", C.c_int), ("r0", C.c_double),
+                ("t0", C.c_double), ("E", C.c_void_p), ("H", C.c_void_p)]
+
+
 class TwoStream(C.Structure):
     _fields_ = [("gamma", C.c_double), ("qDivM", C.c_double), ("n", C.c_int * 3), ("m", C.c_int * 3),
                 ("L", C.c_double * 3), ("id0", C.c_int)]
@@ -153,6 +159,8 @@ def load():
         "mg_run_set_tfsf": [vp, vp],
         "mg_run_snapshot": [vp, vp, vp, vp, C.c_longlong, vp],
         "mg_run_snapshot_wait": [vp],
+        "mg_run_add_mirror": [vp, vp],
+        "mg_run_clear_mirrors": [vp],
         "mg_run_place_two_stream": [vp, vp],
         "mg_run_df_uniform": [vp, C.c_longlong, C.c_longlong, vp],
         "mg_run_shift_velocity": [vp, C.c_longlong, C.c_longlong, vp],
@@ -334,6 +342,18 @@ class Run:
             _check(load().mg_run_snapshot_wait(self.ptr))
             return E, H, m[:n.value]
         return wait
+
+    def add_mirror(self, values, direction, r0, t0, E, H):
+        """Focused-laser mirror (mg_run_add_mirror): the nine values and the
+        direction of a mirror file, units r0 and t0, and its E and H profiles
+        ((n1-9)(n2-9), 4) doubles."""
+        E, H = _f8(E), _f8(H)
+        s = Mirror((C.c_double * 9)(*[float(v) for v in values]), int(direction), float(r0), float(t0),
+                   E.ctypes.data, H.ctypes.data)
+        _check(load().mg_run_add_mirror(self.ptr, C.byref(s)))
+
+    def clear_mirrors(self):
+        _check(load().mg_run_clear_mirrors(self.ptr))
 
     def place_two_stream(self, gamma, qDivM, n, m, L, id0=1):
         """[DF:two-stream] markers (mg_run_place_two_stream)."""

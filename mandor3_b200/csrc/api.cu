@@ -467,6 +467,10 @@ extern "C" int mg_run_destroy (mg_run_t *r)
    if (r->probe_ptrs) cudaFree (r->probe_ptrs);
    mg_tfsf_free (r);
    free_snapshot (r);
+   for (int q = 0 ; q < r->nmirrors ; ++q) {
+      cudaFree (r->mirrors[q].E);
+      cudaFree (r->mirrors[q].H);
+   }
    for (int q = 0 ; q < 2 ; ++q)
       if (r->gauss_rho[q]) cudaFree (r->gauss_rho[q]);
    if (r->gauss_out) cudaFree (r->gauss_out);
@@ -732,6 +736,69 @@ extern "C" int mg_run_snapshot (mg_run_t *r, double *E, double *H, mg_marker_t *
    r->snap_pending = 1;
    if (n)
       *n = got;
+   return MG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Focused-laser mirrors (scpic/em_mirror.c, scpic/em_sources.c).
+// ---------------------------------------------------------------------------
+extern "C" int mg_run_add_mirror (mg_run_t *r, const mg_mirror_t *s)
+{
+   CHECK_RUN (r);
+   if (!s || !s->E || !s->H || !(s->r0 > 0) || !(s->t0 > 0) || !(s->values[5] > 0)) {
+      mg_set_error ("mg_run_add_mirror: need the profiles, units and a positive duration");
+      return MG_ERR_ARG;
+   }
+   if (r->nmirrors >= MG_MIRRORS) {
+      mg_set_error ("mg_run_add_mirror: at most %d mirrors", MG_MIRRORS);
+      return MG_ERR_ARG;
+   }
+   if (r->g.n[1] < 10 || r->g.n[2] < 10) {
+      mg_set_error ("mg_run_add_mirror: the source plane needs at least 10 cells along y and z");
+      return MG_ERR_ARG;
+   }
+   // read_mirror_parameters (scpic/em_mirror.c:292-332), the values the play
+   // needs; the backward delay subtracts the focus from the cell count, as
+   // the reference does (:330).
+   const double pi = 3.141592653589793238462643;
+   const double e = 4.8032e-10, c = 2.9979e+10, m = 9.1094e-28, wpc = 1e7;   // misc_units.h:34-38
+   const double *v = s->values;
+   double A = v[0];
+   if (A > 0)
+      A = s->r0*e*sqrt (8*pi*A*wpc/c)/(m*c*c);
+   else
+      A *= (-2*pi);
+   const double xf = v[2]*1e-4/s->r0;
+   double dt = v[5]*1e-15/s->t0;
+   const double T0 = v[6]*1e-15/s->t0;
+   dt *= sqrt (2.0/log (2));
+   MirrorDev d;
+   d.A = A;
+   d.dt = dt;
+   d.T0 = T0;
+   d.phi0 = v[7];
+   d.forward = s->direction > 0;
+   d.delay = d.forward ? xf - 5*r->g.h[0] : r->g.n[0] - 5*r->g.h[0] - xf;
+   const size_t bytes = sizeof (double)*4*(size_t) (r->g.n[1] - 9)*(r->g.n[2] - 9);
+   d.E = d.H = nullptr;
+   TRY (mg_dev_alloc (r, (void **) &d.E, bytes));
+   TRY (mg_dev_alloc (r, (void **) &d.H, bytes));
+   MG_CUDA (cudaMemcpy (d.E, s->E, bytes, cudaMemcpyHostToDevice));
+   MG_CUDA (cudaMemcpy (d.H, s->H, bytes, cudaMemcpyHostToDevice));
+   r->mirrors[r->nmirrors++] = d;
+   mg_drop_graphs (r);
+   return MG_OK;
+}
+
+extern "C" int mg_run_clear_mirrors (mg_run_t *r)
+{
+   CHECK_RUN (r);
+   for (int q = 0 ; q < r->nmirrors ; ++q) {
+      cudaFree (r->mirrors[q].E);
+      cudaFree (r->mirrors[q].H);
+   }
+   r->nmirrors = 0;
+   mg_drop_graphs (r);
    return MG_OK;
 }
 

@@ -699,6 +699,32 @@ __global__ void k_gauss_spot (Grid g, T *Ey, T *Ez, GaussSpot s, const DevScalar
    Ez[o] = (T) (s.ez*cos (s.omega*t)*f*exp (-dy*dy - dz_*dz_));
 }
 
+// Focused-laser soft source of one mirror (add_source with add_mirror_H /
+// add_mirror_E, scpic/em_mirror.c:667-717): the H plane i = 5 (backward
+// n0 - 4) takes the E profile at t, the E plane i = 4 (backward n0 - 4) the
+// H profile at t + tau/2, over j, k in [5, n - 5]:
+//   Fy += a (z_cos cos p + z_sin sin p), Fz += a (y_cos cos p + y_sin sin p),
+//   a = exp (-(2 t'/dt)^2) tau/h1, p = 2 pi t' + phi0, t' = t - T0 + delay,
+// in FP64 whatever the field type.
+template <typename T>
+__global__ void k_mirror (Grid g, T *Fy, T *Fz, MirrorDev m, int is_e, const DevScalars *dsc)
+{
+   const int nk = g.n[2] - 9, nj = g.n[1] - 9;
+   const int q = blockIdx.x*blockDim.x + threadIdx.x;
+   if (q >= nj*nk)
+      return;
+   const int j = 5 + q/nk, k = 5 + q % nk;
+   const double t = dsc->time + (is_e ? 0.5*g.tau : 0.0) - m.T0 + m.delay;
+   const double x = 2*t/m.dt, ampl = exp (-(x*x));   // pow (x, 2) of the reference, exactly
+   const double ph = 2*3.141592653589793238462643*t + m.phi0;
+   const double cs = cos (ph), sn = sin (ph), A = ampl*g.tau/g.h[0];
+   const int I = m.forward ? (is_e ? 4 : 5) : g.n[0] - 5 + 1;
+   const double *w = (is_e ? m.H : m.E) + 4*(long) q;
+   const long o = g.at (I, j, k);
+   Fy[o] = (T) ((double) Fy[o] + A*(w[2]*cs + w[3]*sn));
+   Fz[o] = (T) ((double) Fz[o] + A*(w[0]*cs + w[1]*sn));
+}
+
 // The field arrays of one precision form.
 template <typename T>
 struct FS {
@@ -774,6 +800,19 @@ static int launch_e_walls (mg_run_t *r, const FS<T> &fs, int sub_j)
       wall_ops (g, ea, op0, op1);
       k_e_walls<<<B, NT, 0, r->stream>>> (g, f3 (fs.E), f3 (fs.J), w, op0, op1, fs.mur[0][ea],
                                          fs.mur[1][ea], alpha, sub_j);
+      MG_LAUNCH_CHECK ();
+   }
+   return MG_OK;
+}
+
+template <typename T>
+static int launch_mirrors (mg_run_t *r, const FS<T> &fs, int is_e)
+{
+   const long nodes = (long) (r->g.n[1] - 9)*(r->g.n[2] - 9);
+   const int NT = 256, B = (int) ((nodes + NT - 1)/NT);
+   for (int q = 0 ; q < r->nmirrors ; ++q) {
+      k_mirror<T><<<B, NT, 0, r->stream>>> (r->g, is_e ? fs.E[1] : fs.H[1], is_e ? fs.E[2] : fs.H[2],
+                                            r->mirrors[q], is_e, r->dsc);
       MG_LAUNCH_CHECK ();
    }
    return MG_OK;
@@ -884,6 +923,7 @@ template <typename T>
 int fields_h_step (mg_run_t *r, const FS<T> &fs)
 {
    TRY_MG (mg_tfsf_h (r));
+   TRY_MG (launch_mirrors<T> (r, fs, 0));
    TRY_MG (launch_laser<T> (r, fs, 0));
    const Grid &g = r->g;
    for (int ea = 0 ; ea < 3 ; ++ea) {
@@ -911,6 +951,7 @@ int fields_h_both (mg_run_t *r, const FS<T> &fs)
       energy_pick (g), r->dsc);
    MG_LAUNCH_CHECK ();
    TRY_MG (mg_tfsf_h (r));
+   TRY_MG (launch_mirrors<T> (r, fs, 0));
    TRY_MG (launch_laser<T> (r, fs, 0));
    return launch_h_walls<T> (r, fs, 1);
 }
@@ -960,6 +1001,7 @@ template <typename T>
 int fields_e_finish (mg_run_t *r, const FS<T> &fs)
 {
    TRY_MG (mg_tfsf_e (r));
+   TRY_MG (launch_mirrors<T> (r, fs, 1));
    TRY_MG (launch_laser<T> (r, fs, 1));
    const int lo[3] = {-1, -1, -1};
    const int hi[3] = {r->g.n[0] + 1, r->g.n[1] + 1, r->g.n[2] + 1};
@@ -973,12 +1015,12 @@ int fields_e_finish (mg_run_t *r, const FS<T> &fs)
 // Graph path: E += curl H - tau J in one pass away from the rim, E walls,
 // source, then -tau J on the rim.  Bit-identical to the stage path: every
 // node sees the same operations in the same order.  Needs the J walls done.
-// A playing TF/SF interface adds to E between the curl and -tau J on its
-// faces, so with one the graph takes the stage path's two passes.
+// A playing TF/SF interface or a focused-laser mirror adds to E between the
+// curl and -tau J, so with one the graph takes the stage path's two passes.
 template <typename T>
 int fields_e_fused (mg_run_t *r, const FS<T> &fs)
 {
-   if (mg_tfsf_playing (r)) {
+   if (mg_tfsf_playing (r) || r->nmirrors > 0) {
       TRY_MG (fields_e_step<T> (r, fs));
       return fields_e_finish<T> (r, fs);
    }

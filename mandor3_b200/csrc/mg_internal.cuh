@@ -80,6 +80,15 @@ struct GaussSpot {
    int    i;               // x-plane
 };
 
+// A focused-laser mirror (scpic/em_mirror.c) as the step plays it: the
+// values read_mirror_parameters derives and the two device profiles.
+struct MirrorDev {
+   double A, dt, T0, delay, phi0;
+   int    forward;
+   double *E, *H;          // (n1-9)(n2-9) x {y_cos, y_sin, z_cos, z_sin}
+};
+#define MG_MIRRORS 8
+
 // Device-side per-run scalars (one small allocation).
 struct DevScalars {
    double time;            // t = n*tau of the step being advanced
@@ -155,6 +164,10 @@ struct mg_run {
    cudaStream_t snap_stream;
    cudaEvent_t snap_ready, snap_done;
    int         snap_pending;
+
+   // focused-laser mirrors (mg_run_add_mirror)
+   int         nmirrors;
+   MirrorDev   mirrors[MG_MIRRORS];
 
    // TF/SF interface (tfsf.cu), null when off
    struct mg_tfsf_state *tfsf;

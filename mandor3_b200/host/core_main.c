@@ -509,6 +509,62 @@ static double micron_units (void)
    return u[11];
 }
 
+/* init_sources (scpic/em_sources.c:37-52): each .EM_sources/laser/mirror_NN
+ * from 00 up to the first missing one read as mirror_source_is_loaded does
+ * (scpic/em_mirror.c:464-486 with read_mirror_parameters, :292-328): the
+ * title and dashes lines, nine "@ double" lines, an "@ int" line, the
+ * dashes line (whose trailing newline directive, as in the reference, also
+ * skips whitespace bytes at the start of the binary part), then the E and H
+ * profiles of the (n1-9)(n2-9) nodes of the source plane; r0 and t0 are the
+ * 1st and 3rd doubles of binData/units.bin. */
+static int load_mirrors (mg_run_t *run, const domain_t *d)
+{
+   double u[3];
+   int count = 0;
+   for (;; ++count) {
+      char name[64];
+      snprintf (name, sizeof (name), ".EM_sources/laser/mirror_%02d", count);
+      FILE *fp = fopen (name, "rb");
+      if (!fp)
+         break;
+      if (count == 0) {
+         FILE *uf = open_or_die ("binData/units.bin", "rb");
+         read_exact (u, sizeof (u), uf, "binData/units.bin");
+         fclose (uf);
+      }
+      mg_mirror_t m;
+      memset (&m, 0, sizeof (m));
+      if (fscanf (fp, "Mirror focused laser beam #%*d\n") < 0)
+         die ("'%s' is truncated", name);
+      if (fscanf (fp, "---------------------------------------\n") < 0)
+         die ("'%s' is truncated", name);
+      for (int q = 0 ; q < 9 ; ++q)
+         if (fscanf (fp, "@ %le %*[^\n] ", &m.values[q]) != 1)
+            die ("%s: cannot get double number", name);
+      char rest[1024];
+      if (fgetc (fp) != '@' || fscanf (fp, "%d", &m.direction) != 1 || !fgets (rest, sizeof (rest), fp))
+         die ("%s: missing required int parameter", name);
+      if (fscanf (fp, "---------------------------------------\n") < 0)
+         die ("'%s' is truncated", name);
+      const long nodes = (long) (d->dmax[1] - 9)*(d->dmax[2] - 9);
+      double *E = (double *) malloc (sizeof (double)*4*nodes);
+      double *H = (double *) malloc (sizeof (double)*4*nodes);
+      if (!E || !H)
+         die ("%s", "no host memory for the mirror profiles");
+      read_exact (E, sizeof (double)*4*nodes, fp, name);
+      read_exact (H, sizeof (double)*4*nodes, fp, name);
+      fclose (fp);
+      m.r0 = u[0];
+      m.t0 = u[2];
+      m.E = E;
+      m.H = H;
+      check (mg_run_add_mirror (run, &m), "mirror source");
+      free (E);
+      free (H);
+   }
+   return count;
+}
+
 /* probe_allocate + probe_touch (core/diag_probe.c:48-100, 121-395) for one
  * rank: old probe files removed unless the run continues, run_probes.cfg
  * read (point / line / rectangle / volume groups up to 'end'), repeated
@@ -1152,6 +1208,7 @@ int main (int argc, char **argv)
       fclose (gs);
       check (mg_run_set_gauss_spot (run, &s), "gauss spot");
    }
+   const int mirrors = load_mirrors (run, &dom);
    tfsf_t tfsf;
    tfsf_open (&tfsf, run, &dom, time);
    probes_t probes;
@@ -1166,6 +1223,8 @@ int main (int argc, char **argv)
 
    printf ("core_b200.out: %lld markers, %d x %d x %d cells, %s, record %d, t = %.6e\n", nm,
            p.n[0], p.n[1], p.n[2], precision == MG_FP64 ? "FP64" : "FP32-offset", point, time);
+   if (mirrors > 0)
+      printf ("core_b200.out: %d focused-laser source(s)\n", mirrors);
    int fresh_diag = !(cfg.cont && point != 0);
    diag_t diag = {NULL, 0, 0};
    double rows[6*256];

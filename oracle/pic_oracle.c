@@ -32,6 +32,9 @@ struct po_run {
    int    has_laser;
    po_gauss_spot_t gspot;
    int    has_gspot;
+   /* focused-laser mirrors */
+   int    nmirror;
+   struct { double A, dt, T0, delay, phi0; int forward; double *E, *H; } mirror[8];
    /* TF/SF interface */
    int    has_tfsf, tfsf_on, tfsf_frame;
    po_tfsf_t tfsf;
@@ -103,6 +106,10 @@ void po_destroy (po_run_t *r)
    free (r->p);
    free (r->frames);
    free (r->rec);
+   for (int q = 0 ; q < r->nmirror ; ++q) {
+      free (r->mirror[q].E);
+      free (r->mirror[q].H);
+   }
    free (r);
 }
 
@@ -799,12 +806,14 @@ void po_em_h_half (po_run_t *r)
 
 static void tfsf_h (po_run_t *r);
 static void tfsf_e (po_run_t *r);
+static void mirrors (po_run_t *r, int is_e);
 
 /* em_HStep (core/em.c:115-131): H^n -> H^(n+1/2) plus source at t = n*tau. */
 void po_em_h_step (po_run_t *r)
 {
    h_advance (r, 0.5);
    tfsf_h (r);
+   mirrors (r, 0);
    if (r->has_laser)
       laser_h (r, r->time);
    h_bc (r);
@@ -858,6 +867,7 @@ static void gauss_spot_e (po_run_t *r, double t)
 void po_em_e_finish (po_run_t *r)
 {
    tfsf_e (r);
+   mirrors (r, 1);
    if (r->has_laser)
       laser_e (r, r->time + 0.5*r->tau);
    e_sub_current (r);
@@ -1032,6 +1042,69 @@ static void tfsf_e (po_run_t *r)
       tfsf_apply (r, 0, tf + 1, 1.0);
    else
       tfsf_apply (r, 0, last - 1 - tf, -1.0);
+}
+
+/* ------------------------------------------------------------------------
+ * Focused-laser soft sources (scpic/em_mirror.c:292-332, 667-717).
+ * ---------------------------------------------------------------------- */
+
+/* read_mirror_parameters (:292-332) for the values the play needs.  The
+ * backward delay subtracts the focus from the cell count n0, not from the
+ * domain length, as the reference does (:330). */
+void po_add_mirror (po_run_t *r, const double v[9], int direction, double r0, double t0,
+                    const double *E, const double *H)
+{
+   if (r->nmirror >= 8)
+      return;
+   const double pi = 3.141592653589793238462643;
+   const double e = 4.8032e-10, c = 2.9979e+10, m = 9.1094e-28, wpc = 1e7;   /* misc_units.h:34-38 */
+   double A = v[0];
+   if (A > 0)
+      A = r0*e*sqrt (8*pi*A*wpc/c)/(m*c*c);
+   else
+      A *= (-2*pi);
+   const double xf = v[2]*1e-4/r0;
+   double dt = v[5]*1e-15/t0;
+   const double T0 = v[6]*1e-15/t0;
+   dt *= sqrt (2.0/log (2));
+   const int q = r->nmirror++;
+   r->mirror[q].A = A;
+   r->mirror[q].dt = dt;
+   r->mirror[q].T0 = T0;
+   r->mirror[q].phi0 = v[7];
+   r->mirror[q].forward = direction > 0;
+   r->mirror[q].delay = r->mirror[q].forward ? xf - 5*r->h[0] : r->n[0] - 5*r->h[0] - xf;
+   const long nodes = (long) (r->n[1] - 9)*(r->n[2] - 9)*4;
+   r->mirror[q].E = (double *) malloc (sizeof (double)*nodes);
+   r->mirror[q].H = (double *) malloc (sizeof (double)*nodes);
+   memcpy (r->mirror[q].E, E, sizeof (double)*nodes);
+   memcpy (r->mirror[q].H, H, sizeof (double)*nodes);
+}
+
+/* add_mirror_H / add_mirror_E with add_source: the H plane i = 5 (backward
+ * n0 - 4) gets the E profile at t, the E plane i = 4 (backward n0 - 4) the
+ * H profile at t + tau/2, over j, k in [5, n - 5]:
+ *   Fy += a (z_cos cos p + z_sin sin p), Fz += a (y_cos cos p + y_sin sin p),
+ *   a = exp (-(2 t'/dt)^2) tau/h1, p = 2 pi t' + phi0, t' = t - T0 + delay. */
+static void mirrors (po_run_t *r, int is_e)
+{
+   const double pi = 3.141592653589793238462643;
+   for (int q = 0 ; q < r->nmirror ; ++q) {
+      const double t = r->time + (is_e ? 0.5*r->tau : 0.0) - r->mirror[q].T0 + r->mirror[q].delay;
+      const double ampl = exp (-pow (2*t/r->mirror[q].dt, 2));
+      const int I = r->mirror[q].forward ? (is_e ? 4 : 5) : r->n[0] - 5 + 1;
+      const double cs = cos (2*pi*t + r->mirror[q].phi0), sn = sin (2*pi*t + r->mirror[q].phi0);
+      const double A = ampl*r->tau/r->h[0];
+      const double *src = is_e ? r->mirror[q].H : r->mirror[q].E;
+      double *Fy = is_e ? r->e[1] : r->b[1], *Fz = is_e ? r->e[2] : r->b[2];
+      const int nk = r->n[2] - 9;
+      for (int j = 5 ; j <= r->n[1] - 5 ; ++j)
+         for (int k = 5 ; k <= r->n[2] - 5 ; ++k) {
+            const double *w = src + 4*((long) (j - 5)*nk + (k - 5));
+            Fy[IX (r, I, j, k)] += A*(w[2]*cs + w[3]*sn);
+            Fz[IX (r, I, j, k)] += A*(w[0]*cs + w[1]*sn);
+         }
+   }
 }
 
 /* One step in core/main.c:353-478 order. */

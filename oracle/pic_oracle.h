@@ -94,6 +94,16 @@ long po_tfsf_faces (const po_run_t *r, int *regions);
 /* Frames recorded so far (record mode), copied to out when out != NULL. */
 long po_tfsf_recorded (const po_run_t *r, double *out);
 
+/* Focused-laser soft source of a parabolic mirror (scpic/em_mirror.c,
+ * scpic/em_sources.c): v = the nine "@" doubles of a .EM_sources/laser
+ * mirror file in its order (amplitude, f-number, focus x, y, z [micron],
+ * duration [fs], arrival [fs], phase, radius ratio), direction = its last
+ * value; r0, t0 = units(mc_r0), units(mc_t0) (binData/units.bin values 0
+ * and 2); E, H = the file's two profiles, (n1-9)(n2-9) records {y_cos,
+ * y_sin, z_cos, z_sin} each, j-major.  Up to 8 mirrors. */
+void po_add_mirror (po_run_t *r, const double v[9], int direction, double r0, double t0,
+                    const double *E, const double *H);
+
 /* em_init / cap_init equivalent: ghost fill and Mur history from E. */
 void po_init (po_run_t *r);
 

@@ -385,11 +385,53 @@ def make_setup_tags():
     print("setup tags: %s" % sorted(out))
 
 
+# The reference's focused-laser soft source (scpic/em_mirror.c): setup.out
+# computes the mirror profiles ([focused laser], setup/tag_laser.c) into
+# .EM_sources/laser/mirror_00, core.out plays them in an empty Mur box;
+# once along +x, once along -x.
+MIRROR_N = (24, 20, 20)
+MIRROR_L_UM = (1.2, 1.0, 1.0)
+MIRROR_STEPS = 40
+
+
+def mirror_deck(direction):
+    from refrun import deck_text
+    text = deck_text(MIRROR_N, MIRROR_L_UM, -0.5, (2, 2, 2), (2, 2, 2))
+    text += ("\n[focused laser]\n@ -1.5\tamplitude\n@ 0.9\tf-number\n@ 0.6\tfocus x\n@ 0.5\tfocus y\n"
+             "@ 0.5\tfocus z\n@ 2.0\tduration fs\n@ 3.0\tarrival fs\n@ 0.3\tphase\n@ 10.0\tratio\n"
+             "@ %d\tdirection\n" % direction)
+    return text
+
+
+def make_mirror():
+    out = {}
+    for direction in (1, -1):
+        rr = RefRun()
+        try:
+            with open(rr.path("deck.input"), "w") as fp:
+                fp.write(mirror_deck(direction))
+            rr._run("setup.out", "deck.input", "create")
+            out["file%d" % direction] = np.frombuffer(open(rr.path(".EM_sources", "laser", "mirror_00"), "rb").read(),
+                                                      np.uint8)
+            out["units%d" % direction] = np.frombuffer(open(rr.path("binData", "units.bin"), "rb").read(), "<f8")
+            dom = refrun.read_domain(rr.path("binData", "domain.bin"))
+            out["h"], out["tau"] = dom["h"], dom["tau"]
+            rr.set_state(np.zeros(0, dtype=oracle_port.MARKER_DTYPE))
+            rr.run(MIRROR_STEPS)
+            _, E, H = rr.final()
+            out["E%d" % direction] = E
+            out["H%d" % direction] = H
+        finally:
+            rr.cleanup()
+    np.savez_compressed(os.path.join(HERE, "mirror.npz"), **out)
+    print("mirror: E max %.3e / %.3e" % (np.abs(out["E1"]).max(), np.abs(out["E-1"]).max()))
+
+
 if __name__ == "__main__":
     if not have_reference():
         sys.exit("reference binaries missing: make -C oracle ref REF=<reference tree>")
     for name in (sys.argv[1:] or list(cases.CASES) + ["gauss_spot", "placers", "tecplot", "probes", "tfsf",
-                                                 "setup_tags"]):
+                                                 "setup_tags", "mirror"]):
         if name == "probes":
             make_probes()
             continue
@@ -398,6 +440,9 @@ if __name__ == "__main__":
             continue
         if name == "setup_tags":
             make_setup_tags()
+            continue
+        if name == "mirror":
+            make_mirror()
             continue
         if name == "tecplot":
             make_tecplot()

@@ -38,6 +38,7 @@ def _load():
     lib.po_step.argtypes = [vp, vp]
     lib.po_step_probes.argtypes = [vp, vp, C.c_int, vp, vp]
     lib.po_fields_n.argtypes = [vp, vp, vp]
+    lib.po_add_mirror.argtypes = [vp, vp, C.c_int, C.c_double, C.c_double, vp, vp]
     lib.po_set_tfsf.restype = C.c_int
     lib.po_set_tfsf.argtypes = [vp, vp, vp]
     lib.po_tfsf_faces.restype = C.c_long
@@ -187,6 +188,13 @@ class OracleRun:
             lib().po_step_probes(self.ptr, a.ctypes.data, len(a), out[s].ctypes.data,
                                  np.zeros(5).ctypes.data)
         return out
+
+    def add_mirror(self, values, direction, r0, t0, E, H):
+        """Focused-laser mirror from a .EM_sources/laser file's values and profiles."""
+        v = np.ascontiguousarray(values, dtype="<f8")
+        self._mirrors = getattr(self, "_mirrors", []) + [(np.ascontiguousarray(E, "<f8"), np.ascontiguousarray(H, "<f8"))]
+        e, h = self._mirrors[-1]
+        lib().po_add_mirror(self.ptr, v.ctypes.data, int(direction), float(r0), float(t0), e.ctypes.data, h.ctypes.data)
 
     def fields_n(self):
         """E^n and H^n of the coming step over [0, n]^3 (state unchanged)."""

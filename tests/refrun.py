@@ -122,6 +122,47 @@ def read_tfsf_stream(raw):
     return head, np.frombuffer(raw[44:], "<f8").reshape(-1, vol)
 
 
+_WS = b" \t\n\r\x0b\x0c"
+
+
+def read_mirror(raw, n):
+    """A focused-laser mirror file (scpic/em_mirror.c:393-481) as core.out
+    reads it: the title and dashes lines, nine "@ double" lines, one
+    "@ int" line, the dashes line -- each fscanf whitespace directive also
+    skipping the whitespace that follows -- then the E and H profiles,
+    (n1-9)(n2-9) records of {y_cos, y_sin, z_cos, z_sin}.  Returns (nine
+    values, direction, E (nodes, 4), H (nodes, 4))."""
+    raw = bytes(raw)
+    pos = 0
+
+    def skip_ws(p):
+        while p < len(raw) and raw[p:p + 1] in _WS:
+            p += 1
+        return p
+    title = b"Mirror focused laser beam #"
+    assert raw.startswith(title)
+    pos = raw.index(b"\n") 
+    pos = skip_ws(pos)
+    dashes = b"-" * 39
+    assert raw[pos:pos + 39] == dashes
+    pos = skip_ws(pos + 39)
+    vals = []
+    for _ in range(9):
+        assert raw[pos:pos + 1] == b"@"
+        end = raw.index(b"\n", pos)
+        vals.append(float(raw[pos + 1:end].split()[0]))
+        pos = skip_ws(end)
+    assert raw[pos:pos + 1] == b"@"
+    end = raw.index(b"\n", pos)
+    direction = int(raw[pos + 1:end].split()[0])
+    pos = end + 1
+    assert raw[pos:pos + 39] == dashes
+    pos = skip_ws(pos + 39)
+    nodes = (n[1] - 9) * (n[2] - 9)
+    data = np.frombuffer(raw[pos:pos + 2 * nodes * 32], "<f8").reshape(2, nodes, 4)
+    return vals, direction, data[0], data[1]
+
+
 def read_chunks(raw):
     """A chunk file (type_CFile.c:112-370): the magic, then chunks of
     {INT64 size with header, int deleted, int name length, '\\n', name,
