@@ -436,6 +436,11 @@ __device__ __forceinline__ void cp_async_wait1 ()
    asm volatile ("cp.async.wait_group 1;" ::: "memory");
 }
 
+__device__ __forceinline__ void cp_async_wait_all ()
+{
+   asm volatile ("cp.async.wait_all;" ::: "memory");
+}
+
 // Starts the copy of marker n's nine pushed arrays into buffer b (the lane's
 // column of the warp's staging area); n < 0: nothing to copy.
 __device__ __forceinline__ void stage_marker (float *b, int lane, const Markers32 &m, int n)
@@ -513,7 +518,7 @@ __device__ __forceinline__ void scatter_s (int *Jt, int q, const float w[12], fl
    }
 }
 
-template <int TX, int TY, int TZ, int ROUNDS, bool PER>
+template <int TX, int TY, int TZ, int GROUP, bool PER>
 __global__ void __launch_bounds__ (256, 3)
 k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, DevScalars *dsc)
 {
@@ -528,6 +533,7 @@ k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, De
    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
    const int soff = lane < 12 ? slot_offset<D> (lane) : 0;
    const float rmax = 1.125f*dsc->rho_max;
+   const float vol = (float) c.vol;
    double Wx = 0, Wy = 0, Wz = 0;
    long long dead = 0;
 
@@ -542,19 +548,22 @@ k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, De
       if (mb < me) {
          const int x0 = (t/(nty*ntz))*TX, y0 = ((t/ntz) % nty)*TY, z0 = (t % ntz)*TZ;
 
-         // Stage E and H nodes [x0-1, x0+TX+3) x ... (inside the ghost layers).
+         // Stage E and H nodes [x0-1, x0+TX+3) x ... (inside the ghost layers),
+         // all copies in flight at once.
          for (int q = threadIdx.x ; q < 6*D::FN ; q += blockDim.x) {
             const int comp = q/D::FN, rem = q - comp*D::FN;
             const int a = rem/D::FYZ, r2 = rem - a*D::FYZ, b = r2/D::FZ, cc = r2 - b*D::FZ;
             const int gi = x0 - 1 + a, gj = y0 - 1 + b, gk = z0 - 1 + cc;
-            float v = 0.0f;
             if (gi <= g.n[0] + MG_GX && gj <= g.n[1] + MG_GX && gk <= g.n[2] + MG_GX) {
                const float *src = comp == 0 ? c.E0 : comp == 1 ? c.E1 : comp == 2 ? c.E2
                                 : comp == 3 ? c.H0 : comp == 4 ? c.H1 : c.H2;
-               v = __ldg (src + g.at (gi, gj, gk));
+               cp_async4 (F + q, src + g.at (gi, gj, gk));
+            } else {
+               F[q] = 0.0f;
             }
-            F[q] = v;
          }
+         cp_async_commit ();
+         cp_async_wait_all ();
 
          for (int cb = mb ; cb < me ; cb += MG_TILE_CHUNK) {
             const int ce = min (cb + MG_TILE_CHUNK, me);
@@ -635,7 +644,7 @@ k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, De
                   const float p2 = px*px + py*py + pz*pz;
                   const float rg = rsqrtf (1.0f + p2);
                   const float gamma = (1.0f + p2)*rg;
-                  const float W = __fdividef (p2, (gamma + 1.0f)*(p2 + 1e-19f))*rho*(float) c.vol/qm;
+                  const float W = __fdividef (p2, (gamma + 1.0f)*(p2 + 1e-19f))*rho*vol/qm;
                   Wx += (double) (W*px*px);
                   Wy += (double) (W*py*py);
                   Wz += (double) (W*pz*pz);
@@ -730,10 +739,11 @@ k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, De
                   }
                }
 
-               // First segment: the weights of lanes that share a cell are
-               // summed across the warp (redux.sync, one per weight) and lane q
-               // adds weight q, for up to ROUNDS cells per warp; the remaining
-               // lanes add their own.
+               // First segment: lanes are grouped by cell (match.any); a group
+               // of at least GROUP lanes sums its weights across the warp
+               // (redux.sync, one per weight) and lane q adds weight q; lanes
+               // of smaller groups (markers that left the cell they were
+               // sorted into) add their own.
                float wgt[12];
                if (valid)
                   weights32 (c, rho, ox, ox + ta*dx, oy, oy + ta*dy, oz, oz + ta*dz, wgt);
@@ -746,10 +756,12 @@ k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, De
 #pragma unroll
                for (int q = 0 ; q < 12 ; ++q)
                   fx[q] = key >= 0 ? fixed (wgt[q], S) : 0;
-               unsigned pend = __ballot_sync (0xffffffffu, key >= 0);
+               const unsigned grp = __match_any_sync (0xffffffffu, key);
+               const bool alone = key >= 0 && __popc (grp) < GROUP;
+               unsigned heads = __ballot_sync (0xffffffffu, key >= 0 && !alone && (grp & ((1u << lane) - 1)) == 0);
 #pragma unroll 1
-               for (int round = 0 ; pend && round < ROUNDS ; ++round) {
-                  const int k0 = __shfl_sync (0xffffffffu, key, __ffs (pend) - 1);
+               while (heads) {
+                  const int k0 = __shfl_sync (0xffffffffu, key, __ffs (heads) - 1);
                   const bool mine = (key == k0);
                   int sum = 0;
 #pragma unroll
@@ -759,9 +771,9 @@ k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, De
                   }
                   if (lane < 12 && sum)
                      atomicAdd (Jt + k0 + soff, sum);
-                  pend &= ~__ballot_sync (0xffffffffu, mine);
+                  heads &= heads - 1;
                }
-               if ((pend >> lane) & 1) {
+               if (alone) {
 #pragma unroll
                   for (int q = 0 ; q < 12 ; ++q)
                      atomicAdd (Jt + key + slot_offset<D> (q), fx[q]);
@@ -793,8 +805,11 @@ k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, De
 
 } // namespace
 
-#ifndef MG_TILE_ROUNDS
-#define MG_TILE_ROUNDS 3
+// Smallest group of lanes in one cell whose first-segment weights are summed
+// across the warp (measured on the 128^3 two-stream plasma, 64 markers per
+// cell: 8 beats 3, 5, 12 and 16 lanes, and three rounds by first lane).
+#ifndef MG_TILE_GROUP
+#define MG_TILE_GROUP 8
 #endif
 
 #define TRY32(x)                                                             \
@@ -810,8 +825,8 @@ template <int TX, int TY, int TZ>
 static int launch_tiles (mg_run_t *r, const Ctx32 &c, bool per)
 {
    using D = TileDims<TX, TY, TZ>;
-   auto kp = k_push32_tiles<TX, TY, TZ, MG_TILE_ROUNDS, true>;
-   auto kn = k_push32_tiles<TX, TY, TZ, MG_TILE_ROUNDS, false>;
+   auto kp = k_push32_tiles<TX, TY, TZ, MG_TILE_GROUP, true>;
+   auto kn = k_push32_tiles<TX, TY, TZ, MG_TILE_GROUP, false>;
    static int attr_dev = -1;
    static int per_sm = 1, sms = 148;
    if (attr_dev != r->device) {
