@@ -391,9 +391,12 @@ extern "C" int mg_run_create (const mg_params_t *params, mg_run_t **out)
          r->tiles[a] = (params->n[a] + T[a] - 1)/T[a];
          r->ntiles *= r->tiles[a];
       }
-      rc = mg_dev_alloc (r, (void **) &r->tile_start, sizeof (int)*(r->ntiles + 2));
-      if (rc == MG_OK)
-         cudaMemsetAsync (r->tile_start, 0, sizeof (int)*(r->ntiles + 2), r->stream);
+      const size_t tb = sizeof (int)*(2*(size_t) r->ntiles + 4);
+      rc = mg_dev_alloc (r, (void **) &r->tile_start, tb);
+      if (rc == MG_OK) {
+         cudaMemsetAsync (r->tile_start, 0, tb, r->stream);
+         r->tile_list = r->tile_start + r->ntiles + 2;
+      }
    }
    if (rc == MG_OK) rc = mg_dev_alloc (r, (void **) &r->dsc, sizeof (DevScalars));
    if (rc == MG_OK) rc = mg_dev_alloc (r, (void **) &r->ring, sizeof (double)*6*MG_RING);
@@ -580,6 +583,7 @@ extern "C" int mg_run_set_markers (mg_run_t *r, const mg_marker_t *m, long long 
       MG_LAUNCH_CHECK ();
    }
    r->np = n;
+   r->tiles_ok = 0;
    MG_CUDA (cudaMemsetAsync (&r->dsc->dead, 0, sizeof (long long), r->stream));
    MG_CUDA (cudaStreamSynchronize (r->stream));
    return MG_OK;
@@ -1551,5 +1555,6 @@ extern "C" int mg_run_place_uniform (mg_run_t *r, const mg_place_t *s)
    }
    r->np += count;
    r->inited = 0;
+   r->tiles_ok = 0;
    return MG_OK;
 }

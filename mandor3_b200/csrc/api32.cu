@@ -286,6 +286,15 @@ __global__ void k_tile_start (const long long *offset, int ntiles, int lc, int *
       tile_start[t] = (int) offset[t <= ntiles ? (long long) t << lc : ((long long) ntiles << lc) + 1];
 }
 
+// The tiles that hold markers, appended to list (count in list[ntiles],
+// zero on entry); the pushes hand out only these.
+__global__ void k_tile_list (const long long *offset, int ntiles, int lc, int *list)
+{
+   for (int t = blockIdx.x*blockDim.x + threadIdx.x ; t < ntiles ; t += gridDim.x*blockDim.x)
+      if (offset[(long long) (t + 1) << lc] > offset[(long long) t << lc])
+         list[atomicAdd (list + ntiles, 1)] = t;
+}
+
 // Moves every marker to its place in the other buffer set: the first free
 // slot of its key (a run of equal keys in a warp takes consecutive slots);
 // fill counts the slots taken per key.
@@ -622,6 +631,18 @@ void mg_convert64to32 (mg_run_t *r, const Markers64 &v, long long c, long long a
    k_convert<<<mg_blocks_for (c, 256, 8), 256, 0, r->stream>>> (r->g, v, c, r->m32, at);
 }
 
+// tile_start and tile_list of a run from the exclusive scan of its sort
+// keys (lc: log2 of the cells per tile).
+int mg_tile_list (mg_run_t *r, const long long *offset, int lc)
+{
+   const int T = 256;
+   k_tile_start<<<mg_blocks_for (r->ntiles + 2, T, 8), T, 0, r->stream>>> (offset, r->ntiles, lc, r->tile_start);
+   MG_CUDA (cudaMemsetAsync (r->tile_list + r->ntiles, 0, sizeof (int), r->stream));
+   k_tile_list<<<mg_blocks_for (r->ntiles, T, 8), T, 0, r->stream>>> (offset, r->ntiles, lc, r->tile_list);
+   MG_LAUNCH_CHECK ();
+   return MG_OK;
+}
+
 // Sorts the markers by tile and cell into the other buffer set and makes
 // that set current; removed markers go to the end.
 // Exclusive scan of the len counters (spread layout, kp keys per region)
@@ -640,7 +661,7 @@ int mg_scan_counts (mg_run_t *r, const int *count, long long kp, long long len, 
 int mg_sort32 (mg_run_t *r)
 {
    if (r->np == 0) {
-      MG_CUDA (cudaMemsetAsync (r->tile_start, 0, sizeof (int)*(r->ntiles + 2), r->stream));
+      MG_CUDA (cudaMemsetAsync (r->tile_start, 0, sizeof (int)*(2*(size_t) r->ntiles + 4), r->stream));
       r->tiles_ok = 1;
       r->steps_since_sort = 0;
       return MG_OK;
@@ -679,7 +700,7 @@ int mg_sort32 (mg_run_t *r)
    k_scan_blocks<<<nb, 256, 0, r->stream>>> (count, kp, cells, bsum);
    k_scan_sums<<<1, 1024, 0, r->stream>>> (bsum, nb);
    k_scan_apply<<<nb, 256, 0, r->stream>>> (count, kp, cells, bsum, offset);
-   k_tile_start<<<mg_blocks_for (r->ntiles + 2, T, 8), T, 0, r->stream>>> (offset, r->ntiles, tk.lc, r->tile_start);
+   TRY32 (mg_tile_list (r, offset, tk.lc));
    // The counters become the per-key fill counts of the scatter.
    MG_CUDA (cudaMemsetAsync (count, 0, (size_t) kp*8*4, r->stream));
    k_scatter<<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (tk, r->m32, r->m32b, r->np, offset, count, kp);

@@ -143,6 +143,8 @@ struct mg_run {
                            // tile t holds [tile_start[t], tile_start[t+1]),
                            // then the markers outside the mesh, then the
                            // removed ones
+   int       *tile_list;   // ntiles + 1: the tiles holding markers, then
+                           // their count (after tile_start, same allocation)
    int        tiles_ok;    // tile_start describes the marker order
 
    // scalars and energy ring
@@ -243,6 +245,7 @@ int mg_push64 (mg_run_t *r);
 int mg_gauss_rho (mg_run_t *r, double *rho);
 int mg_probes_enqueue (mg_run_t *r);
 int mg_sort64 (mg_run_t *r);
+int mg_tile_list (mg_run_t *r, const long long *offset, int lc);
 #define SCAN_CHUNK 4096
 int mg_scan_counts (mg_run_t *r, const int *count, long long kp, long long len, long long *offset,
                     long long *bsum);

@@ -419,6 +419,13 @@ __global__ void k_walls32 (Grid g, Markers32 m, long long np, DevScalars *dsc)
 // 2^-17 at the 16384-marker limit.
 #define MG_TILE_CHUNK 16384
 
+// Fewest markers in a tile for the shared-memory staging of its fields and
+// currents (about 13 staged values per marker at 256 markers of an 8x8x4
+// tile); sparser tiles take the global-memory gather and current sums.
+#ifndef MG_TILE_DENSE
+#define MG_TILE_DENSE 256
+#endif
+
 // Asynchronous 4-byte copies global -> shared (completion per thread).
 __device__ __forceinline__ void cp_async4 (void *sm, const void *gm)
 {
@@ -471,7 +478,10 @@ struct TileDims {
    static constexpr int JYZ = JY*JZ, JN = JX*JYZ;
    // Per warp: two buffers of the nine marker arrays a push reads, 32 lanes each.
    static constexpr int STAGE = 2*9*32;
-   static constexpr size_t BYTES = (6*FN + 3*JN + 8*STAGE)*sizeof (float);
+   // Per warp: a queue of QCAP markers that crossed cell faces, eight words
+   // each (offsets, displacement, weight, packed cell and crossings).
+   static constexpr int QCAP = 40, QUEUE = 8*QCAP;
+   static constexpr size_t BYTES = (6*FN + 3*JN + 8*STAGE + 8*QUEUE)*sizeof (float);
 };
 
 template <int SX, int SY>
@@ -518,9 +528,62 @@ __device__ __forceinline__ void scatter_s (int *Jt, int q, const float w[12], fl
    }
 }
 
+// Segments after the first of a marker that crossed cell faces: the
+// crossing times in increasing order (ties keep the x, y, z order), then one
+// in-cell segment per crossing, into the shared tile (FAST, node jq of the
+// start cell) or into J (cell i, j, k).
+template <class D, bool FAST>
+__device__ __forceinline__ void later_segments (const Ctx32 &c, int *Jt, int jq, float S, int i, int j,
+                                                int k, float ox, float oy, float oz, float dx, float dy,
+                                                float dz, int di, int dj, int dk, float rho)
+{
+   float t0 = 2.0f, t1 = 2.0f, t2 = 2.0f;
+   int a0 = 0, a1 = 1, a2 = 2;
+   if (di) t0 = __fdividef ((di > 0 ? 1.0f : 0.0f) - ox, dx);
+   if (dj) t1 = __fdividef ((dj > 0 ? 1.0f : 0.0f) - oy, dy);
+   if (dk) t2 = __fdividef ((dk > 0 ? 1.0f : 0.0f) - oz, dz);
+   CSWAP (t0, a0, t1, a1);
+   CSWAP (t1, a1, t2, a2);
+   CSWAP (t0, a0, t1, a1);
+   int si = 0, sj = 0, sk = 0;
+   float tb = t0;
+   const int d3[3] = {di, dj, dk};
+   const int ax3[3] = {a0, a1, a2};
+   const float ts[4] = {t0, t1, t2, 2.0f};
+#pragma unroll
+   for (int p = 0 ; p < 3 ; ++p) {
+      if (ts[p] <= 1.0f) {
+         const int a = ax3[p];
+         si += (a == 0) ? d3[0] : 0;
+         sj += (a == 1) ? d3[1] : 0;
+         sk += (a == 2) ? d3[2] : 0;
+         const float te = fminf (ts[p + 1], 1.0f);
+         float w[12];
+         weights32 (c, rho, ox + tb*dx - si, ox + te*dx - si, oy + tb*dy - sj,
+                    oy + te*dy - sj, oz + tb*dz - sk, oz + te*dz - sk, w);
+         if (FAST)
+            scatter_s<D> (Jt, jq + si*D::JYZ + sj*D::JZ + sk, w, S);
+         else
+            scatter32 (c, i + si, j + sj, k + sk, w);
+         tb = te;
+      }
+   }
+}
+
+// The later segments of queue entry e of a warp's queue q.
+template <class D>
+__device__ __forceinline__ void queued_segments (const Ctx32 &c, int *Jt, const float *q, int e, float S)
+{
+   const int kb = __float_as_int (q[7*D::QCAP + e]);
+   later_segments<D, true> (c, Jt, kb & 4095, S, 0, 0, 0, q[e], q[D::QCAP + e], q[2*D::QCAP + e],
+                            q[3*D::QCAP + e], q[4*D::QCAP + e], q[5*D::QCAP + e], ((kb >> 12) & 3) - 1,
+                            ((kb >> 14) & 3) - 1, ((kb >> 16) & 3) - 1, q[6*D::QCAP + e]);
+}
+
 template <int TX, int TY, int TZ, int GROUP, bool PER>
 __global__ void __launch_bounds__ (256, 3)
-k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, DevScalars *dsc)
+k_push32_tiles (Ctx32 c, const int *tile_start, const int *tile_list, int nty, int ntz, int ntiles,
+                DevScalars *dsc)
 {
    const Markers32 m = dsc->m32;
    using D = TileDims<TX, TY, TZ>;
@@ -528,6 +591,7 @@ k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, De
    float *F = smem;                           // Ex Ey Ez Hx Hy Hz, D::FN each
    int *Jt = (int *) (smem + 6*D::FN);        // Jx Jy Jz, D::JN each
    float *stg = smem + 6*D::FN + 3*D::JN + (threadIdx.x >> 5)*D::STAGE;
+   float *que = smem + 6*D::FN + 3*D::JN + 8*D::STAGE + (threadIdx.x >> 5)*D::QUEUE;
    __shared__ int s_tile;
    const Grid &g = c.g;
    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -538,19 +602,25 @@ k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, De
    long long dead = 0;
 
    for (;;) {
-      if (threadIdx.x == 0)
-         s_tile = atomicAdd (&dsc->tile_next, 1);
+      if (threadIdx.x == 0) {
+         const int q = atomicAdd (&dsc->tile_next, 1);
+         s_tile = q < tile_list[ntiles] ? tile_list[q] : -1;
+      }
       __syncthreads ();
       const int t = s_tile;
-      if (t >= ntiles)
+      if (t < 0)
          break;
       const int mb = tile_start[t], me = tile_start[t + 1];
       if (mb < me) {
          const int x0 = (t/(nty*ntz))*TX, y0 = ((t/ntz) % nty)*TY, z0 = (t % ntz)*TZ;
 
+         // A tile with few markers skips the staging: its markers gather
+         // from and add to global memory.
+         const bool dense = me - mb >= MG_TILE_DENSE;
+
          // Stage E and H nodes [x0-1, x0+TX+3) x ... (inside the ghost layers),
          // all copies in flight at once.
-         for (int q = threadIdx.x ; q < 6*D::FN ; q += blockDim.x) {
+         for (int q = threadIdx.x ; dense && q < 6*D::FN ; q += blockDim.x) {
             const int comp = q/D::FN, rem = q - comp*D::FN;
             const int a = rem/D::FYZ, r2 = rem - a*D::FYZ, b = r2/D::FZ, cc = r2 - b*D::FZ;
             const int gi = x0 - 1 + a, gj = y0 - 1 + b, gk = z0 - 1 + cc;
@@ -569,14 +639,14 @@ k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, De
             const int ce = min (cb + MG_TILE_CHUNK, me);
             const float Q = fminf (2097152.0f, 1073741824.0f/(float) (ce - cb));
             const float S = rmax > 0.0f ? Q/rmax : 0.0f;
-            for (int q = threadIdx.x ; q < 3*D::JN ; q += blockDim.x)
+            for (int q = threadIdx.x ; dense && q < 3*D::JN ; q += blockDim.x)
                Jt[q] = 0;
             __syncthreads ();
 
             // Each warp copies its next 32 markers into shared memory while
             // it pushes the current ones.
             stage_marker (stg, lane, m, cb + wid*32 + lane < ce ? cb + wid*32 + lane : -1);
-            int it = 0;
+            int it = 0, qn = 0;
             for (int base = cb + wid*32 ; base < ce ; base += nw*32, ++it) {
                const int n = base + lane;
                const int nn = n + nw*32;
@@ -597,7 +667,7 @@ k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, De
                   i = unpack (cell, 20);
                   j = unpack (cell, 10);
                   k = unpack (cell, 0);
-                  fast = (unsigned) (i - x0 + 1) <= (unsigned) (TX + 1) &&
+                  fast = dense && (unsigned) (i - x0 + 1) <= (unsigned) (TX + 1) &&
                          (unsigned) (j - y0 + 1) <= (unsigned) (TY + 1) &&
                          (unsigned) (k - z0 + 1) <= (unsigned) (TZ + 1);
                   if (!fast && (i < -1 || i > g.n[0] || j < -1 || j > g.n[1] || k < -1 || k > g.n[2])) {
@@ -698,46 +768,19 @@ k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, De
                   }
                }
 
-               // Crossing times, sorted (see k_push32).
-               float t0 = 2.0f, t1 = 2.0f, t2 = 2.0f;
-               int a0 = 0, a1 = 1, a2 = 2;
+               // The first crossing time (see k_push32); markers of the tile
+               // that crossed a face queue their later segments, the others
+               // add theirs now.
+               float tmin = 2.0f;
                if (valid) {
-                  if (di) t0 = __fdividef ((di > 0 ? 1.0f : 0.0f) - ox, dx);
-                  if (dj) t1 = __fdividef ((dj > 0 ? 1.0f : 0.0f) - oy, dy);
-                  if (dk) t2 = __fdividef ((dk > 0 ? 1.0f : 0.0f) - oz, dz);
-                  CSWAP (t0, a0, t1, a1);
-                  CSWAP (t1, a1, t2, a2);
-                  CSWAP (t0, a0, t1, a1);
+                  if (di) tmin = __fdividef ((di > 0 ? 1.0f : 0.0f) - ox, dx);
+                  if (dj) tmin = fminf (tmin, __fdividef ((dj > 0 ? 1.0f : 0.0f) - oy, dy));
+                  if (dk) tmin = fminf (tmin, __fdividef ((dk > 0 ? 1.0f : 0.0f) - oz, dz));
                }
-               const float ta = fminf (t0, 1.0f);
+               const float ta = fminf (tmin, 1.0f);
                const int jq = ((i - x0 + 2)*D::JY + (j - y0 + 2))*D::JZ + (k - z0 + 2);
-
-               // Segments after the first, lane by lane.
-               if (valid && t0 <= 1.0f) {
-                  int si = 0, sj = 0, sk = 0;
-                  float tb = t0;
-                  const int d3[3] = {di, dj, dk};
-                  const int ax3[3] = {a0, a1, a2};
-                  const float ts[4] = {t0, t1, t2, 2.0f};
-#pragma unroll
-                  for (int p = 0 ; p < 3 ; ++p) {
-                     if (ts[p] <= 1.0f) {
-                        const int a = ax3[p];
-                        si += (a == 0) ? d3[0] : 0;
-                        sj += (a == 1) ? d3[1] : 0;
-                        sk += (a == 2) ? d3[2] : 0;
-                        const float te = fminf (ts[p + 1], 1.0f);
-                        float w[12];
-                        weights32 (c, rho, ox + tb*dx - si, ox + te*dx - si, oy + tb*dy - sj,
-                                   oy + te*dy - sj, oz + tb*dz - sk, oz + te*dz - sk, w);
-                        if (fast)
-                           scatter_s<D> (Jt, jq + si*D::JYZ + sj*D::JZ + sk, w, S);
-                        else
-                           scatter32 (c, i + si, j + sj, k + sk, w);
-                        tb = te;
-                     }
-                  }
-               }
+               if (valid && !fast && tmin <= 1.0f)
+                  later_segments<D, false> (c, Jt, 0, S, i, j, k, ox, oy, oz, dx, dy, dz, di, dj, dk, rho);
 
                // First segment: lanes are grouped by cell (match.any); a group
                // of at least GROUP lanes sums its weights across the warp
@@ -778,12 +821,47 @@ k_push32_tiles (Ctx32 c, const int *tile_start, int nty, int ntz, int ntiles, De
                   for (int q = 0 ; q < 12 ; ++q)
                      atomicAdd (Jt + key + slot_offset<D> (q), fx[q]);
                }
+
+               // Queue the crossing markers; a full warp of them adds its
+               // later segments at once.
+               const bool cross = valid && fast && tmin <= 1.0f;
+               const unsigned cm = __ballot_sync (0xffffffffu, cross);
+               if (cm) {
+                  const int nq = __popc (cm);
+                  if (qn + nq > D::QCAP) {
+                     if (lane < qn)
+                        queued_segments<D> (c, Jt, que, lane, S);
+                     qn = 0;
+                     __syncwarp ();
+                  }
+                  if (cross) {
+                     const int e = qn + __popc (cm & ((1u << lane) - 1));
+                     que[e] = ox;
+                     que[D::QCAP + e] = oy;
+                     que[2*D::QCAP + e] = oz;
+                     que[3*D::QCAP + e] = dx;
+                     que[4*D::QCAP + e] = dy;
+                     que[5*D::QCAP + e] = dz;
+                     que[6*D::QCAP + e] = rho;
+                     que[7*D::QCAP + e] = __int_as_float (jq | ((di + 1) << 12) | ((dj + 1) << 14) |
+                                                          ((dk + 1) << 16));
+                  }
+                  qn += nq;
+                  __syncwarp ();
+                  if (qn >= 32) {
+                     qn -= 32;
+                     queued_segments<D> (c, Jt, que, qn + lane, S);
+                     __syncwarp ();
+                  }
+               }
             }
+            if (qn > 0 && lane < qn)
+               queued_segments<D> (c, Jt, que, lane, S);
             __syncthreads ();
 
             // Add the chunk's currents to J.
             const float unit = S > 0.0f ? 1.0f/S : 0.0f;
-            for (int q = threadIdx.x ; q < 3*D::JN ; q += blockDim.x) {
+            for (int q = threadIdx.x ; dense && q < 3*D::JN ; q += blockDim.x) {
                const int v = Jt[q];
                if (v == 0)
                   continue;
@@ -842,8 +920,8 @@ static int launch_tiles (mg_run_t *r, const Ctx32 &c, bool per)
    if (blocks > r->ntiles)
       blocks = r->ntiles;
    MG_CUDA (cudaMemsetAsync (&r->dsc->tile_next, 0, sizeof (int), r->stream));
-   (per ? kp : kn)<<<blocks, 256, D::BYTES, r->stream>>> (c, r->tile_start, r->tiles[1], r->tiles[2],
-                                                            r->ntiles, r->dsc);
+   (per ? kp : kn)<<<blocks, 256, D::BYTES, r->stream>>> (c, r->tile_start, r->tile_list, r->tiles[1],
+                                                            r->tiles[2], r->ntiles, r->dsc);
    MG_LAUNCH_CHECK ();
    return MG_OK;
 }
