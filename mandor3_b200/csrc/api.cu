@@ -1202,7 +1202,7 @@ static int build_graph (mg_run_t *r)
 }
 
 // Precision form: markers are re-sorted by tile and cell every sort_every
-// steps (default 8) so that tiles stay compact and warps keep sharing cells;
+// steps (default 16) so that tiles stay compact and warps keep sharing cells;
 // the sort runs between graph launches on the run's stream.
 // The plain form is put in cell order every sort_every steps (default 16)
 // for the gather's locality (mg_sort64).
@@ -1210,7 +1210,7 @@ static int maybe_sort (mg_run_t *r)
 {
    if (r->prm.sort_every < 0)
       return MG_OK;
-   const int every = r->prm.sort_every > 0 ? r->prm.sort_every : (is32 (r) ? 8 : 16);
+   const int every = r->prm.sort_every > 0 ? r->prm.sort_every : 16;
    if (r->steps_since_sort++ < every)
       return MG_OK;
    return is32 (r) ? mg_sort32 (r) : mg_sort64 (r);
