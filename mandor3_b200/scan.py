@@ -218,7 +218,7 @@ class Server:
         self.peak_used = 0
         # Host seconds spent admitting (building runs), rebuilding batches and
         # stepping rounds.
-        self.stats = dict(admit_s=0.0, batch_s=0.0, step_s=0.0, rounds=0)
+        self.stats = dict(admit_s=0.0, batch_s=0.0, step_s=0.0, retire_s=0.0, idle_s=0.0, rounds=0)
 
     def serve(self, stream):
         pending = sorted(((float(t), i, s) for i, (t, s) in enumerate(stream)), key=lambda x: (x[0], x[1]))
@@ -251,7 +251,9 @@ class Server:
                 changed = True
             if not active:
                 if pending:
+                    ti = time.perf_counter()
                     time.sleep(max(0.0, min(0.05, pending[0][0] - now())))
+                    self.stats["idle_s"] += time.perf_counter() - ti
                 continue
             if changed or batch is None:
                 tb = time.perf_counter()
@@ -264,6 +266,7 @@ class Server:
             rows = batch.step(k)
             self.stats["step_s"] += time.perf_counter() - ts
             self.stats["rounds"] += 1
+            tr = time.perf_counter()
             still = []
             for a, rw in zip(active, rows):
                 a["rows"].append(rw)
@@ -281,6 +284,7 @@ class Server:
                     if a["done"] >= a["spec"].steps:
                         a["run"].close()
             active = still
+            self.stats["retire_s"] += time.perf_counter() - tr
         if batch is not None:
             batch.close()
         return [results[i] for i in range(len(stream))]
