@@ -670,13 +670,16 @@ def end_to_end(w, device, steps, warmup, world):
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    marks = [t0]
     r.set_fields(hE, hH)
     r.set_markers(hm)
     r.init()
+    marks.append(time.perf_counter())
     lib = mg.load()
     rc = lib.mg_run_step(r.ptr, steps, rows.ctypes.data)
     if rc:
         raise mg.MandorError(rc, lib.mg_last_error().decode())
+    marks.append(time.perf_counter())
     import ctypes
     got = ctypes.c_longlong()
     rc = lib.mg_run_get_markers(r.ptr, out_m.ctypes.data, len(out_m), ctypes.byref(got))
@@ -686,6 +689,8 @@ def end_to_end(w, device, steps, warmup, world):
     if rc:
         raise mg.MandorError(rc, lib.mg_last_error().decode())
     sec = time.perf_counter() - t0
+    marks.append(t0 + sec)
+    phases = {k: round(b - a, 4) for k, a, b in zip(("upload_init_s", "steps_s", "download_s"), marks, marks[1:])}
     r.close()
     sec = dist_max(sec, world)
     ps = dist_sum(0.5 * (len(markers) + got.value) * steps, world)
@@ -693,7 +698,8 @@ def end_to_end(w, device, steps, warmup, world):
     d2h = got.value * 64 + hE.nbytes + hH.nbytes + rows.nbytes
     return {"value": ps / sec, "unit": "particle-steps/s",
             "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps,
-            "seconds": sec, "note": "wall clock, max over ranks; upload + %d steps + download" % steps}
+            "seconds": sec, "phases": phases,
+            "note": "wall clock, max over ranks; upload + %d steps + download" % steps}
 
 
 if __name__ == "__main__":
