@@ -154,6 +154,40 @@ def test_tiled_push_matches_untiled_push(tile):
         assert np.max(np.abs(got[ax] - want[ax])) < 1e-4 * 0.05
 
 
+def slabs(sort_every, steps=20):
+    """A dense slab (24 markers per cell) and a sparse one (2 per cell, two
+    cells thick): the tiles over the sparse slab hold fewer markers than the
+    shared-memory staging threshold, those over the dense one more."""
+    n = (32, 16, 16)
+    hh = 0.05 / (2 * math.pi)
+    h = (hh, hh, hh)
+    tau = 0.5 / math.sqrt(sum(1 / x ** 2 for x in h))
+    r = mg.Run(n, h, tau, (0, 0, 0), (0, 0, 0), precision=mg.FP32_OFFSET, sort_every=sort_every)
+    z = np.zeros(r.field_shape())
+    r.set_fields(z, z)
+    rho = -4 * math.pi ** 2 / 24
+    r.place_uniform((2, 0, 0), (10, 16, 16), 24, rho, -1.0, drift=(0.3, 0.1, 0.0),
+                    uth=(0.05, 0.05, 0.05), seed=(11, 22))
+    r.place_uniform((21, 0, 0), (23, 16, 16), 2, 12 * rho, -1.0, drift=(-0.3, 0.0, 0.1),
+                    uth=(0.05, 0.05, 0.05), seed=(33, 44), id0=10 ** 6)
+    r.init()
+    rows = r.step(steps)
+    return r, rows
+
+
+def test_sparse_and_dense_tiles_match_the_untiled_push():
+    rt, a = slabs(0)
+    ru, b = slabs(-1)
+    scale = float(np.max(np.abs(b[:, 1:6].sum(1))))
+    np.testing.assert_allclose(a[:, 1:], b[:, 1:], rtol=1e-5, atol=1e-6 * scale)
+    Jt, Ju = rt.current(), ru.current()
+    assert np.max(np.abs(Jt - Ju)) <= 1e-4 * np.max(np.abs(Ju))
+    got, want = parity.by_id(rt.markers()), parity.by_id(ru.markers())
+    assert np.array_equal(got["id"], want["id"])
+    for ax in "xyz":
+        assert np.max(np.abs(got[ax] - want[ax])) < 1e-4 * 0.05
+
+
 def test_tiled_push_handles_markers_far_from_their_tile():
     # Sorted once at init: after 120 steps at 0.6c most markers sit several
     # cells away from the tile they were sorted into.
