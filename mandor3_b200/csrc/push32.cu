@@ -580,6 +580,14 @@ __device__ __forceinline__ void queued_segments (const Ctx32 &c, int *Jt, const 
                             ((kb >> 14) & 3) - 1, ((kb >> 16) & 3) - 1, q[6*D::QCAP + e]);
 }
 
+// The tiled push: persistent blocks take tiles holding markers from the
+// list built at the sort; per tile, the E and H nodes around it go to shared
+// memory, each warp pushes its 32-marker rows from a cp.async double buffer,
+// first-segment currents are summed per cell group into a fixed-point copy
+// of the tile's J nodes, crossing markers queue their later segments, and
+// the copy is added to J at the end of each chunk.  Tiles with fewer than
+// MG_TILE_DENSE markers, and markers more than a cell outside their tile,
+// gather from and add to global memory.
 template <int TX, int TY, int TZ, int GROUP, bool PER>
 __global__ void __launch_bounds__ (256, 3)
 k_push32_tiles (Ctx32 c, const int *tile_start, const int *tile_list, int nty, int ntz, int ntiles,
