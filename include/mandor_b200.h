@@ -49,9 +49,8 @@ extern "C" {
 #define MG_ERR_CAPACITY  (-5)   /* marker capacity exceeded                  */
 #define MG_ERR_BOUNDS    (-6)   /* device bounds check tripped (marker left
                                    the J ghost layers: Courant violated)     */
-#define MG_ERR_IO        (-7)   /* file error in the host driver             */
+#define MG_ERR_IO        (-7)   /* input file error: core_b200.out exits 7   */
 #define MG_ERR_ADMISSION (-8)   /* serving admission refused (HBM budget)    */
-#define MG_ERR_TIMEOUT   (-9)   /* bounded device wait gave up               */
 
 /* Boundary condition codes, same values as misc_parameters.h:38-42. */
 enum { MG_BC_PERIODIC = 0, MG_BC_MIRROR = 1, MG_BC_OPEN = 2 };
@@ -422,21 +421,27 @@ typedef struct {
 
 /* Writes the markers of `spec` (the placement rule of mg_place_t, cell box
  * measured with steps h) to out[0 .. count), allocating nothing on the
- * device or the host: for callers that cannot call cudaMalloc -- code that
- * runs while a stream is being captured into a CUDA graph (where
- * allocation calls are not allowed), or hosts that have handed all of HBM
- * to their own memory pool and pass this library slices of it.  The
- * generator start states go through a file-scope device array of at most
- * 4096 states (1.59 MB, resident on every GPU that loads the library until
- * the process exits); `threads` (0 = 4096) sets how many states, i.e.
- * parallel generator streams, are used and is rejected above 4096.  The
- * first call on a device looks up that array's device address, so make the
- * first call before any stream capture.  Calls run on `stream` (a
- * cudaStream_t, NULL for the legacy stream) of the current device and
- * return after the kernel has finished; the scratch is shared by every call
- * in the process (calls are serialised by a lock) and overwritten each
- * time, so launches that overlap on the GPU from outside this process would
- * race on it.  Output is bit-identical to mg_run_place_uniform. */
+ * device or the host.  It serves callers that cannot call cudaMalloc: a
+ * host application whose caching allocator has already reserved the
+ * GPU's memory and hands this library slices of it (a cudaMalloc there
+ * fails or evicts the host's pool), and code that must not take the
+ * implicit device-wide synchronisation of cudaMalloc/cudaFree while other
+ * streams of the process are running.  The generator start states go
+ * through a file-scope device array of at most 4096 states (1.59 MB,
+ * resident on every GPU that loads the library until the process exits);
+ * `threads` (0 = 4096) sets how many states, i.e. parallel generator
+ * streams, are used and is rejected above 4096 with MG_ERR_ARG; output
+ * arrays shorter than the box's marker count are rejected with
+ * MG_ERR_CAPACITY.  The first call on a device looks up that array's device
+ * address with the device current and keeps it, so make that first call
+ * before any stream capture, and do not call it again on a device after
+ * cudaDeviceReset.  A call runs on `stream` (a cudaStream_t, NULL for the
+ * legacy stream) of the current device: it copies the start states there
+ * from pageable host memory, launches one kernel and waits for the stream
+ * before returning.  The array is shared by every call in the process
+ * (calls are serialised by a lock) and overwritten each time, so other
+ * work that overlapped a call on the GPU and used the array would race on
+ * it.  Output is bit-identical to mg_run_place_uniform. */
 int  mg_place_uniform_static (const mg_place_t *spec, const double h[3],
                               const mg_device_markers_t *out, long long capacity,
                               int threads, void *stream);

@@ -269,9 +269,14 @@ int mg_place64 (mg_run_t *r, const mg_place_t *spec, long long at, long long cou
 // 97 words, 1.59 MB, held by every GPU that loads the library until the
 // process exits), and the host-side jump-ahead works in static host buffers.
 // Every call overwrites the states it uses, so nothing needs clearing.
-// Calls are serialised inside the process by a mutex and each call waits for
-// its kernel before returning; work launched concurrently on the same device
-// by two processes, or by another user of this array, would race on it.
+// Calls are serialised inside the process by a mutex; each call copies the
+// start states from pageable static host memory and waits for its stream
+// before returning, so the next call may reuse both buffers.  Work that
+// touches the array concurrently from outside these calls would race on it.
+// The array's device address is looked up once per device (first call with
+// that device current) and kept: after cudaDeviceReset of that device the
+// kept address is stale, so a process that resets a device must not call
+// this entry point on it again.
 // ---------------------------------------------------------------------------
 static __device__ __align__ (256) uint32_t g_place_states[MG_PLACE_STATIC_STATES*RM_LAG];
 
@@ -331,12 +336,12 @@ extern "C" int mg_place_uniform_static (const mg_place_t *spec, const double h[3
                     "holds at most %d", threads, MG_PLACE_STATIC_STATES);
       return MG_ERR_ARG;
    }
-   if (count == 0)
-      return MG_OK;
    if (spec->seed_ij < 0 || spec->seed_ij > 31328 || spec->seed_kl < 0 || spec->seed_kl > 30081) {
       mg_set_error ("ranmar seeds must satisfy 0 <= ij <= 31328, 0 <= kl <= 30081 (misc_ranmar.c:81-84)");
       return MG_ERR_ARG;
    }
+   if (count == 0)
+      return MG_OK;
    int dev = 0;
    if (cudaGetDevice (&dev) != cudaSuccess || dev < 0 || dev >= 64) {
       mg_set_error ("mg_place_uniform_static: no current CUDA device");

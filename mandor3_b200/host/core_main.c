@@ -41,19 +41,22 @@
 
 #define HEADER_BYTES 112            /* 6 ints of valid region + 88-byte mesh_t */
 
+/* Errors end the run like the reference's DIE (log.h:44-62), with a
+ * non-zero status that names the kind: -MG_ERR_IO (7) for a missing,
+ * truncated or malformed input file, -rc for a failed library call. */
 static void die (const char *fmt, const char *arg)
 {
    fprintf (stderr, "core_b200.out: ");
    fprintf (stderr, fmt, arg);
    fprintf (stderr, "\n");
-   exit (EXIT_FAILURE);
+   exit (-MG_ERR_IO);
 }
 
 static void check (int rc, const char *what)
 {
    if (rc != MG_OK) {
       fprintf (stderr, "core_b200.out: %s: %s\n", what, mg_last_error ());
-      exit (EXIT_FAILURE);
+      exit (rc < 0 && rc > -128 ? -rc : EXIT_FAILURE);
    }
 }
 
@@ -188,6 +191,8 @@ static mg_marker_t *read_markers (const char *path, long long *n)
    FILE *fp = open_or_die (path, "rb");
    long count = 0;
    read_exact (&count, sizeof (long), fp, path);
+   if (count < 0)
+      die ("'%s': negative marker count", path);
    mg_marker_t *m = (mg_marker_t *) malloc (sizeof (mg_marker_t)*(count > 0 ? count : 1));
    if (count > 0)
       read_exact (m, sizeof (mg_marker_t)*count, fp, path);

@@ -24,8 +24,10 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import (FP32_OFFSET, FP64, BC_OPEN, BC_PERIODIC, Batch, Run, estimate_bytes,
+from . import (FP32_OFFSET, FP64, BC_OPEN, BC_PERIODIC, Batch, MandorError, Run, estimate_bytes,
                load)
+
+ERR_ADMISSION = -8               # MG_ERR_ADMISSION (include/mandor_b200.h)
 
 N_CR = 4 * math.pi ** 2          # critical density in code units
 
@@ -236,7 +238,8 @@ class Server:
                 arrival, i, spec = queue[0]
                 need = footprint(spec)
                 if need > self.budget:
-                    raise ValueError("solve %d needs %d bytes, more than the budget %d" % (i, need, self.budget))
+                    raise MandorError(ERR_ADMISSION, "solve %d needs %d bytes of device memory, more than "
+                                      "the whole admission budget of %d bytes" % (i, need, self.budget))
                 if used + need > self.budget:
                     break
                 queue.pop(0)

@@ -427,11 +427,123 @@ def make_mirror():
     print("mirror: E max %.3e / %.3e" % (np.abs(out["E1"]).max(), np.abs(out["E-1"]).max()))
 
 
+# Runs at the benchmark configurations' sizes and the field-only runs of
+# tests/cases.py.
+def make_resonator():
+    """The cavity eigenmode set up by the reference's own setup.out
+    ([EMResonator] Yee_2nd_order) and run by core.out: the initial fields,
+    the fields after the run and its diag.dat rows."""
+    c = cases.RESONATOR
+    rr = RefRun()
+    try:
+        with open(rr.path("deck.input"), "w") as fp:
+            fp.write(cases.resonator_deck())
+        rr._run("setup.out", "deck.input", "create")
+        dom = refrun.read_domain(rr.path("binData", "domain.bin"))
+        _, _, E0 = refrun.read_mesh(rr.path("binData", "sys_E_000000(000).bin"))
+        _, _, H0 = refrun.read_mesh(rr.path("binData", "sys_H_000000(000).bin"))
+        rr.set_state(np.zeros(0, dtype=oracle_port.MARKER_DTYPE))
+        rr.run(c["steps"])
+        _, E, H = rr.final()
+        np.savez_compressed(os.path.join(HERE, "resonator.npz"), h=dom["h"], tau=dom["tau"], E0=E0, H0=H0,
+                            E=E, H=H, diag=rr.diag())
+        print("resonator: |E0| %.3e, |E| %.3e after %d steps" % (np.abs(E0).max(), np.abs(E).max(), c["steps"]))
+    finally:
+        rr.cleanup()
+
+
+def _run_records(rr, steps, period):
+    with open(rr.path("run_mandor.cfg"), "w") as fp:
+        fp.write("@ %d\ttotal steps\n@ %d\tcheckpoint period\n@ -1\ttecplot\n@ 0\tcontinue\n"
+                 "@ %d\tstop-flag period\n@ -100\tspectral dumps\n" % (steps, period, 10 ** 8))
+    rr._run("core.out")
+
+
+def make_mur_pulse():
+    """The free pulse of cases.MUR_PULSE in an empty Mur box: the
+    reference's E and H at every checkpoint and its diag.dat rows."""
+    c = cases.MUR_PULSE
+    n = c["n"]
+    rr = RefRun()
+    try:
+        dom = rr.setup(n, [v * c["h"] for v in n], c["tau"], c["bc"], c["bc"])
+        E0, H0 = cases.mur_pulse_fields()
+        rr.set_state(np.zeros(0, dtype=oracle_port.MARKER_DTYPE), E0, H0)
+        _run_records(rr, c["period"] * c["records"], c["period"])
+        out = {}
+        for q in range(1, c["records"] + 1):
+            _, out["E%d" % q], out["H%d" % q] = rr.final(q)
+        np.savez_compressed(os.path.join(HERE, "mur_pulse.npz"), h=dom["h"], tau=dom["tau"], diag=rr.diag(), **out)
+        print("mur_pulse: |E| %s" % ["%.3e" % np.abs(out["E%d" % q]).max() for q in range(1, c["records"] + 1)])
+    finally:
+        rr.cleanup()
+
+
+def make_thermal_c1():
+    """BASELINE configuration 1 (cases.THERMAL_C1) through core.out: the
+    diag.dat history of all 200 steps, every 64th marker by id, E and H at
+    4096 seeded nodes and the shell power spectra of E and H at the end."""
+    c = cases.THERMAL_C1
+    n = c["n"]
+    rr = RefRun()
+    try:
+        dom = rr.setup(n, [v * cases.H_LAMBDA for v in n], c["tau"], c["bc"], c["bc"])
+        m0 = cases.thermal_c1_markers(dom["h"])
+        z = np.zeros((n[0] + 1, n[1] + 1, n[2] + 1, 3))
+        rr.set_state(m0, z, z)
+        rr.run(c["steps"])
+        m, E, H = rr.final()
+        m = np.sort(m, order="id")
+        keep = m[(m["id"] - 1) % c["sample_every"] == 0]
+        nodes = cases.field_sample(n, 4096, 1)
+        sel = tuple(nodes.T)
+        np.savez_compressed(os.path.join(HERE, "thermal_c1.npz"), h=dom["h"], tau=dom["tau"], diag=rr.diag(),
+                            n_markers=len(m), markers=keep.tobytes(), nodes=nodes, E=E[sel], H=H[sel],
+                            spec_E=cases.shell_spectrum(E, n), spec_H=cases.shell_spectrum(H, n))
+        print("thermal_c1: %d markers, %d sampled, diag rows %d" % (len(m), len(keep), len(rr.diag())))
+    finally:
+        rr.cleanup()
+
+
+def make_foil_c2():
+    """The grid and foil of BASELINE configuration 2 (cases.FOIL_C2),
+    warm, through core.out for 10 steps: every 1024th marker by id, E and
+    H at 8192 seeded nodes around the foil and 4096 anywhere, the diag.dat
+    rows."""
+    c = cases.FOIL_C2
+    n = c["n"]
+    rr = RefRun()
+    try:
+        dom = rr.setup(n, [v * c["h"] for v in n], c["tau"], c["bc"], c["bc"])
+        m0 = cases.foil_c2_markers(dom["h"])
+        rr.set_state(m0)
+        rr.run(c["steps"])
+        m, E, H = rr.final()
+        m = np.sort(m, order="id")
+        keep = m[(m["id"] - 1) % c["sample_every"] == 0]
+        nodes = np.concatenate([cases.field_sample(n, 8192, 2, ((115, 0, 0), (135, n[1], n[2]))),
+                                cases.field_sample(n, 4096, 3)])
+        sel = tuple(nodes.T)
+        np.savez_compressed(os.path.join(HERE, "foil_c2.npz"), h=dom["h"], tau=dom["tau"], diag=rr.diag(),
+                            n_markers=len(m), markers=keep.tobytes(), nodes=nodes, E=E[sel], H=H[sel],
+                            E_max=np.abs(E).max(axis=(0, 1, 2)), H_max=np.abs(H).max(axis=(0, 1, 2)))
+        print("foil_c2: %d -> %d markers, %d sampled, |E| %.3e" % (len(m0), len(m), len(keep), np.abs(E).max()))
+    finally:
+        rr.cleanup()
+
+
+CONFIG_RUNS = {"resonator": make_resonator, "mur_pulse": make_mur_pulse, "thermal_c1": make_thermal_c1,
+               "foil_c2": make_foil_c2}
+
+
 if __name__ == "__main__":
     if not have_reference():
         sys.exit("reference binaries missing: make -C oracle ref REF=<reference tree>")
     for name in (sys.argv[1:] or list(cases.CASES) + ["gauss_spot", "placers", "tecplot", "probes", "tfsf",
-                                                 "setup_tags", "mirror"]):
+                                                 "setup_tags", "mirror"] + list(CONFIG_RUNS)):
+        if name in CONFIG_RUNS:
+            CONFIG_RUNS[name]()
+            continue
         if name == "probes":
             make_probes()
             continue

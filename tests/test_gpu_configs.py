@@ -1,0 +1,216 @@
+"""The CUDA path against the reference on the field-only runs and at the
+benchmark configurations' sizes (goldens frozen from the reference's
+core.out by tests/golden/make_golden.py; the CPU restatement is pinned to
+the same goldens in tests/test_config_oracle.py):
+
+* cavity resonator set up by the reference's [EMResonator] Yee_2nd_order
+  tag (setup/tag_EMResonator.c:31-116): FP64 fields within 1e-12 of the
+  reference after 60 steps, and every node following the mode's discrete
+  frequency omega = (2/tau) asin(tau |D_r| / 2) to round-off;
+* a free pulse absorbed by first-order Mur walls on all six faces
+  (core/emCap_Mur.c:56-175): FP64 fields within 1e-12 at both checkpoints;
+* BASELINE configuration 1 at full size (32^3 thermal plasma, 8 ppc, 200
+  steps): the diag.dat energy history to its printed digits, sampled
+  markers, fields and shell spectra of E and H;
+* the grid and foil of BASELINE configuration 2 (256 x 128 x 128, 4.46e6
+  markers, 10 steps): sampled markers matched by id, cells bit-exact.
+
+Tolerances beyond 1e-12 are stated at each test with their reason."""
+import os
+
+import numpy as np
+import pytest
+
+import cases
+from refrun import MARKER_DTYPE
+
+pytestmark = pytest.mark.gpu
+
+mg = pytest.importorskip("mandor3_b200")
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def golden(name):
+    return np.load(os.path.join(HERE, "golden", name + ".npz"))
+
+
+def rel(a, b):
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / max(np.max(np.abs(b)), 1e-300))
+
+
+def diag_close(rows, diag, cols=5, tol=2e-6, scale=None):
+    """Energy rows against diag.dat, which prints 7 significant digits
+    (core/diag_WDensity.c:103-104): within `tol` of each quantity's largest
+    magnitude (or of `scale`).  diag.dat row s is the step after row s."""
+    for q in range(cols):
+        s = scale or max(float(np.max(np.abs(diag[:, 1 + q]))), 1e-300)
+        err = float(np.max(np.abs(rows[1:len(diag) + 1, 1 + q] - diag[:, 1 + q]))) / s
+        assert err < tol, (q, err)
+
+
+def zero_fields(n):
+    return np.zeros((n[0] + 1, n[1] + 1, n[2] + 1, 3))
+
+
+def test_resonator_fp64_matches_reference():
+    g = golden("resonator")
+    c = cases.RESONATOR
+    with mg.Run(c["n"], g["h"], float(g["tau"]), c["bc"], c["bc"]) as r:
+        r.set_fields(g["E0"], g["H0"])
+        r.init()
+        rows = r.step(c["steps"])
+        E, H = r.fields()
+    assert rel(E, g["E"]) < 1e-12 and rel(H, g["H"]) < 1e-12
+    diag_close(rows, g["diag"], cols=2)
+
+
+@pytest.mark.parametrize("precision,tol", [("FP64", 1e-12), ("FP32_OFFSET", 2e-6)])
+def test_resonator_follows_the_yee_eigenfrequency(precision, tol):
+    """E^(n+1) + E^(n-1) = 2 cos(omega tau) E^n at every node for the
+    discrete eigenmode (the leapfrog recurrence of the mode's amplitude),
+    checked over 40 steps relative to the mode amplitude.  FP32 fields
+    round each update at 6e-8 of the amplitude; over 40 steps that
+    stays below 2e-6."""
+    g = golden("resonator")
+    c = cases.RESONATOR
+    tau = float(g["tau"])
+    w = cases.resonator_omega(g["h"], tau)
+    c2 = 2 * np.cos(w * tau)
+    ex = []
+    with mg.Run(c["n"], g["h"], tau, c["bc"], c["bc"], precision=getattr(mg, precision)) as r:
+        r.set_fields(g["E0"], g["H0"])
+        r.init()
+        ex.append(r.fields()[0][..., 0])
+        for _ in range(40):
+            r.step(1)
+            ex.append(r.fields()[0][..., 0])
+    ex = np.array(ex)
+    amp = np.max(np.abs(g["E0"]))
+    res = np.max(np.abs(ex[2:] + ex[:-2] - c2 * ex[1:-1])) / amp
+    assert res < tol, res
+    # A frequency 1e-3 off leaves a residual far above the tolerance.
+    c2b = 2 * np.cos(1.001 * w * tau)
+    assert np.max(np.abs(ex[2:] + ex[:-2] - c2b * ex[1:-1])) / amp > 5 * tol
+
+
+def test_mur_pulse_fp64_matches_reference():
+    g = golden("mur_pulse")
+    c = cases.MUR_PULSE
+    E0, H0 = cases.mur_pulse_fields()
+    rows = []
+    with mg.Run(c["n"], g["h"], float(g["tau"]), c["bc"], c["bc"]) as r:
+        r.set_fields(E0, H0)
+        r.init()
+        for q in range(1, c["records"] + 1):
+            rows.append(r.step(c["period"]))
+            E, H = r.fields()
+            assert rel(E, g["E%d" % q]) < 1e-12 and rel(H, g["H%d" % q]) < 1e-12, q
+    rows = np.concatenate(rows)
+    diag_close(rows, g["diag"], cols=2)
+    w0 = rows[1, 1] + rows[1, 2]
+    assert rows[-1, 1] + rows[-1, 2] < 2e-3 * w0          # the walls absorbed the pulse
+
+
+def test_mur_pulse_fp32_tracks_reference():
+    """Precision form: fields within 1e-5 of the initial amplitude at both
+    checkpoints (FP32 rounding of 6e-8 per update over 120 steps)."""
+    g = golden("mur_pulse")
+    c = cases.MUR_PULSE
+    E0, H0 = cases.mur_pulse_fields()
+    amp = np.max(np.abs(E0))
+    with mg.Run(c["n"], g["h"], float(g["tau"]), c["bc"], c["bc"], precision=mg.FP32_OFFSET) as r:
+        r.set_fields(E0, H0)
+        r.init()
+        for q in range(1, c["records"] + 1):
+            r.step(c["period"])
+            E, H = r.fields()
+            assert np.max(np.abs(E - g["E%d" % q])) < 1e-5 * amp, q
+            assert np.max(np.abs(H - g["H%d" % q])) < 1e-5 * amp, q
+
+
+def c1_run(precision, steps):
+    g = golden("thermal_c1")
+    c = cases.THERMAL_C1
+    n, h = c["n"], g["h"]
+    r = mg.Run(n, h, float(g["tau"]), c["bc"], c["bc"], precision=precision)
+    r.set_fields(zero_fields(n), zero_fields(n))
+    r.set_markers(cases.thermal_c1_markers(h))
+    r.init()
+    return g, c, r, r.step(steps)
+
+
+def test_thermal_c1_fp64_matches_reference():
+    """200 steps of BASELINE configuration 1.  The restatement, which sums
+    currents in the reference's marker order, agrees with the reference to
+    3e-14 (fields) and 6e-17 (markers); the device sums a cell's currents
+    in another order (warp runs, atomics), so the bounds below allow 1e-10
+    relative for fields and spectra (a thermal plasma at omega_p t = 2.9
+    does not yet amplify round-off) and 1e-13 for marker state."""
+    g, c, r, rows = c1_run(mg.FP64, cases.THERMAL_C1["steps"])
+    diag_close(rows, g["diag"])
+    E, H = r.fields()
+    n = c["n"]
+    sel = tuple(g["nodes"].T)
+    assert rel(E[sel], g["E"]) < 1e-10 and rel(H[sel], g["H"]) < 1e-10
+    for F, key in ((E, "spec_E"), (H, "spec_H")):
+        s = cases.shell_spectrum(F, n)
+        assert np.max(np.abs(s - g[key]) / g[key].max(axis=1, keepdims=True)) < 1e-10, key
+    m = np.sort(r.markers(), order="id")
+    r.close()
+    want = np.frombuffer(g["markers"].tobytes(), MARKER_DTYPE)
+    got = m[(m["id"] - 1) % c["sample_every"] == 0]
+    assert np.array_equal(got["id"], want["id"])
+    for a, f in enumerate("xyz"):
+        assert np.array_equal(np.floor(got[f] / g["h"][a]), np.floor(want[f] / g["h"][a]))
+    for f in ("x", "y", "z", "vx", "vy", "vz"):
+        assert np.max(np.abs(got[f] - want[f])) < 1e-13 * max(np.max(np.abs(want[f])), 1e-2), f
+
+
+def test_thermal_c1_fp32_energy_history_within_1e4_of_reference():
+    """The precision form on configuration 1: total and thermal energy
+    within 1e-4 of the reference's diag.dat history relative to each
+    quantity; the field energies (thermal noise, 1e-3 of the total) within
+    1e-4 of the total energy."""
+    g, c, r, rows = c1_run(mg.FP32_OFFSET, cases.THERMAL_C1["steps"])
+    r.close()
+    d = g["diag"]
+    m = len(d)
+    tot = rows[1:m + 1, 1] + rows[1:m + 1, 2] + rows[1:m + 1, 3:6].sum(1)
+    tot_ref = d[:, 1] + d[:, 2] + d[:, 3:6].sum(1)
+    assert np.max(np.abs(tot - tot_ref) / np.abs(tot_ref)) < 1e-4
+    wt, wt_ref = rows[1:m + 1, 3:6].sum(1), d[:, 3:6].sum(1)
+    assert np.max(np.abs(wt - wt_ref) / np.abs(wt_ref)) < 1e-4
+    for q in (1, 2):
+        assert np.max(np.abs(rows[1:m + 1, q] - d[:, q])) < 1e-4 * np.max(np.abs(tot_ref))
+
+
+def test_foil_c2_grid_matches_reference():
+    """Configuration 2's grid and foil, warm, 10 steps: sampled markers by
+    id with cells bit-exact, positions and momenta within 1e-12 of their
+    scale, E and H at sampled nodes within 1e-12 of each component's
+    largest magnitude, energy rows to diag.dat's printed digits."""
+    g = golden("foil_c2")
+    c = cases.FOIL_C2
+    n, h = c["n"], g["h"]
+    m0 = cases.foil_c2_markers(h)
+    with mg.Run(n, h, float(g["tau"]), c["bc"], c["bc"], capacity=len(m0)) as r:
+        r.set_fields(zero_fields(n), zero_fields(n))
+        r.set_markers(m0)
+        r.init()
+        rows = r.step(c["steps"])
+        E, H = r.fields()
+        m = np.sort(r.markers(), order="id")
+    assert len(m) == int(g["n_markers"])
+    diag_close(rows, g["diag"])
+    sel = tuple(g["nodes"].T)
+    for q in range(3):
+        assert np.max(np.abs(E[sel][:, q] - g["E"][:, q])) < 1e-12 * g["E_max"][q]
+        assert np.max(np.abs(H[sel][:, q] - g["H"][:, q])) < 1e-12 * g["H_max"][q]
+    want = np.frombuffer(g["markers"].tobytes(), MARKER_DTYPE)
+    got = m[(m["id"] - 1) % c["sample_every"] == 0]
+    assert np.array_equal(got["id"], want["id"])
+    for a, f in enumerate("xyz"):
+        assert np.array_equal(np.floor(got[f] / h[a]), np.floor(want[f] / h[a]))
+    for f in ("x", "y", "z", "vx", "vy", "vz"):
+        assert np.max(np.abs(got[f] - want[f])) < 1e-12 * max(np.max(np.abs(want[f])), 1.0), f
