@@ -203,9 +203,24 @@ def ncu_traffic(w, markers):
 # ---------------------------------------------------------------------------
 # Reference CPU path (the reference core.out built from its sources).
 # ---------------------------------------------------------------------------
-def reference_sample(w, steps):
-    """Runs the reference core_fast.out on the workload's grid and markers for
-    `steps` steps; returns (particle-steps/s, seconds, markers, description)."""
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def reference_sample(w, steps, procs=None):
+    """Runs the reference core_fast.out on the workload's grid and markers
+    for `steps` steps as `procs` independent single-rank processes at once
+    (default: one per host core, fewer if host memory is short).  The
+    reference's only parallelism is MPI domain decomposition and no MPI
+    library exists on these hosts, so independent copies are the way it
+    uses every core.  Returns a dict: aggregate particle-steps/s (all
+    copies' work over the slowest copy's main loop, the reference's own
+    timer core/main.c:479-480), the slowest copy's seconds, the marker
+    count, the number of copies and the median copy's own rate; or None
+    without the reference binaries."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_port
     from refrun import RefRun, have_reference
@@ -213,20 +228,54 @@ def reference_sample(w, steps):
     if not have_reference() or not os.path.exists(exe):
         return None
     m = np.concatenate([oracle_port.place(h=w["h"], **s) for s in w["species"]])
-    rr = RefRun(tempfile.mkdtemp(prefix="mandor_bench_ref_"))
+    if procs is None:
+        procs = host_cores()
+        try:
+            import psutil
+            per = 3.0 * (m.nbytes + 12 * 8 * int(np.prod([v + 5 for v in w["n"]])))
+            procs = max(1, min(procs, int(0.7 * psutil.virtual_memory().available / per)))
+        except ImportError:
+            pass
+    base = RefRun(tempfile.mkdtemp(prefix="mandor_bench_ref_"))
+    runs = []
     try:
-        h_um = [v for v in w["h"]]
-        L_um = [w["n"][a] * h_um[a] for a in range(3)]
-        rr.setup(w["n"], L_um, -0.5, w["bc"], w["bc"])
-        rr.set_state(m)
-        out = rr.run(steps, exe="core_fast.out", timeout=1800)
+        L_um = [w["n"][a] * w["h"][a] for a in range(3)]
+        base.setup(w["n"], L_um, -0.5, w["bc"], w["bc"])
+        base.set_state(m)
+        big = ("plasma_000000_000.bin", "sys_E_000000(000).bin", "sys_H_000000(000).bin")
+        for q in range(procs):
+            rr = RefRun(tempfile.mkdtemp(prefix="mandor_bench_ref%d_" % q))
+            for f in os.listdir(base.path("binData")):
+                src, dst = base.path("binData", f), rr.path("binData", f)
+                if f in big:
+                    os.link(src, dst)          # read only by core.out
+                else:
+                    with open(src, "rb") as a, open(dst, "wb") as b:
+                        b.write(a.read())
+            with open(rr.path("run_mandor.cfg"), "w") as fp:
+                fp.write("@ %d\ttotal steps\n@ %d\tcheckpoint period\n@ -1\ttecplot\n@ 0\tcontinue\n"
+                         "@ %d\tstop-flag period\n@ -100\tspectral dumps\n" % (steps, 10 ** 8, 10 ** 8))
+            runs.append(rr)
+        procs_ = [subprocess.Popen([exe], cwd=rr.dir, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
+                  for rr in runs]
+        secs = []
+        for p in procs_:
+            out, _ = p.communicate(timeout=1800)
+            text = out.decode(errors="replace")
+            if p.returncode != 0:
+                raise RuntimeError("reference core_fast.out failed:\n" + text[-2000:])
+            secs.append(float(re.search(r"main loop have taken ([0-9.eE+-]+) sec", text).group(1)))
     finally:
-        rr.cleanup()
-    sec = float(re.search(r"main loop have taken ([0-9.eE+-]+) sec", out).group(1))
-    desc = ("reference core.out (-O3, single-rank MPI shim, 1 process) on the laser-foil grid "
-            "and markers, %d steps from t=0, laser source omitted (the reference has no "
-            "analytic sin^2 source; the source plane is O(n^2) work)" % steps)
-    return len(m) * steps / sec, sec, len(m), desc
+        base.cleanup()
+        for rr in runs:
+            rr.cleanup()
+    rate = procs * len(m) * steps / max(secs)
+    desc = ("reference core.out (-O3, single-rank MPI shim) as %d independent processes at once, one per "
+            "host core, each on the laser-foil grid and markers for %d steps from t=0; aggregate "
+            "particle-steps over the slowest process's main-loop time; laser source omitted (the "
+            "reference has no analytic sin^2 source; the source plane is O(n^2) work)" % (procs, steps))
+    return {"value": rate, "seconds": max(secs), "markers": len(m), "procs": procs,
+            "per_process": len(m) * steps / statistics.median(secs), "sample": desc}
 
 
 # ---------------------------------------------------------------------------
@@ -289,17 +338,20 @@ def run_reference_arm(args, w, world, rank):
     res = reference_sample(w, steps)
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable":
-                          "reference binaries not built (make -C oracle ref)"}))
+                          "reference binaries not built (make -C oracle ref REF=<reference root>)"}))
         return
-    rate, sec, nm, desc = res
+    rate = res["value"]
     line = {"metric": "particle-steps/s", "value": rate, "unit": "particle-steps/s",
-            "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * sec / steps, "higher_is_better": True, "scaling": "weak",
+            "impl": "reference", "n_gpus": args.gpus, "steps": steps, "warmup": 0,
+            "requested": {"steps": args.steps, "warmup": args.warmup},
+            "ms_per_step": 1e3 * res["seconds"] / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": w["name"], "markers": nm, "grid": list(w["n"]),
-                       "bc": "mur x6", "courant": 0.5},
-            "cpu_baseline": {"value": rate, "unit": "particle-steps/s", "cores": 1,
-                             "kind": "reference", "sample": desc},
+            "config": {"workload": w["name"], "markers": res["markers"], "grid": list(w["n"]),
+                       "bc": "mur x6", "courant": 0.5, "laser": "omitted (no sin^2 source in the reference)",
+                       "copies": res["procs"]},
+            "cpu_baseline": {"value": rate, "unit": "particle-steps/s", "cores": res["procs"],
+                             "kind": "reference", "sample": res["sample"],
+                             "per_process": res["per_process"]},
             "e2e": {"value": rate, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -398,49 +450,54 @@ def batch_bench(args):
     }))
 
 
-def serve_bench(args):
+def serve_measure(requests=24, step_scale=1.0, chaos=True):
     """A Poisson stream (200 requests/s) of laser-foil scan solves served
     with continuous batching in the precision form, against the same solves
-    run one at a time in the plain FP64 form (queued in arrival order)."""
+    run one at a time in the plain FP64 form (queued in arrival order).
+    Accuracy: per solve, the served total-energy history against the FP64
+    solve's, next to the FP64 chaos floor -- the FP64 solve against itself
+    with the laser amplitude moved by one ulp, which bounds how closely any
+    two runs of these chaotic laser-plasmas can agree."""
     import torch
-    import mandor3_b200 as mg
     from mandor3_b200 import scan, FP64
-    specs = serve_specs(count=args.requests, step_scale=args.step_scale)
+    import dataclasses
+    specs = serve_specs(count=requests, step_scale=step_scale)
     stream = scan.poisson_stream(specs, 200.0)
     tuner = scan.Tuner(steps=6, sorts=(8, 16))
+    t = time.perf_counter()
     for s in specs:
         tuner.choose(s)
+    tune_s = time.perf_counter() - t
     srv = scan.Server(chunk=100, tuner=tuner)
     with Clocks(0) as clocks:
         torch.cuda.synchronize()
         t = time.perf_counter()
         res = srv.serve(stream)
         served_s = time.perf_counter() - t
-    # Plain FP64, one solve at a time in arrival order.
-    import dataclasses
-    done, lat, fp64_s, err = 0.0, [], 0.0, []
+    tot = lambda a: a[:, 1] + a[:, 2] + a[:, 3:6].sum(1)
+    done, lat, fp64_s, err, floor = 0.0, [], 0.0, [], []
     for (arr, s), r in zip(stream, res):
         plain = dataclasses.replace(s, precision=FP64)
         rows, count, sec = scan.run_alone(plain)
         fp64_s += sec
         done = max(done, arr) + sec
         lat.append(done - arr)
-        tot = lambda a: a[:, 1] + a[:, 2] + a[:, 3:6].sum(1)
         scale = np.max(np.abs(tot(rows)))
         err.append(float(np.max(np.abs(tot(r.rows) - tot(rows))) / scale))
+        if chaos:
+            nudged = dataclasses.replace(plain, a0=float(np.nextafter(plain.a0, np.inf)))
+            rows2, _, _ = scan.run_alone(nudged)
+            floor.append(float(np.max(np.abs(tot(rows2) - tot(rows))) / scale))
     psteps = sum(s.markers() * s.steps for s in specs)
-    print(json.dumps({
-        "metric": "scan solves/s", "value": len(specs) / served_s, "unit": "solves/s", "n_gpus": 1,
-        "steps": int(sum(s.steps for s in specs)), "warmup": 0, "ms_per_step": None,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic",
-        "config": {"workload": "serve_laser_foil_scan", "requests": len(specs), "rate_per_s": 200.0,
-                   "grids": "(64,32,32) x U{1..4}", "ppc": "4-16", "a0": "U(1,10)",
-                   "thickness": "U(0.1,2) lambda", "density": "U(10,100) n_cr",
-                   "steps": "U{1000..3000} x %g" % args.step_scale, "admission": "device footprint",
-                   "budget_bytes": srv.budget, "peak_admitted_bytes": srv.peak_used,
-                   "server_host_seconds": srv.stats},
+    out = {
+        "workload": "serve_laser_foil_scan", "requests": len(specs), "rate_per_s": 200.0,
+        "grids": "(64,32,32) x U{1..4}", "ppc": "4-16", "a0": "U(1,10)", "thickness": "U(0.1,2) lambda",
+        "density": "U(10,100) n_cr", "steps": "U{1000..3000} x %g" % step_scale,
+        "precision": "int cell + FP32 offset (served) vs plain FP64 (one at a time)",
+        "admission": "device footprint", "budget_bytes": srv.budget, "peak_admitted_bytes": srv.peak_used,
+        "server_host_seconds": srv.stats, "tuning_seconds": tune_s,
         "clocks": clocks.summary(),
+        "solves_per_s": len(specs) / served_s,
         "served": {"seconds": served_s, "particle_steps_per_s": psteps / served_s,
                    "latency_p50_s": scan.percentile([r.latency for r in res], 50),
                    "latency_p99_s": scan.percentile([r.latency for r in res], 99)},
@@ -448,8 +505,80 @@ def serve_bench(args):
                                      "latency_p50_s": scan.percentile(lat, 50),
                                      "latency_p99_s": scan.percentile(lat, 99)},
         "throughput_over_plain": fp64_s / served_s,
-        "total_energy_error_vs_fp64": {"max": max(err), "median": scan.percentile(err, 50)},
-    }))
+        "total_energy_error_vs_fp64": {"max": max(err), "median": scan.percentile(err, 50),
+                                       "per_solve": err},
+    }
+    if chaos:
+        out["fp64_chaos_floor"] = {"max": max(floor), "median": scan.percentile(floor, 50), "per_solve": floor,
+                                   "note": "FP64 solve against itself with a0 one ulp larger: max over the "
+                                           "history of |W_total difference| / max |W_total|"}
+    return out
+
+
+def serve_bench(args):
+    m = serve_measure(args.requests, args.step_scale)
+    steps = None
+    print(json.dumps({
+        "metric": "scan solves/s", "value": m["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
+        "steps": steps, "warmup": 0, "ms_per_step": None,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": {k: m[k] for k in ("workload", "requests", "rate_per_s", "grids", "ppc",
+                                                          "a0", "thickness", "density", "steps", "admission",
+                                                          "budget_bytes", "peak_admitted_bytes")},
+        "clocks": m["clocks"], "serve": m}))
+
+
+def precision_form_measure(device, warmup=3):
+    """BASELINE configuration 3 at full size (256^3 periodic two-stream
+    plasma, 2 x 32 markers per cell = 1.07e9 markers) in the precision form:
+    W warm-up steps, then one sort interval (24 steps, one sort inside) timed
+    with CUDA events on the run's stream; roofline of the tiled push (60 B
+    per marker) and of the whole step (60 B per marker + 72 B per cell);
+    then both forms from t = 0 over the same 24 steps for the energy-history
+    error against FP64."""
+    import torch
+    w = weibel()
+    t = time.perf_counter()
+    r = make_run(w, device)
+    build_s = time.perf_counter() - t
+    r.step(warmup)
+    steps = w["sort_every"]
+    n0 = r.marker_count()
+    stream = torch.cuda.ExternalStream(r.stream(), device=device)
+    r.profile(True)
+    torch.cuda.synchronize()
+    with Clocks(device) as clocks:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r.step_async(steps)
+        e1.record(stream)
+        r.synchronize()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    push_ms, step_ms = r.last_timing()
+    launches = r.kernels_per_step()
+    r.close()
+    peak, peak_kind = hbm_peak()
+    cells = w["n"][0] * w["n"][1] * w["n"][2]
+    push_bytes = w["bytes_per_marker"] * n0
+    step_bytes = push_bytes + 72.0 * cells
+    achieved = push_bytes / (push_ms / 1e3) / 1e9
+    step_achieved = step_bytes / (ms / steps / 1e3) / 1e9
+    out = {"workload": w["name"], "markers": n0, "grid": list(w["n"]), "dtype": "f32",
+           "precision": "int cell + FP32 offset, FP32 u/E/H/J, FP64 reductions",
+           "steps": steps, "warmup": warmup, "sort_every": w["sort_every"], "sorts_in_window": 1,
+           "ms_per_step": ms / steps, "value": n0 * steps / (ms / 1e3), "unit": "particle-steps/s",
+           "build_seconds": build_s, "clocks": clocks.summary(), "gpu_launches_per_step": launches,
+           "roofline": {"bound": "hbm", "kernel": "k_push32_tiles", "achieved": achieved, "peak": peak,
+                        "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                        "traffic": ncu_traffic(w, n0), "push_ms": push_ms,
+                        "algorithmic_bytes_per_launch": push_bytes},
+           "step_roofline": {"achieved": step_achieved, "peak": peak, "unit": "GB/s", "frac": step_achieved / peak,
+                             "algorithmic_bytes_per_step": step_bytes,
+                             "note": "60 B per marker + 72 B per cell over the whole step, its sort included"}}
+    out["fp64_comparison"] = compare_fp64(w, device, steps)
+    return out
 
 
 def main():
@@ -462,6 +591,8 @@ def main():
     ap.add_argument("--ref-steps", type=int, default=12)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the precision-form (configuration 3) and serving sub-objects of the default line")
     ap.add_argument("--requests", type=int, default=24, help="serve workload: solves in the stream")
     ap.add_argument("--step-scale", type=float, default=1.0, help="serve workload: scale of the solves' steps")
     ap.add_argument("--compare-fp64", type=int, default=0, metavar="K",
@@ -538,13 +669,26 @@ def main():
     if args.compare_fp64 > 0 and w["precision"] != 0:
         compare = compare_fp64(w, device, args.compare_fp64)
 
+    # The other north-star forms, on rank 0 of a single-GPU run: the
+    # precision form at configuration 3's full size and the served scan.
+    extras = {}
+    if world == 1 and w["precision"] == 0 and not args.no_extras:
+        for key, fn in (("precision_form", lambda: precision_form_measure(device)),
+                        ("serve", lambda: serve_measure(args.requests, args.step_scale))):
+            t = time.perf_counter()
+            try:
+                extras[key] = fn()
+            except Exception as e:                      # report, keep the headline line
+                extras[key] = {"error": "%s: %s" % (type(e).__name__, e)}
+            extras[key]["wall_seconds"] = time.perf_counter() - t
+            torch.cuda.empty_cache()
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         res = reference_sample(w, args.ref_steps)
         if res:
-            rate, sec, nm, desc = res
-            cpu = {"value": rate, "unit": "particle-steps/s", "cores": 1, "kind": "reference",
-                   "sample": desc}
+            cpu = {"value": res["value"], "unit": "particle-steps/s", "cores": res["procs"],
+                   "kind": "reference", "sample": res["sample"], "per_process": res["per_process"]}
     barrier(world)
     if rank != 0:
         return
@@ -558,6 +702,7 @@ def main():
             "cpu_baseline": cpu}
     if compare:
         line["fp64_comparison"] = compare
+    line.update(extras)
     print(json.dumps(line), flush=True)
 
 
