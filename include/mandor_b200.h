@@ -51,6 +51,7 @@ extern "C" {
                                    the J ghost layers: Courant violated)     */
 #define MG_ERR_IO        (-7)   /* input file error: core_b200.out exits 7   */
 #define MG_ERR_ADMISSION (-8)   /* serving admission refused (HBM budget)    */
+#define MG_ERR_TIMEOUT   (-9)   /* a bounded device wait gave up             */
 
 /* Boundary condition codes, same values as misc_parameters.h:38-42. */
 enum { MG_BC_PERIODIC = 0, MG_BC_MIRROR = 1, MG_BC_OPEN = 2 };
@@ -107,7 +108,10 @@ typedef struct {
 /* Uniform random marker placement driven by the reference's ranmar
  * generator (misc_ranmar.c:79-146).  Cells [lo, hi) per axis, i-major and
  * k-minor; per marker seven consecutive draws: three in-cell offsets, then
- * two Box-Muller pairs whose first three normals scale uth.  The stream is
+ * two Box-Muller pairs (r = sqrt(-2 log(1 - u)), angle 2 pi u') whose first
+ * three normals scale uth.  The logarithm, sine and cosine are the
+ * library's own series in IEEE +, -, *, /, sqrt only, so positions and
+ * momenta are the same bits as a C restatement on the host.  The stream is
  * ranmar(seed_ij, seed_kl) after `skip` draws; marker m of the box uses
  * draws [skip + 7m, skip + 7m + 7). */
 typedef struct {

@@ -29,7 +29,7 @@ MARKER_DTYPE = np.dtype([("x", "<f8"), ("y", "<f8"), ("z", "<f8"),
                          ("pad", "<i4")])
 
 ERRORS = {-1: "cuda", -2: "argument", -3: "out of memory", -4: "stage order",
-          -5: "capacity", -6: "bounds", -7: "io", -8: "admission"}
+          -5: "capacity", -6: "bounds", -7: "io", -8: "admission", -9: "timeout"}
 
 
 class MandorError(RuntimeError):

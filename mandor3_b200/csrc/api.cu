@@ -3,6 +3,8 @@
 // API that mirrors core/main.c's step, and the graph-replayed step loop.
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include <stdarg.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -128,7 +130,7 @@ __global__ void k_markers_out (Markers64 m, long long from, long long n, mg_mark
       p.qDivM = qm;
       p.id = m.id[o];
       p.pad_ = 0;
-      dst[slot[t]] = p;
+      dst[slot ? slot[t] : t] = p;
    }
 }
 
@@ -212,6 +214,70 @@ int mg_ensure_stage (mg_run_t *r, size_t bytes)
    }
    TRY (mg_dev_alloc (r, &r->stage, bytes));
    r->stage_bytes = bytes;
+   return MG_OK;
+}
+
+// The copy stream and its events (created on first use).
+static int ensure_xfer (mg_run_t *r)
+{
+   if (r->xfer)
+      return MG_OK;
+   MG_CUDA (cudaStreamCreateWithFlags (&r->xfer, cudaStreamNonBlocking));
+   for (int b = 0 ; b < 2 ; ++b)
+      for (int e = 0 ; e < 2 ; ++e)
+         MG_CUDA (cudaEventCreateWithFlags (&r->xev[b][e], cudaEventDisableTiming));
+   return MG_OK;
+}
+
+// Device -> host through the two halves of the staging buffer: chunk q is
+// converted on the run's stream into half q % 2 (`convert` launches the
+// kernel for chunk q, of `bytes[q]` bytes), then copied to host[q] on the
+// copy stream while the run's stream converts chunk q + 1.
+template <class Convert>
+static int pipelined_d2h (mg_run_t *r, int chunks, size_t half, Convert convert, void *const *host,
+                          const size_t *bytes)
+{
+   TRY (ensure_xfer (r));
+   TRY (mg_ensure_stage (r, 2*half));
+   for (int q = 0 ; q < chunks ; ++q) {
+      const int b = q & 1;
+      char *buf = (char *) r->stage + b*half;
+      if (q >= 2)
+         MG_CUDA (cudaStreamWaitEvent (r->stream, r->xev[b][1], 0));    // copy q-2 done with buf
+      convert (q, buf);
+      MG_LAUNCH_CHECK ();
+      MG_CUDA (cudaEventRecord (r->xev[b][0], r->stream));
+      MG_CUDA (cudaStreamWaitEvent (r->xfer, r->xev[b][0], 0));
+      MG_CUDA (cudaMemcpyAsync (host[q], buf, bytes[q], cudaMemcpyDeviceToHost, r->xfer));
+      MG_CUDA (cudaEventRecord (r->xev[b][1], r->xfer));
+   }
+   MG_CUDA (cudaStreamSynchronize (r->xfer));
+   return MG_OK;
+}
+
+// Host -> device, the same two halves the other way: chunk q is copied on
+// the copy stream into half q % 2, then converted on the run's stream while
+// chunk q + 1 is copied.
+template <class Convert>
+static int pipelined_h2d (mg_run_t *r, int chunks, size_t half, Convert convert, const void *const *host,
+                          const size_t *bytes)
+{
+   TRY (ensure_xfer (r));
+   TRY (mg_ensure_stage (r, 2*half));
+   MG_CUDA (cudaEventRecord (r->xev[0][1], r->stream));     // earlier work on the stage is ordered first
+   MG_CUDA (cudaStreamWaitEvent (r->xfer, r->xev[0][1], 0));
+   for (int q = 0 ; q < chunks ; ++q) {
+      const int b = q & 1;
+      char *buf = (char *) r->stage + b*half;
+      if (q >= 2)
+         MG_CUDA (cudaStreamWaitEvent (r->xfer, r->xev[b][1], 0));      // conversion q-2 done with buf
+      MG_CUDA (cudaMemcpyAsync (buf, host[q], bytes[q], cudaMemcpyHostToDevice, r->xfer));
+      MG_CUDA (cudaEventRecord (r->xev[b][0], r->xfer));
+      MG_CUDA (cudaStreamWaitEvent (r->stream, r->xev[b][0], 0));
+      convert (q, buf);
+      MG_LAUNCH_CHECK ();
+      MG_CUDA (cudaEventRecord (r->xev[b][1], r->stream));
+   }
    return MG_OK;
 }
 
@@ -314,7 +380,8 @@ extern "C" long long mg_estimate_bytes (const mg_params_t *p, long long markers)
 {
    if (!p)
       return -1;
-   Grid g = make_grid (p->n, p->h, p->tau, p->bc_min, p->bc_max);
+   Grid g = make_grid (p->n, p->h, p->tau, p->bc_min, p->bc_max,
+                       p->precision == MG_FP64 ? MG_GZ_FRONT : MG_GZ_FRONT32);
    const long long elt = (p->precision == MG_FP64) ? 8 : 4;
    long long b = 12LL*g.total*elt;
    for (int a = 0 ; a < 3 ; ++a)
@@ -351,7 +418,8 @@ extern "C" int mg_run_create (const mg_params_t *params, mg_run_t **out)
    mg_run_t *r = (mg_run_t *) calloc (1, sizeof (mg_run_t));
    r->prm = *params;
    r->device = params->device;
-   r->g = make_grid (params->n, params->h, params->tau, params->bc_min, params->bc_max);
+   r->g = make_grid (params->n, params->h, params->tau, params->bc_min, params->bc_max,
+                     params->precision == MG_FP64 ? MG_GZ_FRONT : MG_GZ_FRONT32);
    r->time = params->time;
    if (cudaStreamCreateWithFlags (&r->stream, cudaStreamNonBlocking) != cudaSuccess) {
       free (r);
@@ -479,6 +547,13 @@ extern "C" int mg_run_destroy (mg_run_t *r)
    if (r->gauss_out) cudaFree (r->gauss_out);
    for (int e = 0 ; e < 4 ; ++e)
       if (r->ev[e]) cudaEventDestroy (r->ev[e]);
+   if (r->xfer) {
+      cudaStreamSynchronize (r->xfer);
+      for (int b = 0 ; b < 2 ; ++b)
+         for (int e = 0 ; e < 2 ; ++e)
+            if (r->xev[b][e]) cudaEventDestroy (r->xev[b][e]);
+      cudaStreamDestroy (r->xfer);
+   }
    if (r->stream) cudaStreamDestroy (r->stream);
    free (r);
    return MG_OK;
@@ -495,17 +570,16 @@ extern "C" int mg_run_set_fields (mg_run_t *r, const double *E, const double *H)
    }
    const long vol = (long) (r->g.n[0] + 1)*(r->g.n[1] + 1)*(r->g.n[2] + 1);
    const size_t bytes = (size_t) vol*3*sizeof (double);
-   TRY (mg_ensure_stage (r, bytes));
-   const double *src[2] = {E, H};
-   double **dst[2] = {r->E, r->H};
-   for (int f = 0 ; f < 2 ; ++f) {
-      if (!src[f])
-         continue;
-      MG_CUDA (cudaMemcpyAsync (r->stage, src[f], bytes, cudaMemcpyHostToDevice, r->stream));
-      k_fields_in<<<mg_blocks_for (vol, 256, 8), 256, 0, r->stream>>> (r->g, (const double *) r->stage,
-                                                                       dst[f][0], dst[f][1], dst[f][2]);
-      MG_LAUNCH_CHECK ();
-   }
+   const void *host[2];
+   double **dst[2];
+   size_t sizes[2] = {bytes, bytes};
+   int nf = 0;
+   if (E) { host[nf] = E; dst[nf++] = r->E; }
+   if (H) { host[nf] = H; dst[nf++] = r->H; }
+   TRY (pipelined_h2d (r, nf, bytes, [&] (int q, char *buf) {
+      k_fields_in<<<mg_blocks_for (vol, 256, 8), 256, 0, r->stream>>> (r->g, (const double *) buf,
+                                                                       dst[q][0], dst[q][1], dst[q][2]);
+   }, host, sizes));
    MG_CUDA (cudaStreamSynchronize (r->stream));
    r->inited = 0;
    return MG_OK;
@@ -519,23 +593,32 @@ int mg_fields_out (mg_run_t *r, double *E, double *H, bool dev)
       return mg_fields_out32 (r, E, H, dev);
    const long vol = (long) (r->g.n[0] + 1)*(r->g.n[1] + 1)*(r->g.n[2] + 1);
    const size_t bytes = (size_t) vol*3*sizeof (double);
-   if (!dev)
-      TRY (mg_ensure_stage (r, bytes));
    double *dst[2] = {E, H};
    // Between mg_em_HHalfStep and mg_em_HStep the reference's H is H^n.
    double **src[2] = {r->E, (r->stage_no >= 1 && r->stage_no <= 3) ? r->Hn : r->H};
-   for (int f = 0 ; f < 2 ; ++f) {
-      if (!dst[f])
-         continue;
-      k_fields_out<<<mg_blocks_for (vol, 256, 8), 256, 0, r->stream>>> (r->g, dev ? dst[f] : (double *) r->stage,
-                                                                        src[f][0], src[f][1], src[f][2], 0);
-      MG_LAUNCH_CHECK ();
-      if (!dev) {
-         MG_CUDA (cudaMemcpyAsync (dst[f], r->stage, bytes, cudaMemcpyDeviceToHost, r->stream));
-         MG_CUDA (cudaStreamSynchronize (r->stream));
+   if (dev) {
+      for (int f = 0 ; f < 2 ; ++f) {
+         if (!dst[f])
+            continue;
+         k_fields_out<<<mg_blocks_for (vol, 256, 8), 256, 0, r->stream>>> (r->g, dst[f], src[f][0], src[f][1],
+                                                                           src[f][2], 0);
+         MG_LAUNCH_CHECK ();
       }
+      return MG_OK;
    }
-   return MG_OK;
+   void *host[2];
+   double **from[2];
+   size_t sizes[2] = {bytes, bytes};
+   int nf = 0;
+   for (int f = 0 ; f < 2 ; ++f)
+      if (dst[f]) {
+         host[nf] = dst[f];
+         from[nf++] = src[f];
+      }
+   return pipelined_d2h (r, nf, bytes, [&] (int q, char *buf) {
+      k_fields_out<<<mg_blocks_for (vol, 256, 8), 256, 0, r->stream>>> (r->g, (double *) buf, from[q][0],
+                                                                        from[q][1], from[q][2], 0);
+   }, host, sizes);
 }
 
 extern "C" int mg_run_get_fields (mg_run_t *r, double *E, double *H)
@@ -562,6 +645,7 @@ extern "C" int mg_run_get_current (mg_run_t *r, double *J)
 }
 
 static const long long CHUNK = 1LL << 22;   // markers per staged transfer
+static const long long XCHUNK = 1LL << 20;  // markers per half of a pipelined transfer (64 MB)
 
 extern "C" int mg_run_set_markers (mg_run_t *r, const mg_marker_t *m, long long n)
 {
@@ -574,14 +658,19 @@ extern "C" int mg_run_set_markers (mg_run_t *r, const mg_marker_t *m, long long 
       return mg_run_set_markers32 (r, m, n);
    }
    TRY (ensure_capacity (r, n));
-   const long long chunk = n < CHUNK ? n : CHUNK;
-   TRY (mg_ensure_stage (r, (size_t) (chunk > 0 ? chunk : 1)*sizeof (mg_marker_t)));
-   for (long long at = 0 ; at < n ; at += CHUNK) {
-      const long long c = (n - at < CHUNK) ? n - at : CHUNK;
-      MG_CUDA (cudaMemcpyAsync (r->stage, m + at, c*sizeof (mg_marker_t), cudaMemcpyHostToDevice, r->stream));
-      k_markers_in<<<mg_blocks_for (c, 256, 8), 256, 0, r->stream>>> ((const mg_marker_t *) r->stage, c, r->m64, at);
-      MG_LAUNCH_CHECK ();
+   const int chunks = (int) ((n + XCHUNK - 1)/XCHUNK);
+   std::vector<const void *> host (chunks);
+   std::vector<size_t> sizes (chunks);
+   for (int q = 0 ; q < chunks ; ++q) {
+      const long long at = q*XCHUNK, c = (n - at < XCHUNK) ? n - at : XCHUNK;
+      host[q] = m + at;
+      sizes[q] = (size_t) c*sizeof (mg_marker_t);
    }
+   TRY (pipelined_h2d (r, chunks, (size_t) XCHUNK*sizeof (mg_marker_t), [&] (int q, char *buf) {
+      const long long c = (long long) (sizes[q]/sizeof (mg_marker_t));
+      k_markers_in<<<mg_blocks_for (c, 256, 8), 256, 0, r->stream>>> ((const mg_marker_t *) buf, c, r->m64,
+                                                                       q*XCHUNK);
+   }, host.data (), sizes.data ()));
    r->np = n;
    r->tiles_ok = 0;
    MG_CUDA (cudaMemsetAsync (&r->dsc->dead, 0, sizeof (long long), r->stream));
@@ -624,6 +713,23 @@ int mg_markers_out (mg_run_t *r, mg_marker_t *out, long long cap, long long *n, 
    if (cap < live) {
       mg_set_error ("mg_run_get_markers: buffer holds %lld markers, %lld live", cap, live);
       return MG_ERR_CAPACITY;
+   }
+   if (live == r->np && !dev) {
+      // No marker removed: nothing to compact, chunks go straight through
+      // the pipelined copy.
+      const int chunks = (int) ((r->np + XCHUNK - 1)/XCHUNK);
+      std::vector<void *> host (chunks);
+      std::vector<size_t> sizes (chunks);
+      for (int q = 0 ; q < chunks ; ++q) {
+         const long long at = q*XCHUNK, c = (r->np - at < XCHUNK) ? r->np - at : XCHUNK;
+         host[q] = out + at;
+         sizes[q] = (size_t) c*sizeof (mg_marker_t);
+      }
+      return pipelined_d2h (r, chunks, (size_t) XCHUNK*sizeof (mg_marker_t), [&] (int q, char *buf) {
+         const long long c = (long long) (sizes[q]/sizeof (mg_marker_t));
+         k_markers_out<<<mg_blocks_for (c, 256, 8), 256, 0, r->stream>>> (r->m64, q*XCHUNK, c,
+                                                                         (mg_marker_t *) buf, nullptr);
+      }, host.data (), sizes.data ());
    }
    const long long chunk = r->np < CHUNK ? r->np : CHUNK;
    const size_t need = (size_t) (chunk > 0 ? chunk : 1)*(sizeof (mg_marker_t) + sizeof (long long)) + 64;
@@ -972,6 +1078,11 @@ static int check_err (mg_run_t *r)
    if (info[0] & 4) {
       mg_set_error ("TF/SF frame %d is not on the device (mg_run_tfsf_put_frames)", info[1]);
       return MG_ERR_STATE;
+   }
+   if (info[0] & 8) {
+      mg_set_error ("the tiled push gave up waiting for the TMA copy of a field tile (bounded wait); "
+                    "the step is invalid");
+      return MG_ERR_TIMEOUT;
    }
    if (info[0]) {
       mg_set_error ("marker %d left the mesh or moved more than one cell per step "

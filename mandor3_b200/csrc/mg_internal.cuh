@@ -42,8 +42,14 @@ struct Grid {
    }
 };
 
+// Nodes in front of k = 0 in a row: 4 for FP64 (k = 0 starts a 32-byte
+// sector); 5 for FP32, so that the row offset of k = z0 - 1 is a multiple
+// of 4 floats whenever z0 is, as a tensor-memory-access (TMA) tile copy
+// starting there needs (16-byte aligned innermost coordinate).
+#define MG_GZ_FRONT32 5
+
 static inline Grid make_grid (const int n[3], const double h[3], double tau,
-                              const int bc_min[3], const int bc_max[3])
+                              const int bc_min[3], const int bc_max[3], int front = MG_GZ_FRONT)
 {
    Grid g;
    for (int a = 0 ; a < 3 ; ++a) {
@@ -53,12 +59,12 @@ static inline Grid make_grid (const int n[3], const double h[3], double tau,
       g.bc[1][a] = bc_max[a];
    }
    g.tau = tau;
-   long row = MG_GZ_FRONT + n[2] + 1 + MG_GX;
-   row = (row + 3) & ~3L;                       // 32-byte rows
+   long row = front + n[2] + 1 + MG_GX;
+   row = (row + 3) & ~3L;                       // rows of a multiple of 4 elements
    g.sy = row;
    g.sx = row*(n[1] + 1 + 2*MG_GX);
    g.total = g.sx*(n[0] + 1 + 2*MG_GX);
-   g.origin = MG_GX*g.sx + MG_GX*g.sy + MG_GZ_FRONT;
+   g.origin = MG_GX*g.sx + MG_GX*g.sy + front;
    return g;
 }
 
@@ -165,6 +171,11 @@ struct mg_run {
    long long   snap_cap;
    cudaStream_t snap_stream;
    cudaEvent_t snap_ready, snap_done;
+   // Host transfers: a copy stream beside the run's stream and, per half of
+   // the staging buffer, "converted" and "copied" events, so that the
+   // layout conversion of one chunk overlaps the copy of the previous one.
+   cudaStream_t xfer;
+   cudaEvent_t  xev[2][2];
    int         snap_pending;
 
    // focused-laser mirrors (mg_run_add_mirror)

@@ -19,6 +19,7 @@
 #include <string.h>
 
 #include "mg_internal.cuh"
+#include "placer_math.cuh"
 
 #define RM_LAG 97
 #define RM_MASK 0xFFFFFFu
@@ -137,11 +138,12 @@ k_place (PlaceArgs a, const uint32_t *states, Markers64 m)
       m.x[o] = (i + u[0])*a.h[0];
       m.y[o] = (j + u[1])*a.h[1];
       m.z[o] = (k + u[2])*a.h[2];
-      const double r1 = sqrt (-2.0*log (1.0 - u[3])), t1 = 2*M_PI*u[4];
-      const double r2 = sqrt (-2.0*log (1.0 - u[5])), t2 = 2*M_PI*u[6];
-      m.ux[o] = a.s.drift[0] + a.s.uth[0]*(r1*cos (t1));
-      m.uy[o] = a.s.drift[1] + a.s.uth[1]*(r1*sin (t1));
-      m.uz[o] = a.s.drift[2] + a.s.uth[2]*(r2*cos (t2));
+      double gx, gy, gz, gw;
+      pm_box_muller (u[3], u[4], &gx, &gy);
+      pm_box_muller (u[5], u[6], &gz, &gw);
+      m.ux[o] = a.s.drift[0] + a.s.uth[0]*gx;
+      m.uy[o] = a.s.drift[1] + a.s.uth[1]*gy;
+      m.uz[o] = a.s.drift[2] + a.s.uth[2]*gz;
       m.rho[o] = (float) a.s.rho;
       m.qm[o] = (float) a.s.qDivM;
       m.id[o] = a.s.id0 + (int) n;

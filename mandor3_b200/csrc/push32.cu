@@ -12,7 +12,9 @@
 //
 // Marker cells are packed as ((i+1) << 20) | ((j+1) << 10) | (k+1) with
 // i in [-1, 1022]: one 32-bit word, unpacked with shifts.
+#include <cuda.h>                // CUtensorMap and the tensor-map encoder's types
 #include <cuda_runtime.h>
+#include <stdint.h>
 
 #include "mg_internal.cuh"
 
@@ -25,6 +27,13 @@ struct Ctx32 {
    float  tau, rh[3];            // tau, 1/h
    float  kj[3];                 // h_a / tau: current prefactor per unit rho and cell-unit displacement
    double vol;                   // h1 h2 h3 for the thermal tally
+   int    kfront;                // nodes in front of k = 0 in a row (MG_GZ_FRONT32)
+};
+
+// Tensor maps of the six FP32 field arrays (Ex Ey Ez, Hx Hy Hz at t = n tau)
+// of this GPU's run, for the tiled push's TMA copies of a tile's nodes.
+struct TileMaps {
+   CUtensorMap m[6];
 };
 
 __device__ __forceinline__ int unpack (int c, int s) { return ((c >> s) & 1023) - 1; }
@@ -443,9 +452,58 @@ __device__ __forceinline__ void cp_async_wait1 ()
    asm volatile ("cp.async.wait_group 1;" ::: "memory");
 }
 
-__device__ __forceinline__ void cp_async_wait_all ()
+
+// ---- TMA tile copies and their mbarrier ----------------------------------------
+__device__ __forceinline__ unsigned smem_u32 (const void *p)
 {
-   asm volatile ("cp.async.wait_all;" ::: "memory");
+   return (unsigned) __cvta_generic_to_shared (p);
+}
+
+__device__ __forceinline__ void mbar_init (uint64_t *bar, unsigned count)
+{
+   asm volatile ("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r" (smem_u32 (bar)), "r" (count) : "memory");
+   asm volatile ("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// One arrival that also announces `bytes` of copies completing on the barrier.
+__device__ __forceinline__ void mbar_expect_tx (uint64_t *bar, unsigned bytes)
+{
+   asm volatile ("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                 :: "r" (smem_u32 (bar)), "r" (bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait (uint64_t *bar, unsigned parity)
+{
+   unsigned ok;
+   asm volatile ("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r" (ok) : "r" (smem_u32 (bar)), "r" (parity) : "memory");
+   return ok != 0;
+}
+
+// Waits for the barrier's phase `parity` to complete, for at most
+// MG_TMA_WAIT_CYCLES clock cycles (about 20 ms); false if it gave up.
+#define MG_TMA_WAIT_CYCLES 40000000LL
+__device__ __forceinline__ bool mbar_wait_bounded (uint64_t *bar, unsigned parity)
+{
+   const long long t0 = clock64 ();
+   while (!mbar_try_wait (bar, parity))
+      if (clock64 () - t0 > MG_TMA_WAIT_CYCLES)
+         return false;
+   return true;
+}
+
+// A 3D tile of a tensor map into shared memory (no multicast: the map
+// covers this GPU's own field array), completing on `bar`.  c0 is the
+// innermost (k) coordinate and must be a multiple of 4 floats.
+__device__ __forceinline__ void tma_load3 (void *dst, const CUtensorMap *map, int c0, int c1, int c2,
+                                           uint64_t *bar)
+{
+   asm volatile ("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%2, %3, %4}], [%5];"
+                 :: "r" (smem_u32 (dst)), "l" (map), "r" (c0), "r" (c1), "r" (c2), "r" (smem_u32 (bar))
+                 : "memory");
 }
 
 // Starts the copy of marker n's nine pushed arrays into buffer b (the lane's
@@ -590,12 +648,13 @@ __device__ __forceinline__ void queued_segments (const Ctx32 &c, int *Jt, const 
 // gather from and add to global memory.
 template <int TX, int TY, int TZ, int GROUP, bool PER>
 __global__ void __launch_bounds__ (256, 3)
-k_push32_tiles (Ctx32 c, const int *tile_start, const int *tile_list, int nty, int ntz, int ntiles,
-                DevScalars *dsc)
+k_push32_tiles (Ctx32 c, const __grid_constant__ TileMaps maps, const int *tile_start, const int *tile_list,
+                int nty, int ntz, int ntiles, DevScalars *dsc)
 {
    const Markers32 m = dsc->m32;
    using D = TileDims<TX, TY, TZ>;
-   extern __shared__ float smem[];
+   extern __shared__ __align__ (128) float smem[];
+   __shared__ __align__ (8) uint64_t s_bar;   // completion of a tile's six TMA copies
    float *F = smem;                           // Ex Ey Ez Hx Hy Hz, D::FN each
    int *Jt = (int *) (smem + 6*D::FN);        // Jx Jy Jz, D::JN each
    float *stg = smem + 6*D::FN + 3*D::JN + (threadIdx.x >> 5)*D::STAGE;
@@ -608,6 +667,10 @@ k_push32_tiles (Ctx32 c, const int *tile_start, const int *tile_list, int nty, i
    const float vol = (float) c.vol;
    double Wx = 0, Wy = 0, Wz = 0;
    long long dead = 0;
+   unsigned phase = 0;
+   if (threadIdx.x == 0)
+      mbar_init (&s_bar, 1);
+   __syncthreads ();
 
    for (;;) {
       if (threadIdx.x == 0) {
@@ -626,22 +689,31 @@ k_push32_tiles (Ctx32 c, const int *tile_start, const int *tile_list, int nty, i
          // from and add to global memory.
          const bool dense = me - mb >= MG_TILE_DENSE;
 
-         // Stage E and H nodes [x0-1, x0+TX+3) x ... (inside the ghost layers),
-         // all copies in flight at once.
-         for (int q = threadIdx.x ; dense && q < 6*D::FN ; q += blockDim.x) {
-            const int comp = q/D::FN, rem = q - comp*D::FN;
-            const int a = rem/D::FYZ, r2 = rem - a*D::FYZ, b = r2/D::FZ, cc = r2 - b*D::FZ;
-            const int gi = x0 - 1 + a, gj = y0 - 1 + b, gk = z0 - 1 + cc;
-            if (gi <= g.n[0] + MG_GX && gj <= g.n[1] + MG_GX && gk <= g.n[2] + MG_GX) {
-               const float *src = comp == 0 ? c.E0 : comp == 1 ? c.E1 : comp == 2 ? c.E2
-                                : comp == 3 ? c.H0 : comp == 4 ? c.H1 : c.H2;
-               cp_async4 (F + q, src + g.at (gi, gj, gk));
-            } else {
-               F[q] = 0.0f;
+         // Stage E and H nodes [x0-1, x0+TX+3) x ... : six TMA tile copies
+         // (one per component, box FZ x FY x FX in allocation coordinates,
+         // nodes past the arrays' ends read as zero) issued by one thread,
+         // all threads waiting on the tile's mbarrier.  The barrier at the
+         // end of the previous tile ordered every read of the old tile
+         // before this proxy fence and the copies.
+         if (dense) {
+            if (threadIdx.x == 0) {
+               asm volatile ("fence.proxy.async.shared::cta;" ::: "memory");
+               mbar_expect_tx (&s_bar, 6*D::FN*(unsigned) sizeof (float));
+#pragma unroll
+               for (int comp = 0 ; comp < 6 ; ++comp)
+                  tma_load3 (F + comp*D::FN, &maps.m[comp], z0 - 1 + c.kfront, y0 - 1 + MG_GX,
+                             x0 - 1 + MG_GX, &s_bar);
+            }
+            const bool late = !mbar_wait_bounded (&s_bar, phase);
+            phase ^= 1;
+            if (__syncthreads_or (late)) {
+               // The copies did not complete in time: report it and stop
+               // this block (the step is flagged invalid on the host).
+               if (threadIdx.x == 0)
+                  atomicOr (&dsc->err, 8);
+               break;
             }
          }
-         cp_async_commit ();
-         cp_async_wait_all ();
 
          for (int cb = mb ; cb < me ; cb += MG_TILE_CHUNK) {
             const int ce = min (cb + MG_TILE_CHUNK, me);
@@ -905,12 +977,74 @@ k_push32_tiles (Ctx32 c, const int *tile_start, const int *tile_list, int nty, i
          return rc_;                                                         \
    } while (0)
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no
+// link against the driver library).
+typedef CUresult (*EncodeTiled) (CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
+                                 CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                 CUtensorMapFloatOOBfill);
+
+static EncodeTiled tensor_map_encoder ()
+{
+   static EncodeTiled fn = nullptr;
+   if (!fn) {
+      void *p = nullptr;
+      cudaDriverEntryPointQueryResult q;
+      if (cudaGetDriverEntryPoint ("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+          q == cudaDriverEntryPointSuccess)
+         fn = (EncodeTiled) p;
+   }
+   return fn;
+}
+
+// The six field arrays as 3D tensors (k, j, i in allocation coordinates;
+// k extent up to the last ghost node, so the row padding reads as zero)
+// with a box of the tile's staged nodes.
+template <int TX, int TY, int TZ>
+static int make_tile_maps (const Ctx32 &c, TileMaps &tm)
+{
+   static_assert (TZ % 4 == 0, "TMA tile copies start at k = z0 - 1: z0 must be a multiple of 4");
+   static_assert (MG_GZ_FRONT32 % 4 == 1, "k = z0 - 1 must fall on a multiple of 4 floats");
+   const EncodeTiled enc = tensor_map_encoder ();
+   if (!enc) {
+      mg_set_error ("cuTensorMapEncodeTiled is not available from the CUDA driver");
+      return MG_ERR_CUDA;
+   }
+   const Grid &g = c.g;
+   const cuuint64_t dims[3] = {(cuuint64_t) (c.kfront + g.n[2] + 1 + MG_GX),
+                               (cuuint64_t) (g.n[1] + 1 + 2*MG_GX), (cuuint64_t) (g.n[0] + 1 + 2*MG_GX)};
+   const cuuint64_t strides[2] = {(cuuint64_t) g.sy*sizeof (float), (cuuint64_t) g.sx*sizeof (float)};
+   const cuuint32_t box[3] = {TZ + 4, TY + 4, TX + 4};
+   const cuuint32_t estr[3] = {1, 1, 1};
+   const float *arr[6] = {c.E0, c.E1, c.E2, c.H0, c.H1, c.H2};
+   if (strides[0] % 16 || strides[1] % 16) {
+      mg_set_error ("field rows of %lld bytes cannot be copied by TMA", (long long) strides[0]);
+      return MG_ERR_ARG;
+   }
+   for (int q = 0 ; q < 6 ; ++q) {
+      if (((uintptr_t) arr[q]) % 16) {
+         mg_set_error ("field array %d is not 16-byte aligned", q);
+         return MG_ERR_ARG;
+      }
+      const CUresult e = enc (&tm.m[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *) arr[q], dims, strides, box,
+                              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (e != CUDA_SUCCESS) {
+         mg_set_error ("cuTensorMapEncodeTiled failed (%d) for field array %d", (int) e, q);
+         return MG_ERR_CUDA;
+      }
+   }
+   return MG_OK;
+}
+
 // Launches the tiled push of one tile size: persistent CTAs, as many as fit
 // on the GPU (at most one per tile).
 template <int TX, int TY, int TZ>
 static int launch_tiles (mg_run_t *r, const Ctx32 &c, bool per)
 {
    using D = TileDims<TX, TY, TZ>;
+   TileMaps tm;
+   TRY32 ((make_tile_maps<TX, TY, TZ> (c, tm)));
    auto kp = k_push32_tiles<TX, TY, TZ, MG_TILE_GROUP, true>;
    auto kn = k_push32_tiles<TX, TY, TZ, MG_TILE_GROUP, false>;
    static int attr_dev = -1;
@@ -928,7 +1062,7 @@ static int launch_tiles (mg_run_t *r, const Ctx32 &c, bool per)
    if (blocks > r->ntiles)
       blocks = r->ntiles;
    MG_CUDA (cudaMemsetAsync (&r->dsc->tile_next, 0, sizeof (int), r->stream));
-   (per ? kp : kn)<<<blocks, 256, D::BYTES, r->stream>>> (c, r->tile_start, r->tile_list, r->tiles[1],
+   (per ? kp : kn)<<<blocks, 256, D::BYTES, r->stream>>> (c, tm, r->tile_start, r->tile_list, r->tiles[1],
                                                             r->tiles[2], r->ntiles, r->dsc);
    MG_LAUNCH_CHECK ();
    return MG_OK;
@@ -949,6 +1083,7 @@ int mg_push32 (mg_run_t *r)
       c.kj[a] = (float) (r->g.h[a]/r->g.tau);
    }
    c.vol = r->g.h[0]*r->g.h[1]*r->g.h[2];
+   c.kfront = (int) (r->g.origin - MG_GX*r->g.sx - MG_GX*r->g.sy);
    const int T = 256;
    if (!r->tiles_ok) {
       k_push32<<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (c, r->np, nullptr, r->dsc);

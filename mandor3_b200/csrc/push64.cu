@@ -18,9 +18,12 @@
 // the periodic sort), so consecutive lanes of a warp usually start in the
 // same cell.  The twelve contributions of each marker's first segment (which
 // always lies in its start cell) are summed across lanes that share the
-// cell with a segmented warp scan, and one lane per run of equal cells
-// issues the twelve atomics.  Further segments of cell-crossing markers add
-// their contributions directly.
+// cell with a segmented warp scan (only as many rounds as the warp's longest
+// run needs), and one lane per run of equal cells issues the twelve
+// atomics.  (Letting every lane add its own weights when a warp spans many
+// cells measured slower late in the laser-foil run: neighbouring cells
+// share current nodes, so those atomics collide.)  Further segments of
+// cell-crossing markers add their contributions directly.
 #include <cuda_runtime.h>
 #include <stdlib.h>
 
@@ -73,6 +76,20 @@ __device__ __forceinline__ double div_by (double a, double b, double y)
 }
 
 #define R12 (1.0/12.0)
+
+// 1/b for the thermal tally: the hardware's approximate reciprocal refined
+// by two Newton-Raphson steps y <- y + y (1 - b y), each roughly doubling
+// the correct bits (about 2^-23 after the first, below 2^-50 after the
+// second), for |b| in the normal range.
+__device__ __forceinline__ double recip (double b)
+{
+   double y;
+   asm ("rcp.approx.ftz.f64 %0, %1;" : "=d" (y) : "d" (b));
+   double e = __fma_rn (-b, y, 1.0);
+   y = __fma_rn (y, e, y);
+   e = __fma_rn (-b, y, 1.0);
+   return __fma_rn (y, e, y);
+}
 
 __device__ __forceinline__ double cic (const double *F, const Grid &g, int i, double sx,
                                        int j, double sy, int k, double sz)
@@ -265,18 +282,6 @@ __device__ __forceinline__ double warp_sum (double v)
    return v;
 }
 
-// Segmented inclusive sum over lanes: lanes [seg_start, lane] of the run of
-// equal keys that contains this lane.
-__device__ __forceinline__ double seg_scan (double v, int lane, int seg_start)
-{
-#pragma unroll
-   for (int d = 1 ; d < 32 ; d <<= 1) {
-      const double t = __shfl_up_sync (0xffffffffu, v, d);
-      if (lane - d >= seg_start)
-         v += t;
-   }
-   return v;
-}
 
 // One wall of core/plasma_walls.c:27-104; returns true if the marker goes.
 // Once removed, later walls leave it alone (it is dropped by the caller).
@@ -355,7 +360,11 @@ k_push64 (Ctx c, Markers64 m, long long np, DevScalars *dsc)
             const double tm = 0.5*tau*qm;
             const double px = m.ux[n] + tm*Ex, py = m.uy[n] + tm*Ey, pz = m.uz[n] + tm*Ez;
             const double gamma = sqrt (1.0 + px*px + py*py + pz*pz);
-            const double W = (gamma - 1.0)*rho/(px*px + py*py + pz*pz + 1e-19)*h1*h2*h3/qm;
+            // The tally's two divisions (core/plasma.c:140) by one
+            // reciprocal: W is summed over markers and blocks in an order of
+            // its own anyway, so a last-place difference per marker is
+            // below the sums' own rounding.
+            const double W = (gamma - 1.0)*rho*h1*h2*h3*recip ((px*px + py*py + pz*pz + 1e-19)*qm);
             Wx += W*px*px;
             Wy += W*py*py;
             Wz += W*pz*pz;
@@ -456,9 +465,17 @@ k_push64 (Ctx c, Markers64 m, long long np, DevScalars *dsc)
       const unsigned heads = __ballot_sync (0xffffffffu, head);
       const unsigned le = (lane == 31) ? 0xffffffffu : ((1u << (lane + 1)) - 1);
       const int seg_start = 31 - __clz (heads & le);
+      // Scan rounds up to the longest run of the warp (a cold, sorted foil
+      // has runs of 16 lanes: four rounds instead of five).
+      const unsigned longest = __reduce_max_sync (0xffffffffu, (unsigned) (lane - seg_start + 1));
+      for (int d = 1 ; d < (int) longest ; d <<= 1) {
 #pragma unroll
-      for (int q = 0 ; q < 12 ; ++q)
-         wgt[q] = seg_scan (wgt[q], lane, seg_start);
+         for (int q = 0 ; q < 12 ; ++q) {
+            const double t = __shfl_up_sync (0xffffffffu, wgt[q], d);
+            if (lane - d >= seg_start)
+               wgt[q] += t;
+         }
+      }
       if (valid && tail)
          scatter12 (c, i, j, k, wgt);
    }

@@ -1340,6 +1340,75 @@ void po_ranmar (po_ranmar_t *g, double *out, long n)
    }
 }
 
+/* The placer's Box-Muller transform (the rule of mg_place_t): its own
+ * logarithm and sine/cosine from IEEE +, -, *, /, sqrt only, restated here
+ * in the same operation order as the device's, so the momenta agree to
+ * the bit.  log v: v = m 2^e, m in [sqrt(1/2), sqrt(2)), log v =
+ * e ln2 + 2 s (1 + s^2/3 + ... + s^24/25), s = (m-1)/(m+1); (cos, sin) of
+ * 2 pi u: quadrant q = floor(4u), f = 4u - q, angle (pi/2) min(f, 1-f) in
+ * [0, pi/4], Taylor series of sin (to t^17) and cos (to t^18), then the
+ * complementary swap and the quadrant rotation. */
+static double po_log (double v)
+{
+   int e = 0;
+   double m = frexp (v, &e);
+   if (m < 0x1.6a09e667f3bcdp-1) {
+      m = m*2.0;
+      e = e - 1;
+   }
+   const double s = (m - 1.0)/(m + 1.0);
+   const double z = s*s;
+   static const double c[12] = {
+      0x1.642c8590b2164p-5, 0x1.8618618618618p-5, 0x1.af286bca1af28p-5, 0x1.e1e1e1e1e1e1ep-5,
+      0x1.1111111111111p-4, 0x1.3b13b13b13b14p-4, 0x1.745d1745d1746p-4, 0x1.c71c71c71c71cp-4,
+      0x1.2492492492492p-3, 0x1.999999999999ap-3, 0x1.5555555555555p-2, 1.0};
+   double p = 0x1.47ae147ae147bp-5;
+   for (int q = 0 ; q < 12 ; ++q)
+      p = p*z + c[q];
+   const double de = (double) e;
+   return de*0x1.62e42fee00000p-1 + (de*0x1.a39ef35793c76p-33 + 2.0*s*p);
+}
+
+static void po_sincos_2pi (double u, double *sn, double *cs)
+{
+   const double x = 4.0*u;
+   const double q = floor (x);
+   double f = x - q;
+   const int swap = f > 0.5;
+   if (swap)
+      f = 1.0 - f;
+   const double t = f*0x1.921fb54442d18p+0;
+   const double z = t*t;
+   static const double cs_[8] = {
+      -0x1.ae7f3e733b81fp-41, 0x1.6124613a86d09p-33, -0x1.ae64567f544e4p-26, 0x1.71de3a556c734p-19,
+      -0x1.a01a01a01a01ap-13, 0x1.1111111111111p-7, -0x1.5555555555555p-3, 1.0};
+   static const double cc_[9] = {
+      0x1.ae7f3e733b81fp-45, -0x1.93974a8c07c9dp-37, 0x1.1eed8eff8d898p-29, -0x1.27e4fb7789f5cp-22,
+      0x1.a01a01a01a01ap-16, -0x1.6c16c16c16c17p-10, 0x1.5555555555555p-5, -0.5, 1.0};
+   double ps = 0x1.952c77030ad4ap-49, pc = -0x1.6827863b97d97p-53;
+   for (int k = 0 ; k < 8 ; ++k)
+      ps = ps*z + cs_[k];
+   for (int k = 0 ; k < 9 ; ++k)
+      pc = pc*z + cc_[k];
+   const double st = t*ps;
+   const double s0 = swap ? pc : st, c0 = swap ? st : pc;
+   switch ((int) q) {
+   case 0:  *sn = s0;  *cs = c0;  break;
+   case 1:  *sn = c0;  *cs = -s0; break;
+   case 2:  *sn = -s0; *cs = -c0; break;
+   default: *sn = -c0; *cs = s0;  break;
+   }
+}
+
+static void po_box_muller (double u_r, double u_t, double *a, double *b)
+{
+   const double r = sqrt (-2.0*po_log (1.0 - u_r));
+   double sn, cs;
+   po_sincos_2pi (u_t, &sn, &cs);
+   *a = r*cs;
+   *b = r*sn;
+}
+
 long po_place_count (const po_place_t *s)
 {
    long cells = 1;
@@ -1368,11 +1437,12 @@ long po_place (const po_place_t *s, const double h[3], po_marker_t *out)
       m->x = (i + d[0])*h[0];
       m->y = (j + d[1])*h[1];
       m->z = (k + d[2])*h[2];
-      const double r1 = sqrt (-2.0*log (1.0 - d[3])), t1 = 2*M_PI*d[4];
-      const double r2 = sqrt (-2.0*log (1.0 - d[5])), t2 = 2*M_PI*d[6];
-      m->vx = s->drift[0] + s->uth[0]*(r1*cos (t1));
-      m->vy = s->drift[1] + s->uth[1]*(r1*sin (t1));
-      m->vz = s->drift[2] + s->uth[2]*(r2*cos (t2));
+      double gx, gy, gz, gw;
+      po_box_muller (d[3], d[4], &gx, &gy);
+      po_box_muller (d[5], d[6], &gz, &gw);
+      m->vx = s->drift[0] + s->uth[0]*gx;
+      m->vy = s->drift[1] + s->uth[1]*gy;
+      m->vz = s->drift[2] + s->uth[2]*gz;
       m->rho = (float) s->rho;
       m->qDivM = (float) s->qDivM;
       m->id = s->id0 + (int) n;

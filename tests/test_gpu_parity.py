@@ -137,10 +137,8 @@ def test_device_placer_is_bit_exact():
     want = parity.by_id(oracle_port.place(h=h, **spec))
     assert len(got) == len(want)
     assert np.array_equal(got["id"], want["id"])
-    for ax in "xyz":
-        assert np.array_equal(got[ax], want[ax]), ax          # bit-exact positions
-    for ax in ("vx", "vy", "vz"):
-        np.testing.assert_allclose(got[ax], want[ax], rtol=1e-14, atol=1e-16)
+    for ax in ("x", "y", "z", "vx", "vy", "vz", "rho", "qDivM"):
+        assert np.array_equal(got[ax], want[ax]), ax          # bit-exact positions and momenta
 
 
 def test_stage_order_is_enforced():

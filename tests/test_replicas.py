@@ -28,7 +28,8 @@ class A:
     ref_steps = 1; gpus = world; steps = 1; warmup = 0
 printed = []
 orig = bench.reference_sample
-bench.reference_sample = lambda w, steps: (123.0, 1.0, 7, "stub")
+bench.reference_sample = lambda w, steps: dict(value=123.0, seconds=1.0, markers=7, procs=2,
+                                               per_process=61.5, sample="stub")
 import io, contextlib
 buf = io.StringIO()
 with contextlib.redirect_stdout(buf):
