@@ -583,10 +583,11 @@ int mg_push64 (mg_run_t *r)
    c.rjy = 1.0/c.jdy;
    c.rjz = 1.0/c.jdz;
    const int T = 256;
-   // Three blocks of 256 per SM (80 registers, a few spilled): the extra
-   // warps hide the gather latency better than a spill-free 128-register
-   // build with two blocks (measured about 10% faster on the laser-foil run).
-   k_push64<3><<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (c, r->m64, r->np, r->dsc);
+   // Two blocks of 256 per SM (no register cap that spills): over the whole
+   // 2000-step laser-foil run 0.376 ms per push against 0.387 with three
+   // blocks (80 registers) and 0.403 with four (64 registers); early in the
+   // run, with a cold sorted foil, four blocks lead (0.335 against 0.351).
+   k_push64<2><<<mg_blocks_for (r->np, T, 8), T, 0, r->stream>>> (c, r->m64, r->np, r->dsc);
    MG_LAUNCH_CHECK ();
    return MG_OK;
 }
