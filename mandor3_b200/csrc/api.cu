@@ -3,6 +3,7 @@
 // API that mirrors core/main.c's step, and the graph-replayed step loop.
 #include <cuda_runtime.h>
 
+#include <mutex>
 #include <vector>
 
 #include <stdarg.h>
@@ -189,17 +190,86 @@ __global__ void k_end_step (DevScalars *dsc, double *ring, double volume, double
 // ---------------------------------------------------------------------------
 // Allocation.
 // ---------------------------------------------------------------------------
+// Run state comes from one stream-ordered memory pool per device.  A run
+// that finishes returns its buffers to the pool, and the next run created
+// on that device reuses them: no page mapping or unmapping and no
+// device-wide synchronisation per buffer, which cudaMalloc and cudaFree
+// would cost every solve a server admits and retires.  The pool keeps up to
+// MG_POOL_KEEP bytes of freed memory for reuse and returns the rest to the
+// device at the next synchronisation.
+#define MG_POOL_KEEP (16ull << 30)
+
+static std::mutex    g_pool_mutex;
+static cudaMemPool_t g_pool[64];
+
+static int device_pool (int dev, cudaMemPool_t *out)
+{
+   if (dev < 0 || dev >= 64) {
+      mg_set_error ("device %d: no memory pool slot", dev);
+      return MG_ERR_ARG;
+   }
+   std::lock_guard<std::mutex> lock (g_pool_mutex);
+   if (!g_pool[dev]) {
+      cudaMemPoolProps props;
+      memset (&props, 0, sizeof (props));
+      props.allocType = cudaMemAllocationTypePinned;
+      props.handleTypes = cudaMemHandleTypeNone;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = dev;
+      cudaMemPool_t pool;
+      cudaError_t e = cudaMemPoolCreate (&pool, &props);
+      if (e != cudaSuccess) {
+         cudaGetLastError ();
+         mg_set_error ("cannot create the memory pool of device %d: %s", dev, cudaGetErrorString (e));
+         return MG_ERR_CUDA;
+      }
+      uint64_t keep = MG_POOL_KEEP;
+      cudaMemPoolSetAttribute (pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      g_pool[dev] = pool;
+   }
+   *out = g_pool[dev];
+   return MG_OK;
+}
+
+// Allocates on the run's stream and waits for the allocation, so that the
+// buffer is usable from any stream when this returns.
 int mg_dev_alloc (mg_run_t *r, void **p, size_t bytes)
 {
-   cudaError_t e = cudaMalloc (p, bytes ? bytes : 16);
+   *p = nullptr;
+   cudaMemPool_t pool;
+   TRY (device_pool (r->device, &pool));
+   cudaError_t e = cudaMallocFromPoolAsync (p, bytes ? bytes : 16, pool, r->stream);
+   if (e == cudaSuccess)
+      e = cudaStreamSynchronize (r->stream);
    if (e != cudaSuccess) {
       cudaGetLastError ();
       mg_set_error ("device allocation of %.3f GB failed: %s", bytes/1e9, cudaGetErrorString (e));
       *p = nullptr;
       return MG_ERR_OOM;
    }
+   if ((uintptr_t) *p & 255) {            // TMA and the padded rows rely on this
+      cudaFreeAsync (*p, r->stream);
+      *p = nullptr;
+      mg_set_error ("device allocation not 256-byte aligned");
+      return MG_ERR_CUDA;
+   }
    r->dev_bytes += bytes;
    return MG_OK;
+}
+
+// Returns a buffer of the run to the pool.  Kernels and copies on the run's
+// stream that use it are ordered before the free; the transfer and
+// snapshot streams are waited for here.
+void mg_dev_free (mg_run_t *r, void *p)
+{
+   if (!p)
+      return;
+   if (r->xfer)
+      cudaStreamSynchronize (r->xfer);
+   if (r->snap_stream)
+      cudaStreamSynchronize (r->snap_stream);
+   if (cudaFreeAsync (p, r->stream) != cudaSuccess)
+      cudaGetLastError ();
 }
 
 int mg_ensure_stage (mg_run_t *r, size_t bytes)
@@ -207,7 +277,7 @@ int mg_ensure_stage (mg_run_t *r, size_t bytes)
    if (r->stage_bytes >= bytes)
       return MG_OK;
    if (r->stage) {
-      cudaFree (r->stage);
+      mg_dev_free (r, r->stage);
       r->dev_bytes -= r->stage_bytes;
       r->stage = nullptr;
       r->stage_bytes = 0;
@@ -287,7 +357,7 @@ static void free_markers (mg_run_t *r)
                    r->m64.rho, r->m64.qm, r->m64.id};
    for (void *p : ptrs)
       if (p)
-         cudaFree (p);
+         mg_dev_free (r, p);
    memset (&r->m64, 0, sizeof (r->m64));
 }
 
@@ -511,40 +581,40 @@ extern "C" int mg_run_destroy (mg_run_t *r)
       free (r->pev);
    }
    for (int c = 0 ; c < 3 ; ++c) {
-      if (r->E[c]) cudaFree (r->E[c]);
-      if (r->H[c]) cudaFree (r->H[c]);
-      if (r->J[c]) cudaFree (r->J[c]);
-      if (r->Hn[c]) cudaFree (r->Hn[c]);
-      if (r->E32[c]) cudaFree (r->E32[c]);
-      if (r->H32[c]) cudaFree (r->H32[c]);
-      if (r->J32[c]) cudaFree (r->J32[c]);
-      if (r->Hn32[c]) cudaFree (r->Hn32[c]);
+      if (r->E[c]) mg_dev_free (r, r->E[c]);
+      if (r->H[c]) mg_dev_free (r, r->H[c]);
+      if (r->J[c]) mg_dev_free (r, r->J[c]);
+      if (r->Hn[c]) mg_dev_free (r, r->Hn[c]);
+      if (r->E32[c]) mg_dev_free (r, r->E32[c]);
+      if (r->H32[c]) mg_dev_free (r, r->H32[c]);
+      if (r->J32[c]) mg_dev_free (r, r->J32[c]);
+      if (r->Hn32[c]) mg_dev_free (r, r->Hn32[c]);
    }
    for (int t = 0 ; t < 2 ; ++t)
       for (int a = 0 ; a < 3 ; ++a)
-         if (r->mur[t][a]) cudaFree (r->mur[t][a]);
+         if (r->mur[t][a]) mg_dev_free (r, r->mur[t][a]);
    for (int t = 0 ; t < 2 ; ++t)
       for (int a = 0 ; a < 3 ; ++a)
-         if (r->mur32[t][a]) cudaFree (r->mur32[t][a]);
+         if (r->mur32[t][a]) mg_dev_free (r, r->mur32[t][a]);
    free_markers (r);
    mg_free_markers32 (r);
-   if (r->dsc) cudaFree (r->dsc);
-   if (r->ring) cudaFree (r->ring);
-   if (r->stage) cudaFree (r->stage);
-   if (r->sort_tmp) cudaFree (r->sort_tmp);
-   if (r->tile_start) cudaFree (r->tile_start);
-   if (r->probe_ijk) cudaFree (r->probe_ijk);
-   if (r->probe_ring) cudaFree (r->probe_ring);
-   if (r->probe_ptrs) cudaFree (r->probe_ptrs);
+   if (r->dsc) mg_dev_free (r, r->dsc);
+   if (r->ring) mg_dev_free (r, r->ring);
+   if (r->stage) mg_dev_free (r, r->stage);
+   if (r->sort_tmp) mg_dev_free (r, r->sort_tmp);
+   if (r->tile_start) mg_dev_free (r, r->tile_start);
+   if (r->probe_ijk) mg_dev_free (r, r->probe_ijk);
+   if (r->probe_ring) mg_dev_free (r, r->probe_ring);
+   if (r->probe_ptrs) mg_dev_free (r, r->probe_ptrs);
    mg_tfsf_free (r);
    free_snapshot (r);
    for (int q = 0 ; q < r->nmirrors ; ++q) {
-      cudaFree (r->mirrors[q].E);
-      cudaFree (r->mirrors[q].H);
+      mg_dev_free (r, r->mirrors[q].E);
+      mg_dev_free (r, r->mirrors[q].H);
    }
    for (int q = 0 ; q < 2 ; ++q)
-      if (r->gauss_rho[q]) cudaFree (r->gauss_rho[q]);
-   if (r->gauss_out) cudaFree (r->gauss_out);
+      if (r->gauss_rho[q]) mg_dev_free (r, r->gauss_rho[q]);
+   if (r->gauss_out) mg_dev_free (r, r->gauss_out);
    for (int e = 0 ; e < 4 ; ++e)
       if (r->ev[e]) cudaEventDestroy (r->ev[e]);
    if (r->xfer) {
@@ -554,7 +624,10 @@ extern "C" int mg_run_destroy (mg_run_t *r)
             if (r->xev[b][e]) cudaEventDestroy (r->xev[b][e]);
       cudaStreamDestroy (r->xfer);
    }
-   if (r->stream) cudaStreamDestroy (r->stream);
+   if (r->stream) {
+      cudaStreamSynchronize (r->stream);          // the frees above reach the pool
+      cudaStreamDestroy (r->stream);
+   }
    free (r);
    return MG_OK;
 }
@@ -771,9 +844,9 @@ static void free_snapshot (mg_run_t *r)
    if (r->snap_pending && r->snap_done)
       cudaEventSynchronize (r->snap_done);
    r->snap_pending = 0;
-   if (r->snap_E) cudaFree (r->snap_E);
-   if (r->snap_H) cudaFree (r->snap_H);
-   if (r->snap_m) cudaFree (r->snap_m);
+   if (r->snap_E) mg_dev_free (r, r->snap_E);
+   if (r->snap_H) mg_dev_free (r, r->snap_H);
+   if (r->snap_m) mg_dev_free (r, r->snap_m);
    r->snap_E = r->snap_H = nullptr;
    r->snap_m = nullptr;
    r->snap_cap = 0;
@@ -822,7 +895,7 @@ extern "C" int mg_run_snapshot (mg_run_t *r, double *E, double *H, mg_marker_t *
    }
    if (m && live > r->snap_cap) {
       if (r->snap_m) {
-         cudaFree (r->snap_m);
+         mg_dev_free (r, r->snap_m);
          r->dev_bytes -= (long long) r->snap_cap*sizeof (mg_marker_t);
          r->snap_m = nullptr;
          r->snap_cap = 0;
@@ -904,8 +977,8 @@ extern "C" int mg_run_clear_mirrors (mg_run_t *r)
 {
    CHECK_RUN (r);
    for (int q = 0 ; q < r->nmirrors ; ++q) {
-      cudaFree (r->mirrors[q].E);
-      cudaFree (r->mirrors[q].H);
+      mg_dev_free (r, r->mirrors[q].E);
+      mg_dev_free (r, r->mirrors[q].H);
    }
    r->nmirrors = 0;
    mg_drop_graphs (r);

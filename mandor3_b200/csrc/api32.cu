@@ -357,12 +357,12 @@ __global__ void k_scatter (TileKey t, Markers32 m, Markers32 o, long long np, co
 
 } // namespace
 
-static void free_set (Markers32 &m)
+static void free_set (mg_run_t *r, Markers32 &m)
 {
    void *ptrs[] = {m.cell, m.ox, m.oy, m.oz, m.ux, m.uy, m.uz, m.rho, m.qm, m.id};
    for (void *p : ptrs)
       if (p)
-         cudaFree (p);
+         mg_dev_free (r, p);
    memset (&m, 0, sizeof (m));
 }
 
@@ -379,8 +379,8 @@ static int alloc_set (mg_run_t *r, Markers32 &m, long long cap)
 
 void mg_free_markers32 (mg_run_t *r)
 {
-   free_set (r->m32);
-   free_set (r->m32b);
+   free_set (r, r->m32);
+   free_set (r, r->m32b);
 }
 
 namespace {
@@ -415,8 +415,8 @@ int mg_ensure_capacity32 (mg_run_t *r, long long need)
    if (rc == MG_OK)
       rc = alloc_set (r, nb, cap);
    if (rc != MG_OK) {
-      free_set (nm);
-      free_set (nb);
+      free_set (r, nm);
+      free_set (r, nb);
       return rc;
    }
    if (r->m32.cell && r->np > 0) {
@@ -682,7 +682,7 @@ int mg_sort32 (mg_run_t *r)
    const size_t need = (size_t) kp*8*4 + (size_t) cells*8 + (size_t) nb*8 + 1024;
    if (r->sort_tmp_bytes < need) {
       if (r->sort_tmp) {
-         cudaFree (r->sort_tmp);
+         mg_dev_free (r, r->sort_tmp);
          r->dev_bytes -= r->sort_tmp_bytes;
          r->sort_tmp = nullptr;
       }

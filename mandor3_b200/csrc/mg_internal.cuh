@@ -308,6 +308,7 @@ int mg_ensure_capacity32 (mg_run_t *r, long long need);
 int mg_publish_markers32 (mg_run_t *r);
 void mg_free_markers32 (mg_run_t *r);
 int mg_dev_alloc (mg_run_t *r, void **p, size_t bytes);
+void mg_dev_free (mg_run_t *r, void *p);
 int mg_ensure_stage (mg_run_t *r, size_t bytes);
 void mg_drop_graphs (mg_run_t *r);
 int mg_run_set_fields32 (mg_run_t *r, const double *E, const double *H);

@@ -241,19 +241,20 @@ int mg_place64 (mg_run_t *r, const mg_place_t *spec, long long at, long long cou
       return rc;
    }
    uint32_t *ds = nullptr;
-   if (cudaMalloc (&ds, (size_t) nthreads*RM_LAG*sizeof (uint32_t)) != cudaSuccess) {
+   const size_t ds_bytes = (size_t) nthreads*RM_LAG*sizeof (uint32_t);
+   if (mg_dev_alloc (r, (void **) &ds, ds_bytes) != MG_OK) {
       free (hs);
-      mg_set_error ("placer: device allocation failed");
       return MG_ERR_OOM;
    }
-   cudaMemcpyAsync (ds, hs, (size_t) nthreads*RM_LAG*sizeof (uint32_t), cudaMemcpyHostToDevice, r->stream);
+   cudaMemcpyAsync (ds, hs, ds_bytes, cudaMemcpyHostToDevice, r->stream);
    const int T = 128, B = (nthreads + T - 1)/T;
    const int smem = T*RM_LAG*sizeof (uint32_t);          // 49,664 bytes
    cudaFuncSetAttribute (k_place, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
    k_place<<<B, T, smem, r->stream>>> (a, ds, r->m64);
    cudaError_t e = cudaGetLastError ();
    cudaStreamSynchronize (r->stream);
-   cudaFree (ds);
+   mg_dev_free (r, ds);
+   r->dev_bytes -= ds_bytes;
    free (hs);
    if (e != cudaSuccess) {
       mg_set_error ("placer launch: %s", cudaGetErrorString (e));

@@ -717,7 +717,7 @@ int mg_sort64 (mg_run_t *r)
    const size_t need = a_count + a_off + a_bsum + a_mark;
    if (r->sort_tmp_bytes < need) {
       if (r->sort_tmp) {
-         cudaFree (r->sort_tmp);
+         mg_dev_free (r, r->sort_tmp);
          r->dev_bytes -= r->sort_tmp_bytes;
          r->sort_tmp = nullptr;
          r->sort_tmp_bytes = 0;

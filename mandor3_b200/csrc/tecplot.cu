@@ -110,9 +110,9 @@ extern "C" int mg_run_set_probes (mg_run_t *r, const int *ijk, int n)
                           a, r->g.n[a]);
             return MG_ERR_ARG;
          }
-   if (r->probe_ijk) cudaFree (r->probe_ijk);
-   if (r->probe_ring) cudaFree (r->probe_ring);
-   if (r->probe_ptrs) cudaFree (r->probe_ptrs);
+   if (r->probe_ijk) mg_dev_free (r, r->probe_ijk);
+   if (r->probe_ring) mg_dev_free (r, r->probe_ring);
+   if (r->probe_ptrs) mg_dev_free (r, r->probe_ptrs);
    r->probe_ijk = nullptr;
    r->probe_ring = nullptr;
    r->probe_ptrs = nullptr;

@@ -136,7 +136,7 @@ bool playing (const mg_run_t *r)
    return r->tfsf && r->tfsf->cfg.mode != MG_TFSF_RECORD;
 }
 
-void free_state (mg_tfsf_state *s)
+void free_state (mg_run_t *r, mg_tfsf_state *s)
 {
    if (!s)
       return;
@@ -144,7 +144,7 @@ void free_state (mg_tfsf_state *s)
                 s->add_src[0], s->add_src[1], s->rec_off, s->rec_comp, s->rec_sf, s->rec_ring};
    for (void *q : p)
       if (q)
-         cudaFree (q);
+         mg_dev_free (r, q);
    delete s;
 }
 
@@ -229,7 +229,7 @@ extern "C" int mg_run_set_tfsf (mg_run_t *r, const mg_tfsf_t *t)
       return MG_ERR_ARG;
    }
    MG_CUDA (cudaSetDevice (r->device));
-   free_state (r->tfsf);
+   free_state (r, r->tfsf);
    r->tfsf = nullptr;
    mg_drop_graphs (r);
    if (!t)
@@ -312,7 +312,7 @@ extern "C" int mg_run_set_tfsf (mg_run_t *r, const mg_tfsf_t *t)
          rc = MG_ERR_CUDA;
    }
    if (rc != MG_OK) {
-      free_state (s);
+      free_state (r, s);
       return rc;
    }
    // Frame counter from the run's time (:455): (int) (t/tau + 0.1).
@@ -380,7 +380,7 @@ extern "C" int mg_run_tfsf_recorded (mg_run_t *r, int nsteps, double *out)
 
 void mg_tfsf_free (mg_run_t *r)
 {
-   free_state (r->tfsf);
+   free_state (r, r->tfsf);
    r->tfsf = nullptr;
 }
 
