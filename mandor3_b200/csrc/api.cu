@@ -1306,12 +1306,14 @@ int mg_enqueue_step64 (mg_run_t *r, int part)
       TRY (mg_tfsf_record (r));
       TRY (mg_fields64_h_both (r));
       TRY (mg_probes_enqueue (r));
-      TRY (mg_fields64_zero_j (r));
+      if (r->np > 0)                       // without markers J stays zero
+         TRY (mg_fields64_zero_j (r));
    }
    if (part < 0 || part == 1)
       TRY (mg_push64 (r));
    if (part < 0 || part == 2) {
-      TRY (mg_fields64_jbc (r));
+      if (r->np > 0)
+         TRY (mg_fields64_jbc_graph (r));
       TRY (mg_fields64_e_fused (r));
       k_end_step<<<1, 1, 0, r->stream>>> (r->dsc, r->ring, r->g.h[0]*r->g.h[1]*r->g.h[2], r->g.tau);
       MG_LAUNCH_CHECK ();
@@ -1363,6 +1365,14 @@ static int build_graph (mg_run_t *r)
    if (r->graph_ok)
       return MG_OK;
    mg_drop_graphs (r);
+   // A step graph without markers neither clears nor folds J and leaves
+   // -tau J out of the E update: clear J once here.
+   if (r->np == 0)
+      for (int c = 0 ; c < 3 ; ++c) {
+         void *J = is32 (r) ? (void *) r->J32[c] : (void *) r->J[c];
+         const size_t elt = is32 (r) ? sizeof (float) : sizeof (double);
+         MG_CUDA (cudaMemsetAsync (J, 0, (size_t) r->g.total*elt, r->stream));
+      }
    for (int q = 0 ; q < 4 ; ++q) {
       MG_CUDA (cudaStreamBeginCapture (r->stream, cudaStreamCaptureModeThreadLocal));
       const int part = q - 1;
@@ -1413,6 +1423,10 @@ static int run_steps (mg_run_t *r, int nsteps, double *host_rows, double *dev_ro
    if (nsteps < 0) {
       mg_set_error ("mg_run_step: nsteps = %d", nsteps);
       return MG_ERR_ARG;
+   }
+   if (r->in_batch) {                     // stepped alone again
+      mg_drop_graphs (r);
+      r->in_batch = 0;
    }
    TRY (build_graph (r));
    double push_sum = 0, step_sum = 0;
@@ -1540,6 +1554,10 @@ extern "C" int mg_batch_create (mg_run_t *const *runs, int n, mg_batch_t **out)
       rc = MG_ERR_CUDA;
    }
    for (int q = 0 ; q < n && rc == MG_OK ; ++q) {
+      if (!runs[q]->in_batch) {           // batch branches take the per-axis walls
+         mg_drop_graphs (runs[q]);
+         runs[q]->in_batch = 1;
+      }
       rc = build_graph (runs[q]);
       cudaGraphNode_t node;
       if (rc == MG_OK && cudaGraphAddChildGraphNode (&node, b->graph, nullptr, 0, runs[q]->gr[0]) != cudaSuccess) {
@@ -1621,6 +1639,10 @@ extern "C" int mg_run_step_gauss (mg_run_t *r, int nsteps, double *rows)
       return MG_ERR_STATE;
    }
    TRY (ensure_gauss (r));
+   if (r->in_batch) {
+      mg_drop_graphs (r);
+      r->in_batch = 0;
+   }
    TRY (build_graph (r));
    // gauss_start: the density at the start (plasma_gaussTest.c:77).
    TRY (mg_gauss_rho (r, r->gauss_rho[1]));

@@ -721,12 +721,14 @@ int mg_enqueue_step32 (mg_run_t *r, int part)
       TRY32 (mg_tfsf_record (r));
       TRY32 (mg_fields32_h_both (r));
       TRY32 (mg_probes_enqueue (r));
-      TRY32 (mg_fields32_zero_j (r));
+      if (r->np > 0)                       // without markers J stays zero
+         TRY32 (mg_fields32_zero_j (r));
    }
    if (part < 0 || part == 1)
       TRY32 (mg_push32 (r));
    if (part < 0 || part == 2) {
-      TRY32 (mg_fields32_jbc (r));
+      if (r->np > 0)
+         TRY32 (mg_fields32_jbc_graph (r));
       TRY32 (mg_fields32_e_fused (r));
       TRY32 (mg_end_step (r));
    }

@@ -22,6 +22,7 @@ int mg_fields32_h_step (mg_run_t *r) { return fields_h_step<float> (r, fs_of (r)
 int mg_fields32_h_both (mg_run_t *r) { return fields_h_both<float> (r, fs_of (r)); }
 int mg_fields32_e_step (mg_run_t *r) { return fields_e_step<float> (r, fs_of (r)); }
 int mg_fields32_jbc (mg_run_t *r) { return fields_jbc<float> (r, fs_of (r)); }
+int mg_fields32_jbc_graph (mg_run_t *r) { return fields_jbc_graph<float> (r, fs_of (r)); }
 int mg_fields32_e_finish (mg_run_t *r) { return fields_e_finish<float> (r, fs_of (r)); }
 int mg_fields32_e_fused (mg_run_t *r) { return fields_e_fused<float> (r, fs_of (r)); }
 int mg_fields32_zero_j (mg_run_t *r) { return fields_zero_j<float> (r, fs_of (r)); }

@@ -22,6 +22,7 @@ int mg_fields64_h_step (mg_run_t *r) { return fields_h_step<double> (r, fs_of (r
 int mg_fields64_h_both (mg_run_t *r) { return fields_h_both<double> (r, fs_of (r)); }
 int mg_fields64_e_step (mg_run_t *r) { return fields_e_step<double> (r, fs_of (r)); }
 int mg_fields64_jbc (mg_run_t *r) { return fields_jbc<double> (r, fs_of (r)); }
+int mg_fields64_jbc_graph (mg_run_t *r) { return fields_jbc_graph<double> (r, fs_of (r)); }
 int mg_fields64_e_finish (mg_run_t *r) { return fields_e_finish<double> (r, fs_of (r)); }
 int mg_fields64_e_fused (mg_run_t *r) { return fields_e_fused<double> (r, fs_of (r)); }
 int mg_fields64_zero_j (mg_run_t *r) { return fields_zero_j<double> (r, fs_of (r)); }

@@ -59,6 +59,7 @@ struct Box {
    long vol;
 };
 
+
 static Box make_box (const int lo[3], const int hi[3])
 {
    Box b;
@@ -84,7 +85,9 @@ struct EnergyPick {
    int hlo[3][3], hhi[3][3];  // same for H picks (after the periodic remap)
 };
 
-template <typename T>
+// HN: keep H^n in Hn (the push, the probes and the stage path read it); a
+// run without markers or probes skips those stores.
+template <typename T, bool HN = true>
 __global__ void __launch_bounds__ (256)
 k_h_fused (Grid g, F3T<T> E, F3T<T> H, F3T<T> Hn, Box b, T c1, T c2, T c3,
            EnergyPick ep, DevScalars *dsc)
@@ -102,9 +105,11 @@ k_h_fused (Grid g, F3T<T> E, F3T<T> H, F3T<T> Hn, Box b, T c1, T c2, T c3,
       const T cy = c1*(ez - Ez[o - sx]) - c3*(ex - Ex[o - 1]);
       const T cz = c2*(ex - Ex[o - sy]) - c1*(ey - Ey[o - sx]);
       const T hx = H.c[0][o] + cx, hy = H.c[1][o] + cy, hz = H.c[2][o] + cz;
-      Hn.c[0][o] = hx;
-      Hn.c[1][o] = hy;
-      Hn.c[2][o] = hz;
+      if (HN) {
+         Hn.c[0][o] = hx;
+         Hn.c[1][o] = hy;
+         Hn.c[2][o] = hz;
+      }
       H.c[0][o] = hx + cx;
       H.c[1][o] = hy + cy;
       H.c[2][o] = hz + cz;
@@ -182,7 +187,8 @@ __device__ __forceinline__ bool rim_node (const Rim &rm, int i, int j, int k)
            k >= rm.laser_lo[1] && k <= rm.laser_hi[1]);
 }
 
-template <typename T>
+// WJ: subtract tau J (a run without markers has J = 0 and skips its reads).
+template <typename T, bool WJ = true>
 __global__ void __launch_bounds__ (256)
 k_e_fused (Grid g, F3T<T> E, F3T<T> H, F3T<T> J, Box b, T c1, T c2, T c3, Rim rm)
 {
@@ -198,7 +204,7 @@ k_e_fused (Grid g, F3T<T> E, F3T<T> H, F3T<T> J, Box b, T c1, T c2, T c3, Rim rm
       T ex = Ex[o] - (c3*(Hy[o + 1] - hy) - c2*(Hz[o + sy] - hz));
       T ey = Ey[o] - (c1*(Hz[o + sx] - hz) - c3*(Hx[o + 1] - hx));
       T ez = Ez[o] - (c2*(Hx[o + sy] - hx) - c1*(Hy[o + sx] - hy));
-      if (!rim_node (rm, i, j, k)) {
+      if (WJ && !rim_node (rm, i, j, k)) {
          ex -= tau*J.c[0][o];
          ey -= tau*J.c[1][o];
          ez -= tau*J.c[2][o];
@@ -373,12 +379,9 @@ __global__ void k_mur_init (Grid g, F3T<T> E, Wall w, int top, T *mur)
 // upper wall (they touch disjoint nodes for n >= 3).  H walls act on both
 // H arrays (H at n and at n+1/2).
 template <typename T>
-__global__ void k_h_walls (Grid g, F3T<T> H, F3T<T> Hn, Wall w, int op_min, int op_max, int both)
+__device__ __forceinline__ void h_line (const Grid &g, F3T<T> &H, F3T<T> &Hn, const Wall &w, int op_min,
+                                        int op_max, int both, long o)
 {
-   long o;
-   int p, q;
-   if (!wall_node (g, w, 0, o, p, q))
-      return;
    const int N = g.n[w.ea];
    const long s = w.s_a;
    for (int arr = 0 ; arr < (both ? 2 : 1) ; ++arr) {
@@ -411,6 +414,16 @@ __global__ void k_h_walls (Grid g, F3T<T> H, F3T<T> Hn, Wall w, int op_min, int 
       if (op_max == OP_MIRROR_MAX)
          Ha[t] = 0;
    }
+}
+
+template <typename T>
+__global__ void k_h_walls (Grid g, F3T<T> H, F3T<T> Hn, Wall w, int op_min, int op_max, int both)
+{
+   long o;
+   int p, q;
+   if (!wall_node (g, w, 0, o, p, q))
+      return;
+   h_line (g, H, Hn, w, op_min, op_max, both, o);
 }
 
 template <typename T>
@@ -648,11 +661,10 @@ __device__ double laser_ey (const mg_laser_t &l, double x, double y, double z,
 // Hz[I] += (tau/h1) * Ey_inc(x = (I-1) h1, t = n tau)   (after the H step)
 // Ey[I-1] += (tau/h1) * Hz_inc(x = (I-1/2) h1, t = (n+1/2) tau)
 template <typename T>
-__global__ void k_laser (Grid g, T *F, mg_laser_t l, const DevScalars *dsc,
-                         int is_e, F3T<T> E, F3T<T> J, int sub_j)
+__device__ __forceinline__ void laser_node (const Grid &g, T *F, const mg_laser_t &l, const DevScalars *dsc,
+                                            int is_e, F3T<T> &E, const F3T<T> &J, int sub_j, long t)
 {
    const int nj = g.n[1] - 2*l.margin + 1, nk = g.n[2] - 2*l.margin + 1;
-   const long t = blockIdx.x*(long) blockDim.x + threadIdx.x;
    if (nj <= 0 || nk <= 0 || t >= (long) nj*nk)
       return;
    const int j = l.margin + (int) (t / nk), k = l.margin + (int) (t % nk);
@@ -670,6 +682,13 @@ __global__ void k_laser (Grid g, T *F, mg_laser_t l, const DevScalars *dsc,
       for (int c = 0 ; c < 3 ; ++c)
          E.c[c][o] -= (T) g.tau*J.c[c][o];
    }
+}
+
+template <typename T>
+__global__ void k_laser (Grid g, T *F, mg_laser_t l, const DevScalars *dsc,
+                         int is_e, F3T<T> E, F3T<T> J, int sub_j)
+{
+   laser_node (g, F, l, dsc, is_e, E, J, sub_j, blockIdx.x*(long) blockDim.x + threadIdx.x);
 }
 
 // Hard gauss-spot source (core/em_gaussSpot.c:129-156) at time t + tau:
@@ -726,6 +745,188 @@ __global__ void k_mirror (Grid g, T *Fy, T *Fz, MirrorDev m, int is_e, const Dev
 }
 
 // The field arrays of one precision form.
+// ---------------------------------------------------------------------------
+// All wall work of one field in one launch (the step graph's path).  A wall
+// phase of axis a (the per-axis kernels above, run in the order x, y, z)
+// reads and writes only nodes whose index along a lies in that axis' band
+// {-2..2, N-2..N+2}.  The wall nodes split into regions that no two phases
+// share work in:
+//   face lines of axis a: both transverse indices outside their bands, so
+//     phase a alone touches them (one thread per line);
+//   edge slices of axes a < b at one index of the third axis outside its
+//     band: the band_a x band_b nodes there, touched by phase a and then
+//     phase b (one warp per slice, __syncwarp between the phases);
+//   the corner band^3: phases x, y, z (one block, __syncthreads between).
+// Each wall operation runs once, after the same operations on its inputs as
+// with the per-axis kernels, so the results are bit-identical.  The E walls
+// subtract tau J on the rim nodes of each region after its last phase (each
+// rim node lies in exactly one region), and the analytic laser plane, which
+// lies outside every band, is added by blocks of its own.
+// ---------------------------------------------------------------------------
+enum { WK_H = 0, WK_E = 1, WK_J = 2 };
+
+struct WallPlan {
+   Wall w[3];
+   int  op0[3], op1[3];
+   int  nface[3], bface[4];     // face lines per axis; first block per axis (bface[3]: first edge block)
+   int  nslice[3], bslice[4];   // edge slices per third axis; first block (bslice[3]: the corner block)
+   int  blaser, nlaser;         // laser blocks and nodes (0: none)
+   int  lo, hi;                 // transverse extent of a line: [lo, n + hi]
+};
+
+template <typename T>
+struct WallArgs {
+   F3T<T> F, F2, J;             // H: H and Hn; E: E (and J); J: J
+   T     *mur[2][3];
+   T      alpha[3];
+   int    flag;                 // H: also Hn; E: subtract tau J on the rim
+   mg_laser_t l;
+   const DevScalars *dsc;
+};
+
+__device__ __forceinline__ int band_at (int u, int N) { return u < 5 ? u - 2 : N - 7 + u; }
+
+// The wall line of axis a whose transverse indices are co[ep], co[eq].
+template <typename T, int KIND>
+__device__ __forceinline__ void wall_line (const Grid &g, WallArgs<T> &A, const WallPlan &P, int a,
+                                           const int co[3])
+{
+   const Wall &w = P.w[a];
+   const int p = co[w.ep], q = co[w.eq];
+   if (p < P.lo || p > g.n[w.ep] + P.hi || q < P.lo || q > g.n[w.eq] + P.hi)
+      return;
+   if (KIND == WK_H) {
+      h_line (g, A.F, A.F2, w, P.op0[a], P.op1[a], A.flag, g.origin + p*w.s_p + q*w.s_q);
+   } else if (KIND == WK_E) {
+      if (p >= 0 && q >= 0) {
+         const long o = g.origin + p*w.s_p + q*w.s_q;
+         e_wall_op (g, A.F, w, P.op0[a], o, p, q, A.mur[0][a], A.alpha[a]);
+         e_wall_op (g, A.F, w, P.op1[a], o, p, q, A.mur[1][a], A.alpha[a]);
+      }
+   } else {
+      const long s[3] = {g.sx, g.sy, 1};
+      const long base = g.origin + p*s[w.ep] + q*s[w.eq];
+      j_fold (g, A.J, a, 0, g.bc[0][a], base, s);
+      j_fold (g, A.J, a, 1, g.bc[1][a], base, s);
+   }
+}
+
+// E -= tau J at one rim node (the order of core/em.c:189-222: after every
+// wall operation on the node).
+template <typename T>
+__device__ __forceinline__ void rim_sub_j (const Grid &g, WallArgs<T> &A, int i, int j, int k)
+{
+   const T tau = (T) g.tau;
+   const long x = g.at (i, j, k);
+   T e[3], jv[3];
+#pragma unroll
+   for (int c = 0 ; c < 3 ; ++c) {
+      e[c] = A.F.c[c][x];
+      jv[c] = __ldg (A.J.c[c] + x);
+   }
+#pragma unroll
+   for (int c = 0 ; c < 3 ; ++c)
+      A.F.c[c][x] = e[c] - tau*jv[c];
+}
+
+__device__ __forceinline__ bool rim_index (int v, int N) { return v < 2 || v > N - 2; }
+
+template <typename T, int KIND>
+__global__ void __launch_bounds__ (256)
+k_walls_all (Grid g, WallArgs<T> A, WallPlan P)
+{
+   const int b = blockIdx.x;
+   const bool sub = (KIND == WK_E) && A.flag;
+   if (b < P.bface[3]) {
+      const int a = b >= P.bface[2] ? 2 : b >= P.bface[1] ? 1 : 0;
+      const long t = (long) (b - P.bface[a])*blockDim.x + threadIdx.x;
+      if (t >= P.nface[a])
+         return;
+      const Wall &w = P.w[a];
+      const int nq = g.n[w.eq] - 5;
+      int co[3];
+      co[a] = 0;
+      co[w.ep] = 3 + (int) (t / nq);
+      co[w.eq] = 3 + (int) (t % nq);
+      wall_line<T, KIND> (g, A, P, a, co);
+      if (sub) {
+         const int N = g.n[a];
+         const int vs[6] = {-1, 0, 1, N - 1, N, N + 1};
+#pragma unroll
+         for (int u = 0 ; u < 6 ; ++u) {
+            co[a] = vs[u];
+            rim_sub_j (g, A, co[0], co[1], co[2]);
+         }
+      }
+      return;
+   }
+   if (b < P.bslice[3]) {
+      const int c = b >= P.bslice[2] ? 2 : b >= P.bslice[1] ? 1 : 0;
+      const int s = (b - P.bslice[c])*(int) (blockDim.x >> 5) + (int) (threadIdx.x >> 5);
+      if (s >= P.nslice[c])
+         return;                                   // whole warps leave together
+      const int lane = threadIdx.x & 31;
+      const int a = (c == 0) ? 1 : 0, bb = (c == 2) ? 1 : 2;     // a < bb, both != c
+      int co[3];
+      co[c] = 3 + s;
+      if (lane < 10) {
+         co[a] = 0;
+         co[bb] = band_at (lane, g.n[bb]);
+         wall_line<T, KIND> (g, A, P, a, co);
+      }
+      __syncwarp ();
+      if (lane < 10) {
+         co[bb] = 0;
+         co[a] = band_at (lane, g.n[a]);
+         wall_line<T, KIND> (g, A, P, bb, co);
+      }
+      __syncwarp ();
+      if (sub)
+         for (int u = lane ; u < 100 ; u += 32) {
+            const int va = band_at (u / 10, g.n[a]), vb = band_at (u % 10, g.n[bb]);
+            if (va < -1 || va > g.n[a] + 1 || vb < -1 || vb > g.n[bb] + 1)
+               continue;
+            if (!rim_index (va, g.n[a]) && !rim_index (vb, g.n[bb]))
+               continue;
+            co[a] = va;
+            co[bb] = vb;
+            rim_sub_j (g, A, co[0], co[1], co[2]);
+         }
+      return;
+   }
+   if (b == P.bslice[3]) {
+      for (int a = 0 ; a < 3 ; ++a) {
+         const Wall &w = P.w[a];
+         for (int u = threadIdx.x ; u < 100 ; u += blockDim.x) {
+            int co[3];
+            co[a] = 0;
+            co[w.ep] = band_at (u / 10, g.n[w.ep]);
+            co[w.eq] = band_at (u % 10, g.n[w.eq]);
+            wall_line<T, KIND> (g, A, P, a, co);
+         }
+         __syncthreads ();
+      }
+      if (sub)
+         for (int u = threadIdx.x ; u < 1000 ; u += blockDim.x) {
+            const int v0 = band_at (u / 100, g.n[0]), v1 = band_at ((u / 10) % 10, g.n[1]);
+            const int v2 = band_at (u % 10, g.n[2]);
+            if (v0 < -1 || v0 > g.n[0] + 1 || v1 < -1 || v1 > g.n[1] + 1 || v2 < -1 || v2 > g.n[2] + 1)
+               continue;
+            if (!rim_index (v0, g.n[0]) && !rim_index (v1, g.n[1]) && !rim_index (v2, g.n[2]))
+               continue;
+            rim_sub_j (g, A, v0, v1, v2);
+         }
+      return;
+   }
+   if (KIND != WK_J && P.nlaser > 0) {
+      const long t = (long) (b - P.blaser)*blockDim.x + threadIdx.x;
+      if (KIND == WK_H)
+         laser_node (g, A.F.c[2], A.l, A.dsc, 0, A.F, A.J, 0, t);
+      else
+         laser_node (g, A.F.c[1], A.l, A.dsc, 1, A.F, A.J, A.flag, t);
+   }
+}
+
 template <typename T>
 struct FS {
    T *E[3], *H[3], *Hn[3], *J[3];
@@ -830,6 +1031,86 @@ static int launch_laser (mg_run_t *r, const FS<T> &fs, int is_e, int sub_j = 0)
    const int NT = 256, B = (int) ((nj*nk + NT - 1)/NT);
    k_laser<<<B, NT, 0, r->stream>>> (r->g, is_e ? fs.E[1] : fs.H[2], l, r->dsc, is_e,
                                     f3 (fs.E), f3 (fs.J), sub_j);
+   MG_LAUNCH_CHECK ();
+   return MG_OK;
+}
+
+// The merged wall launch needs the two bands of every axis apart (n >= 6).
+// A run stepped as one branch of a batch graph keeps the per-axis kernels:
+// there the other runs' kernels fill the launch gaps, and the merged
+// kernel's serial corner block (three phases, then the rim) lengthens each
+// run's chain (served scan of 24 solves on one box: 7.6 s per-axis against
+// 8.1-8.9 s merged; one run stepped alone: merged 2 % faster on the
+// laser-foil step, 8 % on the served solves run one at a time).
+static bool walls_merge (const mg_run_t *r)
+{
+   return !r->in_batch && r->g.n[0] >= 6 && r->g.n[1] >= 6 && r->g.n[2] >= 6;
+}
+
+// The analytic laser's planes (H at x index `plane`, E at `plane` - 1, over
+// j, k in [margin, n - margin]) outside every wall band: they commute with
+// the walls and join the merged launch.
+static bool laser_merge (const mg_run_t *r)
+{
+   if (!r->has_laser)
+      return false;
+   const mg_laser_t &l = r->laser;
+   return l.margin >= 3 && l.plane >= 4 && l.plane <= r->g.n[0] - 3 &&
+          r->g.n[1] - 2*l.margin + 1 > 0 && r->g.n[2] - 2*l.margin + 1 > 0;
+}
+
+// One launch of k_walls_all for the field of KIND; flag: H also walls Hn,
+// E subtracts tau J on the rim; laser: the H (KIND = WK_H) or E source too.
+template <typename T, int KIND>
+static int launch_walls_all (mg_run_t *r, const FS<T> &fs, int flag, bool laser)
+{
+   const Grid &g = r->g;
+   const int NT = 256;
+   WallPlan P;
+   int blocks = 0;
+   for (int a = 0 ; a < 3 ; ++a) {
+      P.w[a] = make_wall (g, a);
+      wall_ops (g, a, P.op0[a], P.op1[a]);
+      P.nface[a] = (g.n[P.w[a].ep] - 5)*(g.n[P.w[a].eq] - 5);
+      P.bface[a] = blocks;
+      blocks += (P.nface[a] + NT - 1)/NT;
+   }
+   P.bface[3] = blocks;
+   for (int c = 0 ; c < 3 ; ++c) {
+      P.nslice[c] = g.n[c] - 5;
+      P.bslice[c] = blocks;
+      blocks += (P.nslice[c] + NT/32 - 1)/(NT/32);
+   }
+   P.bslice[3] = blocks++;
+   P.blaser = blocks;
+   P.nlaser = 0;
+   if (laser && KIND != WK_J) {
+      const mg_laser_t &l = r->laser;
+      P.nlaser = (g.n[1] - 2*l.margin + 1)*(g.n[2] - 2*l.margin + 1);
+      blocks += (P.nlaser + NT - 1)/NT;
+   }
+   P.lo = KIND == WK_H ? 0 : KIND == WK_E ? -1 : -2;
+   P.hi = KIND == WK_J ? 2 : 1;
+   WallArgs<T> A;
+   memset (&A, 0, sizeof (A));
+   if (KIND == WK_H) {
+      A.F = f3 (fs.H);
+      A.F2 = f3 (fs.Hn);
+   } else {
+      A.F = f3 (fs.E);
+      A.F2 = f3 (fs.E);
+   }
+   A.J = f3 (fs.J);
+   for (int a = 0 ; a < 3 ; ++a) {
+      A.mur[0][a] = fs.mur[0][a];
+      A.mur[1][a] = fs.mur[1][a];
+      A.alpha[a] = (T) ((g.tau - g.h[a])/(g.tau + g.h[a]));
+   }
+   A.flag = flag;
+   if (r->has_laser)
+      A.l = r->laser;
+   A.dsc = r->dsc;
+   k_walls_all<T, KIND><<<blocks, NT, 0, r->stream>>> (g, A, P);
    MG_LAUNCH_CHECK ();
    return MG_OK;
 }
@@ -939,21 +1220,34 @@ int fields_h_step (mg_run_t *r, const FS<T> &fs)
 }
 
 // Graph path: both half steps, the source on H^(n+1/2), walls on both.
+// H^n is kept only where something reads it: the push (markers) or the
+// probes; a field-only run moves E and H once each per half-update.
 template <typename T>
 int fields_h_both (mg_run_t *r, const FS<T> &fs)
 {
    const Grid &g = r->g;
    Box b = h_box (g);
    const int NT = 256;
+   const bool hn = r->np > 0 || r->probe_ring;
    MG_CUDA (cudaMemsetAsync (r->dsc->acc, 0, 2*sizeof (double), r->stream));
-   k_h_fused<<<mg_blocks_for (b.vol, NT, 8), NT, 0, r->stream>>> (
-      g, f3 (fs.E), f3 (fs.H), f3 (fs.Hn), b, (T) (0.5*g.tau/g.h[0]), (T) (0.5*g.tau/g.h[1]), (T) (0.5*g.tau/g.h[2]),
-      energy_pick (g), r->dsc);
+   const T c1 = (T) (0.5*g.tau/g.h[0]), c2 = (T) (0.5*g.tau/g.h[1]), c3 = (T) (0.5*g.tau/g.h[2]);
+   if (hn)
+      k_h_fused<T, true><<<mg_blocks_for (b.vol, NT, 8), NT, 0, r->stream>>> (
+         g, f3 (fs.E), f3 (fs.H), f3 (fs.Hn), b, c1, c2, c3, energy_pick (g), r->dsc);
+   else
+      k_h_fused<T, false><<<mg_blocks_for (b.vol, NT, 8), NT, 0, r->stream>>> (
+         g, f3 (fs.E), f3 (fs.H), f3 (fs.Hn), b, c1, c2, c3, energy_pick (g), r->dsc);
    MG_LAUNCH_CHECK ();
    TRY_MG (mg_tfsf_h (r));
    TRY_MG (launch_mirrors<T> (r, fs, 0));
+   if (walls_merge (r)) {
+      const bool lm = laser_merge (r);
+      if (!lm)
+         TRY_MG (launch_laser<T> (r, fs, 0));
+      return launch_walls_all<T, WK_H> (r, fs, hn ? 1 : 0, lm);
+   }
    TRY_MG (launch_laser<T> (r, fs, 0));
-   return launch_h_walls<T> (r, fs, 1);
+   return launch_h_walls<T> (r, fs, hn ? 1 : 0);
 }
 
 // Stage path: E += curl H only, then the E walls (Mur history before -tau J).
@@ -982,6 +1276,16 @@ int fields_jbc (mg_run_t *r, const FS<T> &fs)
    }
    return MG_OK;
 }
+
+// Step graph: the three axes' current folding in one launch where it can.
+template <typename T>
+int fields_jbc_graph (mg_run_t *r, const FS<T> &fs)
+{
+   if (walls_merge (r))
+      return launch_walls_all<T, WK_J> (r, fs, 0, false);
+   return fields_jbc<T> (r, fs);
+}
+
 
 template <typename T>
 static int launch_gauss_spot (mg_run_t *r, const FS<T> &fs)
@@ -1028,11 +1332,26 @@ int fields_e_fused (mg_run_t *r, const FS<T> &fs)
    Box b = e_box (g);
    Rim rm = rim (r);
    const int NT = 256;
-   k_e_fused<<<mg_blocks_for (b.vol, NT, 8), NT, 0, r->stream>>> (
-      g, f3 (fs.E), f3 (fs.H), f3 (fs.J), b, (T) (g.tau/g.h[0]), (T) (g.tau/g.h[1]), (T) (g.tau/g.h[2]), rm);
+   // Without markers J stays zero (cleared when the step graph is built)
+   // and -tau J is left out.
+   const bool wj = r->np > 0;
+   const T c1 = (T) (g.tau/g.h[0]), c2 = (T) (g.tau/g.h[1]), c3 = (T) (g.tau/g.h[2]);
+   if (wj)
+      k_e_fused<T, true><<<mg_blocks_for (b.vol, NT, 8), NT, 0, r->stream>>> (
+         g, f3 (fs.E), f3 (fs.H), f3 (fs.J), b, c1, c2, c3, rm);
+   else
+      k_e_fused<T, false><<<mg_blocks_for (b.vol, NT, 8), NT, 0, r->stream>>> (
+         g, f3 (fs.E), f3 (fs.H), f3 (fs.J), b, c1, c2, c3, rm);
    MG_LAUNCH_CHECK ();
-   TRY_MG (launch_e_walls<T> (r, fs, 1));
-   TRY_MG (launch_laser<T> (r, fs, 1, 1));
+   if (walls_merge (r)) {
+      const bool lm = laser_merge (r);
+      TRY_MG ((launch_walls_all<T, WK_E> (r, fs, wj ? 1 : 0, lm)));
+      if (!lm)
+         TRY_MG (launch_laser<T> (r, fs, 1, wj ? 1 : 0));
+   } else {
+      TRY_MG (launch_e_walls<T> (r, fs, wj ? 1 : 0));
+      TRY_MG (launch_laser<T> (r, fs, 1, wj ? 1 : 0));
+   }
    return launch_gauss_spot<T> (r, fs);
 }
 

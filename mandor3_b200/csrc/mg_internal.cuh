@@ -203,6 +203,7 @@ struct mg_run {
    cudaGraph_t     gr[4];      // whole step, then its three parts
    cudaGraphExec_t gexec[4];
    int             graph_ok;
+   int             in_batch;       // step graph built for a batch branch (per-axis wall kernels)
    int             kernels_per_step;
 
    // stage ordering (like core/em.c:32's emStage)
@@ -247,6 +248,7 @@ int mg_fields64_energy (mg_run_t *r);
 int mg_fields64_h_step (mg_run_t *r);
 int mg_fields64_e_step (mg_run_t *r);
 int mg_fields64_jbc (mg_run_t *r);
+int mg_fields64_jbc_graph (mg_run_t *r);
 int mg_fields64_e_finish (mg_run_t *r);
 int mg_fields64_init (mg_run_t *r);
 int mg_fields64_zero_j (mg_run_t *r);
@@ -294,6 +296,7 @@ int mg_fields32_energy (mg_run_t *r);
 int mg_fields32_h_step (mg_run_t *r);
 int mg_fields32_e_step (mg_run_t *r);
 int mg_fields32_jbc (mg_run_t *r);
+int mg_fields32_jbc_graph (mg_run_t *r);
 int mg_fields32_e_finish (mg_run_t *r);
 int mg_fields32_init (mg_run_t *r);
 int mg_fields32_zero_j (mg_run_t *r);

@@ -331,11 +331,16 @@ k_push64 (Ctx c, Markers64 m, long long np, DevScalars *dsc)
          z1 = m.z[n];
          double sX = div_by (x1, h1, c.rh[0]), sY = div_by (y1, h2, c.rh[1]), sZ = div_by (z1, h3, c.rh[2]);
          double sX_ = sX + 0.5, sY_ = sY + 0.5, sZ_ = sZ + 0.5;
-         double fi_, fj_, fk_;
          i = cell_of (sX, fi);
          j = cell_of (sY, fj);
          k = cell_of (sZ, fk);
-         const int i_ = cell_of (sX_, fi_), j_ = cell_of (sY_, fj_), k_ = cell_of (sZ_, fk_);
+         // The half-shifted cell floor(s + 1/2) is the cell plus one when
+         // the offset s - floor(s) reaches 1/2: for s >= 0 the offset is
+         // exact and s + 1/2 rounds to no other integer part; for s in
+         // [-1, 0) both sides are exact near the threshold.
+         const int hx = (sX - fi >= 0.5), hy = (sY - fj >= 0.5), hz = (sZ - fk >= 0.5);
+         const int i_ = i + hx, j_ = j + hy, k_ = k + hz;
+         const double fi_ = fi + hx, fj_ = fj + hy, fk_ = fk + hz;
          // Start cells outside [-1, n] would read or write past the two
          // ghost layers: flag and skip the marker.
          if (i < -1 || i > g.n[0] || j < -1 || j > g.n[1] || k < -1 || k > g.n[2]) {
