@@ -410,7 +410,7 @@ def batch_bench(args):
     t = time.perf_counter()
     choice = [tuner.choose(s) for s in specs]
     tune_s = time.perf_counter() - t
-    runs = [s.build(0, tile=c[0], sort_every=c[1]) for s, c in zip(specs, choice)]
+    runs = [s.build(0, tile=c[0], sort_every=c[1], warps=c[2]) for s, c in zip(specs, choice)]
     markers = sum(r.marker_count() for r in runs)
     b = mg.Batch(runs)
     b.step(args.warmup)
@@ -426,7 +426,7 @@ def batch_bench(args):
     # Same runs, one at a time.
     alone_s = 0.0
     for s, c in zip(specs, choice):
-        r = s.build(0, tile=c[0], sort_every=c[1])
+        r = s.build(0, tile=c[0], sort_every=c[1], warps=c[2])
         r.step(args.warmup)
         torch.cuda.synchronize()
         t = time.perf_counter()

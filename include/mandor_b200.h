@@ -88,6 +88,9 @@ typedef struct {
                              untiled push)                               */
    int       tile[3];     /* precision form: tile of the push in cells,
                              {8,8,4} (also {0,0,0}), {4,4,4} or {8,8,8} */
+   int       tile_warps;  /* precision form: warps per block of the tiled
+                             push (markers of a tile pushed at once / 32):
+                             8 (also 0), 4 or 16                          */
 } mg_params_t;
 
 /* Analytic laser source: paraxial Gaussian beam, Ey polarised, moving along

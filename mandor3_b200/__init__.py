@@ -42,7 +42,7 @@ class Params(C.Structure):
     _fields_ = [("n", C.c_int * 3), ("h", C.c_double * 3), ("tau", C.c_double),
                 ("bc_min", C.c_int * 3), ("bc_max", C.c_int * 3), ("time", C.c_double),
                 ("precision", C.c_int), ("device", C.c_int), ("capacity", C.c_longlong),
-                ("sort_every", C.c_int), ("tile", C.c_int * 3)]
+                ("sort_every", C.c_int), ("tile", C.c_int * 3), ("tile_warps", C.c_int)]
 
 
 class Laser(C.Structure):
@@ -206,7 +206,7 @@ class Run:
     marker array, core/main.c:90-91, core/plasma.c:40-43)."""
 
     def __init__(self, n, h, tau, bc_min, bc_max, time=0.0, precision=FP64,
-                 device=0, capacity=0, sort_every=0, tile=(0, 0, 0)):
+                 device=0, capacity=0, sort_every=0, tile=(0, 0, 0), tile_warps=0):
         lib = load()
         self.n = tuple(int(v) for v in n)
         self.h = tuple(float(v) for v in h)
@@ -215,7 +215,7 @@ class Run:
         p = Params((C.c_int * 3)(*self.n), (C.c_double * 3)(*self.h), self.tau,
                    (C.c_int * 3)(*bc_min), (C.c_int * 3)(*bc_max), float(time),
                    int(precision), int(device), int(capacity), int(sort_every),
-                   (C.c_int * 3)(*tile))
+                   (C.c_int * 3)(*tile), int(tile_warps))
         self._params = p
         ptr = C.c_void_p()
         _check(lib.mg_run_create(C.byref(p), C.byref(ptr)))

@@ -442,6 +442,11 @@ static int check_params (const mg_params_t *p)
          mg_set_error ("tile %dx%dx%d: the push is built for 8x8x4, 4x4x4 and 8x8x8", t[0], t[1], t[2]);
          return MG_ERR_ARG;
       }
+      const int w = p->tile_warps;
+      if (w != 0 && w != 4 && w != 8 && w != 16) {
+         mg_set_error ("tile_warps %d: the tiled push is built for 4, 8 and 16 warps a block", w);
+         return MG_ERR_ARG;
+      }
    }
    return MG_OK;
 }

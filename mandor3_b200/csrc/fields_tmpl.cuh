@@ -59,6 +59,37 @@ struct Box {
    long vol;
 };
 
+// Node indices of a grid-stride walk over a box without a division per
+// node: the stride's own decomposition is added with one carry per axis
+// (each digit of the stride is below its extent).
+struct BoxWalk {
+   int i, j, k;              // box coordinates of the current node
+   int si, sj, sk;           // the stride in box coordinates
+};
+
+__device__ __forceinline__ void walk_init (BoxWalk &w, long t, long stride, const Box &b)
+{
+   w.k = (int) (t % b.ext[2]);
+   t /= b.ext[2];
+   w.j = (int) (t % b.ext[1]);
+   w.i = (int) (t / b.ext[1]);
+   w.sk = (int) (stride % b.ext[2]);
+   stride /= b.ext[2];
+   w.sj = (int) (stride % b.ext[1]);
+   w.si = (int) (stride / b.ext[1]);
+}
+
+__device__ __forceinline__ void walk_step (BoxWalk &w, const Box &b)
+{
+   w.k += w.sk;
+   int c = w.k >= b.ext[2];
+   if (c) w.k -= b.ext[2];
+   w.j += w.sj + c;
+   c = w.j >= b.ext[1];
+   if (c) w.j -= b.ext[1];
+   w.i += w.si + c;
+}
+
 
 static Box make_box (const int lo[3], const int hi[3])
 {
@@ -87,44 +118,97 @@ struct EnergyPick {
 
 // HN: keep H^n in Hn (the push, the probes and the stage path read it); a
 // run without markers or probes skips those stores.
+// MG_BULK_NODES nodes per thread and iteration, all loads issued before
+// the first store (a node writes only itself, so no load aliases an earlier
+// store): twice the bytes in flight per thread.  The energy sums keep the
+// node order of one node per iteration.
+#ifndef MG_BULK_NODES
+#define MG_BULK_NODES 2
+#endif
+
 template <typename T, bool HN = true>
 __global__ void __launch_bounds__ (256)
 k_h_fused (Grid g, F3T<T> E, F3T<T> H, F3T<T> Hn, Box b, T c1, T c2, T c3,
            EnergyPick ep, DevScalars *dsc)
 {
+   constexpr int NU = MG_BULK_NODES;
    __shared__ double sw[2][8];
    const T *Ex = E.c[0], *Ey = E.c[1], *Ez = E.c[2];
    const long sx = g.sx, sy = g.sy;
+   const long stride = (long) gridDim.x*blockDim.x;
    double we = 0, wb = 0;   // FP64 reductions in both forms
-   for (long t = blockIdx.x*(long) blockDim.x + threadIdx.x ; t < b.vol ; t += (long) gridDim.x*blockDim.x) {
-      int i, j, k;
-      box_index (t, b.lo, b.ext, i, j, k);
-      const long o = g.at (i, j, k);
-      const T ex = Ex[o], ey = Ey[o], ez = Ez[o];
-      const T cx = c3*(ey - Ey[o - 1]) - c2*(ez - Ez[o - sy]);
-      const T cy = c1*(ez - Ez[o - sx]) - c3*(ex - Ex[o - 1]);
-      const T cz = c2*(ex - Ex[o - sy]) - c1*(ey - Ey[o - sx]);
-      const T hx = H.c[0][o] + cx, hy = H.c[1][o] + cy, hz = H.c[2][o] + cz;
-      if (HN) {
-         Hn.c[0][o] = hx;
-         Hn.c[1][o] = hy;
-         Hn.c[2][o] = hz;
-      }
-      H.c[0][o] = hx + cx;
-      H.c[1][o] = hy + cy;
-      H.c[2][o] = hz + cz;
-      const int I[3] = {i, j, k};
-      const T ev[3] = {ex, ey, ez}, hv[3] = {hx, hy, hz};
+   BoxWalk wk;
+   walk_init (wk, blockIdx.x*(long) blockDim.x + threadIdx.x, stride, b);
+   for (long t0 = blockIdx.x*(long) blockDim.x + threadIdx.x ; t0 < b.vol ; t0 += NU*stride) {
+      long o[NU];
+      int I[NU][3];
+      T ex[NU], ey[NU], ez[NU], dy[NU], dzy[NU], dzx[NU], dx[NU], dxy[NU], dyx[NU], h0[NU], h1[NU], h2[NU];
 #pragma unroll
-      for (int c = 0 ; c < 3 ; ++c) {
-         bool in_e = true, in_h = true;
-#pragma unroll
-         for (int a = 0 ; a < 3 ; ++a) {
-            in_e &= (I[a] >= ep.lo[c][a]) & (I[a] <= ep.hi[c][a]);
-            in_h &= (I[a] >= ep.hlo[c][a]) & (I[a] <= ep.hhi[c][a]);
+      for (int u = 0 ; u < NU ; ++u) {
+         const long t = t0 + u*stride;
+         o[u] = -1;
+         I[u][0] = b.lo[0] + wk.i;
+         I[u][1] = b.lo[1] + wk.j;
+         I[u][2] = b.lo[2] + wk.k;
+         walk_step (wk, b);
+         if (t < b.vol) {
+            const long x = g.at (I[u][0], I[u][1], I[u][2]);
+            o[u] = x;
+            ex[u] = Ex[x];
+            ey[u] = Ey[x];
+            ez[u] = Ez[x];
+            dy[u] = Ey[x - 1];
+            dzy[u] = Ez[x - sy];
+            dzx[u] = Ez[x - sx];
+            dx[u] = Ex[x - 1];
+            dxy[u] = Ex[x - sy];
+            dyx[u] = Ey[x - sx];
+            h0[u] = H.c[0][x];
+            h1[u] = H.c[1][x];
+            h2[u] = H.c[2][x];
          }
-         if (in_e) we += (double) ev[c]*(double) ev[c];
-         if (in_h) wb += (double) hv[c]*(double) hv[c];
+      }
+      // The precision form sums an iteration's squares in FP32 and adds
+      // them to the FP64 totals once; the FP64 form adds every square.
+      float se = 0.0f, sb = 0.0f;
+#pragma unroll
+      for (int u = 0 ; u < NU ; ++u) {
+         if (o[u] < 0)
+            continue;
+         const long x = o[u];
+         const T cx = c3*(ey[u] - dy[u]) - c2*(ez[u] - dzy[u]);
+         const T cy = c1*(ez[u] - dzx[u]) - c3*(ex[u] - dx[u]);
+         const T cz = c2*(ex[u] - dxy[u]) - c1*(ey[u] - dyx[u]);
+         const T hx = h0[u] + cx, hy = h1[u] + cy, hz = h2[u] + cz;
+         if (HN) {
+            Hn.c[0][x] = hx;
+            Hn.c[1][x] = hy;
+            Hn.c[2][x] = hz;
+         }
+         H.c[0][x] = hx + cx;
+         H.c[1][x] = hy + cy;
+         H.c[2][x] = hz + cz;
+         const T ev[3] = {ex[u], ey[u], ez[u]}, hv[3] = {hx, hy, hz};
+#pragma unroll
+         for (int c = 0 ; c < 3 ; ++c) {
+            bool in_e = true, in_h = true;
+#pragma unroll
+            for (int a = 0 ; a < 3 ; ++a) {
+               in_e &= (I[u][a] >= ep.lo[c][a]) & (I[u][a] <= ep.hi[c][a]);
+               in_h &= (I[u][a] >= ep.hlo[c][a]) & (I[u][a] <= ep.hhi[c][a]);
+            }
+            if (sizeof (T) == sizeof (float)) {
+               if (in_e) se += (float) ev[c]*(float) ev[c];
+               if (in_h) sb += (float) hv[c]*(float) hv[c];
+            } else {
+               if (in_e) we += (double) ev[c]*(double) ev[c];
+               if (in_h) wb += (double) hv[c]*(double) hv[c];
+            }
+         }
+      }
+      if (sizeof (T) == sizeof (float)) {
+         we += (double) se;
+         wb += (double) sb;
       }
    }
    for (int d = 16 ; d > 0 ; d >>= 1) {
@@ -192,26 +276,65 @@ template <typename T, bool WJ = true>
 __global__ void __launch_bounds__ (256)
 k_e_fused (Grid g, F3T<T> E, F3T<T> H, F3T<T> J, Box b, T c1, T c2, T c3, Rim rm)
 {
+   constexpr int NU = MG_BULK_NODES;
    T *Ex = E.c[0], *Ey = E.c[1], *Ez = E.c[2];
    const T *Hx = H.c[0], *Hy = H.c[1], *Hz = H.c[2];
    const long sx = g.sx, sy = g.sy;
    const T tau = (T) g.tau;
-   for (long t = blockIdx.x*(long) blockDim.x + threadIdx.x ; t < b.vol ; t += (long) gridDim.x*blockDim.x) {
-      int i, j, k;
-      box_index (t, b.lo, b.ext, i, j, k);
-      const long o = g.at (i, j, k);
-      const T hx = Hx[o], hy = Hy[o], hz = Hz[o];
-      T ex = Ex[o] - (c3*(Hy[o + 1] - hy) - c2*(Hz[o + sy] - hz));
-      T ey = Ey[o] - (c1*(Hz[o + sx] - hz) - c3*(Hx[o + 1] - hx));
-      T ez = Ez[o] - (c2*(Hx[o + sy] - hx) - c1*(Hy[o + sx] - hy));
-      if (WJ && !rim_node (rm, i, j, k)) {
-         ex -= tau*J.c[0][o];
-         ey -= tau*J.c[1][o];
-         ez -= tau*J.c[2][o];
+   const long stride = (long) gridDim.x*blockDim.x;
+   BoxWalk wk;
+   walk_init (wk, blockIdx.x*(long) blockDim.x + threadIdx.x, stride, b);
+   for (long t0 = blockIdx.x*(long) blockDim.x + threadIdx.x ; t0 < b.vol ; t0 += NU*stride) {
+      long o[NU];
+      bool sub[NU];
+      T e0[NU], e1[NU], e2[NU], hx[NU], hy[NU], hz[NU], hy1[NU], hzy[NU], hzx[NU], hx1[NU], hxy[NU], hyx[NU];
+      T j0[NU], j1[NU], j2[NU];
+#pragma unroll
+      for (int u = 0 ; u < NU ; ++u) {
+         const long t = t0 + u*stride;
+         o[u] = -1;
+         const int i = b.lo[0] + wk.i, j = b.lo[1] + wk.j, k = b.lo[2] + wk.k;
+         walk_step (wk, b);
+         if (t < b.vol) {
+            const long x = g.at (i, j, k);
+            o[u] = x;
+            hx[u] = Hx[x];
+            hy[u] = Hy[x];
+            hz[u] = Hz[x];
+            hy1[u] = Hy[x + 1];
+            hzy[u] = Hz[x + sy];
+            hzx[u] = Hz[x + sx];
+            hx1[u] = Hx[x + 1];
+            hxy[u] = Hx[x + sy];
+            hyx[u] = Hy[x + sx];
+            e0[u] = Ex[x];
+            e1[u] = Ey[x];
+            e2[u] = Ez[x];
+            sub[u] = WJ && !rim_node (rm, i, j, k);
+            if (sub[u]) {
+               j0[u] = J.c[0][x];
+               j1[u] = J.c[1][x];
+               j2[u] = J.c[2][x];
+            }
+         }
       }
-      Ex[o] = ex;
-      Ey[o] = ey;
-      Ez[o] = ez;
+#pragma unroll
+      for (int u = 0 ; u < NU ; ++u) {
+         if (o[u] < 0)
+            continue;
+         const long x = o[u];
+         T ex = e0[u] - (c3*(hy1[u] - hy[u]) - c2*(hzy[u] - hz[u]));
+         T ey = e1[u] - (c1*(hzx[u] - hz[u]) - c3*(hx1[u] - hx[u]));
+         T ez = e2[u] - (c2*(hxy[u] - hx[u]) - c1*(hyx[u] - hy[u]));
+         if (sub[u]) {
+            ex -= tau*j0[u];
+            ey -= tau*j1[u];
+            ez -= tau*j2[u];
+         }
+         Ex[x] = ex;
+         Ey[x] = ey;
+         Ez[x] = ez;
+      }
    }
 }
 

@@ -524,7 +524,7 @@ __device__ __forceinline__ void stage_marker (float *b, int lane, const Markers3
    cp_async_commit ();
 }
 
-template <int TX, int TY, int TZ>
+template <int TX, int TY, int TZ, int NW = 8>
 struct TileDims {
    // E, H nodes [x0-1, x0+TX+3): cells x0-1 .. x0+TX and the CIC stencil of
    // the half-shifted components.
@@ -539,7 +539,10 @@ struct TileDims {
    // Per warp: a queue of QCAP markers that crossed cell faces, eight words
    // each (offsets, displacement, weight, packed cell and crossings).
    static constexpr int QCAP = 40, QUEUE = 8*QCAP;
-   static constexpr size_t BYTES = (6*FN + 3*JN + 8*STAGE + 8*QUEUE)*sizeof (float);
+   static constexpr size_t BYTES = (6*FN + 3*JN + NW*STAGE + NW*QUEUE)*sizeof (float);
+   // Registers: at most 85 a thread for 4 and 8 warps a block, 64 for 16
+   // (two blocks of 512 threads on an SM).
+   static constexpr int MINB = NW == 4 ? 6 : NW == 8 ? 3 : 2;
 };
 
 template <int SX, int SY>
@@ -646,19 +649,19 @@ __device__ __forceinline__ void queued_segments (const Ctx32 &c, int *Jt, const 
 // the copy is added to J at the end of each chunk.  Tiles with fewer than
 // MG_TILE_DENSE markers, and markers more than a cell outside their tile,
 // gather from and add to global memory.
-template <int TX, int TY, int TZ, int GROUP, bool PER>
-__global__ void __launch_bounds__ (256, 3)
+template <int TX, int TY, int TZ, int GROUP, bool PER, int NW>
+__global__ void __launch_bounds__ (NW*32, (TileDims<TX, TY, TZ, NW>::MINB))
 k_push32_tiles (Ctx32 c, const __grid_constant__ TileMaps maps, const int *tile_start, const int *tile_list,
                 int nty, int ntz, int ntiles, DevScalars *dsc)
 {
    const Markers32 m = dsc->m32;
-   using D = TileDims<TX, TY, TZ>;
+   using D = TileDims<TX, TY, TZ, NW>;
    extern __shared__ __align__ (128) float smem[];
    __shared__ __align__ (8) uint64_t s_bar;   // completion of a tile's six TMA copies
    float *F = smem;                           // Ex Ey Ez Hx Hy Hz, D::FN each
    int *Jt = (int *) (smem + 6*D::FN);        // Jx Jy Jz, D::JN each
    float *stg = smem + 6*D::FN + 3*D::JN + (threadIdx.x >> 5)*D::STAGE;
-   float *que = smem + 6*D::FN + 3*D::JN + 8*D::STAGE + (threadIdx.x >> 5)*D::QUEUE;
+   float *que = smem + 6*D::FN + 3*D::JN + NW*D::STAGE + (threadIdx.x >> 5)*D::QUEUE;
    __shared__ int s_tile;
    const Grid &g = c.g;
    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -1037,22 +1040,22 @@ static int make_tile_maps (const Ctx32 &c, TileMaps &tm)
    return MG_OK;
 }
 
-// Launches the tiled push of one tile size: persistent CTAs, as many as fit
-// on the GPU (at most one per tile).
-template <int TX, int TY, int TZ>
+// Launches the tiled push of one tile size and block size (NW warps):
+// persistent CTAs, as many as fit on the GPU (at most one per tile).
+template <int TX, int TY, int TZ, int NW>
 static int launch_tiles (mg_run_t *r, const Ctx32 &c, bool per)
 {
-   using D = TileDims<TX, TY, TZ>;
+   using D = TileDims<TX, TY, TZ, NW>;
    TileMaps tm;
    TRY32 ((make_tile_maps<TX, TY, TZ> (c, tm)));
-   auto kp = k_push32_tiles<TX, TY, TZ, MG_TILE_GROUP, true>;
-   auto kn = k_push32_tiles<TX, TY, TZ, MG_TILE_GROUP, false>;
+   auto kp = k_push32_tiles<TX, TY, TZ, MG_TILE_GROUP, true, NW>;
+   auto kn = k_push32_tiles<TX, TY, TZ, MG_TILE_GROUP, false, NW>;
    static int attr_dev = -1;
    static int per_sm = 1, sms = 148;
    if (attr_dev != r->device) {
       MG_CUDA (cudaFuncSetAttribute (kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) D::BYTES));
       MG_CUDA (cudaFuncSetAttribute (kn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) D::BYTES));
-      MG_CUDA (cudaOccupancyMaxActiveBlocksPerMultiprocessor (&per_sm, kn, 256, D::BYTES));
+      MG_CUDA (cudaOccupancyMaxActiveBlocksPerMultiprocessor (&per_sm, kn, NW*32, D::BYTES));
       MG_CUDA (cudaDeviceGetAttribute (&sms, cudaDevAttrMultiProcessorCount, r->device));
       if (per_sm < 1)
          per_sm = 1;
@@ -1062,10 +1065,20 @@ static int launch_tiles (mg_run_t *r, const Ctx32 &c, bool per)
    if (blocks > r->ntiles)
       blocks = r->ntiles;
    MG_CUDA (cudaMemsetAsync (&r->dsc->tile_next, 0, sizeof (int), r->stream));
-   (per ? kp : kn)<<<blocks, 256, D::BYTES, r->stream>>> (c, tm, r->tile_start, r->tile_list, r->tiles[1],
-                                                            r->tiles[2], r->ntiles, r->dsc);
+   (per ? kp : kn)<<<blocks, NW*32, D::BYTES, r->stream>>> (c, tm, r->tile_start, r->tile_list, r->tiles[1],
+                                                              r->tiles[2], r->ntiles, r->dsc);
    MG_LAUNCH_CHECK ();
    return MG_OK;
+}
+
+template <int TX, int TY, int TZ>
+static int launch_tiles_nw (mg_run_t *r, const Ctx32 &c, bool per)
+{
+   switch (r->prm.tile_warps) {
+   case 4:  return launch_tiles<TX, TY, TZ, 4> (r, c, per);
+   case 16: return launch_tiles<TX, TY, TZ, 16> (r, c, per);
+   default: return launch_tiles<TX, TY, TZ, 8> (r, c, per);
+   }
 }
 
 int mg_push32 (mg_run_t *r)
@@ -1095,11 +1108,11 @@ int mg_push32 (mg_run_t *r)
       per = per && r->g.bc[0][a] == MG_BC_PERIODIC && r->g.bc[1][a] == MG_BC_PERIODIC;
    const int *td = r->tdim;
    if (td[0] == 4 && td[1] == 4 && td[2] == 4)
-      TRY32 ((launch_tiles<4, 4, 4> (r, c, per)));
+      TRY32 ((launch_tiles_nw<4, 4, 4> (r, c, per)));
    else if (td[0] == 8 && td[1] == 8 && td[2] == 8)
-      TRY32 ((launch_tiles<8, 8, 8> (r, c, per)));
+      TRY32 ((launch_tiles_nw<8, 8, 8> (r, c, per)));
    else
-      TRY32 ((launch_tiles<8, 8, 4> (r, c, per)));
+      TRY32 ((launch_tiles_nw<8, 8, 4> (r, c, per)));
    int sms = 148;
    MG_CUDA (cudaDeviceGetAttribute (&sms, cudaDevAttrMultiProcessorCount, r->device));
    // Markers outside the mesh at the last sort: global-memory path.

@@ -6,6 +6,7 @@ None of this has a counterpart in the reference, which runs one simulation
 per `core.out` process (core/main.c:195-480); a scan there is a sequence of
 runs.  Here many solves share the device:
 
+* `Tuner` picks tile shape, block size and sort interval per class of solve;
 * `Batch` (C ABI `mg_batch_*`) steps a fixed set of runs with one graph
   launch per step;
 * `Server` admits solves from a request stream while memory allows (each
@@ -71,11 +72,12 @@ class FoilSolve:
         return dict(n=n, h=(self.h,) * 3, tau=self.tau(), bc_min=(BC_OPEN,) * 3,
                     bc_max=(BC_OPEN,) * 3)
 
-    def build(self, device=0, tile=(0, 0, 0), sort_every=0):
+    def build(self, device=0, tile=(0, 0, 0), sort_every=0, warps=0):
         n, lo, hi = self.geometry()
         p = self.params()
         r = Run(p["n"], p["h"], p["tau"], p["bc_min"], p["bc_max"], precision=self.precision,
-                device=device, capacity=self.markers(), sort_every=sort_every, tile=tile)
+                device=device, capacity=self.markers(), sort_every=sort_every, tile=tile,
+                tile_warps=warps)
         # Fields start at zero (mg_run_create clears them).
         waist = 0.25 * min(n[1], n[2]) * self.h
         r.set_laser(a0=self.a0, waist=waist, x_focus=lo[0] * self.h, duration=10.0, t_start=0.0,
@@ -111,10 +113,11 @@ class PeriodicSolve:
         return dict(n=n, h=(hh,) * 3, tau=0.5 / math.sqrt(3 / hh ** 2), bc_min=(BC_PERIODIC,) * 3,
                     bc_max=(BC_PERIODIC,) * 3)
 
-    def build(self, device=0, tile=(0, 0, 0), sort_every=0):
+    def build(self, device=0, tile=(0, 0, 0), sort_every=0, warps=0):
         p = self.params()
         r = Run(p["n"], p["h"], p["tau"], p["bc_min"], p["bc_max"], precision=self.precision,
-                device=device, capacity=self.markers(), sort_every=sort_every, tile=tile)
+                device=device, capacity=self.markers(), sort_every=sort_every, tile=tile,
+                tile_warps=warps)
         # Fields start at zero (mg_run_create clears them).
         r.place_uniform((0, 0, 0), p["n"], self.ppc, -self.density * N_CR / self.ppc, -1.0,
                         uth=(self.uth,) * 3, seed=self.seed)
@@ -130,19 +133,23 @@ def footprint(spec):
 
 
 class Tuner:
-    """Picks the tile shape and sort interval of precision-form solves by
-    timing each candidate for a few steps on a solve of the same class
-    (grid-size and markers-per-cell bucket) and keeping the fastest; FP64
-    solves have nothing to tune."""
+    """Picks the tile shape, the block size of the tiled push (warps per
+    block, i.e. markers of a tile pushed at once / 32) and the sort interval
+    of precision-form solves by timing each candidate for a few steps on a
+    solve of the same class (grid-size and markers-per-cell bucket) and
+    keeping the fastest, one knob after the other; FP64 solves have nothing
+    to tune."""
 
     TILES = ((8, 8, 4), (4, 4, 4), (8, 8, 8))
+    WARPS = (8, 4, 16)
     SORTS = (4, 8, 16)
 
-    def __init__(self, device=0, steps=12, tiles=TILES, sorts=SORTS):
+    def __init__(self, device=0, steps=12, tiles=TILES, sorts=SORTS, warps=WARPS):
         self.device = device
         self.steps = steps
         self.tiles = tiles
         self.sorts = sorts
+        self.warps = warps
         self.table = {}
 
     @staticmethod
@@ -151,34 +158,29 @@ class Tuner:
         return (type(spec).__name__, spec.precision, int(math.log2(max(cells, 1))) // 2,
                 int(math.log2(max(spec.markers() / max(cells, 1), 1))))
 
+    def _time(self, spec, steps, which, **kw):
+        r = spec.build(self.device, **kw)
+        r.step(2)
+        r.profile(True)
+        r.step(steps)
+        push, step = r.last_timing()
+        r.close()
+        return push if which == "push" else step
+
     def choose(self, spec):
-        """(tile, sort_every) for this solve."""
+        """(tile, sort_every, warps) for this solve."""
         if spec.precision == FP64:
-            return (0, 0, 0), 0
+            return (0, 0, 0), 0, 0
         k = self.key(spec)
         if k not in self.table:
-            best = None
-            for tile in self.tiles:
-                r = spec.build(self.device, tile=tile, sort_every=min(self.sorts))
-                r.step(2)
-                r.profile(True)
-                r.step(self.steps)
-                push, _ = r.last_timing()
-                r.close()
-                if best is None or push < best[0]:
-                    best = (push, tile)
-            tile = best[1]
-            best = None
-            for every in self.sorts:
-                r = spec.build(self.device, tile=tile, sort_every=every)
-                r.step(2)
-                r.profile(True)
-                r.step(max(self.steps, 2 * every))
-                _, step = r.last_timing()
-                r.close()
-                if best is None or step < best[0]:
-                    best = (step, every)
-            self.table[k] = (tile, best[1])
+            every0 = min(self.sorts)
+            tile = min(self.tiles, key=lambda t: self._time(spec, self.steps, "push", tile=t,
+                                                            sort_every=every0, warps=self.warps[0]))
+            warps = min(self.warps, key=lambda w: self._time(spec, self.steps, "push", tile=tile,
+                                                             sort_every=every0, warps=w))
+            every = min(self.sorts, key=lambda e: self._time(spec, max(self.steps, 2 * e), "step",
+                                                             tile=tile, sort_every=e, warps=warps))
+            self.table[k] = (tile, every, warps)
         return self.table[k]
 
 
@@ -244,8 +246,8 @@ class Server:
                     break
                 queue.pop(0)
                 ta = time.perf_counter()
-                tile, every = self.tuner.choose(spec) if self.tuner else ((0, 0, 0), 0)
-                run = spec.build(self.device, tile=tile, sort_every=every)
+                tile, every, warps = self.tuner.choose(spec) if self.tuner else ((0, 0, 0), 0, 0)
+                run = spec.build(self.device, tile=tile, sort_every=every, warps=warps)
                 self.stats["admit_s"] += time.perf_counter() - ta
                 active.append(dict(i=i, spec=spec, run=run, rows=[], done=0, need=need,
                                    arrival=arrival, admitted=now()))
@@ -293,12 +295,12 @@ class Server:
         return [results[i] for i in range(len(stream))]
 
 
-def run_alone(spec, device=0, tile=(0, 0, 0), sort_every=0):
+def run_alone(spec, device=0, tile=(0, 0, 0), sort_every=0, warps=0):
     """One solve on its own: (energy rows, final marker count, seconds)."""
     import torch
     torch.cuda.synchronize(device)
     t = time.perf_counter()
-    r = spec.build(device, tile=tile, sort_every=sort_every)
+    r = spec.build(device, tile=tile, sort_every=sort_every, warps=warps)
     rows = r.step(spec.steps)
     count = r.marker_count()
     r.close()

@@ -80,3 +80,32 @@ def test_estimate_bytes(lib):
     import mandor3_b200 as mg
     b = mg.estimate_bytes((256, 128, 128), (0.05,) * 3, 0.02, (2, 2, 2), (2, 2, 2), 4_500_000)
     assert 3e8 < b < 2e9
+
+
+# ctypes mirrors of the header's structures: same size and field offsets as
+# the C compiler lays them out (a field added on one side only fails here).
+STRUCTS = [("Params", "mg_params_t"), ("Laser", "mg_laser_t"), ("GaussSpot", "mg_gauss_spot_t"),
+           ("Tfsf", "mg_tfsf_t"), ("Mirror", "mg_mirror_t"), ("TwoStream", "mg_two_stream_t"),
+           ("DfUniform", "mg_df_uniform_t"), ("Maxwell", "mg_maxwell_t"), ("Foil", "mg_foil_t"),
+           ("Place", "mg_place_t")]
+
+
+def test_ctypes_structures_match_the_header(tmp_path):
+    import mandor3_b200 as mg
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "mandor_b200.h"', 'int main (void) {']
+    for py, c in STRUCTS:
+        lines.append('printf ("%s size %%zu\\n", sizeof (%s));' % (py, c))
+        for f, _ in getattr(mg, py)._fields_:
+            lines.append('printf ("%s %s %%zu\\n", offsetof (%s, %s));' % (py, f, c, f))
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], stdout=subprocess.PIPE, check=True).stdout.decode().split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for py, _ in STRUCTS:
+        cls = getattr(mg, py)
+        assert got[(py, "size")] == ctypes.sizeof(cls), py
+        for f, _ in cls._fields_:
+            assert got[(py, f)] == getattr(cls, f).offset, (py, f)

@@ -119,13 +119,14 @@ def test_fp32_device_placer_matches_fp64_placement():
         assert np.max(np.abs(a[ax] - b[ax])) < 1e-7 * h[q]
 
 
-def beams(sort_every, n=(20, 12, 28), bc=(0, 1, 0), drift=0.3, steps=20, tile=(0, 0, 0)):
+def beams(sort_every, n=(20, 12, 28), bc=(0, 1, 0), drift=0.3, steps=20, tile=(0, 0, 0), warps=0):
     """Two counter-drifting electron beams on a grid whose sides are not
     multiples of the tile, mirror walls on y, 6 markers per cell each."""
     hh = 0.05 / (2 * math.pi)
     h = (hh, 1.1 * hh, 0.9 * hh)
     tau = 0.5 / math.sqrt(sum(1 / x ** 2 for x in h))
-    r = mg.Run(n, h, tau, bc, bc, precision=mg.FP32_OFFSET, sort_every=sort_every, tile=tile)
+    r = mg.Run(n, h, tau, bc, bc, precision=mg.FP32_OFFSET, sort_every=sort_every, tile=tile,
+               tile_warps=warps)
     z = np.zeros(r.field_shape())
     r.set_fields(z, z)
     rho = -4 * math.pi ** 2 / 12
@@ -138,11 +139,13 @@ def beams(sort_every, n=(20, 12, 28), bc=(0, 1, 0), drift=0.3, steps=20, tile=(0
     return r, rows
 
 
-@pytest.mark.parametrize("tile", [(0, 0, 0), (4, 4, 4), (8, 8, 8)])
-def test_tiled_push_matches_untiled_push(tile):
+@pytest.mark.parametrize("tile,warps", [((0, 0, 0), 0), ((4, 4, 4), 0), ((8, 8, 8), 0),
+                                        ((0, 0, 0), 4), ((0, 0, 0), 16), ((4, 4, 4), 16)])
+def test_tiled_push_matches_untiled_push(tile, warps):
     # The tiled push sums currents in fixed point per tile, the untiled one
-    # in FP32 atomics: the two agree to single-precision round-off.
-    rt, a = beams(0, tile=tile)
+    # in FP32 atomics: the two agree to single-precision round-off, for every
+    # tile shape and block size the push is built for.
+    rt, a = beams(0, tile=tile, warps=warps)
     ru, b = beams(-1)
     scale = float(np.max(np.abs(b[:, 1:6].sum(1))))
     np.testing.assert_allclose(a[:, 1:], b[:, 1:], rtol=1e-5, atol=1e-6 * scale)
@@ -203,3 +206,6 @@ def test_tile_shape_outside_the_built_set_is_rejected():
     with pytest.raises(mg.MandorError) as e:
         mg.Run((8, 8, 8), (0.1,) * 3, 0.02, (0, 0, 0), (0, 0, 0), precision=mg.FP32_OFFSET, tile=(2, 4, 4))
     assert e.value.code == -2
+    with pytest.raises(mg.MandorError) as e:
+        mg.Run((8, 8, 8), (0.1,) * 3, 0.02, (0, 0, 0), (0, 0, 0), precision=mg.FP32_OFFSET, tile_warps=6)
+    assert e.value.code == -2 and "warps" in str(e.value)

@@ -51,9 +51,9 @@ def test_admission_keeps_footprints_within_the_budget():
 def test_tuned_solve_matches_the_default_one():
     s = scan.FoilSolve((48, 24, 24), 2, 2.0, 0.25, 20.0, 40)
     t = scan.Tuner(steps=4, sorts=(4, 8))
-    tile, every = t.choose(s)
-    assert tile in scan.Tuner.TILES and every in (4, 8)
-    rows, count, _ = scan.run_alone(s, tile=tile, sort_every=every)
+    tile, every, warps = t.choose(s)
+    assert tile in scan.Tuner.TILES and every in (4, 8) and warps in scan.Tuner.WARPS
+    rows, count, _ = scan.run_alone(s, tile=tile, sort_every=every, warps=warps)
     ref, count0, _ = scan.run_alone(s)
     close(rows, ref, s.precision)
     assert count == count0
