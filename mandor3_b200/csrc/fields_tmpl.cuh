@@ -339,6 +339,189 @@ k_e_fused (Grid g, F3T<T> E, F3T<T> H, F3T<T> J, Box b, T c1, T c2, T c3, Rim rm
 }
 
 
+// ---------------------------------------------------------------------------
+// Precision form: the two bulk passes on float4 slots.  A row's node k sits
+// at offset origin + i sx + j sy + k with origin = 1 (mod 4) and sx, sy
+// multiples of 4, so the slots m = [4m - 1, 4m + 2] are 16-byte aligned;
+// each thread takes one slot (four nodes) of a row, loads every stream of
+// the stencil with one vector load (the k -/+ 1 neighbours of the slot's
+// end nodes with one scalar load each), and stores whole slots inside the
+// box (nodes outside it are computed from in-allocation ghosts and padding
+// and not stored).  The arithmetic per node is that of the scalar kernels.
+// ---------------------------------------------------------------------------
+struct Slots {
+   Box walk;                // (i, j, slot) over the box's rows
+   int m0;                  // first slot of a row
+   int klo, khi;            // the box's k range
+};
+
+static Slots make_slots (const Box &b)
+{
+   Slots s;
+   s.klo = b.lo[2];
+   s.khi = b.lo[2] + b.ext[2] - 1;
+   s.m0 = (s.klo + 1) >> 2;
+   const int m1 = (s.khi + 1) >> 2;
+   s.walk = b;
+   s.walk.lo[2] = 0;
+   s.walk.ext[2] = m1 - s.m0 + 1;
+   s.walk.vol = (long) b.ext[0]*b.ext[1]*s.walk.ext[2];
+   return s;
+}
+
+__device__ __forceinline__ float4 ld4 (const float *p) { return *reinterpret_cast<const float4 *> (p); }
+__device__ __forceinline__ void st4 (float *p, float4 v) { *reinterpret_cast<float4 *> (p) = v; }
+__device__ __forceinline__ float el (const float4 &v, int e) { return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w; }
+
+__device__ __forceinline__ void st_slot (float *p, const float r[4], int k0, int klo, int khi)
+{
+   if (k0 >= klo && k0 + 3 <= khi) {
+      st4 (p, make_float4 (r[0], r[1], r[2], r[3]));
+      return;
+   }
+#pragma unroll
+   for (int e = 0 ; e < 4 ; ++e)
+      if (k0 + e >= klo && k0 + e <= khi)
+         p[e] = r[e];
+}
+
+template <bool HN>
+__global__ void __launch_bounds__ (256)
+k_h_fused4 (Grid g, F3T<float> E, F3T<float> H, F3T<float> Hn, Slots S, float c1, float c2, float c3,
+            EnergyPick ep, DevScalars *dsc)
+{
+   __shared__ double sw[2][8];
+   const float *Ex = E.c[0], *Ey = E.c[1], *Ez = E.c[2];
+   const long sx = g.sx, sy = g.sy;
+   const long stride = (long) gridDim.x*blockDim.x;
+   double we = 0, wb = 0;
+   BoxWalk wk;
+   walk_init (wk, blockIdx.x*(long) blockDim.x + threadIdx.x, stride, S.walk);
+   for (long t = blockIdx.x*(long) blockDim.x + threadIdx.x ; t < S.walk.vol ; t += stride) {
+      const int i = S.walk.lo[0] + wk.i, j = S.walk.lo[1] + wk.j, k0 = 4*(S.m0 + wk.k) - 1;
+      walk_step (wk, S.walk);
+      const long o = g.at (i, j, k0);
+      const float4 ex = ld4 (Ex + o), ey = ld4 (Ey + o), ez = ld4 (Ez + o);
+      const float4 ezy = ld4 (Ez + o - sy), ezx = ld4 (Ez + o - sx);
+      const float4 exy = ld4 (Ex + o - sy), eyx = ld4 (Ey + o - sx);
+      const float4 h0 = ld4 (H.c[0] + o), h1 = ld4 (H.c[1] + o), h2 = ld4 (H.c[2] + o);
+      const float eym = Ey[o - 1], exm = Ex[o - 1];
+      float rx[4], ry[4], rz[4], nx[4], ny[4], nz[4];
+      float se = 0.0f, sb = 0.0f;
+#pragma unroll
+      for (int e = 0 ; e < 4 ; ++e) {
+         const float vex = el (ex, e), vey = el (ey, e), vez = el (ez, e);
+         const float pey = e == 0 ? eym : el (ey, e - 1), pex = e == 0 ? exm : el (ex, e - 1);
+         const float cx = c3*(vey - pey) - c2*(vez - el (ezy, e));
+         const float cy = c1*(vez - el (ezx, e)) - c3*(vex - pex);
+         const float cz = c2*(vex - el (exy, e)) - c1*(vey - el (eyx, e));
+         const float hx = el (h0, e) + cx, hy = el (h1, e) + cy, hz = el (h2, e) + cz;
+         nx[e] = hx;
+         ny[e] = hy;
+         nz[e] = hz;
+         rx[e] = hx + cx;
+         ry[e] = hy + cy;
+         rz[e] = hz + cz;
+         const int k = k0 + e;
+         if (k < S.klo || k > S.khi)
+            continue;
+         const int I[3] = {i, j, k};
+         const float ev[3] = {vex, vey, vez}, hv[3] = {hx, hy, hz};
+#pragma unroll
+         for (int c = 0 ; c < 3 ; ++c) {
+            bool in_e = true, in_h = true;
+#pragma unroll
+            for (int a = 0 ; a < 3 ; ++a) {
+               in_e &= (I[a] >= ep.lo[c][a]) & (I[a] <= ep.hi[c][a]);
+               in_h &= (I[a] >= ep.hlo[c][a]) & (I[a] <= ep.hhi[c][a]);
+            }
+            if (in_e) se += ev[c]*ev[c];
+            if (in_h) sb += hv[c]*hv[c];
+         }
+      }
+      we += (double) se;
+      wb += (double) sb;
+      if (HN) {
+         st_slot (Hn.c[0] + o, nx, k0, S.klo, S.khi);
+         st_slot (Hn.c[1] + o, ny, k0, S.klo, S.khi);
+         st_slot (Hn.c[2] + o, nz, k0, S.klo, S.khi);
+      }
+      st_slot (H.c[0] + o, rx, k0, S.klo, S.khi);
+      st_slot (H.c[1] + o, ry, k0, S.klo, S.khi);
+      st_slot (H.c[2] + o, rz, k0, S.klo, S.khi);
+   }
+   for (int d = 16 ; d > 0 ; d >>= 1) {
+      we += __shfl_xor_sync (0xffffffffu, we, d);
+      wb += __shfl_xor_sync (0xffffffffu, wb, d);
+   }
+   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+   if (lane == 0) {
+      sw[0][wid] = we;
+      sw[1][wid] = wb;
+   }
+   __syncthreads ();
+   if (wid == 0) {
+      we = lane < (int) (blockDim.x >> 5) ? sw[0][lane] : 0;
+      wb = lane < (int) (blockDim.x >> 5) ? sw[1][lane] : 0;
+      for (int d = 16 ; d > 0 ; d >>= 1) {
+         we += __shfl_xor_sync (0xffffffffu, we, d);
+         wb += __shfl_xor_sync (0xffffffffu, wb, d);
+      }
+      if (lane == 0) {
+         atomicAdd (&dsc->acc[0], we);
+         atomicAdd (&dsc->acc[1], wb);
+      }
+   }
+}
+
+template <bool WJ>
+__global__ void __launch_bounds__ (256)
+k_e_fused4 (Grid g, F3T<float> E, F3T<float> H, F3T<float> J, Slots S, float c1, float c2, float c3, Rim rm)
+{
+   const float *Hx = H.c[0], *Hy = H.c[1], *Hz = H.c[2];
+   const long sx = g.sx, sy = g.sy;
+   const float tau = (float) g.tau;
+   const long stride = (long) gridDim.x*blockDim.x;
+   BoxWalk wk;
+   walk_init (wk, blockIdx.x*(long) blockDim.x + threadIdx.x, stride, S.walk);
+   for (long t = blockIdx.x*(long) blockDim.x + threadIdx.x ; t < S.walk.vol ; t += stride) {
+      const int i = S.walk.lo[0] + wk.i, j = S.walk.lo[1] + wk.j, k0 = 4*(S.m0 + wk.k) - 1;
+      walk_step (wk, S.walk);
+      const long o = g.at (i, j, k0);
+      const float4 hx = ld4 (Hx + o), hy = ld4 (Hy + o), hz = ld4 (Hz + o);
+      const float4 hzy = ld4 (Hz + o + sy), hzx = ld4 (Hz + o + sx);
+      const float4 hxy = ld4 (Hx + o + sy), hyx = ld4 (Hy + o + sx);
+      const float hyp = Hy[o + 4], hxp = Hx[o + 4];
+      const float4 e0 = ld4 (E.c[0] + o), e1 = ld4 (E.c[1] + o), e2 = ld4 (E.c[2] + o);
+      float4 j0 = make_float4 (0, 0, 0, 0), j1 = j0, j2 = j0;
+      if (WJ) {
+         j0 = ld4 (J.c[0] + o);
+         j1 = ld4 (J.c[1] + o);
+         j2 = ld4 (J.c[2] + o);
+      }
+      float rx[4], ry[4], rz[4];
+#pragma unroll
+      for (int e = 0 ; e < 4 ; ++e) {
+         const float vhx = el (hx, e), vhy = el (hy, e), vhz = el (hz, e);
+         const float nhy = e == 3 ? hyp : el (hy, e + 1), nhx = e == 3 ? hxp : el (hx, e + 1);
+         float ex = el (e0, e) - (c3*(nhy - vhy) - c2*(el (hzy, e) - vhz));
+         float ey = el (e1, e) - (c1*(el (hzx, e) - vhz) - c3*(nhx - vhx));
+         float ez = el (e2, e) - (c2*(el (hxy, e) - vhx) - c1*(el (hyx, e) - vhy));
+         if (WJ && !rim_node (rm, i, j, k0 + e)) {
+            ex -= tau*el (j0, e);
+            ey -= tau*el (j1, e);
+            ez -= tau*el (j2, e);
+         }
+         rx[e] = ex;
+         ry[e] = ey;
+         rz[e] = ez;
+      }
+      st_slot (E.c[0] + o, rx, k0, S.klo, S.khi);
+      st_slot (E.c[1] + o, ry, k0, S.klo, S.khi);
+      st_slot (E.c[2] + o, rz, k0, S.klo, S.khi);
+   }
+}
+
 // Wall kernels run over the two transverse axes, nodes [0, n+1] each (the
 // flush extent of the reference's caps, core/em_caps.c:140-146).
 struct Wall {
@@ -1354,12 +1537,22 @@ int fields_h_both (mg_run_t *r, const FS<T> &fs)
    const bool hn = r->np > 0 || r->probe_ring;
    MG_CUDA (cudaMemsetAsync (r->dsc->acc, 0, 2*sizeof (double), r->stream));
    const T c1 = (T) (0.5*g.tau/g.h[0]), c2 = (T) (0.5*g.tau/g.h[1]), c3 = (T) (0.5*g.tau/g.h[2]);
-   if (hn)
+   if constexpr (sizeof (T) == sizeof (float)) {
+      const Slots sl = make_slots (b);
+      const int B = mg_blocks_for (sl.walk.vol, NT, 8);
+      if (hn)
+         k_h_fused4<true><<<B, NT, 0, r->stream>>> (g, f3 (fs.E), f3 (fs.H), f3 (fs.Hn), sl, c1, c2, c3,
+                                                    energy_pick (g), r->dsc);
+      else
+         k_h_fused4<false><<<B, NT, 0, r->stream>>> (g, f3 (fs.E), f3 (fs.H), f3 (fs.Hn), sl, c1, c2, c3,
+                                                     energy_pick (g), r->dsc);
+   } else if (hn) {
       k_h_fused<T, true><<<mg_blocks_for (b.vol, NT, 8), NT, 0, r->stream>>> (
          g, f3 (fs.E), f3 (fs.H), f3 (fs.Hn), b, c1, c2, c3, energy_pick (g), r->dsc);
-   else
+   } else {
       k_h_fused<T, false><<<mg_blocks_for (b.vol, NT, 8), NT, 0, r->stream>>> (
          g, f3 (fs.E), f3 (fs.H), f3 (fs.Hn), b, c1, c2, c3, energy_pick (g), r->dsc);
+   }
    MG_LAUNCH_CHECK ();
    TRY_MG (mg_tfsf_h (r));
    TRY_MG (launch_mirrors<T> (r, fs, 0));
@@ -1459,12 +1652,20 @@ int fields_e_fused (mg_run_t *r, const FS<T> &fs)
    // and -tau J is left out.
    const bool wj = r->np > 0;
    const T c1 = (T) (g.tau/g.h[0]), c2 = (T) (g.tau/g.h[1]), c3 = (T) (g.tau/g.h[2]);
-   if (wj)
+   if constexpr (sizeof (T) == sizeof (float)) {
+      const Slots sl = make_slots (b);
+      const int B = mg_blocks_for (sl.walk.vol, NT, 8);
+      if (wj)
+         k_e_fused4<true><<<B, NT, 0, r->stream>>> (g, f3 (fs.E), f3 (fs.H), f3 (fs.J), sl, c1, c2, c3, rm);
+      else
+         k_e_fused4<false><<<B, NT, 0, r->stream>>> (g, f3 (fs.E), f3 (fs.H), f3 (fs.J), sl, c1, c2, c3, rm);
+   } else if (wj) {
       k_e_fused<T, true><<<mg_blocks_for (b.vol, NT, 8), NT, 0, r->stream>>> (
          g, f3 (fs.E), f3 (fs.H), f3 (fs.J), b, c1, c2, c3, rm);
-   else
+   } else {
       k_e_fused<T, false><<<mg_blocks_for (b.vol, NT, 8), NT, 0, r->stream>>> (
          g, f3 (fs.E), f3 (fs.H), f3 (fs.J), b, c1, c2, c3, rm);
+   }
    MG_LAUNCH_CHECK ();
    if (walls_merge (r)) {
       const bool lm = laser_merge (r);
