@@ -522,6 +522,125 @@ k_e_fused4 (Grid g, F3T<float> E, F3T<float> H, F3T<float> J, Slots S, float c1,
    }
 }
 
+// ---------------------------------------------------------------------------
+// Plain FP64 form: the H pass on double2 slots.  With four nodes in front
+// of k = 0 the FP64 origin is a multiple of 4 elements, so the slots
+// [2m, 2m + 1] are 16-byte aligned; the per-node arithmetic (compiled
+// without contraction) is the scalar kernel's, so H and H^n are
+// bit-identical to it.  The energy sums add the same squares, in slot order.
+// ---------------------------------------------------------------------------
+static Slots make_slots2 (const Box &b)
+{
+   Slots s;
+   s.klo = b.lo[2];
+   s.khi = b.lo[2] + b.ext[2] - 1;
+   s.m0 = s.klo >> 1;
+   const int m1 = s.khi >> 1;
+   s.walk = b;
+   s.walk.lo[2] = 0;
+   s.walk.ext[2] = m1 - s.m0 + 1;
+   s.walk.vol = (long) b.ext[0]*b.ext[1]*s.walk.ext[2];
+   return s;
+}
+
+__device__ __forceinline__ double2 ld2 (const double *p) { return *reinterpret_cast<const double2 *> (p); }
+
+__device__ __forceinline__ void st_slot2 (double *p, double a, double b, int k0, int klo, int khi)
+{
+   if (k0 >= klo && k0 + 1 <= khi) {
+      *reinterpret_cast<double2 *> (p) = make_double2 (a, b);
+      return;
+   }
+   if (k0 >= klo && k0 <= khi) p[0] = a;
+   if (k0 + 1 >= klo && k0 + 1 <= khi) p[1] = b;
+}
+
+template <bool HN>
+__global__ void __launch_bounds__ (256)
+k_h_fused2 (Grid g, F3T<double> E, F3T<double> H, F3T<double> Hn, Slots S, double c1, double c2, double c3,
+            EnergyPick ep, DevScalars *dsc)
+{
+   __shared__ double sw[2][8];
+   const double *Ex = E.c[0], *Ey = E.c[1], *Ez = E.c[2];
+   const long sx = g.sx, sy = g.sy;
+   const long stride = (long) gridDim.x*blockDim.x;
+   double we = 0, wb = 0;
+   BoxWalk wk;
+   walk_init (wk, blockIdx.x*(long) blockDim.x + threadIdx.x, stride, S.walk);
+   for (long t = blockIdx.x*(long) blockDim.x + threadIdx.x ; t < S.walk.vol ; t += stride) {
+      const int i = S.walk.lo[0] + wk.i, j = S.walk.lo[1] + wk.j, k0 = 2*(S.m0 + wk.k);
+      walk_step (wk, S.walk);
+      const long o = g.at (i, j, k0);
+      const double2 ex = ld2 (Ex + o), ey = ld2 (Ey + o), ez = ld2 (Ez + o);
+      const double2 ezy = ld2 (Ez + o - sy), ezx = ld2 (Ez + o - sx);
+      const double2 exy = ld2 (Ex + o - sy), eyx = ld2 (Ey + o - sx);
+      const double2 h0 = ld2 (H.c[0] + o), h1 = ld2 (H.c[1] + o), h2 = ld2 (H.c[2] + o);
+      const double eym = Ey[o - 1], exm = Ex[o - 1];
+      double rx[2], ry[2], rz[2], nx[2], ny[2], nz[2];
+#pragma unroll
+      for (int e = 0 ; e < 2 ; ++e) {
+         const double vex = e ? ex.y : ex.x, vey = e ? ey.y : ey.x, vez = e ? ez.y : ez.x;
+         const double pey = e ? ey.x : eym, pex = e ? ex.x : exm;
+         const double cx = c3*(vey - pey) - c2*(vez - (e ? ezy.y : ezy.x));
+         const double cy = c1*(vez - (e ? ezx.y : ezx.x)) - c3*(vex - pex);
+         const double cz = c2*(vex - (e ? exy.y : exy.x)) - c1*(vey - (e ? eyx.y : eyx.x));
+         const double hx = (e ? h0.y : h0.x) + cx, hy = (e ? h1.y : h1.x) + cy, hz = (e ? h2.y : h2.x) + cz;
+         nx[e] = hx;
+         ny[e] = hy;
+         nz[e] = hz;
+         rx[e] = hx + cx;
+         ry[e] = hy + cy;
+         rz[e] = hz + cz;
+         const int k = k0 + e;
+         if (k < S.klo || k > S.khi)
+            continue;
+         const int I[3] = {i, j, k};
+         const double ev[3] = {vex, vey, vez}, hv[3] = {hx, hy, hz};
+#pragma unroll
+         for (int c = 0 ; c < 3 ; ++c) {
+            bool in_e = true, in_h = true;
+#pragma unroll
+            for (int a = 0 ; a < 3 ; ++a) {
+               in_e &= (I[a] >= ep.lo[c][a]) & (I[a] <= ep.hi[c][a]);
+               in_h &= (I[a] >= ep.hlo[c][a]) & (I[a] <= ep.hhi[c][a]);
+            }
+            if (in_e) we += ev[c]*ev[c];
+            if (in_h) wb += hv[c]*hv[c];
+         }
+      }
+      if (HN) {
+         st_slot2 (Hn.c[0] + o, nx[0], nx[1], k0, S.klo, S.khi);
+         st_slot2 (Hn.c[1] + o, ny[0], ny[1], k0, S.klo, S.khi);
+         st_slot2 (Hn.c[2] + o, nz[0], nz[1], k0, S.klo, S.khi);
+      }
+      st_slot2 (H.c[0] + o, rx[0], rx[1], k0, S.klo, S.khi);
+      st_slot2 (H.c[1] + o, ry[0], ry[1], k0, S.klo, S.khi);
+      st_slot2 (H.c[2] + o, rz[0], rz[1], k0, S.klo, S.khi);
+   }
+   for (int d = 16 ; d > 0 ; d >>= 1) {
+      we += __shfl_xor_sync (0xffffffffu, we, d);
+      wb += __shfl_xor_sync (0xffffffffu, wb, d);
+   }
+   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+   if (lane == 0) {
+      sw[0][wid] = we;
+      sw[1][wid] = wb;
+   }
+   __syncthreads ();
+   if (wid == 0) {
+      we = lane < (int) (blockDim.x >> 5) ? sw[0][lane] : 0;
+      wb = lane < (int) (blockDim.x >> 5) ? sw[1][lane] : 0;
+      for (int d = 16 ; d > 0 ; d >>= 1) {
+         we += __shfl_xor_sync (0xffffffffu, we, d);
+         wb += __shfl_xor_sync (0xffffffffu, wb, d);
+      }
+      if (lane == 0) {
+         atomicAdd (&dsc->acc[0], we);
+         atomicAdd (&dsc->acc[1], wb);
+      }
+   }
+}
+
 // Wall kernels run over the two transverse axes, nodes [0, n+1] each (the
 // flush extent of the reference's caps, core/em_caps.c:140-146).
 struct Wall {
@@ -1546,12 +1665,15 @@ int fields_h_both (mg_run_t *r, const FS<T> &fs)
       else
          k_h_fused4<false><<<B, NT, 0, r->stream>>> (g, f3 (fs.E), f3 (fs.H), f3 (fs.Hn), sl, c1, c2, c3,
                                                      energy_pick (g), r->dsc);
-   } else if (hn) {
-      k_h_fused<T, true><<<mg_blocks_for (b.vol, NT, 8), NT, 0, r->stream>>> (
-         g, f3 (fs.E), f3 (fs.H), f3 (fs.Hn), b, c1, c2, c3, energy_pick (g), r->dsc);
    } else {
-      k_h_fused<T, false><<<mg_blocks_for (b.vol, NT, 8), NT, 0, r->stream>>> (
-         g, f3 (fs.E), f3 (fs.H), f3 (fs.Hn), b, c1, c2, c3, energy_pick (g), r->dsc);
+      const Slots sl = make_slots2 (b);
+      const int B = mg_blocks_for (sl.walk.vol, NT, 8);
+      if (hn)
+         k_h_fused2<true><<<B, NT, 0, r->stream>>> (g, f3 (fs.E), f3 (fs.H), f3 (fs.Hn), sl, c1, c2, c3,
+                                                    energy_pick (g), r->dsc);
+      else
+         k_h_fused2<false><<<B, NT, 0, r->stream>>> (g, f3 (fs.E), f3 (fs.H), f3 (fs.Hn), sl, c1, c2, c3,
+                                                     energy_pick (g), r->dsc);
    }
    MG_LAUNCH_CHECK ();
    TRY_MG (mg_tfsf_h (r));
