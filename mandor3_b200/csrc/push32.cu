@@ -877,11 +877,13 @@ k_push32_tiles (Ctx32 c, const __grid_constant__ TileMaps maps, const int *tile_
                   for (int q = 0 ; q < 12 ; ++q) wgt[q] = 0.0f;
                if (valid && !fast)
                   scatter32 (c, i, j, k, wgt);
+               // Lanes with key -1 (invalid, or pushed through global memory)
+               // take part in no group sum, so their fx are never read.
                const int key = (valid && fast) ? jq : -1;
                int fx[12];
 #pragma unroll
                for (int q = 0 ; q < 12 ; ++q)
-                  fx[q] = key >= 0 ? fixed (wgt[q], S) : 0;
+                  fx[q] = fixed (wgt[q], S);
                const unsigned grp = __match_any_sync (0xffffffffu, key);
                const bool alone = key >= 0 && __popc (grp) < GROUP;
                unsigned heads = __ballot_sync (0xffffffffu, key >= 0 && !alone && (grp & ((1u << lane) - 1)) == 0);
