@@ -1460,7 +1460,8 @@ static int launch_laser (mg_run_t *r, const FS<T> &fs, int is_e, int sub_j = 0)
    return MG_OK;
 }
 
-// The merged wall launch needs the two bands of every axis apart (n >= 6).
+// The merged wall launch needs the two bands of every axis apart (n >= 6;
+// a run has at least 8 cells per axis, so this holds for every run).
 // A run stepped as one branch of a batch graph keeps the per-axis kernels:
 // there the other runs' kernels fill the launch gaps, and the merged
 // kernel's serial corner block (three phases, then the rim) lengthens each

@@ -24,9 +24,9 @@ WALLS = [((0, 0, 0), (0, 0, 0)), ((1, 1, 1), (1, 1, 1)), ((2, 2, 2), (2, 2, 2)),
          ((2, 0, 1), (2, 0, 1)), ((1, 2, 0), (2, 1, 0)), ((2, 1, 2), (1, 2, 1))]
 
 
-def fields():
-    i, j, k = np.meshgrid(*[np.arange(v + 1) / v for v in N], indexing="ij")
-    E = np.zeros((N[0] + 1, N[1] + 1, N[2] + 1, 3))
+def fields(n=N):
+    i, j, k = np.meshgrid(*[np.arange(v + 1) / v for v in n], indexing="ij")
+    E = np.zeros((n[0] + 1, n[1] + 1, n[2] + 1, 3))
     H = np.zeros_like(E)
     E[..., 0] = np.sin(2 * np.pi * (j + 2 * k)) * np.cos(2 * np.pi * i) + 0.3 * np.exp(-30 * ((i - .4) ** 2 + (k - .6) ** 2))
     E[..., 1] = 0.7 * np.cos(2 * np.pi * (i - k)) + 0.2 * np.sin(6 * np.pi * j)
@@ -52,9 +52,9 @@ def staged(r, steps):
     return np.array(rows)
 
 
-def make(walls, precision):
-    r = mg.Run(N, H_, TAU, walls[0], walls[1], precision=precision)
-    E, H = fields()
+def make(walls, precision, n=N):
+    r = mg.Run(n, H_, TAU, walls[0], walls[1], precision=precision)
+    E, H = fields(n)
     r.set_fields(E, H)
     r.init()
     return r
@@ -70,6 +70,42 @@ def test_graph_step_matches_staged_kernels(walls):
     Eb, Hb = b.fields()
     assert np.array_equal(Ea, Eb) and np.array_equal(Ha, Hb)
     np.testing.assert_allclose(rows[:, 1:3], ref, rtol=1e-13, atol=1e-300)
+
+
+# The smallest grids a run accepts (8 cells per axis, core/plasma.c:392-396)
+# leave the merged wall launch three face lines per axis and three edge
+# slices; odd sides give the slot passes a partial last slot.
+@pytest.mark.parametrize("n", [(8, 9, 11), (9, 8, 8)])
+@pytest.mark.parametrize("walls", [WALLS[0], WALLS[1], WALLS[4], WALLS[5]])
+def test_graph_step_matches_staged_kernels_on_small_grids(walls, n):
+    a = make(walls, mg.FP64, n)
+    rows = a.step(20)
+    b = make(walls, mg.FP64, n)
+    ref = staged(b, 20)
+    Ea, Ha = a.fields()
+    Eb, Hb = b.fields()
+    assert np.array_equal(Ea, Eb) and np.array_equal(Ha, Hb)
+    np.testing.assert_allclose(rows[:, 1:3], ref, rtol=1e-13, atol=1e-300)
+
+
+def test_batch_branch_matches_the_run_alone_bit_for_bit():
+    # A run stepped as a batch branch keeps the per-axis wall kernels, alone
+    # it takes the merged launch: a field-only FP64 run gives the same bits.
+    alone = make(WALLS[4], mg.FP64)
+    alone.step(25)
+    a = make(WALLS[4], mg.FP64)
+    other = make(WALLS[0], mg.FP64)
+    b = mg.Batch([a, other])
+    b.step(25)
+    b.close()
+    Ea, Ha = a.fields()
+    Eb, Hb = alone.fields()
+    assert np.array_equal(Ea, Eb) and np.array_equal(Ha, Hb)
+    a.step(5)                   # alone again after the batch: merged walls
+    alone.step(5)
+    Ea, Ha = a.fields()
+    Eb, Hb = alone.fields()
+    assert np.array_equal(Ea, Eb) and np.array_equal(Ha, Hb)
 
 
 @pytest.mark.parametrize("walls", [WALLS[3], WALLS[5]])
