@@ -682,6 +682,26 @@ __device__ __forceinline__ bool wall_node (const Grid &g, const Wall &w, int a,
 
 enum { OP_PERIODIC = 0, OP_MIRROR_MIN, OP_MIRROR_MAX, OP_OPEN_MIN, OP_OPEN_MAX };
 
+// Wall operations take their axis as a template argument: transverse axes,
+// strides and extents are then compile-time picks among the kernel's
+// parameters.  (Indexing a parameter array with a run-time axis makes the
+// compiler copy the parameters to local memory, on the critical path of
+// these latency-bound kernels.)
+template <int AX> struct Axes {
+   static constexpr int EP = AX == 0 ? 1 : 0, EQ = AX == 2 ? 1 : 2;
+};
+
+template <int AX>
+__device__ __forceinline__ long axis_stride (const Grid &g) { return AX == 0 ? g.sx : AX == 1 ? g.sy : 1; }
+
+// Host side: run the statement with the compile-time axis AX = ea.
+#define MG_AXIS_SWITCH(ea, ...)                                               \
+   switch (ea) {                                                              \
+   case 0: { constexpr int AX = 0; __VA_ARGS__; } break;                      \
+   case 1: { constexpr int AX = 1; __VA_ARGS__; } break;                      \
+   default: { constexpr int AX = 2; __VA_ARGS__; } break;                     \
+   }
+
 // H wall operations (core/emCap_periodic.c:15-37, emCap_mirror.c:17-40,
 // emCap_Mur.c:56-80).
 template <typename T>
@@ -803,27 +823,28 @@ __global__ void k_mur_init (Grid g, F3T<T> E, Wall w, int top, T *mur)
 // All wall operations of one axis in one launch: the lower wall, then the
 // upper wall (they touch disjoint nodes for n >= 3).  H walls act on both
 // H arrays (H at n and at n+1/2).
-template <typename T>
-__device__ __forceinline__ void h_line (const Grid &g, F3T<T> &H, F3T<T> &Hn, const Wall &w, int op_min,
+template <typename T, int AX>
+__device__ __forceinline__ void h_line (const Grid &g, const F3T<T> &H, const F3T<T> &Hn, int op_min,
                                         int op_max, int both, long o)
 {
-   const int N = g.n[w.ea];
-   const long s = w.s_a;
+   constexpr int EP = Axes<AX>::EP, EQ = Axes<AX>::EQ;
+   const int N = g.n[AX];
+   const long s = axis_stride<AX> (g);
    for (int arr = 0 ; arr < (both ? 2 : 1) ; ++arr) {
-      F3T<T> &F = arr ? Hn : H;
-      T *Ha = F.c[w.ea], *Hp = F.c[w.ep], *Hq = F.c[w.eq];
+      T *const F[3] = {arr ? Hn.c[0] : H.c[0], arr ? Hn.c[1] : H.c[1], arr ? Hn.c[2] : H.c[2]};
+      T *Ha = F[AX], *Hp = F[EP], *Hq = F[EQ];
       // Loads first, then stores: the wall nodes never alias the sources.
       if (op_min == OP_PERIODIC) {
          T top[3], one[3];
 #pragma unroll
          for (int c = 0 ; c < 3 ; ++c) {
-            top[c] = F.c[c][o + N*s];
-            one[c] = F.c[c][o + s];
+            top[c] = F[c][o + N*s];
+            one[c] = F[c][o + s];
          }
 #pragma unroll
          for (int c = 0 ; c < 3 ; ++c) {
-            F.c[c][o] = top[c];
-            F.c[c][o + (N + 1)*s] = one[c];
+            F[c][o] = top[c];
+            F[c][o + (N + 1)*s] = one[c];
          }
          continue;
       }
@@ -841,51 +862,55 @@ __device__ __forceinline__ void h_line (const Grid &g, F3T<T> &H, F3T<T> &Hn, co
    }
 }
 
-template <typename T>
+template <typename T, int AX>
 __global__ void k_h_walls (Grid g, F3T<T> H, F3T<T> Hn, Wall w, int op_min, int op_max, int both)
 {
    long o;
    int p, q;
    if (!wall_node (g, w, 0, o, p, q))
       return;
-   h_line (g, H, Hn, w, op_min, op_max, both, o);
+   h_line<T, AX> (g, H, Hn, op_min, op_max, both, o);
 }
 
-template <typename T>
-__device__ __forceinline__ void e_wall_op (const Grid &g, F3T<T> &E, const Wall &w, int op,
-                                           long o, int p, int q, T *mur, T alpha)
+template <typename T, int AX>
+__device__ __forceinline__ void e_wall_op (const Grid &g, const F3T<T> &E, int op, long o, int p, int q,
+                                           T *mur, T alpha)
 {
-   const int N = g.n[w.ea];
-   T *Ea = E.c[w.ea], *Ep = E.c[w.ep], *Eq = E.c[w.eq];
+   constexpr int EP = Axes<AX>::EP, EQ = Axes<AX>::EQ;
+   const int N = g.n[AX];
+   const long sa = axis_stride<AX> (g);
+   const int nq_ = g.n[EQ] + 2;
+   T *Ea = E.c[AX], *Ep = E.c[EP], *Eq = E.c[EQ];
    switch (op) {
    case OP_PERIODIC:
+#pragma unroll
       for (int c = 0 ; c < 3 ; ++c) {
-         E.c[c][o + N*w.s_a] = E.c[c][o];
-         E.c[c][o + (N + 1)*w.s_a] = E.c[c][o + w.s_a];
+         E.c[c][o + N*sa] = E.c[c][o];
+         E.c[c][o + (N + 1)*sa] = E.c[c][o + sa];
       }
       break;
    case OP_MIRROR_MIN:
       Ep[o] = 0;
       Eq[o] = 0;
-      Ea[o] = Ea[o + w.s_a];
+      Ea[o] = Ea[o + sa];
       break;
    case OP_MIRROR_MAX:
-      o += N*w.s_a;
+      o += N*sa;
       Ep[o] = 0;
       Eq[o] = 0;
-      Ea[o + w.s_a] = Ea[o];
+      Ea[o + sa] = Ea[o];
       break;
    case OP_OPEN_MIN:
    case OP_OPEN_MAX: {
       const bool top = (op == OP_OPEN_MAX);
       if (top)
-         o += N*w.s_a;
-      const long in = top ? o - w.s_a : o + w.s_a;
-      T *h = mur + 4*((long) p*w.nq_ + q);
+         o += N*sa;
+      const long in = top ? o - sa : o + sa;
+      T *h = mur + 4*((long) p*nq_ + q);
       if (top)
-         Ea[o + w.s_a] = Ea[o];
+         Ea[o + sa] = Ea[o];
       else
-         Ea[o] = Ea[o + w.s_a];
+         Ea[o] = Ea[o + sa];
       const T ep = h[2] + alpha*(Ep[in] - h[0]);
       const T eq = h[3] + alpha*(Eq[in] - h[1]);
       Ep[o] = ep;
@@ -908,10 +933,11 @@ __device__ __forceinline__ void e_wall_op (const Grid &g, F3T<T> &E, const Wall 
 // later wall reads or writes such a node, so its -tau J comes after every
 // wall operation on it, as in core/em.c:189-222.  Threads cover transverse
 // indices [-1, n+1]; the wall operations act on [0, n+1].
-template <typename T>
+template <typename T, int AX>
 __global__ void k_e_walls (Grid g, F3T<T> E, F3T<T> J, Wall w, int op_min, int op_max, T *mur_min,
                            T *mur_max, T alpha, int sub_j)
 {
+   constexpr int EP = Axes<AX>::EP, EQ = Axes<AX>::EQ;
    const long t = blockIdx.x*(long) blockDim.x + threadIdx.x;
    const int np1 = w.np_ + 1, nq1 = w.nq_ + 1;          // [-1, n+1]
    if (t >= (long) np1*nq1)
@@ -919,18 +945,18 @@ __global__ void k_e_walls (Grid g, F3T<T> E, F3T<T> J, Wall w, int op_min, int o
    const int p = (int) (t / nq1) - 1, q = (int) (t % nq1) - 1;
    const long o = g.origin + p*w.s_p + q*w.s_q;
    if (p >= 0 && q >= 0) {
-      e_wall_op (g, E, w, op_min, o, p, q, mur_min, alpha);
-      e_wall_op (g, E, w, op_max, o, p, q, mur_max, alpha);
+      e_wall_op<T, AX> (g, E, op_min, o, p, q, mur_min, alpha);
+      e_wall_op<T, AX> (g, E, op_max, o, p, q, mur_max, alpha);
    }
    if (!sub_j)
       return;
-   const int N = g.n[w.ea];
-   const int Np = g.n[w.ep], Nq = g.n[w.eq];
+   const int N = g.n[AX];
+   const int Np = g.n[EP], Nq = g.n[EQ];
    const bool p_rim = p < 2 || p > Np - 2, q_rim = q < 2 || q > Nq - 2;
    bool own;
-   if (w.ea == 2)
+   if (AX == 2)
       own = true;
-   else if (w.ea == 1)
+   else if (AX == 1)
       own = !q_rim;                 // eq = z
    else
       own = !p_rim && !q_rim;       // ep = y, eq = z
@@ -941,7 +967,7 @@ __global__ void k_e_walls (Grid g, F3T<T> E, F3T<T> J, Wall w, int op_min, int o
    T e[6][3], jv[6][3];
 #pragma unroll
    for (int u = 0 ; u < 6 ; ++u) {
-      const long x = o + vs[u]*w.s_a;
+      const long x = o + vs[u]*axis_stride<AX> (g);
 #pragma unroll
       for (int c = 0 ; c < 3 ; ++c) {
          e[u][c] = E.c[c][x];
@@ -950,7 +976,7 @@ __global__ void k_e_walls (Grid g, F3T<T> E, F3T<T> J, Wall w, int op_min, int o
    }
 #pragma unroll
    for (int u = 0 ; u < 6 ; ++u) {
-      const long x = o + vs[u]*w.s_a;
+      const long x = o + vs[u]*axis_stride<AX> (g);
 #pragma unroll
       for (int c = 0 ; c < 3 ; ++c)
          E.c[c][x] = e[u][c] - tau*jv[u][c];
@@ -985,15 +1011,15 @@ __device__ __forceinline__ void j_fold_wall (T a[5], T pp[5], T qq[5], int top)
    qq[2 + 2*out] = -qq[2 - 2*out];
 }
 
-template <typename T>
-__device__ __forceinline__ void j_fold (const Grid &g, F3T<T> &J, int ea, int top, int bc, long base,
-                                        const long s[3])
+template <typename T, int AX>
+__device__ __forceinline__ void j_fold (const Grid &g, const F3T<T> &J, int top, int bc, long base)
 {
-   const long st = s[ea];
+   constexpr int EP = Axes<AX>::EP, EQ = Axes<AX>::EQ;
+   const long st = axis_stride<AX> (g);
    if (bc == MG_BC_PERIODIC) {
       if (top)
          return;
-      const long shift = (long) g.n[ea]*st;
+      const long shift = (long) g.n[AX]*st;
       T lo[3][5], hi[3][5];
 #pragma unroll
       for (int c = 0 ; c < 3 ; ++c)
@@ -1012,37 +1038,38 @@ __device__ __forceinline__ void j_fold (const Grid &g, F3T<T> &J, int ea, int to
          }
       return;
    }
-   const int ep = (ea == 0) ? 1 : 0, eq = (ea == 2) ? 1 : 2;
-   const long o = base + (top ? g.n[ea] : 0)*st;
+   const long o = base + (top ? g.n[AX] : 0)*st;
    T a[5], pp[5], qq[5];
 #pragma unroll
    for (int u = 0 ; u < 5 ; ++u) {
-      a[u] = J.c[ea][o + (u - 2)*st];
-      pp[u] = J.c[ep][o + (u - 2)*st];
-      qq[u] = J.c[eq][o + (u - 2)*st];
+      a[u] = J.c[AX][o + (u - 2)*st];
+      pp[u] = J.c[EP][o + (u - 2)*st];
+      qq[u] = J.c[EQ][o + (u - 2)*st];
    }
-   j_fold_wall (a, pp, qq, top);
+   if (top)
+      j_fold_wall (a, pp, qq, 1);
+   else
+      j_fold_wall (a, pp, qq, 0);
 #pragma unroll
    for (int u = 0 ; u < 5 ; ++u) {
-      J.c[ea][o + (u - 2)*st] = a[u];
-      J.c[ep][o + (u - 2)*st] = pp[u];
-      J.c[eq][o + (u - 2)*st] = qq[u];
+      J.c[AX][o + (u - 2)*st] = a[u];
+      J.c[EP][o + (u - 2)*st] = pp[u];
+      J.c[EQ][o + (u - 2)*st] = qq[u];
    }
 }
 
-template <typename T>
-__global__ void k_j_walls (Grid g, F3T<T> J, int ea)
+template <typename T, int AX>
+__global__ void k_j_walls (Grid g, F3T<T> J)
 {
-   const int ep = (ea == 0) ? 1 : 0, eq = (ea == 2) ? 1 : 2;
-   const int np_ = g.n[ep] + 5, nq_ = g.n[eq] + 5;
+   constexpr int EP = Axes<AX>::EP, EQ = Axes<AX>::EQ;
+   const int np_ = g.n[EP] + 5, nq_ = g.n[EQ] + 5;
    const long t = blockIdx.x*(long) blockDim.x + threadIdx.x;
    if (t >= (long) np_*nq_)
       return;
-   const long s[3] = {g.sx, g.sy, 1};
    const int p = (int) (t / nq_) - 2, q = (int) (t % nq_) - 2;
-   const long base = g.origin + p*s[ep] + q*s[eq];
-   j_fold (g, J, ea, 0, g.bc[0][ea], base, s);
-   j_fold (g, J, ea, 1, g.bc[1][ea], base, s);
+   const long base = g.origin + p*axis_stride<EP> (g) + q*axis_stride<EQ> (g);
+   j_fold<T, AX> (g, J, 0, g.bc[0][AX], base);
+   j_fold<T, AX> (g, J, 1, g.bc[1][AX], base);
 }
 
 
@@ -1211,28 +1238,25 @@ struct WallArgs {
 
 __device__ __forceinline__ int band_at (int u, int N) { return u < 5 ? u - 2 : N - 7 + u; }
 
-// The wall line of axis a whose transverse indices are co[ep], co[eq].
-template <typename T, int KIND>
-__device__ __forceinline__ void wall_line (const Grid &g, WallArgs<T> &A, const WallPlan &P, int a,
-                                           const int co[3])
+// The wall line of axis AX whose transverse indices (along Axes<AX>::EP
+// and ::EQ) are p and q.
+template <typename T, int KIND, int AX>
+__device__ __forceinline__ void wall_line (const Grid &g, WallArgs<T> &A, const WallPlan &P, int p, int q)
 {
-   const Wall &w = P.w[a];
-   const int p = co[w.ep], q = co[w.eq];
-   if (p < P.lo || p > g.n[w.ep] + P.hi || q < P.lo || q > g.n[w.eq] + P.hi)
+   constexpr int EP = Axes<AX>::EP, EQ = Axes<AX>::EQ;
+   if (p < P.lo || p > g.n[EP] + P.hi || q < P.lo || q > g.n[EQ] + P.hi)
       return;
+   const long o = g.origin + p*axis_stride<EP> (g) + q*axis_stride<EQ> (g);
    if (KIND == WK_H) {
-      h_line (g, A.F, A.F2, w, P.op0[a], P.op1[a], A.flag, g.origin + p*w.s_p + q*w.s_q);
+      h_line<T, AX> (g, A.F, A.F2, P.op0[AX], P.op1[AX], A.flag, o);
    } else if (KIND == WK_E) {
       if (p >= 0 && q >= 0) {
-         const long o = g.origin + p*w.s_p + q*w.s_q;
-         e_wall_op (g, A.F, w, P.op0[a], o, p, q, A.mur[0][a], A.alpha[a]);
-         e_wall_op (g, A.F, w, P.op1[a], o, p, q, A.mur[1][a], A.alpha[a]);
+         e_wall_op<T, AX> (g, A.F, P.op0[AX], o, p, q, A.mur[0][AX], A.alpha[AX]);
+         e_wall_op<T, AX> (g, A.F, P.op1[AX], o, p, q, A.mur[1][AX], A.alpha[AX]);
       }
    } else {
-      const long s[3] = {g.sx, g.sy, 1};
-      const long base = g.origin + p*s[w.ep] + q*s[w.eq];
-      j_fold (g, A.J, a, 0, g.bc[0][a], base, s);
-      j_fold (g, A.J, a, 1, g.bc[1][a], base, s);
+      j_fold<T, AX> (g, A.J, 0, g.bc[0][AX], o);
+      j_fold<T, AX> (g, A.J, 1, g.bc[1][AX], o);
    }
 }
 
@@ -1256,82 +1280,115 @@ __device__ __forceinline__ void rim_sub_j (const Grid &g, WallArgs<T> &A, int i,
 
 __device__ __forceinline__ bool rim_index (int v, int N) { return v < 2 || v > N - 2; }
 
+// Node (i, j, k) with index v along axis AX and p, q along its transverse axes.
+template <int AX>
+__device__ __forceinline__ void node_of (int v, int p, int q, int &i, int &j, int &k)
+{
+   constexpr int EP = Axes<AX>::EP;
+   i = AX == 0 ? v : EP == 0 ? p : q;
+   j = AX == 1 ? v : EP == 1 ? p : q;
+   k = AX == 2 ? v : q;
+}
+
+template <typename T, int KIND, int AX>
+__device__ __forceinline__ void face_line (const Grid &g, WallArgs<T> &A, const WallPlan &P, long t)
+{
+   constexpr int EQ = Axes<AX>::EQ;
+   if (t >= P.nface[AX])
+      return;
+   const int nq = g.n[EQ] - 5;
+   const int p = 3 + (int) (t / nq), q = 3 + (int) (t % nq);
+   wall_line<T, KIND, AX> (g, A, P, p, q);
+   if (KIND == WK_E && A.flag) {
+      const int N = g.n[AX];
+      const int vs[6] = {-1, 0, 1, N - 1, N, N + 1};
+#pragma unroll
+      for (int u = 0 ; u < 6 ; ++u) {
+         int i, j, k;
+         node_of<AX> (vs[u], p, q, i, j, k);
+         rim_sub_j (g, A, i, j, k);
+      }
+   }
+}
+
+// Edge slice at index tc of axis C: phases of the two other axes, lower
+// index first, on their lines through band x band.
+template <typename T, int KIND, int C>
+__device__ __forceinline__ void edge_slice (const Grid &g, WallArgs<T> &A, const WallPlan &P, int s, int lane)
+{
+   constexpr int AA = C == 0 ? 1 : 0, BB = C == 2 ? 1 : 2;     // AA < BB, both != C
+   if (s >= P.nslice[C])
+      return;                                   // whole warps leave together
+   const int tc = 3 + s;
+   if (lane < 10) {
+      const int tb = band_at (lane, g.n[BB]);
+      // Axis AA's lines: transverse axes {BB, C} in its (EP, EQ) order.
+      if (Axes<AA>::EP == BB)
+         wall_line<T, KIND, AA> (g, A, P, tb, tc);
+      else
+         wall_line<T, KIND, AA> (g, A, P, tc, tb);
+   }
+   __syncwarp ();
+   if (lane < 10) {
+      const int ta = band_at (lane, g.n[AA]);
+      if (Axes<BB>::EP == AA)
+         wall_line<T, KIND, BB> (g, A, P, ta, tc);
+      else
+         wall_line<T, KIND, BB> (g, A, P, tc, ta);
+   }
+   __syncwarp ();
+   if (KIND == WK_E && A.flag)
+      for (int u = lane ; u < 100 ; u += 32) {
+         const int va = band_at (u / 10, g.n[AA]), vb = band_at (u % 10, g.n[BB]);
+         if (va < -1 || va > g.n[AA] + 1 || vb < -1 || vb > g.n[BB] + 1)
+            continue;
+         if (!rim_index (va, g.n[AA]) && !rim_index (vb, g.n[BB]))
+            continue;
+         const int i = AA == 0 ? va : C == 0 ? tc : vb;
+         const int j = AA == 1 ? va : BB == 1 ? vb : tc;
+         const int k = BB == 2 ? vb : tc;
+         rim_sub_j (g, A, i, j, k);
+      }
+}
+
+template <typename T, int KIND, int AX>
+__device__ __forceinline__ void corner_phase (const Grid &g, WallArgs<T> &A, const WallPlan &P)
+{
+   constexpr int EP = Axes<AX>::EP, EQ = Axes<AX>::EQ;
+   for (int u = threadIdx.x ; u < 100 ; u += blockDim.x)
+      wall_line<T, KIND, AX> (g, A, P, band_at (u / 10, g.n[EP]), band_at (u % 10, g.n[EQ]));
+   __syncthreads ();
+}
+
 template <typename T, int KIND>
 __global__ void __launch_bounds__ (256)
 k_walls_all (Grid g, WallArgs<T> A, WallPlan P)
 {
    const int b = blockIdx.x;
-   const bool sub = (KIND == WK_E) && A.flag;
    if (b < P.bface[3]) {
-      const int a = b >= P.bface[2] ? 2 : b >= P.bface[1] ? 1 : 0;
-      const long t = (long) (b - P.bface[a])*blockDim.x + threadIdx.x;
-      if (t >= P.nface[a])
-         return;
-      const Wall &w = P.w[a];
-      const int nq = g.n[w.eq] - 5;
-      int co[3];
-      co[a] = 0;
-      co[w.ep] = 3 + (int) (t / nq);
-      co[w.eq] = 3 + (int) (t % nq);
-      wall_line<T, KIND> (g, A, P, a, co);
-      if (sub) {
-         const int N = g.n[a];
-         const int vs[6] = {-1, 0, 1, N - 1, N, N + 1};
-#pragma unroll
-         for (int u = 0 ; u < 6 ; ++u) {
-            co[a] = vs[u];
-            rim_sub_j (g, A, co[0], co[1], co[2]);
-         }
-      }
+      if (b >= P.bface[2])
+         face_line<T, KIND, 2> (g, A, P, (long) (b - P.bface[2])*blockDim.x + threadIdx.x);
+      else if (b >= P.bface[1])
+         face_line<T, KIND, 1> (g, A, P, (long) (b - P.bface[1])*blockDim.x + threadIdx.x);
+      else
+         face_line<T, KIND, 0> (g, A, P, (long) (b - P.bface[0])*blockDim.x + threadIdx.x);
       return;
    }
    if (b < P.bslice[3]) {
-      const int c = b >= P.bslice[2] ? 2 : b >= P.bslice[1] ? 1 : 0;
-      const int s = (b - P.bslice[c])*(int) (blockDim.x >> 5) + (int) (threadIdx.x >> 5);
-      if (s >= P.nslice[c])
-         return;                                   // whole warps leave together
-      const int lane = threadIdx.x & 31;
-      const int a = (c == 0) ? 1 : 0, bb = (c == 2) ? 1 : 2;     // a < bb, both != c
-      int co[3];
-      co[c] = 3 + s;
-      if (lane < 10) {
-         co[a] = 0;
-         co[bb] = band_at (lane, g.n[bb]);
-         wall_line<T, KIND> (g, A, P, a, co);
-      }
-      __syncwarp ();
-      if (lane < 10) {
-         co[bb] = 0;
-         co[a] = band_at (lane, g.n[a]);
-         wall_line<T, KIND> (g, A, P, bb, co);
-      }
-      __syncwarp ();
-      if (sub)
-         for (int u = lane ; u < 100 ; u += 32) {
-            const int va = band_at (u / 10, g.n[a]), vb = band_at (u % 10, g.n[bb]);
-            if (va < -1 || va > g.n[a] + 1 || vb < -1 || vb > g.n[bb] + 1)
-               continue;
-            if (!rim_index (va, g.n[a]) && !rim_index (vb, g.n[bb]))
-               continue;
-            co[a] = va;
-            co[bb] = vb;
-            rim_sub_j (g, A, co[0], co[1], co[2]);
-         }
+      const int w = (int) (threadIdx.x >> 5), lane = threadIdx.x & 31, nw = (int) (blockDim.x >> 5);
+      if (b >= P.bslice[2])
+         edge_slice<T, KIND, 2> (g, A, P, (b - P.bslice[2])*nw + w, lane);
+      else if (b >= P.bslice[1])
+         edge_slice<T, KIND, 1> (g, A, P, (b - P.bslice[1])*nw + w, lane);
+      else
+         edge_slice<T, KIND, 0> (g, A, P, (b - P.bslice[0])*nw + w, lane);
       return;
    }
    if (b == P.bslice[3]) {
-      for (int a = 0 ; a < 3 ; ++a) {
-         const Wall &w = P.w[a];
-         for (int u = threadIdx.x ; u < 100 ; u += blockDim.x) {
-            int co[3];
-            co[a] = 0;
-            co[w.ep] = band_at (u / 10, g.n[w.ep]);
-            co[w.eq] = band_at (u % 10, g.n[w.eq]);
-            wall_line<T, KIND> (g, A, P, a, co);
-         }
-         __syncthreads ();
-      }
-      if (sub)
+      corner_phase<T, KIND, 0> (g, A, P);
+      corner_phase<T, KIND, 1> (g, A, P);
+      corner_phase<T, KIND, 2> (g, A, P);
+      if (KIND == WK_E && A.flag)
          for (int u = threadIdx.x ; u < 1000 ; u += blockDim.x) {
             const int v0 = band_at (u / 100, g.n[0]), v1 = band_at ((u / 10) % 10, g.n[1]);
             const int v2 = band_at (u % 10, g.n[2]);
@@ -1390,7 +1447,7 @@ static int launch_h_walls (mg_run_t *r, const FS<T> &fs, int both)
       const int NT = 256, B = (int) ((nodes + NT - 1)/NT);
       int op0, op1;
       wall_ops (g, ea, op0, op1);
-      k_h_walls<<<B, NT, 0, r->stream>>> (g, f3 (fs.H), f3 (fs.Hn), w, op0, op1, both);
+      MG_AXIS_SWITCH (ea, k_h_walls<T, AX><<<B, NT, 0, r->stream>>> (g, f3 (fs.H), f3 (fs.Hn), w, op0, op1, both));
       MG_LAUNCH_CHECK ();
    }
    return MG_OK;
@@ -1406,7 +1463,7 @@ static int launch_hn_walls (mg_run_t *r, const FS<T> &fs)
       const int NT = 256, B = (int) ((nodes + NT - 1)/NT);
       int op0, op1;
       wall_ops (g, ea, op0, op1);
-      k_h_walls<<<B, NT, 0, r->stream>>> (g, f3 (fs.Hn), f3 (fs.Hn), w, op0, op1, 0);
+      MG_AXIS_SWITCH (ea, k_h_walls<T, AX><<<B, NT, 0, r->stream>>> (g, f3 (fs.Hn), f3 (fs.Hn), w, op0, op1, 0));
       MG_LAUNCH_CHECK ();
    }
    return MG_OK;
@@ -1424,8 +1481,8 @@ static int launch_e_walls (mg_run_t *r, const FS<T> &fs, int sub_j)
       const T alpha = (T) ((g.tau - g.h[ea])/(g.tau + g.h[ea]));
       int op0, op1;
       wall_ops (g, ea, op0, op1);
-      k_e_walls<<<B, NT, 0, r->stream>>> (g, f3 (fs.E), f3 (fs.J), w, op0, op1, fs.mur[0][ea],
-                                         fs.mur[1][ea], alpha, sub_j);
+      MG_AXIS_SWITCH (ea, k_e_walls<T, AX><<<B, NT, 0, r->stream>>> (g, f3 (fs.E), f3 (fs.J), w, op0, op1, fs.mur[0][ea],
+                                         fs.mur[1][ea], alpha, sub_j));
       MG_LAUNCH_CHECK ();
    }
    return MG_OK;
@@ -1639,7 +1696,7 @@ int fields_h_step (mg_run_t *r, const FS<T> &fs)
       const int NT = 256, B = (int) ((nodes + NT - 1)/NT);
       int op0, op1;
       wall_ops (g, ea, op0, op1);
-      k_h_walls<<<B, NT, 0, r->stream>>> (g, f3 (fs.H), f3 (fs.H), w, op0, op1, 0);
+      MG_AXIS_SWITCH (ea, k_h_walls<T, AX><<<B, NT, 0, r->stream>>> (g, f3 (fs.H), f3 (fs.H), w, op0, op1, 0));
       MG_LAUNCH_CHECK ();
    }
    return MG_OK;
@@ -1710,7 +1767,7 @@ int fields_jbc (mg_run_t *r, const FS<T> &fs)
       const int ep = (ea == 0) ? 1 : 0, eq = (ea == 2) ? 1 : 2;
       const long nodes = (long) (g.n[ep] + 5)*(g.n[eq] + 5);
       const int NT = 256, B = (int) ((nodes + NT - 1)/NT);
-      k_j_walls<<<B, NT, 0, r->stream>>> (g, f3 (fs.J), ea);
+      MG_AXIS_SWITCH (ea, k_j_walls<T, AX><<<B, NT, 0, r->stream>>> (g, f3 (fs.J)));
       MG_LAUNCH_CHECK ();
    }
    return MG_OK;
