@@ -317,8 +317,10 @@ k_push64 (Ctx c, Markers64 m, long long np, DevScalars *dsc)
       const long long n = base + lane;
       bool valid = n < np;
       double qm = 0;
+      // Markers stream through once per step: their loads and stores are
+      // marked evict-first, leaving L1 and L2 to the field gather.
       if (valid) {
-         qm = m.qm[n];
+         qm = __ldcs (m.qm + n);
          valid = (qm != 0.0);             // removed markers carry qDivM = 0
       }
       int i = 0, j = 0, k = 0, i2 = 0, j2 = 0, k2 = 0, nseg = 0;
@@ -326,9 +328,9 @@ k_push64 (Ctx c, Markers64 m, long long np, DevScalars *dsc)
       double x1 = 0, y1 = 0, z1 = 0, x2 = 0, y2 = 0, z2 = 0, rho = 0;
       double xa = 0, ya = 0, za = 0;         // end of the first segment
       if (valid) {
-         x1 = m.x[n];
-         y1 = m.y[n];
-         z1 = m.z[n];
+         x1 = __ldcs (m.x + n);
+         y1 = __ldcs (m.y + n);
+         z1 = __ldcs (m.z + n);
          double sX = div_by (x1, h1, c.rh[0]), sY = div_by (y1, h2, c.rh[1]), sZ = div_by (z1, h3, c.rh[2]);
          double sX_ = sX + 0.5, sY_ = sY + 0.5, sZ_ = sZ + 0.5;
          i = cell_of (sX, fi);
@@ -361,9 +363,9 @@ k_push64 (Ctx c, Markers64 m, long long np, DevScalars *dsc)
             const double Hy = cic (c.H1, g, i_, sX_, j, sY, k_, sZ_);
             const double Hz = cic (c.H2, g, i_, sX_, j_, sY_, k, sZ);
 
-            rho = (double) m.rho[n];
+            rho = (double) __ldcs (m.rho + n);
             const double tm = 0.5*tau*qm;
-            const double px = m.ux[n] + tm*Ex, py = m.uy[n] + tm*Ey, pz = m.uz[n] + tm*Ez;
+            const double px = __ldcs (m.ux + n) + tm*Ex, py = __ldcs (m.uy + n) + tm*Ey, pz = __ldcs (m.uz + n) + tm*Ez;
             const double gamma = sqrt (1.0 + px*px + py*py + pz*pz);
             // The tally's two divisions (core/plasma.c:140) by one
             // reciprocal: W is summed over markers and blocks in an order of
@@ -434,12 +436,12 @@ k_push64 (Ctx c, Markers64 m, long long np, DevScalars *dsc)
             gone |= wall (g.bc[1][0], true, px_, vx_, L0, h1);
             gone |= wall (g.bc[1][1], true, py_, vy_, L1, h2);
             gone |= wall (g.bc[1][2], true, pz_, vz_, L2, h3);
-            m.x[n] = px_;
-            m.y[n] = py_;
-            m.z[n] = pz_;
-            m.ux[n] = vx_;
-            m.uy[n] = vy_;
-            m.uz[n] = vz_;
+            __stcs (m.x + n, px_);
+            __stcs (m.y + n, py_);
+            __stcs (m.z + n, pz_);
+            __stcs (m.ux + n, vx_);
+            __stcs (m.uy + n, vy_);
+            __stcs (m.uz + n, vz_);
             if (gone) {
                m.qm[n] = 0.0f;
                ++dead;
