@@ -84,8 +84,9 @@ typedef struct {
    long long capacity;    /* marker capacity (0: grows on upload)      */
    int       sort_every;  /* re-sort markers every k steps: by tile and cell
                              (precision form) or by cell (plain form);
-                             0 = every 16; < 0 = never (precision form:
-                             untiled push)                               */
+                             0 = every 16 (precision form) or 24 (plain
+                             form); < 0 = never (precision form: untiled
+                             push)                                        */
    int       tile[3];     /* precision form: tile of the push in cells,
                              {8,8,4} (also {0,0,0}), {4,4,4} or {8,8,8} */
    int       tile_warps;  /* precision form: warps per block of the tiled
