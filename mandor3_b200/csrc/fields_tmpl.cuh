@@ -830,36 +830,55 @@ __device__ __forceinline__ void h_line (const Grid &g, const F3T<T> &H, const F3
    constexpr int EP = Axes<AX>::EP, EQ = Axes<AX>::EQ;
    const int N = g.n[AX];
    const long s = axis_stride<AX> (g);
-   for (int arr = 0 ; arr < (both ? 2 : 1) ; ++arr) {
-      T *const F[3] = {arr ? Hn.c[0] : H.c[0], arr ? Hn.c[1] : H.c[1], arr ? Hn.c[2] : H.c[2]};
-      T *Ha = F[AX], *Hp = F[EP], *Hq = F[EQ];
-      // Loads first, then stores: the wall nodes never alias the sources.
-      if (op_min == OP_PERIODIC) {
-         T top[3], one[3];
+   const long t = o + N*s;
+   const int na = both ? 2 : 1;
+   // Every load of both arrays first, then the stores: the wall nodes never
+   // alias the sources, so this is the order of the operations on each node.
+   if (op_min == OP_PERIODIC) {
+      T top[2][3], one[2][3];
 #pragma unroll
-         for (int c = 0 ; c < 3 ; ++c) {
-            top[c] = F[c][o + N*s];
-            one[c] = F[c][o + s];
-         }
+      for (int arr = 0 ; arr < 2 ; ++arr)
 #pragma unroll
-         for (int c = 0 ; c < 3 ; ++c) {
-            F[c][o] = top[c];
-            F[c][o + (N + 1)*s] = one[c];
-         }
-         continue;
-      }
-      const T p1 = Hp[o + s], q1 = Hq[o + s];
-      const long t = o + N*s;
-      const T pN = Hp[t], qN = Hq[t];
-      Hp[o] = p1;
-      Hq[o] = q1;
-      if (op_min == OP_MIRROR_MIN)
-         Ha[o] = 0;
-      Hp[t + s] = pN;
-      Hq[t + s] = qN;
-      if (op_max == OP_MIRROR_MAX)
-         Ha[t] = 0;
+         for (int c = 0 ; c < 3 ; ++c)
+            if (arr < na) {
+               const T *F = arr ? Hn.c[c] : H.c[c];
+               top[arr][c] = F[t];
+               one[arr][c] = F[o + s];
+            }
+#pragma unroll
+      for (int arr = 0 ; arr < 2 ; ++arr)
+#pragma unroll
+         for (int c = 0 ; c < 3 ; ++c)
+            if (arr < na) {
+               T *F = arr ? Hn.c[c] : H.c[c];
+               F[o] = top[arr][c];
+               F[o + (N + 1)*s] = one[arr][c];
+            }
+      return;
    }
+   T p1[2], q1[2], pN[2], qN[2];
+#pragma unroll
+   for (int arr = 0 ; arr < 2 ; ++arr)
+      if (arr < na) {
+         const T *Hp = arr ? Hn.c[EP] : H.c[EP], *Hq = arr ? Hn.c[EQ] : H.c[EQ];
+         p1[arr] = Hp[o + s];
+         q1[arr] = Hq[o + s];
+         pN[arr] = Hp[t];
+         qN[arr] = Hq[t];
+      }
+#pragma unroll
+   for (int arr = 0 ; arr < 2 ; ++arr)
+      if (arr < na) {
+         T *Ha = arr ? Hn.c[AX] : H.c[AX], *Hp = arr ? Hn.c[EP] : H.c[EP], *Hq = arr ? Hn.c[EQ] : H.c[EQ];
+         Hp[o] = p1[arr];
+         Hq[o] = q1[arr];
+         if (op_min == OP_MIRROR_MIN)
+            Ha[o] = 0;
+         Hp[t + s] = pN[arr];
+         Hq[t + s] = qN[arr];
+         if (op_max == OP_MIRROR_MAX)
+            Ha[t] = 0;
+      }
 }
 
 template <typename T, int AX>
@@ -1240,6 +1259,145 @@ __device__ __forceinline__ int band_at (int u, int N) { return u < 5 ? u - 2 : N
 
 // The wall line of axis AX whose transverse indices (along Axes<AX>::EP
 // and ::EQ) are p and q.
+// Both E walls of a line and, with sub, -tau J on its six rim nodes
+// (indices -1, 0, 1, N-1, N, N+1) as one chain: every value is loaded, the
+// wall operations of the per-axis kernels act on registers in their order
+// (lower wall, then upper wall: disjoint nodes), -tau J follows on the
+// post-wall values, then every changed value is stored.
+template <typename T, int AX>
+__device__ __forceinline__ void e_line (const Grid &g, WallArgs<T> &A, const WallPlan &P, int p, int q,
+                                        bool sub)
+{
+   constexpr int EP = Axes<AX>::EP, EQ = Axes<AX>::EQ;
+   const int N = g.n[AX];
+   const long sa = axis_stride<AX> (g);
+   const long o = g.origin + p*axis_stride<EP> (g) + q*axis_stride<EQ> (g);
+   const int op0 = P.op0[AX], op1 = P.op1[AX];
+   const int vs[6] = {-1, 0, 1, N - 1, N, N + 1};
+   T e[6][3], jv[6][3];
+   bool chg[6][3];
+#pragma unroll
+   for (int u = 0 ; u < 6 ; ++u)
+#pragma unroll
+      for (int c = 0 ; c < 3 ; ++c) {
+         e[u][c] = A.F.c[c][o + vs[u]*sa];
+         chg[u][c] = sub;
+         if (sub)
+            jv[u][c] = __ldg (A.J.c[c] + o + vs[u]*sa);
+      }
+   const long hq = 4*((long) p*(g.n[EQ] + 2) + q);
+   T *h0 = op0 == OP_OPEN_MIN ? A.mur[0][AX] + hq : nullptr;
+   T *h1 = op1 == OP_OPEN_MAX ? A.mur[1][AX] + hq : nullptr;
+   T hm[4], hM[4];
+   if (op0 == OP_OPEN_MIN)
+#pragma unroll
+      for (int x = 0 ; x < 4 ; ++x) hm[x] = h0[x];
+   if (op1 == OP_OPEN_MAX)
+#pragma unroll
+      for (int x = 0 ; x < 4 ; ++x) hM[x] = h1[x];
+   const T alpha = A.alpha[AX];
+   // Lower wall: index 0 is row 1, index 1 row 2.
+   if (op0 == OP_PERIODIC) {
+#pragma unroll
+      for (int c = 0 ; c < 3 ; ++c) {
+         e[4][c] = e[1][c];
+         e[5][c] = e[2][c];
+         chg[4][c] = chg[5][c] = true;
+      }
+   } else if (op0 == OP_MIRROR_MIN) {
+      e[1][EP] = 0;
+      e[1][EQ] = 0;
+      e[1][AX] = e[2][AX];
+      chg[1][EP] = chg[1][EQ] = chg[1][AX] = true;
+   } else if (op0 == OP_OPEN_MIN) {
+      e[1][AX] = e[2][AX];
+      const T ep = hm[2] + alpha*(e[2][EP] - hm[0]);
+      const T eq = hm[3] + alpha*(e[2][EQ] - hm[1]);
+      e[1][EP] = ep;
+      e[1][EQ] = eq;
+      hm[0] = ep;
+      hm[1] = eq;
+      hm[2] = e[2][EP];
+      hm[3] = e[2][EQ];
+      chg[1][EP] = chg[1][EQ] = chg[1][AX] = true;
+   }
+   // Upper wall: index N-1 is row 3, N row 4, N+1 row 5.
+   if (op1 == OP_MIRROR_MAX) {
+      e[4][EP] = 0;
+      e[4][EQ] = 0;
+      e[5][AX] = e[4][AX];
+      chg[4][EP] = chg[4][EQ] = chg[5][AX] = true;
+   } else if (op1 == OP_OPEN_MAX) {
+      e[5][AX] = e[4][AX];
+      const T ep = hM[2] + alpha*(e[3][EP] - hM[0]);
+      const T eq = hM[3] + alpha*(e[3][EQ] - hM[1]);
+      e[4][EP] = ep;
+      e[4][EQ] = eq;
+      hM[0] = ep;
+      hM[1] = eq;
+      hM[2] = e[3][EP];
+      hM[3] = e[3][EQ];
+      chg[4][EP] = chg[4][EQ] = chg[5][AX] = true;
+   }
+   if (sub) {
+      const T tau = (T) g.tau;
+#pragma unroll
+      for (int u = 0 ; u < 6 ; ++u)
+#pragma unroll
+         for (int c = 0 ; c < 3 ; ++c)
+            e[u][c] = e[u][c] - tau*jv[u][c];
+   }
+#pragma unroll
+   for (int u = 0 ; u < 6 ; ++u)
+#pragma unroll
+      for (int c = 0 ; c < 3 ; ++c)
+         if (chg[u][c])
+            A.F.c[c][o + vs[u]*sa] = e[u][c];
+   if (op0 == OP_OPEN_MIN)
+#pragma unroll
+      for (int x = 0 ; x < 4 ; ++x) h0[x] = hm[x];
+   if (op1 == OP_OPEN_MAX)
+#pragma unroll
+      for (int x = 0 ; x < 4 ; ++x) h1[x] = hM[x];
+}
+
+// Both current walls of a line (plasma_currentWalls.c:27-121) as one chain:
+// the five nodes around each wall are loaded, folded in registers, stored.
+template <typename T, int AX>
+__device__ __forceinline__ void j_line (const Grid &g, const F3T<T> &J, long base)
+{
+   constexpr int EP = Axes<AX>::EP, EQ = Axes<AX>::EQ;
+   if (g.bc[0][AX] == MG_BC_PERIODIC) {
+      j_fold<T, AX> (g, J, 0, MG_BC_PERIODIC, base);
+      return;
+   }
+   const long st = axis_stride<AX> (g);
+   const long o0 = base, o1 = base + g.n[AX]*st;
+   T a0[5], p0[5], q0[5], a1[5], p1[5], q1[5];
+#pragma unroll
+   for (int u = 0 ; u < 5 ; ++u) {
+      a0[u] = J.c[AX][o0 + (u - 2)*st];
+      p0[u] = J.c[EP][o0 + (u - 2)*st];
+      q0[u] = J.c[EQ][o0 + (u - 2)*st];
+      a1[u] = J.c[AX][o1 + (u - 2)*st];
+      p1[u] = J.c[EP][o1 + (u - 2)*st];
+      q1[u] = J.c[EQ][o1 + (u - 2)*st];
+   }
+   j_fold_wall (a0, p0, q0, 0);
+   j_fold_wall (a1, p1, q1, 1);
+#pragma unroll
+   for (int u = 0 ; u < 5 ; ++u) {
+      J.c[AX][o0 + (u - 2)*st] = a0[u];
+      J.c[EP][o0 + (u - 2)*st] = p0[u];
+      J.c[EQ][o0 + (u - 2)*st] = q0[u];
+      J.c[AX][o1 + (u - 2)*st] = a1[u];
+      J.c[EP][o1 + (u - 2)*st] = p1[u];
+      J.c[EQ][o1 + (u - 2)*st] = q1[u];
+   }
+}
+
+// The wall line of axis AX whose transverse indices (along Axes<AX>::EP
+// and ::EQ) are p and q; the E lines' rim nodes are left to the caller.
 template <typename T, int KIND, int AX>
 __device__ __forceinline__ void wall_line (const Grid &g, WallArgs<T> &A, const WallPlan &P, int p, int q)
 {
@@ -1247,47 +1405,39 @@ __device__ __forceinline__ void wall_line (const Grid &g, WallArgs<T> &A, const 
    if (p < P.lo || p > g.n[EP] + P.hi || q < P.lo || q > g.n[EQ] + P.hi)
       return;
    const long o = g.origin + p*axis_stride<EP> (g) + q*axis_stride<EQ> (g);
-   if (KIND == WK_H) {
+   if (KIND == WK_H)
       h_line<T, AX> (g, A.F, A.F2, P.op0[AX], P.op1[AX], A.flag, o);
-   } else if (KIND == WK_E) {
-      if (p >= 0 && q >= 0) {
-         e_wall_op<T, AX> (g, A.F, P.op0[AX], o, p, q, A.mur[0][AX], A.alpha[AX]);
-         e_wall_op<T, AX> (g, A.F, P.op1[AX], o, p, q, A.mur[1][AX], A.alpha[AX]);
-      }
-   } else {
-      j_fold<T, AX> (g, A.J, 0, g.bc[0][AX], o);
-      j_fold<T, AX> (g, A.J, 1, g.bc[1][AX], o);
-   }
-}
-
-// E -= tau J at one rim node (the order of core/em.c:189-222: after every
-// wall operation on the node).
-template <typename T>
-__device__ __forceinline__ void rim_sub_j (const Grid &g, WallArgs<T> &A, int i, int j, int k)
-{
-   const T tau = (T) g.tau;
-   const long x = g.at (i, j, k);
-   T e[3], jv[3];
-#pragma unroll
-   for (int c = 0 ; c < 3 ; ++c) {
-      e[c] = A.F.c[c][x];
-      jv[c] = __ldg (A.J.c[c] + x);
-   }
-#pragma unroll
-   for (int c = 0 ; c < 3 ; ++c)
-      A.F.c[c][x] = e[c] - tau*jv[c];
+   else if (KIND == WK_E) {
+      if (p >= 0 && q >= 0)
+         e_line<T, AX> (g, A, P, p, q, false);
+   } else
+      j_line<T, AX> (g, A.J, o);
 }
 
 __device__ __forceinline__ bool rim_index (int v, int N) { return v < 2 || v > N - 2; }
 
-// Node (i, j, k) with index v along axis AX and p, q along its transverse axes.
-template <int AX>
-__device__ __forceinline__ void node_of (int v, int p, int q, int &i, int &j, int &k)
+// E -= tau J at up to four rim nodes of a thread (offsets x[u], -1 for
+// none), all loads before the stores (the order of core/em.c:189-222:
+// after every wall operation on the node).
+template <typename T>
+__device__ __forceinline__ void rim_sub_j4 (const Grid &g, WallArgs<T> &A, const long x[4])
 {
-   constexpr int EP = Axes<AX>::EP;
-   i = AX == 0 ? v : EP == 0 ? p : q;
-   j = AX == 1 ? v : EP == 1 ? p : q;
-   k = AX == 2 ? v : q;
+   const T tau = (T) g.tau;
+   T e[4][3], jv[4][3];
+#pragma unroll
+   for (int u = 0 ; u < 4 ; ++u)
+      if (x[u] >= 0)
+#pragma unroll
+         for (int c = 0 ; c < 3 ; ++c) {
+            e[u][c] = A.F.c[c][x[u]];
+            jv[u][c] = __ldg (A.J.c[c] + x[u]);
+         }
+#pragma unroll
+   for (int u = 0 ; u < 4 ; ++u)
+      if (x[u] >= 0)
+#pragma unroll
+         for (int c = 0 ; c < 3 ; ++c)
+            A.F.c[c][x[u]] = e[u][c] - tau*jv[u][c];
 }
 
 template <typename T, int KIND, int AX>
@@ -1298,17 +1448,10 @@ __device__ __forceinline__ void face_line (const Grid &g, WallArgs<T> &A, const 
       return;
    const int nq = g.n[EQ] - 5;
    const int p = 3 + (int) (t / nq), q = 3 + (int) (t % nq);
-   wall_line<T, KIND, AX> (g, A, P, p, q);
-   if (KIND == WK_E && A.flag) {
-      const int N = g.n[AX];
-      const int vs[6] = {-1, 0, 1, N - 1, N, N + 1};
-#pragma unroll
-      for (int u = 0 ; u < 6 ; ++u) {
-         int i, j, k;
-         node_of<AX> (vs[u], p, q, i, j, k);
-         rim_sub_j (g, A, i, j, k);
-      }
-   }
+   if (KIND == WK_E)
+      e_line<T, AX> (g, A, P, p, q, A.flag != 0);    // face lines own their six rim nodes
+   else
+      wall_line<T, KIND, AX> (g, A, P, p, q);
 }
 
 // Edge slice at index tc of axis C: phases of the two other axes, lower
@@ -1337,8 +1480,14 @@ __device__ __forceinline__ void edge_slice (const Grid &g, WallArgs<T> &A, const
          wall_line<T, KIND, BB> (g, A, P, tc, ta);
    }
    __syncwarp ();
-   if (KIND == WK_E && A.flag)
-      for (int u = lane ; u < 100 ; u += 32) {
+   if (KIND == WK_E && A.flag) {
+      long x[4];
+#pragma unroll
+      for (int r = 0 ; r < 4 ; ++r) {
+         const int u = lane + 32*r;
+         x[r] = -1;
+         if (u >= 100)
+            continue;
          const int va = band_at (u / 10, g.n[AA]), vb = band_at (u % 10, g.n[BB]);
          if (va < -1 || va > g.n[AA] + 1 || vb < -1 || vb > g.n[BB] + 1)
             continue;
@@ -1347,8 +1496,10 @@ __device__ __forceinline__ void edge_slice (const Grid &g, WallArgs<T> &A, const
          const int i = AA == 0 ? va : C == 0 ? tc : vb;
          const int j = AA == 1 ? va : BB == 1 ? vb : tc;
          const int k = BB == 2 ? vb : tc;
-         rim_sub_j (g, A, i, j, k);
+         x[r] = g.at (i, j, k);
       }
+      rim_sub_j4 (g, A, x);
+   }
 }
 
 template <typename T, int KIND, int AX>
@@ -1389,14 +1540,23 @@ k_walls_all (Grid g, WallArgs<T> A, WallPlan P)
       corner_phase<T, KIND, 1> (g, A, P);
       corner_phase<T, KIND, 2> (g, A, P);
       if (KIND == WK_E && A.flag)
-         for (int u = threadIdx.x ; u < 1000 ; u += blockDim.x) {
-            const int v0 = band_at (u / 100, g.n[0]), v1 = band_at ((u / 10) % 10, g.n[1]);
-            const int v2 = band_at (u % 10, g.n[2]);
-            if (v0 < -1 || v0 > g.n[0] + 1 || v1 < -1 || v1 > g.n[1] + 1 || v2 < -1 || v2 > g.n[2] + 1)
-               continue;
-            if (!rim_index (v0, g.n[0]) && !rim_index (v1, g.n[1]) && !rim_index (v2, g.n[2]))
-               continue;
-            rim_sub_j (g, A, v0, v1, v2);
+         for (int u0 = threadIdx.x ; u0 < 1000 ; u0 += 4*blockDim.x) {
+            long x[4];
+#pragma unroll
+            for (int r = 0 ; r < 4 ; ++r) {
+               const int u = u0 + r*blockDim.x;
+               x[r] = -1;
+               if (u >= 1000)
+                  continue;
+               const int v0 = band_at (u / 100, g.n[0]), v1 = band_at ((u / 10) % 10, g.n[1]);
+               const int v2 = band_at (u % 10, g.n[2]);
+               if (v0 < -1 || v0 > g.n[0] + 1 || v1 < -1 || v1 > g.n[1] + 1 || v2 < -1 || v2 > g.n[2] + 1)
+                  continue;
+               if (!rim_index (v0, g.n[0]) && !rim_index (v1, g.n[1]) && !rim_index (v2, g.n[2]))
+                  continue;
+               x[r] = g.at (v0, v1, v2);
+            }
+            rim_sub_j4 (g, A, x);
          }
       return;
    }
