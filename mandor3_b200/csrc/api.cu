@@ -590,6 +590,8 @@ extern "C" int mg_run_destroy (mg_run_t *r)
       if (r->H[c]) mg_dev_free (r, r->H[c]);
       if (r->J[c]) mg_dev_free (r, r->J[c]);
       if (r->Hn[c]) mg_dev_free (r, r->Hn[c]);
+      if (r->Ealt[c]) mg_dev_free (r, r->Ealt[c]);
+      if (r->Halt[c]) mg_dev_free (r, r->Halt[c]);
       if (r->E32[c]) mg_dev_free (r, r->E32[c]);
       if (r->H32[c]) mg_dev_free (r, r->H32[c]);
       if (r->J32[c]) mg_dev_free (r, r->J32[c]);
@@ -1307,6 +1309,12 @@ extern "C" int mg_gauss_after (mg_run_t *r, double out[2])
 // (core/main.c:353-478 order).  part < 0 enqueues all three.
 int mg_enqueue_step64 (mg_run_t *r, int part)
 {
+   if (part < 0 && r->fo_graph) {        // field-only: one pass into Ealt, Halt
+      TRY (mg_fields64_one_pass (r));
+      k_end_step<<<1, 1, 0, r->stream>>> (r->dsc, r->ring, r->g.h[0]*r->g.h[1]*r->g.h[2], r->g.tau);
+      MG_LAUNCH_CHECK ();
+      return MG_OK;
+   }
    if (part < 0 || part == 0) {
       TRY (mg_tfsf_record (r));
       TRY (mg_fields64_h_both (r));
@@ -1354,13 +1362,53 @@ static int count_kernels (cudaGraph_t graph)
 
 void mg_drop_graphs (mg_run_t *r)
 {
-   for (int q = 0 ; q < 4 ; ++q) {
+   for (int q = 0 ; q < 5 ; ++q) {
       if (r->gexec[q]) cudaGraphExecDestroy (r->gexec[q]);
       if (r->gr[q]) cudaGraphDestroy (r->gr[q]);
       r->gexec[q] = nullptr;
       r->gr[q] = nullptr;
    }
    r->graph_ok = 0;
+   r->fo_graph = 0;
+}
+
+// The precision form keeps its two float4-slot passes: its one-pass step
+// measured slower (256^3: 0.328 against 0.274 ms per step).
+static bool one_pass_ok (const mg_run_t *r)
+{
+   return !is32 (r) && r->np == 0 && !r->probe_ring && !r->has_laser && !r->has_gspot &&
+          r->nmirrors == 0 && !r->tfsf && !r->in_batch;
+}
+
+template <typename T>
+static void swap3 (T *a[3], T *b[3])
+{
+   for (int c = 0 ; c < 3 ; ++c) {
+      T *t = a[c];
+      a[c] = b[c];
+      b[c] = t;
+   }
+}
+
+static void swap_field_sets (mg_run_t *r)
+{
+   swap3 (r->E, r->Ealt);
+   swap3 (r->H, r->Halt);
+}
+
+// The second E and H arrays, equal to the current ones (nodes no step
+// writes, the outer ghosts, must match in both sets).
+template <typename T>
+static int make_alt_set (mg_run_t *r, T *const E[3], T *const H[3], T *Ea[3], T *Ha[3])
+{
+   const size_t bytes = (size_t) r->g.total*sizeof (T);
+   for (int c = 0 ; c < 3 ; ++c) {
+      if (!Ea[c]) TRY (mg_dev_alloc (r, (void **) &Ea[c], bytes));
+      if (!Ha[c]) TRY (mg_dev_alloc (r, (void **) &Ha[c], bytes));
+      MG_CUDA (cudaMemcpyAsync (Ea[c], E[c], bytes, cudaMemcpyDeviceToDevice, r->stream));
+      MG_CUDA (cudaMemcpyAsync (Ha[c], H[c], bytes, cudaMemcpyDeviceToDevice, r->stream));
+   }
+   return MG_OK;
 }
 
 // Graph 0: the whole step; graphs 1..3: its three parts (profiling mode, so
@@ -1378,12 +1426,24 @@ static int build_graph (mg_run_t *r)
          const size_t elt = is32 (r) ? sizeof (float) : sizeof (double);
          MG_CUDA (cudaMemsetAsync (J, 0, (size_t) r->g.total*elt, r->stream));
       }
-   for (int q = 0 ; q < 4 ; ++q) {
+   // A plain-form run without markers, sources, probes or TF/SF steps its
+   // fields in one pass between two sets of E and H arrays: graph 0 reads
+   // the arrays current now and writes the others, graph 4 the reverse.
+   r->fo_graph = one_pass_ok (r);
+   if (r->fo_graph) {
+      TRY (make_alt_set<double> (r, r->E, r->H, r->Ealt, r->Halt));
+      r->fo_read0 = r->E[0];
+   }
+   for (int q = 0 ; q < (r->fo_graph ? 5 : 4) ; ++q) {
+      if (q == 4)
+         swap_field_sets (r);
       MG_CUDA (cudaStreamBeginCapture (r->stream, cudaStreamCaptureModeThreadLocal));
-      const int part = q - 1;
+      const int part = q == 4 ? -1 : q - 1;
       int rc = is32 (r) ? mg_enqueue_step32 (r, part) : mg_enqueue_step64 (r, part);
       cudaGraph_t g = nullptr;
       cudaError_t e = cudaStreamEndCapture (r->stream, &g);
+      if (q == 4)
+         swap_field_sets (r);
       if (rc != MG_OK) {
          if (g) cudaGraphDestroy (g);
          return rc;
@@ -1397,6 +1457,19 @@ static int build_graph (mg_run_t *r)
    }
    r->kernels_per_step = count_kernels (r->gr[0]);
    r->graph_ok = 1;
+   return MG_OK;
+}
+
+// One whole step from its graph; the one-pass field-only pair alternates
+// with the field arrays it writes.
+static int launch_step_graph (mg_run_t *r)
+{
+   if (!r->fo_graph) {
+      MG_CUDA (cudaGraphLaunch (r->gexec[0], r->stream));
+      return MG_OK;
+   }
+   MG_CUDA (cudaGraphLaunch (r->E[0] == r->fo_read0 ? r->gexec[0] : r->gexec[4], r->stream));
+   swap_field_sets (r);
    return MG_OK;
 }
 
@@ -1456,7 +1529,7 @@ static int run_steps (mg_run_t *r, int nsteps, double *host_rows, double *dev_ro
       } else {
          for (int s = 0 ; s < chunk ; ++s) {
             TRY (maybe_sort (r));
-            MG_CUDA (cudaGraphLaunch (r->gexec[0], r->stream));
+            TRY (launch_step_graph (r));
          }
       }
       if (host_rows)
@@ -1660,7 +1733,7 @@ extern "C" int mg_run_step_gauss (mg_run_t *r, int nsteps, double *rows)
       const double time = r->time;
       TRY (maybe_sort (r));
       MG_CUDA (cudaMemsetAsync (&r->dsc->step, 0, sizeof (int), r->stream));
-      MG_CUDA (cudaGraphLaunch (r->gexec[0], r->stream));
+      TRY (launch_step_graph (r));
       TRY (mg_gauss_rho (r, r->gauss_rho[1]));
       TRY (mg_gauss_residual (r, r->gauss_rho[0], r->gauss_rho[1], r->gauss_out));
       double res[2];

@@ -27,3 +27,4 @@ int mg_fields64_e_finish (mg_run_t *r) { return fields_e_finish<double> (r, fs_o
 int mg_fields64_e_fused (mg_run_t *r) { return fields_e_fused<double> (r, fs_of (r)); }
 int mg_fields64_zero_j (mg_run_t *r) { return fields_zero_j<double> (r, fs_of (r)); }
 int mg_fields64_init (mg_run_t *r) { return fields_init<double> (r, fs_of (r)); }
+int mg_fields64_one_pass (mg_run_t *r) { return fields_one_pass<double> (r, fs_of (r), r->Ealt, r->Halt); }

@@ -340,6 +340,311 @@ k_e_fused (Grid g, F3T<T> E, F3T<T> H, F3T<T> J, Box b, T c1, T c2, T c3, Rim rm
 
 
 // ---------------------------------------------------------------------------
+// Field-only step in one pass (plain form: runs without markers, sources or
+// probes).  E^(n+1) at a node needs H^(n+1/2) at the node and at its +1
+// neighbours, computed from E^n and H^(n-1/2) with the H pass's expressions
+// (the same bits, no contraction in the FP64 build).  E and H are
+// double-buffered: the pass reads the old arrays and writes the new ones, so
+// each node is one read of E and H and one write of each (96 B instead of
+// the two passes' 144 B).
+//
+// Which nodes can skip the walls: the H walls write H at index 0 and n + 1
+// of an axis, and the axis' own component at n (mirror); the new H at any
+// node needs only E^n and H^(n-1/2), so one pass computes it over the whole
+// H box.  The new E at index m of an axis reads the new H at m and, for the
+// components across the axis, at m + 1; for m in [1, n - 1] none of those is
+// a wall's, so the pass computes E over [1, n - 1]^3 as well.  What is left
+// is the single layer of the E box at index 0 (periodic axes) or n (the
+// others), updated from the walled H after the H walls.
+// ---------------------------------------------------------------------------
+struct Slabs {
+   Box  b[6];
+   long start[7];
+};
+
+// Box b minus the box [in_lo, in_hi]^3 (axis-wise), as six slabs.
+static Slabs shell_slabs (const Box &b, const int in_lo[3], const int in_hi[3])
+{
+   int lo[3], hi[3];
+   for (int a = 0 ; a < 3 ; ++a) {
+      lo[a] = b.lo[a];
+      hi[a] = b.lo[a] + b.ext[a] - 1;
+   }
+   Slabs s;
+   int n = 0;
+   auto add = [&] (int l0, int h0, int l1, int h1, int l2, int h2) {
+      const int l[3] = {l0, l1, l2}, h[3] = {h0, h1, h2};
+      s.b[n++] = make_box (l, h);
+   };
+   add (lo[0], in_lo[0] - 1, lo[1], hi[1], lo[2], hi[2]);
+   add (in_hi[0] + 1, hi[0], lo[1], hi[1], lo[2], hi[2]);
+   add (in_lo[0], in_hi[0], lo[1], in_lo[1] - 1, lo[2], hi[2]);
+   add (in_lo[0], in_hi[0], in_hi[1] + 1, hi[1], lo[2], hi[2]);
+   add (in_lo[0], in_hi[0], in_lo[1], in_hi[1], lo[2], in_lo[2] - 1);
+   add (in_lo[0], in_hi[0], in_lo[1], in_hi[1], in_hi[2] + 1, hi[2]);
+   s.start[0] = 0;
+   for (int q = 0 ; q < 6 ; ++q) {
+      if (s.b[q].vol < 0)
+         s.b[q].vol = 0;
+      s.start[q + 1] = s.start[q] + s.b[q].vol;
+   }
+   return s;
+}
+
+__device__ __forceinline__ bool slab_node (const Slabs &S, long t, int &i, int &j, int &k)
+{
+   if (t >= S.start[6])
+      return false;
+   int q = 0;
+   while (t >= S.start[q + 1])
+      ++q;
+   box_index (t - S.start[q], S.b[q].lo, S.b[q].ext, i, j, k);
+   return true;
+}
+
+// Energy sums of one node at its picks (core/em.c:241-247).
+template <typename T>
+__device__ __forceinline__ void energy_add (const EnergyPick &ep, int i, int j, int k, const T ev[3],
+                                            const T hv[3], double &we, double &wb)
+{
+   const int I[3] = {i, j, k};
+#pragma unroll
+   for (int c = 0 ; c < 3 ; ++c) {
+      bool in_e = true, in_h = true;
+#pragma unroll
+      for (int a = 0 ; a < 3 ; ++a) {
+         in_e &= (I[a] >= ep.lo[c][a]) & (I[a] <= ep.hi[c][a]);
+         in_h &= (I[a] >= ep.hlo[c][a]) & (I[a] <= ep.hhi[c][a]);
+      }
+      if (in_e) we += (double) ev[c]*(double) ev[c];
+      if (in_h) wb += (double) hv[c]*(double) hv[c];
+   }
+}
+
+__device__ __forceinline__ void energy_flush (double we, double wb, DevScalars *dsc)
+{
+   __shared__ double sw[2][8];
+   for (int d = 16 ; d > 0 ; d >>= 1) {
+      we += __shfl_xor_sync (0xffffffffu, we, d);
+      wb += __shfl_xor_sync (0xffffffffu, wb, d);
+   }
+   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+   if (lane == 0) {
+      sw[0][wid] = we;
+      sw[1][wid] = wb;
+   }
+   __syncthreads ();
+   if (wid == 0) {
+      we = lane < (int) (blockDim.x >> 5) ? sw[0][lane] : 0;
+      wb = lane < (int) (blockDim.x >> 5) ? sw[1][lane] : 0;
+      for (int d = 16 ; d > 0 ; d >>= 1) {
+         we += __shfl_xor_sync (0xffffffffu, we, d);
+         wb += __shfl_xor_sync (0xffffffffu, wb, d);
+      }
+      if (lane == 0) {
+         atomicAdd (&dsc->acc[0], we);
+         atomicAdd (&dsc->acc[1], wb);
+      }
+   }
+}
+
+// The H box as (y, z) tiles of YT x ZT nodes, each block marching along x
+// over a chunk of planes [i0, i1).  Per plane p the block holds in shared
+// memory E^n of planes p - 1, p (tile plus the -1 and +1 halos), p + 1 and
+// p + 2 (arriving by cp.async while p is computed), and H^(n+1/2) of planes
+// p - 1 and p on the tile plus the +1 halo: it computes the new H of plane p
+// from E^n (planes p - 1, p) and H^(n-1/2), then the new E of plane p - 1
+// from E^n and the new H of planes p - 1, p.  Tiles partition [lo, n - 1] on
+// each axis; the last tile of an axis also owns node n, its +1 halo there.
+// Halo values of the new H are computed again by each tile that needs them,
+// from the same inputs, so they are the same bits.
+template <int YT, int ZT>
+struct YeeTile {
+   static constexpr int NT = YT*ZT;               // threads, one per tile node
+   static constexpr int EW = ZT + 2;              // E row pitch: k in [kb - 1, kb + ZT]
+   static constexpr int EP = (YT + 2)*EW;         // E plane: j in [jb - 1, jb + YT]
+   static constexpr int HW = ZT + 1;              // new-H row pitch: k in [kb, kb + ZT]
+   static constexpr int HP = (YT + 1)*HW;         // new-H plane: j in [jb, jb + YT]
+   static constexpr int XH = YT + ZT + 1;         // +1 halo nodes of the new H
+};
+
+template <typename T>
+__device__ __forceinline__ void cp_async_el (T *sm, const T *gm)
+{
+   asm volatile ("cp.async.ca.shared.global [%0], [%1], %2;"
+                 :: "r" ((unsigned) __cvta_generic_to_shared (sm)), "l" (gm), "n" ((int) sizeof (T))
+                 : "memory");
+}
+
+struct YeeTiles {
+   int lo[3];              // first node of the H box on each axis (0, or 1 at a mirror)
+   int n[3];               // cells: the H box ends at n, the E interior is [1, n - 1]
+   int tj0, ntj, tk0, ntk; // first tile index and tile count along y and z
+   int cx;                 // planes per chunk
+};
+
+template <typename T, int YT, int ZT>
+__global__ void __launch_bounds__ (YT*ZT, 4)
+k_yee_tile (Grid g, F3T<T> E, F3T<T> H, F3T<T> En, F3T<T> Hnw, YeeTiles tl, T c1, T c2, T c3,
+            T d1, T d2, T d3, EnergyPick ep, DevScalars *dsc)
+{
+   using L = YeeTile<YT, ZT>;
+   __shared__ T sE[4][3][L::EP];
+   __shared__ T sH[2][3][L::HP];
+   const int tid = threadIdx.x;
+   int b = blockIdx.x;
+   const int tk = tl.tk0 + b % tl.ntk;
+   b /= tl.ntk;
+   const int tj = tl.tj0 + b % tl.ntj;
+   b /= tl.ntj;
+   const int nx = tl.n[0], ny = tl.n[1], nz = tl.n[2];
+   const int i0 = tl.lo[0] + b*tl.cx, i1 = min (i0 + tl.cx, nx);
+   const bool lasti = i1 == nx;                       // the chunk owns plane n too
+   const int jb = tj*YT, kb = tk*ZT;                  // tile base
+   const int ja = max (jb, tl.lo[1]), je = min (jb + YT - 1, ny - 1);   // rows
+   const int ka = max (kb, tl.lo[2]), ke = min (kb + ZT - 1, nz - 1);   // columns
+   const bool lastj = je == ny - 1, lastk = ke == nz - 1;
+   const long sx = g.sx, sy = g.sy;
+
+   // E^n of plane p into slot s: rows [ja - 1, je + 1], columns [ka - 1, ke + 1].
+   auto load_e = [&] (int p, int s) {
+      for (int q = tid ; q < L::EP ; q += L::NT) {
+         const int r = q/L::EW, c = q - r*L::EW;
+         const int j = jb - 1 + r, k = kb - 1 + c;
+         if (j >= ja - 1 && j <= je + 1 && k >= ka - 1 && k <= ke + 1) {
+            const long o = g.at (p, j, k);
+#pragma unroll
+            for (int e = 0 ; e < 3 ; ++e)
+               cp_async_el (&sE[s][e][q], E.c[e] + o);
+         }
+      }
+   };
+   // This thread's new-H nodes: the tile node (tid / ZT, tid % ZT), and for
+   // the first XH threads one node of the +1 halo (row YT, then column ZT).
+   // Computed where the tile's new E needs them; written where the tile owns
+   // them.
+   const int r0 = tid/ZT, q0 = tid - r0*ZT;
+   const int r1 = tid <= ZT ? YT : tid - ZT - 1, q1 = tid <= ZT ? tid : ZT;
+   const int j0 = jb + r0, k0 = kb + q0, j1 = jb + r1, k1 = kb + q1;
+   const bool need0 = j0 >= ja && j0 <= je + 1 && k0 >= ka && k0 <= ke + 1;
+   const bool need1 = tid < L::XH && j1 >= ja && j1 <= je + 1 && k1 >= ka && k1 <= ke + 1;
+   const bool own0 = need0 && (j0 <= je || lastj) && (k0 <= ke || lastk);
+   const bool own1 = need1 && (j1 <= je || lastj) && (k1 <= ke || lastk);
+   const bool ownE = j0 >= max (ja, 1) && j0 <= je && k0 >= max (ka, 1) && k0 <= ke;
+   T h0[3] = {0, 0, 0}, h1[3] = {0, 0, 0};             // H^(n-1/2) of the next plane
+   auto load_h = [&] (int p) {
+      if (need0) {
+         const long o = g.at (p, j0, k0);
+#pragma unroll
+         for (int e = 0 ; e < 3 ; ++e) h0[e] = H.c[e][o];
+      }
+      if (need1) {
+         const long o = g.at (p, j1, k1);
+#pragma unroll
+         for (int e = 0 ; e < 3 ; ++e) h1[e] = H.c[e][o];
+      }
+   };
+   double we = 0, wb = 0;
+   // The new H at tile-relative node (r, q) of plane p (E slot se, previous
+   // plane's slot sp) into new-H slot sh, k_h_fused's expressions; written
+   // to Hnw with its energy terms where owned.
+   auto h_node = [&] (int p, int r, int q, int se, int sp, int sh, const T ho[3], bool own) {
+      const int e0 = (r + 1)*L::EW + q + 1;        // node in the E slot
+      const T ex = sE[se][0][e0], ey = sE[se][1][e0], ez = sE[se][2][e0];
+      const T cx = c3*(ey - sE[se][1][e0 - 1]) - c2*(ez - sE[se][2][e0 - L::EW]);
+      const T cy = c1*(ez - sE[sp][2][e0]) - c3*(ex - sE[se][0][e0 - 1]);
+      const T cz = c2*(ex - sE[se][0][e0 - L::EW]) - c1*(ey - sE[sp][1][e0]);
+      const T hv[3] = {ho[0] + cx, ho[1] + cy, ho[2] + cz};
+      const T hx = hv[0] + cx, hy = hv[1] + cy, hz = hv[2] + cz;
+      const int hi = r*L::HW + q;
+      sH[sh][0][hi] = hx;
+      sH[sh][1][hi] = hy;
+      sH[sh][2][hi] = hz;
+      if (own) {
+         const int j = jb + r, k = kb + q;
+         const long o = g.at (p, j, k);
+         Hnw.c[0][o] = hx;
+         Hnw.c[1][o] = hy;
+         Hnw.c[2][o] = hz;
+         const T ev[3] = {ex, ey, ez};
+         if (p >= 1 && p < nx && j >= 1 && j < ny && k >= 1 && k < nz) {
+            // Inside every energy pick range.
+            we += (double) ex*(double) ex;
+            we += (double) ey*(double) ey;
+            we += (double) ez*(double) ez;
+            wb += (double) hv[0]*(double) hv[0];
+            wb += (double) hv[1]*(double) hv[1];
+            wb += (double) hv[2]*(double) hv[2];
+         } else {
+            energy_add (ep, p, j, k, ev, hv, we, wb);
+         }
+      }
+   };
+
+   // E slot of plane p: (p - i0 + 1) mod 4.  Groups of copies: planes
+   // i0 - 1 and i0, then one group per plane; at the top of the step for
+   // plane p the latest group is plane p + 1's.
+   load_e (i0 - 1, 0);
+   load_e (i0, 1);
+   asm volatile ("cp.async.commit_group;" ::: "memory");
+   if (i0 + 1 <= i1)
+      load_e (i0 + 1, 2);
+   asm volatile ("cp.async.commit_group;" ::: "memory");
+   load_h (i0);
+   for (int p = i0 ; p <= i1 ; ++p) {
+      const int hs = (p - i0) & 1;                    // new-H slot of plane p
+      const int u = p - i0 + 1, sp = (u - 1) & 3, se = u & 3;
+      asm volatile ("cp.async.wait_group 1;" ::: "memory");
+      __syncthreads ();
+      if (p + 2 <= i1)
+         load_e (p + 2, (u + 2) & 3);
+      asm volatile ("cp.async.commit_group;" ::: "memory");
+      const T ho0[3] = {h0[0], h0[1], h0[2]}, ho1[3] = {h1[0], h1[1], h1[2]};
+      if (p < i1)
+         load_h (p + 1);
+      const bool ownp = p < i1 || lasti;
+      if (need0)
+         h_node (p, r0, q0, se, sp, hs, ho0, own0 && ownp);
+      if (need1)
+         h_node (p, r1, q1, se, sp, hs, ho1, own1 && ownp);
+      __syncthreads ();
+      if (p > i0 && p >= 2 && ownE) {
+         // E^(n+1) of plane p - 1 (in [1, n - 1]) at the tile node.
+         const int pe = (r0 + 1)*L::EW + q0 + 1, ph = r0*L::HW + q0;
+         const int hp = hs ^ 1;
+         const T ex = sE[sp][0][pe], ey = sE[sp][1][pe], ez = sE[sp][2][pe];
+         const T Hx = sH[hp][0][ph], Hy = sH[hp][1][ph], Hz = sH[hp][2][ph];
+         const T Hy_z = sH[hp][1][ph + 1], Hx_z = sH[hp][0][ph + 1];
+         const T Hz_y = sH[hp][2][ph + L::HW], Hx_y = sH[hp][0][ph + L::HW];
+         const T Hz_x = sH[hs][2][ph], Hy_x = sH[hs][1][ph];
+         const long o = g.at (p - 1, j0, k0);
+         En.c[0][o] = ex - (d3*(Hy_z - Hy) - d2*(Hz_y - Hz));
+         En.c[1][o] = ey - (d1*(Hz_x - Hz) - d3*(Hx_z - Hx));
+         En.c[2][o] = ez - (d2*(Hx_y - Hx) - d1*(Hy_x - Hy));
+      }
+   }
+   energy_flush (we, wb, dsc);
+}
+
+// The E update of the shell slabs: old E and the new (walled) H to the new E.
+template <typename T>
+__global__ void __launch_bounds__ (256)
+k_shell_e (Grid g, F3T<T> E, F3T<T> En, F3T<T> Hnw, Slabs S, T d1, T d2, T d3)
+{
+   const long sx = g.sx, sy = g.sy;
+   const T *Hx = Hnw.c[0], *Hy = Hnw.c[1], *Hz = Hnw.c[2];
+   for (long t = blockIdx.x*(long) blockDim.x + threadIdx.x ; t < S.start[6] ; t += (long) gridDim.x*blockDim.x) {
+      int i, j, k;
+      slab_node (S, t, i, j, k);
+      const long o = g.at (i, j, k);
+      const T hx = Hx[o], hy = Hy[o], hz = Hz[o];
+      En.c[0][o] = E.c[0][o] - (d3*(Hy[o + 1] - hy) - d2*(Hz[o + sy] - hz));
+      En.c[1][o] = E.c[1][o] - (d1*(Hz[o + sx] - hz) - d3*(Hx[o + 1] - hx));
+      En.c[2][o] = E.c[2][o] - (d2*(Hx[o + sy] - hx) - d1*(Hy[o + sx] - hy));
+   }
+}
+
+// ---------------------------------------------------------------------------
 // Precision form: the two bulk passes on float4 slots.  A row's node k sits
 // at offset origin + i sx + j sy + k with origin = 1 (mod 4) and sx, sy
 // multiples of 4, so the slots m = [4m - 1, 4m + 2] are 16-byte aligned;
@@ -1904,6 +2209,51 @@ int fields_h_both (mg_run_t *r, const FS<T> &fs)
    }
    TRY_MG (launch_laser<T> (r, fs, 0));
    return launch_h_walls<T> (r, fs, hn ? 1 : 0);
+}
+
+// The one-pass field-only step (plain form): reads fs.E, fs.H, writes the
+// new arrays En, Hw (E^(n+1), H^(n+1/2)); the caller swaps the pointers.
+// Used for runs without markers, sources, probes or TF/SF, stepped alone.
+template <typename T>
+int fields_one_pass (mg_run_t *r, const FS<T> &fs, T *const En[3], T *const Hw[3])
+{
+   const Grid &g = r->g;
+   const int NT = 256;
+   const T c1 = (T) (0.5*g.tau/g.h[0]), c2 = (T) (0.5*g.tau/g.h[1]), c3 = (T) (0.5*g.tau/g.h[2]);
+   const T d1 = (T) (g.tau/g.h[0]), d2 = (T) (g.tau/g.h[1]), d3 = (T) (g.tau/g.h[2]);
+   const Box hb = h_box (g);
+   const int in_lo[3] = {1, 1, 1};
+   const int in_hi[3] = {g.n[0] - 1, g.n[1] - 1, g.n[2] - 1};
+   const Slabs se = shell_slabs (e_box (g), in_lo, in_hi);
+   MG_CUDA (cudaMemsetAsync (r->dsc->acc, 0, 2*sizeof (double), r->stream));
+   constexpr int YT = 8, ZT = 32;
+   YeeTiles tl;
+   for (int a = 0 ; a < 3 ; ++a) {
+      tl.lo[a] = hb.lo[a];
+      tl.n[a] = g.n[a];
+   }
+   tl.tj0 = tl.lo[1]/YT;
+   tl.ntj = (g.n[1] - 1)/YT - tl.tj0 + 1;
+   tl.tk0 = tl.lo[2]/ZT;
+   tl.ntk = (g.n[2] - 1)/ZT - tl.tk0 + 1;
+   tl.cx = 16;
+   const int chunks = (g.n[0] - tl.lo[0] + tl.cx - 1)/tl.cx;
+   k_yee_tile<T, YT, ZT><<<tl.ntj*tl.ntk*chunks, YT*ZT, 0, r->stream>>> (
+      g, f3 (fs.E), f3 (fs.H), f3 (En), f3 (Hw), tl, c1, c2, c3, d1, d2, d3, energy_pick (g), r->dsc);
+   MG_LAUNCH_CHECK ();
+   FS<T> fh = fs;
+   for (int c = 0 ; c < 3 ; ++c)
+      fh.H[c] = Hw[c];
+   TRY_MG ((launch_walls_all<T, WK_H> (r, fh, 0, false)));
+   if (se.start[6] > 0) {
+      k_shell_e<T><<<mg_blocks_for (se.start[6], NT, 8), NT, 0, r->stream>>> (
+         g, f3 (fs.E), f3 (En), f3 (Hw), se, d1, d2, d3);
+      MG_LAUNCH_CHECK ();
+   }
+   FS<T> fe = fs;
+   for (int c = 0 ; c < 3 ; ++c)
+      fe.E[c] = En[c];
+   return launch_walls_all<T, WK_E> (r, fe, 0, false);
 }
 
 // Stage path: E += curl H only, then the E walls (Mur history before -tau J).

@@ -88,6 +88,23 @@ def test_graph_step_matches_staged_kernels_on_small_grids(walls, n):
     np.testing.assert_allclose(rows[:, 1:3], ref, rtol=1e-13, atol=1e-300)
 
 
+# A field-only run steps its fields as (y, z) tiles of 8 x 32 nodes over
+# chunks of 16 x-planes: these grids give several tiles per axis, partial
+# last tiles and chunks, sides that are whole multiples of the tile (the
+# last tile then owns node n through its halo) and a last chunk of one plane.
+@pytest.mark.parametrize("n", [(40, 37, 70), (20, 45, 33), (33, 32, 64)])
+@pytest.mark.parametrize("walls", [WALLS[2], WALLS[3], WALLS[5]])
+def test_graph_step_matches_staged_kernels_on_tiled_grids(walls, n):
+    a = make(walls, mg.FP64, n)
+    rows = a.step(15)
+    b = make(walls, mg.FP64, n)
+    ref = staged(b, 15)
+    Ea, Ha = a.fields()
+    Eb, Hb = b.fields()
+    assert np.array_equal(Ea, Eb) and np.array_equal(Ha, Hb)
+    np.testing.assert_allclose(rows[:, 1:3], ref, rtol=1e-13, atol=1e-300)
+
+
 def test_batch_branch_matches_the_run_alone_bit_for_bit():
     # A run stepped as a batch branch keeps the per-axis wall kernels, alone
     # it takes the merged launch: a field-only FP64 run gives the same bits.
