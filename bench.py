@@ -745,13 +745,12 @@ def yee_bench(args):
     peak, peak_kind = hbm_peak()
     achieved = cells * bpc / (ms / 1e3) / 1e9
     traffic = None
-    if not fp32:
-        try:
-            text = open(os.path.join(ROOT, "profiles", "launches_yee.md")).read()
-            m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", text)
-            traffic = float(m.group(1)) if m else None
-        except OSError:
-            pass
+    try:
+        text = open(os.path.join(ROOT, "profiles", "launches_yee.md")).read()
+        m = re.search(r"traffic_bytes_per_launch_%s:\s*([0-9.eE+]+)" % ("fp32" if fp32 else "fp64"), text)
+        traffic = float(m.group(1)) if m else None
+    except OSError:
+        pass
     r.close()
     print(json.dumps({
         "metric": "Yee cell-updates/s", "value": cells / (ms / 1e3), "unit": "cell-updates/s", "n_gpus": 1,
@@ -761,9 +760,7 @@ def yee_bench(args):
                    "bc": "mur x6", "markers": 0, "l2": "inputs larger than L2 (fields %.1f GB)"
                    % (12 * (n[0] + 5) ** 3 * (4 if fp32 else 8) / 1e9)},
         "clocks": clocks.summary(),
-        "roofline": {"bound": "hbm", "kernel": "whole step (%s)" % (
-                         "k_h_fused4, k_e_fused4, walls" if fp32 else
-                         "one pass k_yee_tile, E shell, walls"),
+        "roofline": {"bound": "hbm", "kernel": "whole step (one pass k_yee_tile, E shell, walls)",
                      "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "traffic_of": None if traffic is None else "k_yee_tile, one launch (ncu)",

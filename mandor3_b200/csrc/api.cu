@@ -592,6 +592,8 @@ extern "C" int mg_run_destroy (mg_run_t *r)
       if (r->Hn[c]) mg_dev_free (r, r->Hn[c]);
       if (r->Ealt[c]) mg_dev_free (r, r->Ealt[c]);
       if (r->Halt[c]) mg_dev_free (r, r->Halt[c]);
+      if (r->Ealt32[c]) mg_dev_free (r, r->Ealt32[c]);
+      if (r->Halt32[c]) mg_dev_free (r, r->Halt32[c]);
       if (r->E32[c]) mg_dev_free (r, r->E32[c]);
       if (r->H32[c]) mg_dev_free (r, r->H32[c]);
       if (r->J32[c]) mg_dev_free (r, r->J32[c]);
@@ -1372,11 +1374,11 @@ void mg_drop_graphs (mg_run_t *r)
    r->fo_graph = 0;
 }
 
-// The precision form keeps its two float4-slot passes: its one-pass step
-// measured slower (256^3: 0.328 against 0.274 ms per step).
+// A run stepped alone without markers, sources, probes or TF/SF takes the
+// one-pass field step (both precisions).
 static bool one_pass_ok (const mg_run_t *r)
 {
-   return !is32 (r) && r->np == 0 && !r->probe_ring && !r->has_laser && !r->has_gspot &&
+   return r->np == 0 && !r->probe_ring && !r->has_laser && !r->has_gspot &&
           r->nmirrors == 0 && !r->tfsf && !r->in_batch;
 }
 
@@ -1392,8 +1394,18 @@ static void swap3 (T *a[3], T *b[3])
 
 static void swap_field_sets (mg_run_t *r)
 {
-   swap3 (r->E, r->Ealt);
-   swap3 (r->H, r->Halt);
+   if (is32 (r)) {
+      swap3 (r->E32, r->Ealt32);
+      swap3 (r->H32, r->Halt32);
+   } else {
+      swap3 (r->E, r->Ealt);
+      swap3 (r->H, r->Halt);
+   }
+}
+
+static const void *field_set_id (const mg_run_t *r)
+{
+   return is32 (r) ? (const void *) r->E32[0] : (const void *) r->E[0];
 }
 
 // The second E and H arrays, equal to the current ones (nodes no step
@@ -1431,8 +1443,11 @@ static int build_graph (mg_run_t *r)
    // the arrays current now and writes the others, graph 4 the reverse.
    r->fo_graph = one_pass_ok (r);
    if (r->fo_graph) {
-      TRY (make_alt_set<double> (r, r->E, r->H, r->Ealt, r->Halt));
-      r->fo_read0 = r->E[0];
+      if (is32 (r))
+         TRY (make_alt_set<float> (r, r->E32, r->H32, r->Ealt32, r->Halt32));
+      else
+         TRY (make_alt_set<double> (r, r->E, r->H, r->Ealt, r->Halt));
+      r->fo_read0 = field_set_id (r);
    }
    for (int q = 0 ; q < (r->fo_graph ? 5 : 4) ; ++q) {
       if (q == 4)
@@ -1468,7 +1483,7 @@ static int launch_step_graph (mg_run_t *r)
       MG_CUDA (cudaGraphLaunch (r->gexec[0], r->stream));
       return MG_OK;
    }
-   MG_CUDA (cudaGraphLaunch (r->E[0] == r->fo_read0 ? r->gexec[0] : r->gexec[4], r->stream));
+   MG_CUDA (cudaGraphLaunch (field_set_id (r) == r->fo_read0 ? r->gexec[0] : r->gexec[4], r->stream));
    swap_field_sets (r);
    return MG_OK;
 }

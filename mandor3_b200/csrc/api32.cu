@@ -717,6 +717,10 @@ int mg_sort32 (mg_run_t *r)
 
 int mg_enqueue_step32 (mg_run_t *r, int part)
 {
+   if (part < 0 && r->fo_graph) {        // field-only: one pass into Ealt32, Halt32
+      TRY32 (mg_fields32_one_pass (r));
+      return mg_end_step (r);
+   }
    if (part < 0 || part == 0) {
       TRY32 (mg_tfsf_record (r));
       TRY32 (mg_fields32_h_both (r));

@@ -27,3 +27,4 @@ int mg_fields32_e_finish (mg_run_t *r) { return fields_e_finish<float> (r, fs_of
 int mg_fields32_e_fused (mg_run_t *r) { return fields_e_fused<float> (r, fs_of (r)); }
 int mg_fields32_zero_j (mg_run_t *r) { return fields_zero_j<float> (r, fs_of (r)); }
 int mg_fields32_init (mg_run_t *r) { return fields_init<float> (r, fs_of (r)); }
+int mg_fields32_one_pass (mg_run_t *r) { return fields_one_pass<float> (r, fs_of (r), r->Ealt32, r->Halt32); }

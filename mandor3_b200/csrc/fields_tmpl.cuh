@@ -458,22 +458,27 @@ __device__ __forceinline__ void energy_flush (double we, double wb, DevScalars *
 // each axis; the last tile of an axis also owns node n, its +1 halo there.
 // Halo values of the new H are computed again by each tile that needs them,
 // from the same inputs, so they are the same bits.
-template <int YT, int ZT>
+// E rows move as 16-byte chunks: rows start at multiples of 4 elements and
+// node k = 0 sits at offset 4 (FP64) or 5 (FP32) of its row, so node kb - A
+// starts a chunk for kb a multiple of 4 (A = 2 for FP64, 1 for FP32); a row
+// of the tile holds k in [kb - A, kb - A + EW).
+template <typename T, int YT, int ZT>
 struct YeeTile {
    static constexpr int NT = YT*ZT;               // threads, one per tile node
-   static constexpr int EW = ZT + 2;              // E row pitch: k in [kb - 1, kb + ZT]
+   static constexpr int V = 16/(int) sizeof (T);  // elements per chunk
+   static constexpr int A = sizeof (T) == 8 ? 2 : 1;
+   static constexpr int EW = (ZT + 1 + A + V - 1)/V*V;   // E row pitch: k in [kb - A, kb + ZT]
+   static constexpr int NCH = EW/V;               // chunks per E row
    static constexpr int EP = (YT + 2)*EW;         // E plane: j in [jb - 1, jb + YT]
    static constexpr int HW = ZT + 1;              // new-H row pitch: k in [kb, kb + ZT]
    static constexpr int HP = (YT + 1)*HW;         // new-H plane: j in [jb, jb + YT]
    static constexpr int XH = YT + ZT + 1;         // +1 halo nodes of the new H
 };
 
-template <typename T>
-__device__ __forceinline__ void cp_async_el (T *sm, const T *gm)
+__device__ __forceinline__ void cp_async16 (void *sm, const void *gm)
 {
-   asm volatile ("cp.async.ca.shared.global [%0], [%1], %2;"
-                 :: "r" ((unsigned) __cvta_generic_to_shared (sm)), "l" (gm), "n" ((int) sizeof (T))
-                 : "memory");
+   asm volatile ("cp.async.cg.shared.global [%0], [%1], 16;"
+                 :: "r" ((unsigned) __cvta_generic_to_shared (sm)), "l" (gm) : "memory");
 }
 
 struct YeeTiles {
@@ -488,8 +493,8 @@ __global__ void __launch_bounds__ (YT*ZT, 4)
 k_yee_tile (Grid g, F3T<T> E, F3T<T> H, F3T<T> En, F3T<T> Hnw, YeeTiles tl, T c1, T c2, T c3,
             T d1, T d2, T d3, EnergyPick ep, DevScalars *dsc)
 {
-   using L = YeeTile<YT, ZT>;
-   __shared__ T sE[4][3][L::EP];
+   using L = YeeTile<T, YT, ZT>;
+   __shared__ __align__ (16) T sE[4][3][L::EP];
    __shared__ T sH[2][3][L::HP];
    const int tid = threadIdx.x;
    int b = blockIdx.x;
@@ -506,16 +511,19 @@ k_yee_tile (Grid g, F3T<T> E, F3T<T> H, F3T<T> En, F3T<T> Hnw, YeeTiles tl, T c1
    const bool lastj = je == ny - 1, lastk = ke == nz - 1;
    const long sx = g.sx, sy = g.sy;
 
-   // E^n of plane p into slot s: rows [ja - 1, je + 1], columns [ka - 1, ke + 1].
+   // E^n of plane p into slot s: the chunks of rows [ja - 1, je + 1] that
+   // meet columns [ka - 1, ke + 1].  A chunk may run up to three elements
+   // past the row into the next one (rows up to n, never the last of the
+   // allocation); those elements are not read.
    auto load_e = [&] (int p, int s) {
-      for (int q = tid ; q < L::EP ; q += L::NT) {
-         const int r = q/L::EW, c = q - r*L::EW;
-         const int j = jb - 1 + r, k = kb - 1 + c;
-         if (j >= ja - 1 && j <= je + 1 && k >= ka - 1 && k <= ke + 1) {
+      for (int q = tid ; q < (YT + 2)*L::NCH ; q += L::NT) {
+         const int r = q/L::NCH, m = q - r*L::NCH;
+         const int j = jb - 1 + r, k = kb - L::A + m*L::V;
+         if (j >= ja - 1 && j <= je + 1 && k + L::V - 1 >= ka - 1 && k <= ke + 1) {
             const long o = g.at (p, j, k);
 #pragma unroll
             for (int e = 0 ; e < 3 ; ++e)
-               cp_async_el (&sE[s][e][q], E.c[e] + o);
+               cp_async16 (&sE[s][e][r*L::EW + m*L::V], E.c[e] + o);
          }
       }
    };
@@ -549,7 +557,7 @@ k_yee_tile (Grid g, F3T<T> E, F3T<T> H, F3T<T> En, F3T<T> Hnw, YeeTiles tl, T c1
    // plane's slot sp) into new-H slot sh, k_h_fused's expressions; written
    // to Hnw with its energy terms where owned.
    auto h_node = [&] (int p, int r, int q, int se, int sp, int sh, const T ho[3], bool own) {
-      const int e0 = (r + 1)*L::EW + q + 1;        // node in the E slot
+      const int e0 = (r + 1)*L::EW + q + L::A;     // node in the E slot
       const T ex = sE[se][0][e0], ey = sE[se][1][e0], ez = sE[se][2][e0];
       const T cx = c3*(ey - sE[se][1][e0 - 1]) - c2*(ez - sE[se][2][e0 - L::EW]);
       const T cy = c1*(ez - sE[sp][2][e0]) - c3*(ex - sE[se][0][e0 - 1]);
@@ -568,13 +576,25 @@ k_yee_tile (Grid g, F3T<T> E, F3T<T> H, F3T<T> En, F3T<T> Hnw, YeeTiles tl, T c1
          Hnw.c[2][o] = hz;
          const T ev[3] = {ex, ey, ez};
          if (p >= 1 && p < nx && j >= 1 && j < ny && k >= 1 && k < nz) {
-            // Inside every energy pick range.
-            we += (double) ex*(double) ex;
-            we += (double) ey*(double) ey;
-            we += (double) ez*(double) ez;
-            wb += (double) hv[0]*(double) hv[0];
-            wb += (double) hv[1]*(double) hv[1];
-            wb += (double) hv[2]*(double) hv[2];
+            // Inside every energy pick range.  The precision form sums a
+            // node's three squares in FP32 (as its field passes do), one
+            // conversion per sum.
+            if (sizeof (T) == sizeof (float)) {
+               float se = (float) ex*(float) ex, sb = (float) hv[0]*(float) hv[0];
+               se += (float) ey*(float) ey;
+               se += (float) ez*(float) ez;
+               sb += (float) hv[1]*(float) hv[1];
+               sb += (float) hv[2]*(float) hv[2];
+               we += (double) se;
+               wb += (double) sb;
+            } else {
+               we += (double) ex*(double) ex;
+               we += (double) ey*(double) ey;
+               we += (double) ez*(double) ez;
+               wb += (double) hv[0]*(double) hv[0];
+               wb += (double) hv[1]*(double) hv[1];
+               wb += (double) hv[2]*(double) hv[2];
+            }
          } else {
             energy_add (ep, p, j, k, ev, hv, we, wb);
          }
@@ -610,7 +630,7 @@ k_yee_tile (Grid g, F3T<T> E, F3T<T> H, F3T<T> En, F3T<T> Hnw, YeeTiles tl, T c1
       __syncthreads ();
       if (p > i0 && p >= 2 && ownE) {
          // E^(n+1) of plane p - 1 (in [1, n - 1]) at the tile node.
-         const int pe = (r0 + 1)*L::EW + q0 + 1, ph = r0*L::HW + q0;
+         const int pe = (r0 + 1)*L::EW + q0 + L::A, ph = r0*L::HW + q0;
          const int hp = hs ^ 1;
          const T ex = sE[sp][0][pe], ey = sE[sp][1][pe], ez = sE[sp][2][pe];
          const T Hx = sH[hp][0][ph], Hy = sH[hp][1][ph], Hz = sH[hp][2][ph];
@@ -2227,6 +2247,9 @@ int fields_one_pass (mg_run_t *r, const FS<T> &fs, T *const En[3], T *const Hw[3
    const Slabs se = shell_slabs (e_box (g), in_lo, in_hi);
    MG_CUDA (cudaMemsetAsync (r->dsc->acc, 0, 2*sizeof (double), r->stream));
    constexpr int YT = 8, ZT = 32;
+   using L = YeeTile<T, YT, ZT>;
+   if ((g.origin - L::A) % L::V != 0 || g.sy % L::V != 0 || g.sx % L::V != 0)
+      return MG_ERR_STATE;               // the grid layout lost its chunk alignment
    YeeTiles tl;
    for (int a = 0 ; a < 3 ; ++a) {
       tl.lo[a] = hb.lo[a];

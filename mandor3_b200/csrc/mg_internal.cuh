@@ -130,10 +130,12 @@ struct mg_run {
    // fields
    double *E[3], *H[3], *J[3];
    double *Hn[3];          // H at t = n tau (H holds n-1/2, then n+1/2)
-   // Second E and H arrays of the one-pass field-only step (plain form): the
-   // step reads E, H and writes Ealt, Halt, then the pointers swap.
+   // Second E and H arrays of the one-pass field-only step: the step reads
+   // E, H (E32, H32) and writes Ealt, Halt (Ealt32, Halt32), then the
+   // pointers swap.
    double *Ealt[3], *Halt[3];
-   const double *fo_read0; // E[0] the first field-only step graph reads
+   float  *Ealt32[3], *Halt32[3];
+   const void *fo_read0;   // E[0] (E32[0]) the first field-only step graph reads
    int     fo_graph;       // the step graphs are the field-only pair
    double *mur[2][3];      // Mur history, 4 doubles per wall node
    float  *E32[3], *H32[3], *J32[3], *Hn32[3];
@@ -255,6 +257,7 @@ int mg_fields64_e_step (mg_run_t *r);
 int mg_fields64_jbc (mg_run_t *r);
 int mg_fields64_jbc_graph (mg_run_t *r);
 int mg_fields64_one_pass (mg_run_t *r);
+int mg_fields32_one_pass (mg_run_t *r);
 int mg_fields64_e_finish (mg_run_t *r);
 int mg_fields64_init (mg_run_t *r);
 int mg_fields64_zero_j (mg_run_t *r);
