@@ -1524,6 +1524,12 @@ static int run_steps (mg_run_t *r, int nsteps, double *host_rows, double *dev_ro
       r->in_batch = 0;
    }
    TRY (build_graph (r));
+   if (r->profile && r->fo_graph && field_set_id (r) != r->fo_read0) {
+      // The part graphs step the set they were captured on and do not
+      // swap: capture them again on the current set.
+      mg_drop_graphs (r);
+      TRY (build_graph (r));
+   }
    double push_sum = 0, step_sum = 0;
    for (int done = 0 ; done < nsteps ; ) {
       int chunk = (nsteps - done < MG_RING) ? nsteps - done : MG_RING;

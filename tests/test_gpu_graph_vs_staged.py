@@ -138,6 +138,29 @@ def test_graph_and_staged_steps_interleave(walls):
     assert np.array_equal(Ea, Eb) and np.array_equal(Ha, Hb)
 
 
+@pytest.mark.parametrize("precision", ["FP64", "FP32_OFFSET"])
+def test_one_pass_pair_and_profiled_parts_interleave(precision):
+    # A field-only run alternates between two sets of E and H arrays; the
+    # profiled step (three part graphs, no swap) taken after an odd number
+    # of steps must continue from the current set.
+    p = getattr(mg, precision)
+    a = make(WALLS[5], p)
+    a.step(3)
+    a.profile(True)
+    a.step(2)
+    a.profile(False)
+    a.step(3)
+    b = make(WALLS[5], p)
+    b.step(8)
+    Ea, Ha = a.fields()
+    Eb, Hb = b.fields()
+    if precision == "FP64":
+        assert np.array_equal(Ea, Eb) and np.array_equal(Ha, Hb)
+    else:
+        scale = max(np.max(np.abs(Eb)), np.max(np.abs(Hb)))
+        assert np.max(np.abs(Ea - Eb)) < 1e-5 * scale and np.max(np.abs(Ha - Hb)) < 1e-5 * scale
+
+
 @pytest.mark.parametrize("walls", [WALLS[0], WALLS[4]])
 def test_graph_step_precision_form(walls):
     a = make(walls, mg.FP32_OFFSET)
