@@ -184,7 +184,9 @@ int  mg_run_stream (mg_run_t *run, void **stream);
 int  mg_run_kernels_per_step (mg_run_t *run, int *count);
 /* Device memory the run holds, bytes.                                     */
 int  mg_run_device_bytes (mg_run_t *run, long long *bytes);
-/* Estimated device bytes for a run with these parameters and markers.     */
+/* Estimated device bytes for a run with these parameters and markers
+ * (without markers it includes the second E and H arrays of the one-pass
+ * field step).                                                            */
 long long mg_estimate_bytes (const mg_params_t *params, long long markers);
 
 /* ---- tecplot dumps (IO_tecplot.c:108-266) --------------------------------

@@ -459,6 +459,8 @@ extern "C" long long mg_estimate_bytes (const mg_params_t *p, long long markers)
                        p->precision == MG_FP64 ? MG_GZ_FRONT : MG_GZ_FRONT32);
    const long long elt = (p->precision == MG_FP64) ? 8 : 4;
    long long b = 12LL*g.total*elt;
+   if (markers == 0)                  // one-pass field step: a second E and H set
+      b += 6LL*g.total*elt;
    for (int a = 0 ; a < 3 ; ++a)
       b += 2LL*4*elt*(p->n[(a + 1) % 3] + 2)*(p->n[(a + 2) % 3] + 2);
    // FP64: SoA records; precision form: two buffer sets (the sort scatters

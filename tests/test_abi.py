@@ -80,6 +80,14 @@ def test_estimate_bytes(lib):
     import mandor3_b200 as mg
     b = mg.estimate_bytes((256, 128, 128), (0.05,) * 3, 0.02, (2, 2, 2), (2, 2, 2), 4_500_000)
     assert 3e8 < b < 2e9
+    # Without markers a run stepped alone keeps a second E and H set (six
+    # more arrays of the padded grid) for its one-pass field step.
+    n = (64, 48, 40)
+    row = (4 + n[2] + 1 + 2 + 3) & ~3
+    total = row * (n[1] + 5) * (n[0] + 5)
+    b0 = mg.estimate_bytes(n, (0.05,) * 3, 0.02, (2, 2, 2), (2, 2, 2), 0)
+    b1 = mg.estimate_bytes(n, (0.05,) * 3, 0.02, (2, 2, 2), (2, 2, 2), 1)
+    assert b0 - b1 == 6 * total * 8 - 60          # less one FP64 marker's 60 bytes
 
 
 # ctypes mirrors of the header's structures: same size and field offsets as
