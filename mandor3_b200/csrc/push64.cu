@@ -316,21 +316,23 @@ k_push64 (Ctx c, Markers64 m, long long np, DevScalars *dsc)
    for (long long base = warp0*32 ; base < np ; base += warps_total*32) {
       const long long n = base + lane;
       bool valid = n < np;
-      double qm = 0;
+      double qm = 0, x1 = 0, y1 = 0, z1 = 0;
       // Markers stream through once per step: their loads and stores are
-      // marked evict-first, leaving L1 and L2 to the field gather.
+      // marked evict-first, leaving L1 and L2 to the field gather.  The
+      // position loads go out with qDivM's, not after it, so that the
+      // gather waits for one round trip to memory, not two.
       if (valid) {
          qm = __ldcs (m.qm + n);
+         x1 = __ldcs (m.x + n);
+         y1 = __ldcs (m.y + n);
+         z1 = __ldcs (m.z + n);
          valid = (qm != 0.0);             // removed markers carry qDivM = 0
       }
       int i = 0, j = 0, k = 0, i2 = 0, j2 = 0, k2 = 0, nseg = 0;
       double fi = 0, fj = 0, fk = 0, fi2 = 0, fj2 = 0, fk2 = 0;   // the same as doubles
-      double x1 = 0, y1 = 0, z1 = 0, x2 = 0, y2 = 0, z2 = 0, rho = 0;
+      double x2 = 0, y2 = 0, z2 = 0, rho = 0;
       double xa = 0, ya = 0, za = 0;         // end of the first segment
       if (valid) {
-         x1 = __ldcs (m.x + n);
-         y1 = __ldcs (m.y + n);
-         z1 = __ldcs (m.z + n);
          double sX = div_by (x1, h1, c.rh[0]), sY = div_by (y1, h2, c.rh[1]), sZ = div_by (z1, h3, c.rh[2]);
          double sX_ = sX + 0.5, sY_ = sY + 0.5, sZ_ = sZ + 0.5;
          i = cell_of (sX, fi);
